@@ -1,0 +1,549 @@
+// Test infrastructure only. A C-ABI harness around the UNMODIFIED emerald
+// reference sources (emerald/z_index, emerald/sph_common, emerald/sph2d_box),
+// compiled from where they lie by oracle/build_oracle.py against the
+// project-written shims in oracle/ref_shim. Tests load the resulting
+// oracle/_ref/libemerald_ref.so through ctypes to pin the C restatement and the
+// CUDA path bit for bit; bench.py's reference arm times it on the host cores.
+// Nothing in the product links or loads this file.
+//
+// The solver sub-step functions are file-static in the reference
+// (emerald/sph2d_box/iisph.cpp:23, dfsph_p.cpp:265, pcisph.cpp:36,
+// iisph_ap.cpp:44, iisph_pseudo_ap.cpp:64), so those translation units are
+// included here to reach them with a fixed dt.
+#include <emerald/sph2d_box/dfsph_p.cpp>
+#include <emerald/sph2d_box/iisph.cpp>
+#include <emerald/sph2d_box/iisph_ap.cpp>
+#include <emerald/sph2d_box/iisph_pseudo_ap.cpp>
+#include <emerald/sph2d_box/pcisph.cpp>
+
+#include <emerald/sph2d_box/colors.h>
+#include <emerald/sph2d_box/forces.h>
+#include <emerald/sph2d_box/initial_state.h>
+#include <emerald/sph2d_box/solids.h>
+#include <emerald/sph_common/common.h>
+#include <emerald/sph_common/neighborhood.h>
+#include <emerald/sph_common/volume.h>
+#include <emerald/z_index/z_index.h>
+
+#include <tbb/tbb_shim.h>
+
+#include <cstring>
+#include <random>
+#include <string>
+
+using namespace emerald;
+using namespace emerald::sph2d_box;
+using namespace emerald::sph_common;
+
+extern "C" {
+
+// Mirrors emerald/sph2d_box/parameters.h:12-41 plus two optional overrides of
+// Simulation_config fields (emerald/sph2d_box/config.h:7-18).
+struct ref_params {
+    uint64_t seed;
+    int64_t time_per_step_flicks;
+    int32_t sub_steps;
+    float length;
+    float support;
+    float gravity;
+    float viscosity;
+    float target_density;
+    int32_t iisph_max_pressure_iterations;
+    float iisph_error_average_threshold;
+    float iisph_error_max_threshold;
+    float iisph_omega;
+    int32_t dfsph_max_correction_iterations;
+    float dfsph_density_error_average_threshold;
+    float dfsph_density_error_max_threshold;
+    float dfsph_divergence_error_average_threshold;
+    float dfsph_divergence_error_max_threshold;
+    float mass_per_particle_override;         // > 0 replaces config.mass_per_particle
+    float pressure_correction_denom_override;  // > 0 replaces the PCISPH denominator
+};
+
+}  // extern "C"
+
+namespace {
+
+Parameters to_parameters(ref_params const& p) {
+    Parameters params;
+    params.seed = p.seed;
+    params.time_per_step = flicks{p.time_per_step_flicks};
+    params.sub_steps = p.sub_steps;
+    params.length = p.length;
+    params.support = p.support;
+    params.gravity = p.gravity;
+    params.viscosity = p.viscosity;
+    params.target_density = p.target_density;
+    params.iisph.max_pressure_iterations = p.iisph_max_pressure_iterations;
+    params.iisph.error_average_threshold = p.iisph_error_average_threshold;
+    params.iisph.error_max_threshold = p.iisph_error_max_threshold;
+    params.iisph.omega = p.iisph_omega;
+    params.dfsph.max_correction_iterations = p.dfsph_max_correction_iterations;
+    params.dfsph.density_error_average_threshold = p.dfsph_density_error_average_threshold;
+    params.dfsph.density_error_max_threshold = p.dfsph_density_error_max_threshold;
+    params.dfsph.divergence_error_average_threshold =
+      p.dfsph_divergence_error_average_threshold;
+    params.dfsph.divergence_error_max_threshold = p.dfsph_divergence_error_max_threshold;
+    return params;
+}
+
+Simulation_config to_config(ref_params const& p) {
+    Simulation_config config{to_parameters(p)};
+    if (p.mass_per_particle_override > 0.0f) {
+        config.mass_per_particle = p.mass_per_particle_override;
+    }
+    if (p.pressure_correction_denom_override > 0.0f) {
+        config.pressure_correction_denom = p.pressure_correction_denom_override;
+    }
+    return config;
+}
+
+struct Ref_sim {
+    Simulation_config config;
+    Solid_state solid_state;
+    State state;
+    Temp_data temp;
+    User_forces_function forces;
+    User_colors_function colors;
+    flicks time{0};
+};
+
+std::vector<V2f> to_v2f(float const* xy, size_t n) {
+    std::vector<V2f> out(n);
+    for (size_t i = 0; i < n; ++i) out[i] = V2f{xy[2 * i], xy[2 * i + 1]};
+    return out;
+}
+
+void copy_out(std::vector<V2f> const& v, float* out) {
+    for (size_t i = 0; i < v.size(); ++i) {
+        out[2 * i] = v[i][0];
+        out[2 * i + 1] = v[i][1];
+    }
+}
+
+void copy_out(std::vector<float> const& v, float* out) {
+    std::memcpy(out, v.data(), v.size() * sizeof(float));
+}
+
+void copy_neighborhood(Neighborhood_vectors const& nb,
+                       size_t n,
+                       uint8_t* counts,
+                       uint32_t* idx,
+                       float* dist,
+                       float* vec,
+                       float* w,
+                       float* gw) {
+    for (size_t i = 0; i < n; ++i) {
+        uint8_t const c = nb.counts[i];
+        if (counts) counts[i] = c;
+        for (size_t k = 0; k < NEIGHBORHOOD_MAX_COUNT; ++k) {
+            size_t const o = i * NEIGHBORHOOD_MAX_COUNT + k;
+            bool const live = k < c;
+            if (idx) idx[o] = live ? static_cast<uint32_t>(nb.indices[i][k]) : 0u;
+            if (dist) dist[o] = live && !nb.distances.empty() ? nb.distances[i][k] : 0.0f;
+            if (vec) {
+                vec[2 * o] = live && !nb.vectors_to.empty() ? nb.vectors_to[i][k][0] : 0.0f;
+                vec[2 * o + 1] = live && !nb.vectors_to.empty() ? nb.vectors_to[i][k][1] : 0.0f;
+            }
+            if (w) w[o] = live && nb.kernels.size() == n ? nb.kernels[i][k] : 0.0f;
+            if (gw) {
+                bool const g = live && nb.kernel_gradients.size() == n;
+                gw[2 * o] = g ? nb.kernel_gradients[i][k][0] : 0.0f;
+                gw[2 * o + 1] = g ? nb.kernel_gradients[i][k][1] : 0.0f;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void ref_set_threads(int n) { tbb_shim::Pool::get().set_threads(n); }
+
+int ref_get_threads() { return tbb_shim::Pool::get().threads(); }
+
+uint64_t ref_z_index(uint32_t x, uint32_t y) { return z_index::z_index(x, y); }
+
+void ref_default_params(ref_params* p) {
+    Parameters const d;
+    p->seed = d.seed;
+    p->time_per_step_flicks = d.time_per_step.count();
+    p->sub_steps = d.sub_steps;
+    p->length = d.length;
+    p->support = d.support;
+    p->gravity = d.gravity;
+    p->viscosity = d.viscosity;
+    p->target_density = d.target_density;
+    p->iisph_max_pressure_iterations = d.iisph.max_pressure_iterations;
+    p->iisph_error_average_threshold = d.iisph.error_average_threshold;
+    p->iisph_error_max_threshold = d.iisph.error_max_threshold;
+    p->iisph_omega = d.iisph.omega;
+    p->dfsph_max_correction_iterations = d.dfsph.max_correction_iterations;
+    p->dfsph_density_error_average_threshold = d.dfsph.density_error_average_threshold;
+    p->dfsph_density_error_max_threshold = d.dfsph.density_error_max_threshold;
+    p->dfsph_divergence_error_average_threshold = d.dfsph.divergence_error_average_threshold;
+    p->dfsph_divergence_error_max_threshold = d.dfsph.divergence_error_max_threshold;
+    p->mass_per_particle_override = 0.0f;
+    p->pressure_correction_denom_override = 0.0f;
+}
+
+// out: seconds_per_sub_step, mass_per_particle, draw_radius,
+// pressure_correction_denom (emerald/sph2d_box/config.cpp:16-132).
+void ref_config(ref_params const* p, float* out) {
+    Simulation_config const c = to_config(*p);
+    out[0] = c.seconds_per_sub_step;
+    out[1] = c.mass_per_particle;
+    out[2] = c.draw_radius;
+    out[3] = c.pressure_correction_denom;
+}
+
+float ref_kernel_w(float r, float h) { return kernels::W(r, h); }
+
+void ref_kernel_grad_w(float dx, float dy, float h, float* out) {
+    V2f const g = kernels::GradW(V2f{dx, dy}, h);
+    out[0] = g[0];
+    out[1] = g[1];
+}
+
+float ref_vec2_length(float x, float y) { return V2f{x, y}.length(); }
+
+// Seeded synthetic block scene: an nx-by-ny fluid lattice at spacing dx with
+// origin offset (x0, y0), each coordinate jittered uniformly by +/- jitter*dx
+// from std::mt19937_64{seed}; x then y per particle.
+void ref_block_scene(uint32_t nx,
+                     uint32_t ny,
+                     float dx,
+                     float x0,
+                     float y0,
+                     float jitter,
+                     uint64_t seed,
+                     float* xy) {
+    std::mt19937_64 gen{seed};
+    std::uniform_real_distribution<float> dist{-jitter * dx, jitter * dx};
+    size_t k = 0;
+    for (uint32_t j = 0; j < ny; ++j) {
+        for (uint32_t i = 0; i < nx; ++i) {
+            float const px = x0 + (static_cast<float>(i) + 0.5f) * dx;
+            float const py = y0 + (static_cast<float>(j) + 0.5f) * dx;
+            float const jx = dist(gen);
+            float const jy = dist(gen);
+            xy[2 * k] = px + jx;
+            xy[2 * k + 1] = py + jy;
+            ++k;
+        }
+    }
+}
+
+void* ref_sim_create(ref_params const* p,
+                     float const* solid_xy,
+                     size_t n_solid,
+                     float const* fluid_xy,
+                     float const* fluid_v,
+                     size_t n_fluid) {
+    auto* sim = new Ref_sim;
+    sim->config = to_config(*p);
+    Parameters const& params = sim->config.params;
+    if (solid_xy) {
+        Solid_state solid;
+        solid.positions = to_v2f(solid_xy, n_solid);
+        solid.velocities.assign(n_solid, V2f{0.0f, 0.0f});
+        solid.colors.assign(n_solid, C4f{0.784f, 0.608f, 0.078f, 1.0f});
+        sim->solid_state = compute_neighbor_data_and_volumes(params, std::move(solid));
+    } else {
+        sim->solid_state = world_walls_initial_solid_state(params);
+    }
+    if (fluid_xy) {
+        sim->state.positions = to_v2f(fluid_xy, n_fluid);
+        if (fluid_v) {
+            sim->state.velocities = to_v2f(fluid_v, n_fluid);
+        } else {
+            sim->state.velocities.assign(n_fluid, V2f{0.0f, 0.0f});
+        }
+        sim->state.colors.assign(n_fluid, C4f{0.5f, 0.5f, 1.0f, 1.0f});
+    } else {
+        sim->state = dam_break_initial_state(params, sim->solid_state);
+    }
+    sim->forces = default_gravity_forces(params.gravity);
+    sim->colors = default_target_density_colors(params.target_density);
+    return sim;
+}
+
+void ref_sim_destroy(void* h) { delete static_cast<Ref_sim*>(h); }
+
+size_t ref_sim_fluid_count(void* h) { return static_cast<Ref_sim*>(h)->state.positions.size(); }
+
+size_t ref_sim_solid_count(void* h) {
+    return static_cast<Ref_sim*>(h)->solid_state.positions.size();
+}
+
+void ref_sim_get_solid(void* h, float* xy, float* volumes) {
+    auto* sim = static_cast<Ref_sim*>(h);
+    if (xy) copy_out(sim->solid_state.positions, xy);
+    if (volumes) copy_out(sim->solid_state.volumes, volumes);
+}
+
+// Replaces the boundary volumes that compute_neighbor_data_and_volumes
+// produced (Solid_state::volumes, emerald/sph2d_box/state.h:31).
+void ref_sim_set_solid_volumes(void* h, float const* volumes) {
+    auto* sim = static_cast<Ref_sim*>(h);
+    std::memcpy(sim->solid_state.volumes.data(), volumes, sim->solid_state.volumes.size() * sizeof(float));
+}
+
+int64_t ref_sim_time(void* h) { return static_cast<Ref_sim*>(h)->time.count(); }
+
+// Method numbering follows EZ_EXAMPLE_SIM::Method
+// (emerald/sph2d_box/simulation.h:25): 0 PCISPH, 1 IISPH, 2 IISPH_AP,
+// 3 IISPH_PSEUDO_AP, 4 DFSPH_P.
+int ref_sim_begin_frame(void* h, int method) {
+    auto* sim = static_cast<Ref_sim*>(h);
+    size_t const n = sim->state.positions.size();
+    switch (method) {
+    case 0: break;
+    case 1: iisph_resize_temp_arrays(n, sim->temp); break;
+    case 2: iisph_ap_resize_temp_arrays(n, sim->temp); break;
+    case 3: iisph_pseudo_ap_resize_temp_arrays(n, sim->temp); break;
+    case 4: dfsph_p_resize_and_init_temp_arrays(n, sim->temp); break;
+    default: return -1;
+    }
+    if (method != 0) {
+        compute_constant_volumes(n,
+                                 sim->config.params.target_density,
+                                 sim->config.mass_per_particle,
+                                 sim->temp.fluid_volumes.data());
+    }
+    return 0;
+}
+
+int ref_sim_sub_step(void* h, int method, float t, float dt) {
+    auto* sim = static_cast<Ref_sim*>(h);
+    switch (method) {
+    case 0:
+        pcisph_sub_step(t, dt, sim->config, sim->state, sim->solid_state, sim->temp, sim->forces);
+        break;
+    case 1:
+        iisph_sub_step(t, dt, sim->config, sim->state, sim->solid_state, sim->temp, sim->forces);
+        break;
+    case 2:
+        iisph_ap_sub_step(
+          t, dt, sim->config, sim->state, sim->solid_state, sim->temp, sim->forces);
+        break;
+    case 3:
+        iisph_pseudo_ap_sub_step(
+          t, dt, sim->config, sim->state, sim->solid_state, sim->temp, sim->forces);
+        break;
+    case 4:
+        dfsph_p_sub_step(t, dt, sim->config, sim->state, sim->solid_state, sim->temp, sim->forces);
+        break;
+    default: return -1;
+    }
+    return 0;
+}
+
+// One frame through the reference's own frame functions, exactly as
+// EZ_EXAMPLE_SIM::step (emerald/sph2d_box/simulation.cpp:41-93) calls them.
+int ref_sim_frame(void* h, int method) {
+    auto* sim = static_cast<Ref_sim*>(h);
+    switch (method) {
+    case 0:
+        sim->state = pcisph_simulation_step(sim->time, sim->config, std::move(sim->state),
+                                            sim->solid_state, sim->temp, sim->forces,
+                                            sim->colors);
+        break;
+    case 1:
+        sim->state = iisph_simulation_step(sim->time, sim->config, std::move(sim->state),
+                                           sim->solid_state, sim->temp, sim->forces,
+                                           sim->colors);
+        break;
+    case 2:
+        sim->state = iisph_ap_simulation_step(sim->time, sim->config, std::move(sim->state),
+                                              sim->solid_state, sim->temp, sim->forces,
+                                              sim->colors);
+        break;
+    case 3:
+        sim->state = iisph_pseudo_ap_simulation_step(sim->time, sim->config,
+                                                     std::move(sim->state), sim->solid_state,
+                                                     sim->temp, sim->forces, sim->colors);
+        break;
+    case 4:
+        sim->state = dfsph_p_simulation_step(sim->time, sim->config, std::move(sim->state),
+                                             sim->solid_state, sim->temp, sim->forces,
+                                             sim->colors);
+        break;
+    default: return -1;
+    }
+    sim->time += sim->config.params.time_per_step;
+    return 0;
+}
+
+void ref_sim_get_state(void* h, float* x, float* v) {
+    auto* sim = static_cast<Ref_sim*>(h);
+    if (x) copy_out(sim->state.positions, x);
+    if (v) copy_out(sim->state.velocities, v);
+}
+
+void ref_sim_set_state(void* h, float const* x, float const* v) {
+    auto* sim = static_cast<Ref_sim*>(h);
+    size_t const n = sim->state.positions.size();
+    if (x) sim->state.positions = to_v2f(x, n);
+    if (v) sim->state.velocities = to_v2f(v, n);
+}
+
+// Copies a per-particle temporary of Temp_data (emerald/sph2d_box/state.h:34-69).
+// Returns the number of floats per particle, 0 when the array is unset, or -1
+// for an unknown name.
+int ref_sim_get_array(void* h, char const* name, float* out) {
+    auto* sim = static_cast<Ref_sim*>(h);
+    auto& t = sim->temp;
+    std::string const s{name};
+    auto scalar = [&](std::vector<float> const& v) -> int {
+        if (v.empty()) return 0;
+        if (out) copy_out(v, out);
+        return 1;
+    };
+    auto vector = [&](std::vector<V2f> const& v) -> int {
+        if (v.empty()) return 0;
+        if (out) copy_out(v, out);
+        return 2;
+    };
+    if (s == "densities") return scalar(t.densities);
+    if (s == "pressures") return scalar(t.pressures);
+    if (s == "new_pressures") return scalar(t.new_pressures);
+    if (s == "density_stars") return scalar(t.density_stars);
+    if (s == "aiis") return scalar(t.aiis);
+    if (s == "alphas") return scalar(t.alphas);
+    if (s == "divergence_kappas") return scalar(t.divergence_kappas);
+    if (s == "density_kappas") return scalar(t.density_kappas);
+    if (s == "fluid_volumes") return scalar(t.fluid_volumes);
+    if (s == "diis") return vector(t.diis);
+    if (s == "sum_dij_pjs") return vector(t.sum_dij_pjs);
+    if (s == "external_forces") return vector(t.external_forces);
+    if (s == "pressure_forces") return vector(t.pressure_forces);
+    if (s == "pressure_accelerations") return vector(t.pressure_accelerations);
+    if (s == "velocity_external_forces") return vector(t.velocity_external_forces);
+    if (s == "position_stars") return vector(t.position_stars);
+    if (s == "velocity_stars") return vector(t.velocity_stars);
+    return -1;
+}
+
+// Fluid (solid == 0) or boundary (solid == 1) neighbourhoods of the last
+// sub-step, 64 slots per particle (emerald/sph_common/neighborhood.h:38).
+void ref_sim_get_neighbors(void* h,
+                           int solid,
+                           uint8_t* counts,
+                           uint32_t* idx,
+                           float* dist,
+                           float* vec,
+                           float* w,
+                           float* gw) {
+    auto* sim = static_cast<Ref_sim*>(h);
+    auto const& nb = solid ? sim->temp.solid_neighborhood : sim->temp.neighborhood;
+    copy_neighborhood(nb, nb.counts.size(), counts, idx, dist, vec, w, gw);
+}
+
+// Sort products of the last neighbour build (emerald/sph2d_box/state.h:34-40).
+size_t ref_sim_get_sort(void* h,
+                        int solid,
+                        int32_t* grid_coords,
+                        uint64_t* z_indices,
+                        uint64_t* pair_z,
+                        uint64_t* pair_index,
+                        uint32_t* block_indices,
+                        uint64_t* blocks) {
+    auto* sim = static_cast<Ref_sim*>(h);
+    auto const& gc = solid ? sim->solid_state.grid_coords : sim->temp.grid_coords;
+    auto const& z = solid ? sim->solid_state.z_indices : sim->temp.z_indices;
+    auto const& pairs = solid ? sim->solid_state.index_pairs : sim->temp.index_pairs;
+    auto const& bi = solid ? sim->solid_state.block_indices : sim->temp.block_indices;
+    auto const& bl = solid ? sim->solid_state.blocks : sim->temp.blocks;
+    for (size_t i = 0; i < gc.size(); ++i) {
+        if (grid_coords) {
+            grid_coords[2 * i] = gc[i][0];
+            grid_coords[2 * i + 1] = gc[i][1];
+        }
+        if (z_indices) z_indices[i] = z[i];
+        if (pair_z) pair_z[i] = pairs[i].first;
+        if (pair_index) pair_index[i] = pairs[i].second;
+        if (block_indices) block_indices[i] = bi[i];
+    }
+    if (blocks) {
+        for (size_t b = 0; b < bl.size(); ++b) {
+            blocks[2 * b] = bl[b].first;
+            blocks[2 * b + 1] = bl[b].second;
+        }
+    }
+    return bl.size();
+}
+
+// Stand-alone neighbour build over one point set against itself, with the
+// grid anchored at the origin: the path of the reference's
+// emerald/sph_common/tests/test_neighborhood.cpp:177-292.
+void ref_self_neighborhoods(float const* xy,
+                            size_t n,
+                            float cell_size,
+                            int32_t* grid_coords,
+                            uint64_t* z_indices,
+                            uint64_t* pair_index,
+                            uint32_t* block_indices,
+                            uint8_t* counts,
+                            uint32_t* idx,
+                            float* dist,
+                            float* vec) {
+    auto const positions = to_v2f(xy, n);
+    std::vector<V2i> gc(n);
+    compute_grid_coords(n, cell_size, V2f{0.0f, 0.0f}, gc.data(), positions.data());
+    std::vector<uint64_t> z(n);
+    compute_z_indices(n, z.data(), gc.data());
+    std::vector<std::pair<uint64_t, size_t>> pairs(n);
+    compute_index_pairs(n, pairs.data(), z.data());
+    sort_index_pairs(n, pairs.data());
+    std::vector<uint32_t> bi(n);
+    compute_block_indices(n, bi.data(), pairs.data());
+    size_t const block_count = n ? bi.back() + 1 : 0;
+    std::vector<std::pair<size_t, size_t>> blocks(block_count);
+    fill_blocks(n, blocks.data(), bi.data());
+    Block_map map{block_count * 2};
+    map = create_block_map(block_count, std::move(map), blocks.data(), pairs.data());
+    Neighborhood_vectors nb;
+    nb.resize(n);
+    create_regular_neighborhoods(n,
+                                 cell_size,
+                                 nb.counts.data(),
+                                 nb.indices.data(),
+                                 nb.distances.data(),
+                                 nb.vectors_to.data(),
+                                 positions.data(),
+                                 gc.data(),
+                                 positions.data(),
+                                 pairs.data(),
+                                 map);
+    nb.kernels.clear();
+    nb.kernel_gradients.clear();
+    for (size_t i = 0; i < n; ++i) {
+        if (grid_coords) {
+            grid_coords[2 * i] = gc[i][0];
+            grid_coords[2 * i + 1] = gc[i][1];
+        }
+        if (z_indices) z_indices[i] = z[i];
+        if (pair_index) pair_index[i] = pairs[i].second;
+        if (block_indices) block_indices[i] = bi[i];
+    }
+    copy_neighborhood(nb, n, counts, idx, dist, vec, nullptr, nullptr);
+}
+
+float ref_max_density_error(size_t n, float target_density, float const* densities) {
+    return max_density_error(n, target_density, densities);
+}
+
+float ref_max_vector_squared_magnitude(size_t n, float const* xy) {
+    auto const v = to_v2f(xy, n);
+    return max_vector_squared_magnitude(n, v.data());
+}
+
+int64_t ref_cfl_maximum_time_step(size_t n, float support, float factor, float const* v_xy) {
+    auto const v = to_v2f(v_xy, n);
+    return cfl_maximum_time_step(n, support, factor, v.data()).count();
+}
+
+}  // extern "C"

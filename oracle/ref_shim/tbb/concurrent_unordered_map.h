@@ -1,0 +1,3 @@
+// Test infrastructure only: see tbb_shim.h.
+#pragma once
+#include <tbb/tbb_shim.h>

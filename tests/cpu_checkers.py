@@ -1,0 +1,420 @@
+"""ctypes bindings for the CPU checkers (test infrastructure only).
+
+``Oracle`` wraps oracle/liboracle_sph.so, the project's C restatement of the
+reference SPH path. ``Reference`` wraps oracle/_ref/libemerald_ref.so, the
+unmodified emerald sources compiled against project-written shims (present
+only where it was built). Only tests, the smoke check and bench.py's CPU
+baseline use these; the product never does.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle_sph.so")
+REF_SO = os.path.join(ORACLE_DIR, "_ref", "libemerald_ref.so")
+
+METHODS = {"pcisph": 0, "iisph": 1, "iisph_ap": 2, "iisph_pseudo_ap": 3, "dfsph_p": 4}
+
+c_f = ctypes.c_float
+c_i32 = ctypes.c_int32
+c_i64 = ctypes.c_int64
+c_u64 = ctypes.c_uint64
+c_sz = ctypes.c_size_t
+c_vp = ctypes.c_void_p
+
+
+def ptr(a):
+    return None if a is None else a.ctypes.data_as(c_vp)
+
+
+def ensure_built():
+    import sys
+    sys.path.insert(0, ORACLE_DIR)
+    try:
+        import build_oracle
+        build_oracle.build_oracle()
+        build_oracle.build_reference()
+    finally:
+        sys.path.pop(0)
+
+
+class OracleParams(ctypes.Structure):
+    _fields_ = [
+        ("time_per_step_flicks", c_i64), ("sub_steps", c_i32), ("support", c_f),
+        ("gravity", c_f), ("viscosity", c_f), ("target_density", c_f),
+        ("iisph_max_pressure_iterations", c_i32), ("iisph_error_average_threshold", c_f),
+        ("iisph_error_max_threshold", c_f), ("iisph_omega", c_f),
+        ("dfsph_max_correction_iterations", c_i32),
+        ("dfsph_density_error_average_threshold", c_f),
+        ("dfsph_density_error_max_threshold", c_f),
+        ("dfsph_divergence_error_average_threshold", c_f),
+        ("dfsph_divergence_error_max_threshold", c_f),
+        ("mass_per_particle", c_f), ("pressure_correction_denom", c_f),
+        ("seconds_per_sub_step", c_f),
+    ]
+
+
+class OracleStats(ctypes.Structure):
+    _fields_ = [("pressure_iterations", c_i32), ("divergence_iterations", c_i32),
+                ("error_average", c_f), ("error_max", c_f),
+                ("divergence_error_average", c_f), ("divergence_error_max", c_f)]
+
+
+class RefParams(ctypes.Structure):
+    _fields_ = [
+        ("seed", c_u64), ("time_per_step_flicks", c_i64), ("sub_steps", c_i32),
+        ("length", c_f), ("support", c_f), ("gravity", c_f), ("viscosity", c_f),
+        ("target_density", c_f), ("iisph_max_pressure_iterations", c_i32),
+        ("iisph_error_average_threshold", c_f), ("iisph_error_max_threshold", c_f),
+        ("iisph_omega", c_f), ("dfsph_max_correction_iterations", c_i32),
+        ("dfsph_density_error_average_threshold", c_f),
+        ("dfsph_density_error_max_threshold", c_f),
+        ("dfsph_divergence_error_average_threshold", c_f),
+        ("dfsph_divergence_error_max_threshold", c_f),
+        ("mass_per_particle_override", c_f), ("pressure_correction_denom_override", c_f),
+    ]
+
+
+_ARRAYS = ["densities", "pressures", "new_pressures", "density_stars", "aiis", "alphas",
+           "divergence_kappas", "density_kappas", "fluid_volumes", "diis", "sum_dij_pjs",
+           "external_forces", "pressure_forces", "pressure_accelerations",
+           "velocity_external_forces", "position_stars", "velocity_stars"]
+
+
+class Oracle:
+    """The C restatement (oracle/sph_oracle.c)."""
+
+    def __init__(self):
+        if not os.path.exists(ORACLE_SO):
+            ensure_built()
+        L = ctypes.CDLL(ORACLE_SO)
+        L.oracle_z_index.restype = c_u64
+        L.oracle_z_index.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
+        L.oracle_kernel_w.restype = c_f
+        L.oracle_kernel_w.argtypes = [c_f, c_f]
+        L.oracle_kernel_grad_w.argtypes = [c_f, c_f, c_f, c_vp]
+        L.oracle_vec2_length.restype = c_f
+        L.oracle_vec2_length.argtypes = [c_f, c_f]
+        L.oracle_neighborhoods.argtypes = [c_vp, c_sz, c_vp, c_sz, ctypes.c_int, c_f,
+                                           c_vp, c_vp, c_vp, c_vp]
+        L.oracle_sort.restype = c_sz
+        L.oracle_sort.argtypes = [c_vp, c_sz, c_f, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]
+        L.oracle_solid_volumes.argtypes = [c_vp, c_sz, c_f, c_f, c_vp]
+        L.oracle_sim_create.restype = c_vp
+        L.oracle_sim_create.argtypes = [ctypes.POINTER(OracleParams), c_vp, c_vp, c_sz,
+                                        c_vp, c_vp, c_sz]
+        L.oracle_sim_destroy.argtypes = [c_vp]
+        L.oracle_set_threads.argtypes = [ctypes.c_int]
+        L.oracle_sim_begin_frame.argtypes = [c_vp, ctypes.c_int]
+        L.oracle_sim_sub_step.argtypes = [c_vp, ctypes.c_int, c_f, c_f,
+                                          ctypes.POINTER(OracleStats)]
+        L.oracle_sim_frame.argtypes = [c_vp, ctypes.c_int]
+        L.oracle_sim_time.restype = c_i64
+        L.oracle_sim_time.argtypes = [c_vp]
+        L.oracle_sim_get_state.argtypes = [c_vp, c_vp, c_vp]
+        L.oracle_sim_set_state.argtypes = [c_vp, c_vp, c_vp]
+        L.oracle_sim_get_array.argtypes = [c_vp, ctypes.c_char_p, c_vp]
+        L.oracle_sim_get_neighbors.argtypes = [c_vp, ctypes.c_int, c_vp, c_vp, c_vp, c_vp]
+        self.L = L
+
+    def z_index(self, x, y):
+        return self.L.oracle_z_index(x & 0xFFFFFFFF, y & 0xFFFFFFFF)
+
+    def kernel_w(self, r, h):
+        return self.L.oracle_kernel_w(r, h)
+
+    def kernel_grad_w(self, dx, dy, h):
+        out = np.zeros(2, np.float32)
+        self.L.oracle_kernel_grad_w(dx, dy, h, ptr(out))
+        return out
+
+    def neighborhoods(self, self_xy, other_xy, same_set, cell_size):
+        self_xy = np.ascontiguousarray(self_xy, np.float32)
+        other_xy = np.ascontiguousarray(other_xy, np.float32)
+        n = len(self_xy)
+        counts = np.zeros(n, np.uint8)
+        idx = np.zeros((n, 64), np.uint32)
+        dist = np.zeros((n, 64), np.float32)
+        vec = np.zeros((n, 64, 2), np.float32)
+        self.L.oracle_neighborhoods(ptr(self_xy), n, ptr(other_xy), len(other_xy),
+                                    int(same_set), cell_size, ptr(counts), ptr(idx),
+                                    ptr(dist), ptr(vec))
+        return counts, idx, dist, vec
+
+    def sort(self, xy, cell_size):
+        xy = np.ascontiguousarray(xy, np.float32)
+        n = len(xy)
+        gc = np.zeros((n, 2), np.int32)
+        z = np.zeros(n, np.uint64)
+        pz = np.zeros(n, np.uint64)
+        pi = np.zeros(n, np.uint64)
+        bi = np.zeros(n, np.uint32)
+        blocks = np.zeros((max(n, 1), 2), np.uint64)
+        nb = self.L.oracle_sort(ptr(xy), n, cell_size, ptr(gc), ptr(z), ptr(pz), ptr(pi),
+                                ptr(bi), ptr(blocks))
+        return dict(grid_coords=gc, z_indices=z, pair_z=pz, pair_index=pi,
+                    block_indices=bi, blocks=blocks[:nb])
+
+    def solid_volumes(self, xy, support, numer=1.7):
+        xy = np.ascontiguousarray(xy, np.float32)
+        out = np.zeros(len(xy), np.float32)
+        self.L.oracle_solid_volumes(ptr(xy), len(xy), support, numer, ptr(out))
+        return out
+
+    def set_threads(self, n):
+        self.L.oracle_set_threads(n)
+
+    def sim(self, params, solid_xy, solid_volumes, fluid_xy, fluid_v=None):
+        return OracleSim(self, params, solid_xy, solid_volumes, fluid_xy, fluid_v)
+
+
+class OracleSim:
+    def __init__(self, lib, params, solid_xy, solid_volumes, fluid_xy, fluid_v):
+        self.lib = lib
+        L = lib.L
+        p = OracleParams()
+        for name, _ in OracleParams._fields_:
+            setattr(p, name, params[name])
+        self._solid = np.ascontiguousarray(solid_xy, np.float32)
+        self._vol = None if solid_volumes is None else np.ascontiguousarray(solid_volumes, np.float32)
+        fx = np.ascontiguousarray(fluid_xy, np.float32)
+        fv = None if fluid_v is None else np.ascontiguousarray(fluid_v, np.float32)
+        self.n = len(fx)
+        self.h = L.oracle_sim_create(ctypes.byref(p), ptr(self._solid), ptr(self._vol),
+                                     len(self._solid), ptr(fx), ptr(fv), self.n)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.L.oracle_sim_destroy(self.h)
+            self.h = None
+
+    def begin_frame(self, method):
+        assert self.lib.L.oracle_sim_begin_frame(self.h, METHODS.get(method, method)) == 0
+
+    def sub_step(self, method, t, dt):
+        st = OracleStats()
+        assert self.lib.L.oracle_sim_sub_step(self.h, METHODS.get(method, method), t, dt,
+                                              ctypes.byref(st)) == 0
+        return {k: getattr(st, k) for k, _ in OracleStats._fields_}
+
+    def frame(self, method):
+        return self.lib.L.oracle_sim_frame(self.h, METHODS.get(method, method))
+
+    def time(self):
+        return self.lib.L.oracle_sim_time(self.h)
+
+    def state(self):
+        x = np.zeros((self.n, 2), np.float32)
+        v = np.zeros((self.n, 2), np.float32)
+        self.lib.L.oracle_sim_get_state(self.h, ptr(x), ptr(v))
+        return x, v
+
+    def set_state(self, x=None, v=None):
+        x = None if x is None else np.ascontiguousarray(x, np.float32)
+        v = None if v is None else np.ascontiguousarray(v, np.float32)
+        self.lib.L.oracle_sim_set_state(self.h, ptr(x), ptr(v))
+
+    def array(self, name):
+        w = self.lib.L.oracle_sim_get_array(self.h, name.encode(), None)
+        if w < 0:
+            raise KeyError(name)
+        n = len(self._solid) if name == "solid_volumes" else self.n
+        out = np.zeros((n, w) if w > 1 else n, np.float32)
+        self.lib.L.oracle_sim_get_array(self.h, name.encode(), ptr(out))
+        return out
+
+    def neighbors(self, solid=False):
+        counts = np.zeros(self.n, np.uint8)
+        idx = np.zeros((self.n, 64), np.uint32)
+        w = np.zeros((self.n, 64), np.float32)
+        gw = np.zeros((self.n, 64, 2), np.float32)
+        self.lib.L.oracle_sim_get_neighbors(self.h, int(solid), ptr(counts), ptr(idx),
+                                            ptr(w), ptr(gw))
+        return counts, idx, w, gw
+
+
+class Reference:
+    """The unmodified emerald reference built against shims (oracle/_ref)."""
+
+    available = os.path.exists(REF_SO)
+
+    def __init__(self):
+        L = ctypes.CDLL(REF_SO)
+        L.ref_z_index.restype = c_u64
+        L.ref_z_index.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
+        L.ref_default_params.argtypes = [ctypes.POINTER(RefParams)]
+        L.ref_config.argtypes = [ctypes.POINTER(RefParams), c_vp]
+        L.ref_kernel_w.restype = c_f
+        L.ref_kernel_w.argtypes = [c_f, c_f]
+        L.ref_kernel_grad_w.argtypes = [c_f, c_f, c_f, c_vp]
+        L.ref_vec2_length.restype = c_f
+        L.ref_vec2_length.argtypes = [c_f, c_f]
+        L.ref_block_scene.argtypes = [ctypes.c_uint32, ctypes.c_uint32, c_f, c_f, c_f, c_f,
+                                      c_u64, c_vp]
+        L.ref_sim_create.restype = c_vp
+        L.ref_sim_create.argtypes = [ctypes.POINTER(RefParams), c_vp, c_sz, c_vp, c_vp, c_sz]
+        L.ref_sim_destroy.argtypes = [c_vp]
+        L.ref_sim_fluid_count.restype = c_sz
+        L.ref_sim_fluid_count.argtypes = [c_vp]
+        L.ref_sim_solid_count.restype = c_sz
+        L.ref_sim_solid_count.argtypes = [c_vp]
+        L.ref_sim_get_solid.argtypes = [c_vp, c_vp, c_vp]
+        L.ref_sim_set_solid_volumes.argtypes = [c_vp, c_vp]
+        L.ref_sim_time.restype = c_i64
+        L.ref_sim_time.argtypes = [c_vp]
+        L.ref_sim_begin_frame.argtypes = [c_vp, ctypes.c_int]
+        L.ref_sim_sub_step.argtypes = [c_vp, ctypes.c_int, c_f, c_f]
+        L.ref_sim_frame.argtypes = [c_vp, ctypes.c_int]
+        L.ref_sim_get_state.argtypes = [c_vp, c_vp, c_vp]
+        L.ref_sim_set_state.argtypes = [c_vp, c_vp, c_vp]
+        L.ref_sim_get_array.argtypes = [c_vp, ctypes.c_char_p, c_vp]
+        L.ref_sim_get_neighbors.argtypes = [c_vp, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                            c_vp]
+        L.ref_sim_get_sort.restype = c_sz
+        L.ref_sim_get_sort.argtypes = [c_vp, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]
+        L.ref_self_neighborhoods.argtypes = [c_vp, c_sz, c_f, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                             c_vp, c_vp, c_vp]
+        L.ref_set_threads.argtypes = [ctypes.c_int]
+        L.ref_max_density_error.restype = c_f
+        L.ref_max_density_error.argtypes = [c_sz, c_f, c_vp]
+        L.ref_max_vector_squared_magnitude.restype = c_f
+        L.ref_max_vector_squared_magnitude.argtypes = [c_sz, c_vp]
+        L.ref_cfl_maximum_time_step.restype = c_i64
+        L.ref_cfl_maximum_time_step.argtypes = [c_sz, c_f, c_f, c_vp]
+        self.L = L
+
+    def default_params(self):
+        p = RefParams()
+        self.L.ref_default_params(ctypes.byref(p))
+        return {k: getattr(p, k) for k, _ in RefParams._fields_}
+
+    def config(self, params):
+        p = self._params(params)
+        out = np.zeros(4, np.float32)
+        self.L.ref_config(ctypes.byref(p), ptr(out))
+        return dict(seconds_per_sub_step=out[0], mass_per_particle=out[1], draw_radius=out[2],
+                    pressure_correction_denom=out[3])
+
+    @staticmethod
+    def _params(params):
+        p = RefParams()
+        for name, _ in RefParams._fields_:
+            setattr(p, name, params[name])
+        return p
+
+    def z_index(self, x, y):
+        return self.L.ref_z_index(x & 0xFFFFFFFF, y & 0xFFFFFFFF)
+
+    def block_scene(self, nx, ny, dx, x0=0.0, y0=0.0, jitter=0.01, seed=1):
+        xy = np.zeros((nx * ny, 2), np.float32)
+        self.L.ref_block_scene(nx, ny, dx, x0, y0, jitter, seed, ptr(xy))
+        return xy
+
+    def self_neighborhoods(self, xy, cell_size):
+        xy = np.ascontiguousarray(xy, np.float32)
+        n = len(xy)
+        out = dict(grid_coords=np.zeros((n, 2), np.int32), z_indices=np.zeros(n, np.uint64),
+                   pair_index=np.zeros(n, np.uint64), block_indices=np.zeros(n, np.uint32),
+                   counts=np.zeros(n, np.uint8), idx=np.zeros((n, 64), np.uint32),
+                   dist=np.zeros((n, 64), np.float32), vec=np.zeros((n, 64, 2), np.float32))
+        self.L.ref_self_neighborhoods(ptr(xy), n, cell_size, ptr(out["grid_coords"]),
+                                      ptr(out["z_indices"]), ptr(out["pair_index"]),
+                                      ptr(out["block_indices"]), ptr(out["counts"]),
+                                      ptr(out["idx"]), ptr(out["dist"]), ptr(out["vec"]))
+        return out
+
+    def set_threads(self, n):
+        self.L.ref_set_threads(n)
+
+    def sim(self, params, solid_xy=None, fluid_xy=None, fluid_v=None, solid_volumes=None):
+        return RefSim(self, params, solid_xy, fluid_xy, fluid_v, solid_volumes)
+
+
+class RefSim:
+    def __init__(self, lib, params, solid_xy, fluid_xy, fluid_v, solid_volumes):
+        self.lib = lib
+        L = lib.L
+        p = Reference._params(params)
+        s = None if solid_xy is None else np.ascontiguousarray(solid_xy, np.float32)
+        f = None if fluid_xy is None else np.ascontiguousarray(fluid_xy, np.float32)
+        v = None if fluid_v is None else np.ascontiguousarray(fluid_v, np.float32)
+        self.h = L.ref_sim_create(ctypes.byref(p), ptr(s), 0 if s is None else len(s), ptr(f),
+                                  ptr(v), 0 if f is None else len(f))
+        self.n = L.ref_sim_fluid_count(self.h)
+        self.ns = L.ref_sim_solid_count(self.h)
+        if solid_volumes is not None:
+            vol = np.ascontiguousarray(solid_volumes, np.float32)
+            assert len(vol) == self.ns
+            L.ref_sim_set_solid_volumes(self.h, ptr(vol))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.L.ref_sim_destroy(self.h)
+            self.h = None
+
+    def solid(self):
+        xy = np.zeros((self.ns, 2), np.float32)
+        vol = np.zeros(self.ns, np.float32)
+        self.lib.L.ref_sim_get_solid(self.h, ptr(xy), ptr(vol))
+        return xy, vol
+
+    def begin_frame(self, method):
+        assert self.lib.L.ref_sim_begin_frame(self.h, METHODS.get(method, method)) == 0
+
+    def sub_step(self, method, t, dt):
+        assert self.lib.L.ref_sim_sub_step(self.h, METHODS.get(method, method), t, dt) == 0
+
+    def frame(self, method):
+        assert self.lib.L.ref_sim_frame(self.h, METHODS.get(method, method)) == 0
+
+    def time(self):
+        return self.lib.L.ref_sim_time(self.h)
+
+    def state(self):
+        x = np.zeros((self.n, 2), np.float32)
+        v = np.zeros((self.n, 2), np.float32)
+        self.lib.L.ref_sim_get_state(self.h, ptr(x), ptr(v))
+        return x, v
+
+    def set_state(self, x=None, v=None):
+        x = None if x is None else np.ascontiguousarray(x, np.float32)
+        v = None if v is None else np.ascontiguousarray(v, np.float32)
+        self.lib.L.ref_sim_set_state(self.h, ptr(x), ptr(v))
+
+    def array(self, name):
+        w = self.lib.L.ref_sim_get_array(self.h, name.encode(), None)
+        if w < 0:
+            raise KeyError(name)
+        if w == 0:
+            return None
+        out = np.zeros((self.n, w) if w > 1 else self.n, np.float32)
+        self.lib.L.ref_sim_get_array(self.h, name.encode(), ptr(out))
+        return out
+
+    def neighbors(self, solid=False):
+        n = self.n
+        counts = np.zeros(n, np.uint8)
+        idx = np.zeros((n, 64), np.uint32)
+        dist = np.zeros((n, 64), np.float32)
+        vec = np.zeros((n, 64, 2), np.float32)
+        w = np.zeros((n, 64), np.float32)
+        gw = np.zeros((n, 64, 2), np.float32)
+        self.lib.L.ref_sim_get_neighbors(self.h, int(solid), ptr(counts), ptr(idx), ptr(dist),
+                                         ptr(vec), ptr(w), ptr(gw))
+        return counts, idx, w, gw
+
+    def sort(self, solid=False):
+        n = self.ns if solid else self.n
+        gc = np.zeros((n, 2), np.int32)
+        z = np.zeros(n, np.uint64)
+        pz = np.zeros(n, np.uint64)
+        pi = np.zeros(n, np.uint64)
+        bi = np.zeros(n, np.uint32)
+        blocks = np.zeros((max(n, 1), 2), np.uint64)
+        nb = self.lib.L.ref_sim_get_sort(self.h, int(solid), ptr(gc), ptr(z), ptr(pz), ptr(pi),
+                                         ptr(bi), ptr(blocks))
+        return dict(grid_coords=gc, z_indices=z, pair_z=pz, pair_index=pi, block_indices=bi,
+                    blocks=blocks[:nb])
