@@ -1,0 +1,375 @@
+"""Benchmark of the emerald 2D SPH step on B200.
+
+Workload (N=1): the DFSPH_P dam break of 512x512 = 262144 fluid particles at
+dx = 1/1024 in a [0,1]^2 tank with three boundary rows on the floor and side
+walls, CFL-adaptive sub-steps capped at 5e-4 s (time_per_step = 2e-3 s,
+DFSPH's 60/4 denominators), divergence tolerance 0.1%/s, density tolerance
+0.05%. A step is one solver sub-step; the metric is fluid particle-steps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With --gpus N > 1 (launched by torch.distributed.run) every rank advances its
+own replica of the scene (the single-scene path does not shard); the value
+is the sum over ranks, timed as the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "2D SPH particle-steps/s at 0.1% density error; batched scenes/s, p50/p99 step"
+N_SIDE = 512
+DX = np.float32(1.0 / 1024)
+TPS_FLICKS = 1411200  # 2e-3 s: DFSPH sub-steps between tps/60 and tps/4 = 5e-4 s
+WORKLOAD = ("DFSPH_P dam break, 512x512=262144 fluid particles, dx=1/1024, support=dx, "
+            "3 boundary rows, CFL dt<=5e-4 s, div tol 0.1%/s, density tol 0.05%")
+
+
+def scene_kwargs():
+    return dict(dx=DX, seed=1, time_per_step_flicks=TPS_FLICKS, sub_steps=4,
+                dfsph_divergence_error_average_threshold=np.float32(0.001),
+                dfsph_density_error_average_threshold=np.float32(0.0005))
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def clock_sampler(gpu_index, path):
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    try:
+        f = open(path, "w")
+        p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + q,
+                              "--format=csv,noheader,nounits", "-lms", "200"], stdout=f,
+                             stderr=subprocess.DEVNULL)
+        return p, f
+    except Exception:
+        return None, None
+
+
+def summarize_clocks(path):
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    try:
+        for line in open(path):
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+    except OSError:
+        pass
+    if not sm:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+    return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_from_profile(kernel):
+    """dram bytes per launch of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "ncu_summary.json")
+    try:
+        d = json.load(open(path))
+        k = d["kernels"][kernel]
+        return float(k["dram_bytes_per_launch"]) * float(d.get("scale_to_bench", 1.0))
+    except Exception:
+        return None
+
+
+# Algorithmic bytes per launch (each element a kernel must touch, once, plus
+# the neighbour lists it streams: 4 B index + 8 B kernel gradient per entry,
+# 4 B kernel value where used).
+def algorithmic_bytes(kernel, n, nnz_f, nnz_s, n_s):
+    per_entry = 12.0 * (nnz_f + nnz_s)
+    vols = 4.0 * n_s
+    table = {
+        "apply_pressures": per_entry + vols + n * (2 + 4 + 8 + 8),
+        "apply_pressures_ext": per_entry + vols + n * (2 + 4 + 8 + 8),
+        "dfsph_divergence": per_entry + vols + 8.0 * n_s + n * (2 + 8 + 4 + 4 + 4 + 4 + 4),
+        "dfsph_density": per_entry + vols + 8.0 * n_s + n * (2 + 8 + 4 + 4 + 4 + 4 + 4),
+        "dfsph_density_alpha": 16.0 * (nnz_f + nnz_s) + vols + n * (2 + 4 + 4 + 4 + 4 + 4 + 4),
+        "neighbors_fluid": 16.0 * nnz_f + n * (8 + 4 + 1),
+        "neighbors_solid": 16.0 * nnz_s + n * (8 + 1) + 12.0 * n_s,
+    }
+    return table.get(kernel)
+
+
+def run_gpu(args):
+    import torch
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import emerald_b200 as E
+
+    scene = E.BlockScene(N_SIDE, **scene_kwargs())
+    sim = E.Simulation.from_block_scene(scene)
+    n = sim.n
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        sim.advance("dfsph_p", 1, stats=False)
+    barrier()
+
+    # device-resident timing: one event pair per sub-step, L2 flushed between
+    clocks_path = "/tmp/emerald_clocks_%d.csv" % rank
+    smi, smi_file = clock_sampler(local, clocks_path)
+    launches0 = E.kernel_launches()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        ev[k][0].record()
+        sim.advance("dfsph_p", 1, stats=False)
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    launches = E.kernel_launches() - launches0
+    total_ms = sum(a.elapsed_time(b) for a, b in ev)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    if smi is not None:
+        smi.terminate()
+        smi.wait()
+        smi_file.close()
+    clocks = summarize_clocks(clocks_path)
+    last = sim.advance("dfsph_p", 0)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * n * args.steps / (max_ms / 1000.0)
+
+    # end to end through the C ABI: pinned host state in, sub-step, state out
+    x_h = torch.empty((n, 2), dtype=torch.float32).pin_memory()
+    v_h = torch.empty((n, 2), dtype=torch.float32).pin_memory()
+    xs, vs = sim.state()
+    x_h.numpy()[:] = xs
+    v_h.numpy()[:] = vs
+    e2e_steps = max(1, min(args.steps, 100))
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(e2e_steps):
+        sim.set_state(x_h.numpy(), v_h.numpy())
+        sim.advance("dfsph_p", 1, stats=False)
+        xo, vo = sim.state()
+        x_h.numpy()[:] = xo
+        v_h.numpy()[:] = vo
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    t2 = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e_value = world * n * e2e_steps / (float(t2.item()) / 1000.0)
+
+    # per-kernel device times (events around every launch) for the roofline
+    sim.enable_timing(True)
+    rsteps = max(3, min(args.steps, 50))
+    for _ in range(rsteps):
+        flush.zero_()
+        sim.advance("dfsph_p", 1, stats=False)
+    times = sim.kernel_times()
+    sim.enable_timing(False)
+    counts_f, _, _, _ = sim.neighbors(False)
+    counts_s, _, _, _ = sim.neighbors(True)
+    nnz_f = float(counts_f.sum())
+    nnz_s = float(counts_s.sum())
+    n_s = sim.ns
+    ranked = sorted(times.items(), key=lambda kv: -kv[1][0])
+    top_name, (top_ms, top_launches) = ranked[0]
+    per_launch_s = top_ms / top_launches / 1000.0
+    alg = algorithmic_bytes(top_name, n, nnz_f, nnz_s, n_s)
+    peak, peak_kind = measured_peak()
+    roofline = None
+    if alg is not None:
+        achieved = alg / per_launch_s / 1e9
+        roofline = {"bound": "hbm", "kernel": top_name, "achieved": round(achieved, 1),
+                    "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                    "peak_source": peak_kind, "traffic": traffic_from_profile(top_name),
+                    "algorithmic_bytes_per_launch": alg,
+                    "avg_launch_us": round(per_launch_s * 1e6, 2)}
+    kernel_table = {k: {"ms_total": round(v[0], 3), "launches": v[1],
+                        "share": round(v[0] / sum(x[0] for x in times.values()), 4)}
+                    for k, v in ranked[:12]}
+
+    result = None
+    if rank == 0:
+        result = {
+            "metric": METRIC, "value": round(value, 1), "unit": "particle-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(max_ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "fluid_particles": n, "boundary_particles": n_s,
+                       "neighbours_per_particle": round(nnz_f / n, 2),
+                       "parallelism": "replicas" if world > 1 else "single scene",
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "p50_step_ms": round(float(np.percentile(step_ms, 50)), 4),
+                       "p99_step_ms": round(float(np.percentile(step_ms, 99)), 4),
+                       "last_step": {k: last[k] for k in ("dt", "pressure_iterations",
+                                                          "divergence_iterations",
+                                                          "error_average", "error_max")}},
+            "roofline": roofline,
+            "kernels": kernel_table,
+            "e2e": {"value": round(e2e_value, 1), "unit": "particle-steps/s",
+                    "h2d_bytes_per_step": int(2 * n * 8), "d2h_bytes_per_step": int(2 * n * 8),
+                    "steps": e2e_steps},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline(args, sample_seconds=args.cpu_seconds)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def reference_sim(threads):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import emerald_b200 as E
+    from cpu_checkers import Reference
+    if not Reference.available:
+        return None, None, None
+    R = Reference()
+    R.set_threads(threads)
+    scene = E.BlockScene(N_SIDE, **scene_kwargs())
+    rp = R.default_params()
+    p = scene.params.as_dict()
+    for k in rp:
+        if k in p:
+            rp[k] = p[k]
+    rp["mass_per_particle_override"] = p["mass_per_particle"]
+    rp["pressure_correction_denom_override"] = p["pressure_correction_denom"]
+    sim = R.sim(rp, scene.solid, scene.fluid, None, scene.solid_volumes)
+    return R, sim, scene
+
+
+def cpu_baseline(args, sample_seconds=15.0):
+    """The reference's own CPU code (oracle/_ref: emerald sources with TBB
+    replaced by a std::thread pool) on this host's cores: DFSPH frames of the
+    same scene from its initial state."""
+    threads = os.cpu_count() or 1
+    R, sim, scene = reference_sim(threads)
+    if sim is None:
+        return {"value": None, "unit": "particle-steps/s", "cores": threads,
+                "kind": "reference", "sample": "unavailable: oracle/_ref not built"}
+    import emerald_b200 as E
+    t0 = time.perf_counter()
+    frames = 0
+    while time.perf_counter() - t0 < sample_seconds and frames < 200:
+        sim.frame("dfsph_p")
+        frames += 1
+    elapsed = time.perf_counter() - t0
+    # The GPU path is bit-identical, so its frame statistics give the
+    # reference's sub-step count for the same frames (counted untimed).
+    gsim = E.Simulation.from_block_scene(scene)
+    substeps = sum(gsim.frame("dfsph_p")["sub_steps"] for _ in range(frames))
+    n = sim.n
+    return {"value": round(n * substeps / elapsed, 1), "unit": "particle-steps/s",
+            "cores": threads, "kind": "reference",
+            "sample": "%d DFSPH frames (%d sub-steps) of the same scene from its initial state, "
+                      "%.1f s; TBB replaced by a std::thread pool of %d threads" % (
+                          frames, substeps, elapsed, threads)}
+
+
+def run_reference(args):
+    world, rank, local = dist_env()
+    if rank != 0:
+        return None
+    threads = os.cpu_count() or 1
+    R, sim, scene = reference_sim(threads)
+    if sim is None:
+        return {"impl": "reference", "unavailable": "oracle/_ref (reference compiled with shims) "
+                "is not built on this machine"}
+    import emerald_b200 as E
+    dt = np.float32(5e-4)
+    # one step = one DFSPH sub-step; bounded so the run ends within minutes
+    per_step = None
+    sim.begin_frame("dfsph_p")
+    for k in range(min(args.warmup, 3)):
+        sim.sub_step("dfsph_p", np.float32(k * dt), dt)
+    budget = 120.0
+    done = 0
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        if k % 4 == 0:
+            sim.begin_frame("dfsph_p")
+        sim.sub_step("dfsph_p", np.float32(k * dt), dt)
+        done += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    elapsed = time.perf_counter() - t0
+    value = sim.n * done / elapsed
+    sample = ("%d of %d requested DFSPH sub-steps at dt=5e-4 s (frames of 4), %.1f s, "
+              "%d host threads" % (done, args.steps, elapsed, threads))
+    return {"impl": "reference", "metric": METRIC, "value": round(value, 1),
+            "unit": "particle-steps/s", "n_gpus": world, "steps": done, "warmup": args.warmup,
+            "ms_per_step": round(elapsed * 1000.0 / done, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "fluid_particles": sim.n},
+            "cpu_baseline": {"value": round(value, 1), "unit": "particle-steps/s",
+                             "cores": threads, "kind": "reference", "sample": sample},
+            "e2e": {"value": round(value, 1), "unit": "particle-steps/s",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        out = run_reference(args)
+    else:
+        out = run_gpu(args)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,348 @@
+"""emerald_b200: B200 implementation of the emerald 2D SPH step.
+
+A Python mirror of the reference's solver API (emerald/sph2d_box/simulation.h,
+EZ_EXAMPLE_SIM and the X_simulation_step functions) over the C ABI in
+include/emerald_sph.h. All compute runs in libemerald_b200.so on the GPU;
+this module only marshals arrays. Importing it fails loudly when the library
+is missing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libemerald_b200.so")
+
+METHODS = {"pcisph": 0, "iisph": 1, "iisph_ap": 2, "iisph_pseudo_ap": 3, "dfsph_p": 4}
+FLICKS_PER_SECOND = 705600000
+
+c_f = ctypes.c_float
+c_i32 = ctypes.c_int32
+c_i64 = ctypes.c_int64
+c_u32 = ctypes.c_uint32
+c_u64 = ctypes.c_uint64
+c_sz = ctypes.c_size_t
+c_vp = ctypes.c_void_p
+
+
+class EmeraldError(RuntimeError):
+    pass
+
+
+class Params(ctypes.Structure):
+    """emerald_params (mirrors emerald/sph2d_box/parameters.h:12-41)."""
+
+    _fields_ = [
+        ("seed", c_u64), ("time_per_step_flicks", c_i64), ("sub_steps", c_i32),
+        ("length", c_f), ("support", c_f), ("gravity", c_f), ("viscosity", c_f),
+        ("target_density", c_f), ("iisph_max_pressure_iterations", c_i32),
+        ("iisph_error_average_threshold", c_f), ("iisph_error_max_threshold", c_f),
+        ("iisph_omega", c_f), ("dfsph_max_correction_iterations", c_i32),
+        ("dfsph_density_error_average_threshold", c_f),
+        ("dfsph_density_error_max_threshold", c_f),
+        ("dfsph_divergence_error_average_threshold", c_f),
+        ("dfsph_divergence_error_max_threshold", c_f),
+        ("mass_per_particle", c_f), ("pressure_correction_denom", c_f),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [
+        ("sub_steps", c_i32), ("pressure_iterations", c_i32), ("error_average", c_f),
+        ("error_max", c_f), ("divergence_iterations", c_i32), ("divergence_error_average", c_f),
+        ("divergence_error_max", c_f), ("dt", c_f), ("time_seconds", ctypes.c_double),
+        ("error_flags", c_i32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+EXPORTS = {
+    "emerald_default_params": (c_i32, [ctypes.POINTER(Params)]),
+    "emerald_config": (c_i32, [ctypes.POINTER(Params), c_vp]),
+    "emerald_lattice_config": (c_i32, [ctypes.POINTER(Params), c_f, c_f, c_vp]),
+    "emerald_z_index": (c_u64, [c_u32, c_u32]),
+    "emerald_block_scene": (c_sz, [c_u32, c_u32, c_f, c_f, c_f, c_f, c_u64, c_vp]),
+    "emerald_wall_scene": (c_sz, [c_f, c_f, c_i32, c_vp]),
+    "emerald_world_walls": (c_sz, [ctypes.POINTER(Params), c_vp]),
+    "emerald_dam_break": (c_sz, [ctypes.POINTER(Params), c_vp, c_sz, c_vp]),
+    "emerald_sim_create": (c_i32, [ctypes.POINTER(Params), c_vp, c_vp, c_sz, c_vp, c_vp, c_sz,
+                                   ctypes.POINTER(c_vp)]),
+    "emerald_sim_destroy": (c_i32, [c_vp]),
+    "emerald_sim_begin_frame": (c_i32, [c_vp, c_i32]),
+    "emerald_sim_sub_step": (c_i32, [c_vp, c_i32, c_f, c_f, ctypes.POINTER(StepStats)]),
+    "emerald_sim_frame": (c_i32, [c_vp, c_i32, ctypes.POINTER(StepStats)]),
+    "emerald_sim_advance": (c_i32, [c_vp, c_i32, c_i32, ctypes.POINTER(StepStats)]),
+    "emerald_sim_counts": (c_i32, [c_vp, ctypes.POINTER(c_sz), ctypes.POINTER(c_sz)]),
+    "emerald_sim_time": (c_i32, [c_vp, ctypes.POINTER(c_i64)]),
+    "emerald_sim_get_state": (c_i32, [c_vp, c_vp, c_vp]),
+    "emerald_sim_set_state": (c_i32, [c_vp, c_vp, c_vp]),
+    "emerald_sim_get_solid": (c_i32, [c_vp, c_vp, c_vp]),
+    "emerald_sim_get_array": (c_i32, [c_vp, ctypes.c_char_p, c_vp, ctypes.POINTER(c_i32)]),
+    "emerald_sim_get_neighbors": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp]),
+    "emerald_sim_get_sort": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                     ctypes.POINTER(c_sz)]),
+    "emerald_sim_set_stream": (c_i32, [c_vp, c_vp]),
+    "emerald_sim_device_state": (c_i32, [c_vp, ctypes.POINTER(c_vp), ctypes.POINTER(c_vp)]),
+    "emerald_sim_enable_timing": (c_i32, [c_vp, c_i32]),
+    "emerald_sim_kernel_times": (c_i32, [c_vp, ctypes.c_char_p, c_sz, c_vp, c_vp,
+                                         ctypes.POINTER(c_i32)]),
+    "emerald_kernel_launches": (c_i64, []),
+    "emerald_last_error": (ctypes.c_char_p, []),
+}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            "emerald_b200: %s is missing; build it with `python -m emerald_b200.build` "
+            "(there is no CPU fallback)" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in EXPORTS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(c_vp)
+
+
+def _check(rc, what):
+    if rc != 0:
+        msg = lib.emerald_last_error()
+        raise EmeraldError("%s failed (%d): %s" % (what, rc, msg.decode() if msg else ""))
+
+
+def _f32(a, shape_tail=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a
+
+
+def method_id(method):
+    return METHODS[method] if isinstance(method, str) else int(method)
+
+
+def default_params(**overrides):
+    p = Params()
+    _check(lib.emerald_default_params(ctypes.byref(p)), "emerald_default_params")
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+def config(params):
+    """Simulation_config values: seconds_per_sub_step, mass_per_particle,
+    draw_radius, pressure_correction_denom (emerald/sph2d_box/config.cpp)."""
+    out = np.zeros(4, np.float32)
+    _check(lib.emerald_config(ctypes.byref(params), _ptr(out)), "emerald_config")
+    return dict(seconds_per_sub_step=out[0], mass_per_particle=out[1], draw_radius=out[2],
+                pressure_correction_denom=out[3])
+
+
+def lattice_config(params, dx, dt):
+    out = np.zeros(2, np.float32)
+    _check(lib.emerald_lattice_config(ctypes.byref(params), dx, dt, _ptr(out)),
+           "emerald_lattice_config")
+    return out[0], out[1]
+
+
+def z_index(x, y):
+    return lib.emerald_z_index(x & 0xFFFFFFFF, y & 0xFFFFFFFF)
+
+
+def block_scene(nx, ny, dx, x0=0.0, y0=0.0, jitter=0.01, seed=1):
+    xy = np.zeros((nx * ny, 2), np.float32)
+    lib.emerald_block_scene(nx, ny, dx, x0, y0, jitter, seed, _ptr(xy))
+    return xy
+
+
+def wall_scene(dx, length=1.0, layers=3):
+    n = lib.emerald_wall_scene(dx, length, layers, None)
+    xy = np.zeros((n, 2), np.float32)
+    lib.emerald_wall_scene(dx, length, layers, _ptr(xy))
+    return xy
+
+
+def world_walls(params):
+    n = lib.emerald_world_walls(ctypes.byref(params), None)
+    xy = np.zeros((n, 2), np.float32)
+    lib.emerald_world_walls(ctypes.byref(params), _ptr(xy))
+    return xy
+
+
+def dam_break(params, solid_xy):
+    solid_xy = _f32(solid_xy)
+    n = lib.emerald_dam_break(ctypes.byref(params), _ptr(solid_xy), len(solid_xy), None)
+    xy = np.zeros((n, 2), np.float32)
+    lib.emerald_dam_break(ctypes.byref(params), _ptr(solid_xy), len(solid_xy), _ptr(xy))
+    return xy
+
+
+def kernel_launches():
+    return lib.emerald_kernel_launches()
+
+
+class BlockScene:
+    """A seeded dam-break block scene: an nx-by-ny fluid lattice at spacing dx
+    (jitter +/- jitter*dx from std::mt19937_64{seed}) inside a [0, length]^2
+    tank with `layers` boundary rows at the same spacing on the floor and side
+    walls. support = support_ratio * dx. Boundary volumes are the fluid
+    particle volume (the rows act as frozen fluid at the lattice spacing) and
+    the mass per particle gives the unjittered lattice the target density."""
+
+    def __init__(self, n_side, dx=None, ny=None, length=1.0, support_ratio=1.0, jitter=0.01,
+                 seed=1, layers=3, dt=5e-4, **param_overrides):
+        self.nx = n_side
+        self.ny = ny or n_side
+        self.dx = np.float32(dx if dx is not None else 1.0 / (2 * n_side))
+        self.support = np.float32(support_ratio * self.dx)
+        self.params = default_params(support=self.support, length=length, seed=seed)
+        for k, v in param_overrides.items():
+            setattr(self.params, k, v)
+        mass, denom = lattice_config(self.params, self.dx, dt)
+        self.params.mass_per_particle = mass
+        self.params.pressure_correction_denom = denom
+        self.fluid = block_scene(self.nx, self.ny, self.dx, 0.0, 0.0, jitter, seed)
+        self.solid = wall_scene(self.dx, length, layers)
+        self.solid_volumes = np.full(len(self.solid), np.float32(mass) / np.float32(
+            self.params.target_density), np.float32)
+
+
+class Simulation:
+    """One scene on the GPU: the EZ_EXAMPLE_SIM state
+    (emerald/sph2d_box/simulation.h:24-44) with step functions."""
+
+    def __init__(self, params, solid_xy, fluid_xy, fluid_v=None, solid_volumes=None):
+        self.params = params
+        s = _f32(solid_xy).reshape(-1, 2)
+        f = _f32(fluid_xy).reshape(-1, 2)
+        v = None if fluid_v is None else _f32(fluid_v).reshape(-1, 2)
+        vol = None if solid_volumes is None else _f32(solid_volumes)
+        h = c_vp()
+        _check(lib.emerald_sim_create(ctypes.byref(params), _ptr(s), _ptr(vol), len(s), _ptr(f),
+                                      _ptr(v), len(f), ctypes.byref(h)), "emerald_sim_create")
+        self._h = h
+        self.n = len(f)
+        self.ns = len(s)
+
+    @classmethod
+    def from_block_scene(cls, scene):
+        return cls(scene.params, scene.solid, scene.fluid, None, scene.solid_volumes)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib.emerald_sim_destroy(self._h)
+            self._h = c_vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def begin_frame(self, method):
+        _check(lib.emerald_sim_begin_frame(self._h, method_id(method)), "begin_frame")
+
+    def sub_step(self, method, t, dt):
+        st = StepStats()
+        _check(lib.emerald_sim_sub_step(self._h, method_id(method), t, dt, ctypes.byref(st)),
+               "sub_step")
+        return st.as_dict()
+
+    def frame(self, method):
+        st = StepStats()
+        _check(lib.emerald_sim_frame(self._h, method_id(method), ctypes.byref(st)), "frame")
+        return st.as_dict()
+
+    def advance(self, method, n_substeps, stats=True):
+        st = StepStats()
+        _check(lib.emerald_sim_advance(self._h, method_id(method), n_substeps,
+                                       ctypes.byref(st) if stats else None), "advance")
+        return st.as_dict()
+
+    def time(self):
+        t = c_i64()
+        _check(lib.emerald_sim_time(self._h, ctypes.byref(t)), "time")
+        return t.value
+
+    def state(self):
+        x = np.zeros((self.n, 2), np.float32)
+        v = np.zeros((self.n, 2), np.float32)
+        _check(lib.emerald_sim_get_state(self._h, _ptr(x), _ptr(v)), "get_state")
+        return x, v
+
+    def set_state(self, x=None, v=None):
+        x = None if x is None else _f32(x)
+        v = None if v is None else _f32(v)
+        _check(lib.emerald_sim_set_state(self._h, _ptr(x), _ptr(v)), "set_state")
+
+    def solid(self):
+        xy = np.zeros((self.ns, 2), np.float32)
+        vol = np.zeros(self.ns, np.float32)
+        _check(lib.emerald_sim_get_solid(self._h, _ptr(xy), _ptr(vol)), "get_solid")
+        return xy, vol
+
+    def array(self, name):
+        w = c_i32()
+        _check(lib.emerald_sim_get_array(self._h, name.encode(), None, ctypes.byref(w)),
+               "get_array")
+        out = np.zeros((self.n, w.value) if w.value > 1 else self.n, np.float32)
+        _check(lib.emerald_sim_get_array(self._h, name.encode(), _ptr(out), ctypes.byref(w)),
+               "get_array")
+        return out
+
+    def neighbors(self, solid=False):
+        counts = np.zeros(self.n, np.uint8)
+        idx = np.zeros((self.n, 64), np.uint32)
+        w = np.zeros((self.n, 64), np.float32)
+        gw = np.zeros((self.n, 64, 2), np.float32)
+        _check(lib.emerald_sim_get_neighbors(self._h, int(solid), _ptr(counts), _ptr(idx),
+                                             _ptr(w), _ptr(gw)), "get_neighbors")
+        return counts, idx, w, gw
+
+    def sort(self, solid=False):
+        n = self.ns if solid else self.n
+        gc = np.zeros((n, 2), np.int32)
+        z = np.zeros(n, np.uint64)
+        pz = np.zeros(n, np.uint64)
+        pi = np.zeros(n, np.uint64)
+        bi = np.zeros(n, np.uint32)
+        blocks = np.zeros((max(n, 1), 2), np.uint64)
+        nb = c_sz()
+        _check(lib.emerald_sim_get_sort(self._h, int(solid), _ptr(gc), _ptr(z), _ptr(pz), _ptr(pi),
+                                        _ptr(bi), _ptr(blocks), ctypes.byref(nb)), "get_sort")
+        return dict(grid_coords=gc, z_indices=z, pair_z=pz, pair_index=pi, block_indices=bi,
+                    blocks=blocks[:nb.value])
+
+    def set_stream(self, stream_ptr):
+        _check(lib.emerald_sim_set_stream(self._h, stream_ptr), "set_stream")
+
+    def device_state(self):
+        x = c_vp()
+        v = c_vp()
+        _check(lib.emerald_sim_device_state(self._h, ctypes.byref(x), ctypes.byref(v)),
+               "device_state")
+        return x.value, v.value
+
+    def enable_timing(self, on=True):
+        _check(lib.emerald_sim_enable_timing(self._h, int(on)), "enable_timing")
+
+    def kernel_times(self):
+        count = c_i32(256)
+        ms = np.zeros(256, np.float64)
+        launches = np.zeros(256, np.int32)
+        names = ctypes.create_string_buffer(1 << 16)
+        _check(lib.emerald_sim_kernel_times(self._h, names, len(names), _ptr(ms), _ptr(launches),
+                                            ctypes.byref(count)), "kernel_times")
+        keys = names.value.decode().split("\n") if names.value else []
+        return {k: (float(ms[i]), int(launches[i])) for i, k in enumerate(keys[:count.value])}

@@ -1,0 +1,376 @@
+// Neighbour build on the GPU: Morton keys, cell binning, cell ranges and the
+// per-particle neighbour lists of emerald/sph_common/neighborhood.{h,cpp}.
+//
+// The reference sorts (z, index) pairs and keeps a hash map from z to the
+// [begin, end) range of each cell (neighborhood.cpp:10-124). Here each scene
+// has an open-addressing table keyed by z; binning counts the members of
+// every cell, an exclusive scan turns the counts into ranges, and each
+// cell's member list is ordered by index, which is exactly the order the
+// sorted pairs give inside a cell. The neighbour search then walks the 3x3
+// cells in the reference's row-major order, keeps the first 64 accepted
+// candidates and orders them by (distance, index) (neighborhood.h:199-282),
+// so the lists are bit-identical.
+#include "engine_types.cuh"
+#include "kernels.cuh"
+#include "sph_math.cuh"
+
+namespace emerald {
+
+namespace {
+
+__device__ __forceinline__ uint32_t cell_hash(uint64_t z, uint32_t log2cap) {
+    return static_cast<uint32_t>((z * 0x9E3779B97F4A7C15ull) >> (64u - log2cap));
+}
+
+// Inserts z into the table (capacity 2^log2cap plus one extra slot reserved
+// for z == kEmptyKey, the key of cell (-1, -1)). Returns the slot or
+// UINT32_MAX when the table is full; the probe loop is bounded.
+__device__ uint32_t table_insert(uint64_t* keys, uint32_t log2cap, uint64_t z) {
+    uint32_t const cap = 1u << log2cap;
+    if (z == kEmptyKey) return cap;
+    uint32_t h = cell_hash(z, log2cap);
+    for (uint32_t probe = 0; probe < cap; ++probe) {
+        unsigned long long const prev = atomicCAS(
+          reinterpret_cast<unsigned long long*>(keys + h), kEmptyKey, z);
+        if (prev == kEmptyKey || prev == z) return h;
+        h = (h + 1u) & (cap - 1u);
+    }
+    return UINT32_MAX;
+}
+
+__device__ __forceinline__ bool table_find(uint64_t const* keys,
+                                           uint32_t log2cap,
+                                           uint64_t z,
+                                           uint32_t& slot) {
+    uint32_t const cap = 1u << log2cap;
+    if (z == kEmptyKey) {
+        slot = cap;
+        return true;
+    }
+    uint32_t h = cell_hash(z, log2cap);
+    for (uint32_t probe = 0; probe < cap; ++probe) {
+        uint64_t const k = keys[h];
+        if (k == z) {
+            slot = h;
+            return true;
+        }
+        if (k == kEmptyKey) return false;
+        h = (h + 1u) & (cap - 1u);
+    }
+    return false;
+}
+
+struct OtherSet {
+    float2 const* x;
+    uint64_t const* keys;
+    uint32_t const* count;
+    uint32_t const* start;
+    uint32_t const* members;
+    uint32_t log2cap;
+    uint32_t begin;
+};
+
+// The neighbour search of create_neighborhoods
+// (emerald/sph_common/neighborhood.h:199-282). Accepted candidates are kept
+// in `list` as (distance bits << 32 | scene-local index), sorted ascending,
+// which is the reference's (distance, index) order for non-negative
+// distances. Returns the count.
+__device__ int find_neighbors(float2 pos,
+                              uint32_t self,
+                              bool same_set,
+                              float cell,
+                              float max_distance,
+                              OtherSet const& o,
+                              uint64_t (&list)[kMaxNeighbors]) {
+    int32_t gx, gy;
+    grid_coord(pos, cell, gx, gy);
+    int cnt = 0;
+    for (int32_t j = gy - 1; cnt < kMaxNeighbors && j <= gy + 1; ++j) {
+        for (int32_t k = gx - 1; cnt < kMaxNeighbors && k <= gx + 1; ++k) {
+            uint32_t slot;
+            uint64_t const z = morton2(static_cast<uint32_t>(k), static_cast<uint32_t>(j));
+            if (!table_find(o.keys, o.log2cap, z, slot)) continue;
+            uint32_t const b = o.start[slot];
+            uint32_t const e = b + o.count[slot];
+            for (uint32_t m = b; cnt < kMaxNeighbors && m != e; ++m) {
+                uint32_t const other = o.members[m];
+                if (same_set && other == self) continue;
+                float2 const vec = sub2(o.x[other], pos);
+                float const dist = length2f(vec);
+                if (dist >= max_distance) continue;
+                uint64_t const key = (static_cast<uint64_t>(__float_as_uint(dist)) << 32) |
+                                     static_cast<uint64_t>(other - o.begin);
+                int p = cnt;
+                while (p > 0 && list[p - 1] > key) {
+                    list[p] = list[p - 1];
+                    --p;
+                }
+                list[p] = key;
+                ++cnt;
+            }
+        }
+    }
+    return cnt;
+}
+
+template <bool SOLID>
+__global__ void k_bin(Arena a) {
+    int32_t const s = (SOLID ? a.stile_scene : a.tile_scene)[blockIdx.x];
+    if (s < 0) return;
+    SceneParams const& P = a.sp[s];
+    if (!SOLID && !a.ss[s].active) return;
+    uint32_t const i = blockIdx.x * kTile + threadIdx.x;
+    uint32_t const begin = SOLID ? P.solid_begin : P.fluid_begin;
+    uint32_t const count = SOLID ? P.solid_count : P.fluid_count;
+    if (i - begin >= count) return;
+    float2 const p = SOLID ? a.xs[i] : a.x[i];
+    int32_t gx, gy;
+    grid_coord(p, P.cell_size, gx, gy);
+    uint64_t const z = morton2(static_cast<uint32_t>(gx), static_cast<uint32_t>(gy));
+    (SOLID ? a.szkey : a.zkey)[i] = z;
+    uint32_t const tb = SOLID ? P.stab_begin : P.ftab_begin;
+    uint32_t const lg = SOLID ? P.stab_log2 : P.ftab_log2;
+    uint32_t const slot = table_insert((SOLID ? a.skeys : a.fkeys) + tb, lg, z);
+    uint32_t* out_slot = SOLID ? a.sslot : a.slot;
+    if (slot == UINT32_MAX) {
+        atomicOr(&a.ss[s].error, kErrTableFull);
+        out_slot[i] = UINT32_MAX;
+        return;
+    }
+    uint32_t const r = atomicAdd((SOLID ? a.scount : a.fcount) + tb + slot, 1u);
+    out_slot[i] = tb + slot;
+    (SOLID ? a.srank : a.rank)[i] = r;
+}
+
+template <bool SOLID>
+__global__ void k_scatter(Arena a) {
+    int32_t const s = (SOLID ? a.stile_scene : a.tile_scene)[blockIdx.x];
+    if (s < 0) return;
+    SceneParams const& P = a.sp[s];
+    if (!SOLID && !a.ss[s].active) return;
+    uint32_t const i = blockIdx.x * kTile + threadIdx.x;
+    uint32_t const begin = SOLID ? P.solid_begin : P.fluid_begin;
+    uint32_t const count = SOLID ? P.solid_count : P.fluid_count;
+    if (i - begin >= count) return;
+    uint32_t const slot = (SOLID ? a.sslot : a.slot)[i];
+    if (slot == UINT32_MAX) return;
+    uint32_t const pos = (SOLID ? a.sstart : a.fstart)[slot] + (SOLID ? a.srank : a.rank)[i];
+    (SOLID ? a.smembers : a.members)[pos] = i;
+}
+
+// Orders every cell's members by index (the within-cell order of the
+// reference's sorted (z, index) pairs).
+__global__ void k_sort_cells(uint32_t const* count,
+                             uint32_t const* start,
+                             uint32_t* members,
+                             uint32_t total) {
+    uint32_t const e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    uint32_t const c = count[e];
+    if (c < 2) return;
+    uint32_t* m = members + start[e];
+    for (uint32_t q = 1; q < c; ++q) {
+        uint32_t const v = m[q];
+        uint32_t p = q;
+        while (p > 0 && m[p - 1] > v) {
+            m[p] = m[p - 1];
+            --p;
+        }
+        m[p] = v;
+    }
+}
+
+template <bool SOLID_OTHER>
+__global__ void k_neighbors(Arena a, int write_kernels) {
+    int32_t const s = a.tile_scene[blockIdx.x];
+    if (s < 0) return;
+    SceneParams const& P = a.sp[s];
+    if (!a.ss[s].active) return;
+    uint32_t const i = blockIdx.x * kTile + threadIdx.x;
+    if (i - P.fluid_begin >= P.fluid_count) return;
+    float const h = P.support;
+    float const cell = P.cell_size;
+    OtherSet o;
+    if (SOLID_OTHER) {
+        o = OtherSet{a.xs, a.skeys + P.stab_begin, a.scount + P.stab_begin, a.sstart + P.stab_begin,
+                     a.smembers, P.stab_log2, P.solid_begin};
+    } else {
+        o = OtherSet{a.x, a.fkeys + P.ftab_begin, a.fcount + P.ftab_begin, a.fstart + P.ftab_begin,
+                     a.members, P.ftab_log2, P.fluid_begin};
+    }
+    float2 const pos = a.x[i];
+    uint64_t list[kMaxNeighbors];
+    int const cnt = (SOLID_OTHER && P.solid_count == 0)
+                      ? 0
+                      : find_neighbors(pos, i, !SOLID_OTHER, cell, cell, o, list);
+    uint8_t* cnt_out = SOLID_OTHER ? a.ns_cnt : a.nf_cnt;
+    uint32_t* idx_out = SOLID_OTHER ? a.ns_idx : a.nf_idx;
+    float* w_out = SOLID_OTHER ? a.ns_w : a.nf_w;
+    float2* gw_out = SOLID_OTHER ? a.ns_gw : a.nf_gw;
+    cnt_out[i] = static_cast<uint8_t>(cnt);
+    size_t const stride = a.stride;
+    for (int k = 0; k < cnt; ++k) {
+        uint32_t const j = o.begin + static_cast<uint32_t>(list[k] & 0xffffffffu);
+        size_t const e = static_cast<size_t>(k) * stride + i;
+        idx_out[e] = j;
+        if (write_kernels) {
+            float const dist = __uint_as_float(static_cast<uint32_t>(list[k] >> 32));
+            w_out[e] = kernel_w(dist, h);
+            gw_out[e] = kernel_grad_w(neg2(sub2(o.x[j], pos)), h);
+        }
+    }
+}
+
+// compute_volumes (emerald/sph2d_box/solids.cpp:52-74) over the solid-solid
+// neighbourhood of compute_neighbor_data_and_volumes (:76-137):
+// V = numer / (W(0) + sum W) in list order, 1/W(0) without neighbours.
+__global__ void k_solid_volumes(Arena a, float numer, int only_scene) {
+    int32_t const s = a.stile_scene[blockIdx.x];
+    if (s < 0 || s != only_scene) return;
+    SceneParams const& P = a.sp[s];
+    uint32_t const i = blockIdx.x * kTile + threadIdx.x;
+    if (i - P.solid_begin >= P.solid_count) return;
+    OtherSet const o{a.xs, a.skeys + P.stab_begin, a.scount + P.stab_begin, a.sstart + P.stab_begin,
+                     a.smembers, P.stab_log2, P.solid_begin};
+    uint64_t list[kMaxNeighbors];
+    int const cnt = find_neighbors(a.xs[i], i, true, P.cell_size, P.cell_size, o, list);
+    float const w0 = kernel_w(0.0f, P.support);
+    if (!cnt) {
+        a.vols[i] = 1.0f / w0;
+        return;
+    }
+    float m = w0;
+    for (int k = 0; k < cnt; ++k) {
+        m += kernel_w(__uint_as_float(static_cast<uint32_t>(list[k] >> 32)), P.support);
+    }
+    a.vols[i] = numer / m;
+}
+
+// Exclusive scan of uint32 counts: per-block sums, a single-block scan of
+// the sums, then per-block scans offset by the scanned sums.
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanBlock = kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t v) {
+    int const lane = threadIdx.x & 31;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t const t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Block-wide exclusive scan of one value per thread; returns the block total.
+__device__ uint32_t block_exclusive_scan(uint32_t v, uint32_t& excl) {
+    __shared__ uint32_t warp_sums[kScanThreads / 32];
+    int const lane = threadIdx.x & 31;
+    int const warp = threadIdx.x >> 5;
+    uint32_t const incl = warp_inclusive_scan(v);
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kScanThreads / 32 ? warp_sums[lane] : 0u;
+        w = warp_inclusive_scan(w);
+        if (lane < kScanThreads / 32) warp_sums[lane] = w;
+    }
+    __syncthreads();
+    uint32_t const warp_off = warp ? warp_sums[warp - 1] : 0u;
+    excl = warp_off + incl - v;
+    uint32_t const total = warp_sums[kScanThreads / 32 - 1];
+    __syncthreads();
+    return total;
+}
+
+__global__ void k_scan_reduce(uint32_t const* in, uint32_t n, uint32_t* sums) {
+    size_t const base = static_cast<size_t>(blockIdx.x) * kScanBlock + threadIdx.x * kScanItems;
+    uint32_t t = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        size_t const e = base + k;
+        if (e < n) t += in[e];
+    }
+    uint32_t excl;
+    uint32_t const total = block_exclusive_scan(t, excl);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_sums(uint32_t* sums, uint32_t nblocks) {
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < nblocks; base += kScanThreads) {
+        uint32_t const e = base + threadIdx.x;
+        uint32_t const v = e < nblocks ? sums[e] : 0u;
+        uint32_t excl;
+        uint32_t const total = block_exclusive_scan(v, excl);
+        if (e < nblocks) sums[e] = carry + excl;
+        carry += total;
+    }
+}
+
+__global__ void k_scan_apply(uint32_t const* in, uint32_t n, uint32_t const* sums, uint32_t* out) {
+    size_t const base = static_cast<size_t>(blockIdx.x) * kScanBlock + threadIdx.x * kScanItems;
+    uint32_t vals[kScanItems];
+    uint32_t t = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        size_t const e = base + k;
+        vals[k] = e < n ? in[e] : 0u;
+        t += vals[k];
+    }
+    uint32_t excl;
+    block_exclusive_scan(t, excl);
+    uint32_t run = sums[blockIdx.x] + excl;
+    for (int k = 0; k < kScanItems; ++k) {
+        size_t const e = base + k;
+        if (e < n) out[e] = run;
+        run += vals[k];
+    }
+}
+
+}  // namespace
+
+uint32_t scan_scratch_words(uint32_t n) { return (n + kScanBlock - 1) / kScanBlock + 1; }
+
+void launch_exclusive_scan(uint32_t const* in, uint32_t n, uint32_t* out, uint32_t* scratch,
+                           cudaStream_t st) {
+    if (n == 0) return;
+    uint32_t const nb = (n + kScanBlock - 1) / kScanBlock;
+    k_scan_reduce<<<nb, kScanThreads, 0, st>>>(in, n, scratch);
+    k_scan_sums<<<1, kScanThreads, 0, st>>>(scratch, nb);
+    k_scan_apply<<<nb, kScanThreads, 0, st>>>(in, n, scratch, out);
+}
+
+void launch_build_cells(Arena const& a, bool solid, uint32_t tiles, uint32_t* scan_scratch,
+                        cudaStream_t st) {
+    if (solid) {
+        cudaMemsetAsync(a.skeys, 0xff, sizeof(uint64_t) * a.stab_total, st);
+        cudaMemsetAsync(a.scount, 0, sizeof(uint32_t) * a.stab_total, st);
+        k_bin<true><<<tiles, kTile, 0, st>>>(a);
+        launch_exclusive_scan(a.scount, a.stab_total, a.sstart, scan_scratch, st);
+        k_scatter<true><<<tiles, kTile, 0, st>>>(a);
+        k_sort_cells<<<(a.stab_total + 255) / 256, 256, 0, st>>>(a.scount, a.sstart, a.smembers,
+                                                                 a.stab_total);
+    } else {
+        cudaMemsetAsync(a.fkeys, 0xff, sizeof(uint64_t) * a.ftab_total, st);
+        cudaMemsetAsync(a.fcount, 0, sizeof(uint32_t) * a.ftab_total, st);
+        k_bin<false><<<tiles, kTile, 0, st>>>(a);
+        launch_exclusive_scan(a.fcount, a.ftab_total, a.fstart, scan_scratch, st);
+        k_scatter<false><<<tiles, kTile, 0, st>>>(a);
+        k_sort_cells<<<(a.ftab_total + 255) / 256, 256, 0, st>>>(a.fcount, a.fstart, a.members,
+                                                                 a.ftab_total);
+    }
+}
+
+void launch_neighbors(Arena const& a, uint32_t tiles, bool solid_other, bool write_kernels,
+                      cudaStream_t st) {
+    if (solid_other) {
+        k_neighbors<true><<<tiles, kTile, 0, st>>>(a, write_kernels ? 1 : 0);
+    } else {
+        k_neighbors<false><<<tiles, kTile, 0, st>>>(a, write_kernels ? 1 : 0);
+    }
+}
+
+void launch_solid_volumes(Arena const& a, uint32_t solid_tiles, float numer, int scene,
+                          cudaStream_t st) {
+    k_solid_volumes<<<solid_tiles, kTile, 0, st>>>(a, numer, scene);
+}
+
+}  // namespace emerald

@@ -1,0 +1,350 @@
+// extern "C" entry points of include/emerald_sph.h over the Engine.
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/emerald_sph.h"
+#include "engine.hpp"
+
+namespace emerald {
+void lattice_config(emerald_params const& p, float dx, float dt, float& mass, float& denom);
+size_t block_scene(uint32_t nx, uint32_t ny, float dx, float x0, float y0, float jitter,
+                   uint64_t seed, float* xy);
+size_t wall_scene(float dx, float length, int layers, float* xy);
+std::vector<float2> world_walls(emerald_params const& p);
+std::vector<float2> dam_break(emerald_params const& p, float2 const* solid, size_t n_solid);
+}  // namespace emerald
+
+using namespace emerald;
+
+struct emerald_sim {
+    Engine engine;
+    int scene;
+    emerald_params params;
+    emerald_sim(uint32_t n, uint32_t ns) : engine(n, ns, 1), scene(-1), params{} {}
+};
+
+namespace {
+
+thread_local std::string t_error;
+
+int fail(int code, std::string const& msg) {
+    t_error = msg;
+    return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        return f();
+    } catch (std::bad_alloc const&) {
+        return fail(EMERALD_ENOMEM, "device or host allocation failed");
+    } catch (std::exception const& e) {
+        return fail(EMERALD_ECUDA, e.what());
+    }
+}
+
+bool valid_method(int32_t m) { return m >= 0 && m <= 4; }
+
+int check_params(emerald_params const* p) {
+    if (!p) return fail(EMERALD_EINVAL, "params is NULL");
+    if (!(p->support > 0.0f)) return fail(EMERALD_EINVAL, "support must be positive");
+    if (!(p->target_density > 0.0f)) return fail(EMERALD_EINVAL, "target_density must be positive");
+    if (p->time_per_step_flicks <= 0) return fail(EMERALD_EINVAL, "time_per_step must be positive");
+    if (p->sub_steps <= 0) return fail(EMERALD_EINVAL, "sub_steps must be positive");
+    return EMERALD_OK;
+}
+
+void fill_stats(SceneState const& s, emerald_step_stats* out, int substeps) {
+    if (!out) return;
+    out->sub_steps = substeps;
+    out->pressure_iterations = s.stat_iters;
+    out->error_average = s.stat_avg;
+    out->error_max = s.stat_max;
+    out->divergence_iterations = s.stat_div_iters;
+    out->divergence_error_average = s.stat_div_avg;
+    out->divergence_error_max = s.stat_div_max;
+    out->dt = s.dt;
+    out->time_seconds = double(s.frame_time + s.elapsed) / 705600000.0;
+    out->error_flags = s.error;
+}
+
+}  // namespace
+
+extern "C" {
+
+char const* emerald_last_error(void) { return t_error.c_str(); }
+
+int64_t emerald_kernel_launches(void) { return kernel_launch_count(); }
+
+int emerald_default_params(emerald_params* out) {
+    if (!out) return fail(EMERALD_EINVAL, "out is NULL");
+    default_params(*out);
+    return EMERALD_OK;
+}
+
+int emerald_config(emerald_params const* params, float* out) {
+    if (int rc = check_params(params)) return rc;
+    if (!out) return fail(EMERALD_EINVAL, "out is NULL");
+    DerivedConfig const c = derive_config(*params);
+    out[0] = c.seconds_per_sub_step;
+    out[1] = c.mass_per_particle;
+    out[2] = c.draw_radius;
+    out[3] = c.pressure_correction_denom;
+    return EMERALD_OK;
+}
+
+int emerald_lattice_config(emerald_params const* params, float dx, float dt, float* out) {
+    if (int rc = check_params(params)) return rc;
+    if (!out || !(dx > 0.0f)) return fail(EMERALD_EINVAL, "bad lattice arguments");
+    lattice_config(*params, dx, dt, out[0], out[1]);
+    return EMERALD_OK;
+}
+
+uint64_t emerald_z_index(uint32_t x, uint32_t y) { return morton2(x, y); }
+
+size_t emerald_block_scene(uint32_t nx, uint32_t ny, float dx, float x0, float y0, float jitter,
+                           uint64_t seed, float* xy) {
+    return block_scene(nx, ny, dx, x0, y0, jitter, seed, xy);
+}
+
+size_t emerald_wall_scene(float dx, float length, int32_t layers, float* xy) {
+    if (!(dx > 0.0f) || layers < 0) return 0;
+    return wall_scene(dx, length, layers, xy);
+}
+
+size_t emerald_world_walls(emerald_params const* params, float* xy) {
+    if (check_params(params)) return 0;
+    auto const pts = world_walls(*params);
+    if (xy) std::memcpy(xy, pts.data(), pts.size() * sizeof(float2));
+    return pts.size();
+}
+
+size_t emerald_dam_break(emerald_params const* params, float const* solid_xy, size_t n_solid,
+                         float* xy) {
+    if (check_params(params)) return 0;
+    auto const pts = dam_break(*params, reinterpret_cast<float2 const*>(solid_xy), n_solid);
+    if (xy) std::memcpy(xy, pts.data(), pts.size() * sizeof(float2));
+    return pts.size();
+}
+
+int emerald_sim_create(emerald_params const* params,
+                       float const* solid_xy,
+                       float const* solid_volumes,
+                       size_t n_solid,
+                       float const* fluid_xy,
+                       float const* fluid_v,
+                       size_t n_fluid,
+                       emerald_sim** out) {
+    if (int rc = check_params(params)) return rc;
+    if (!out) return fail(EMERALD_EINVAL, "out is NULL");
+    if ((n_fluid && !fluid_xy) || (n_solid && !solid_xy)) {
+        return fail(EMERALD_EINVAL, "particle arrays are NULL");
+    }
+    if (n_fluid > (1u << 30) || n_solid > (1u << 30)) return fail(EMERALD_EINVAL, "too many particles");
+    return guarded([&] {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(EMERALD_ECUDA, "no CUDA device");
+        }
+        auto* sim = new emerald_sim(uint32_t(n_fluid), uint32_t(n_solid));
+        sim->params = *params;
+        SceneSpec spec;
+        spec.params = *params;
+        spec.method = kDfsph;
+        spec.mode = kFrame;
+        spec.solid_xy = solid_xy;
+        spec.solid_volumes = solid_volumes;
+        spec.n_solid = uint32_t(n_solid);
+        spec.fluid_xy = fluid_xy;
+        spec.fluid_v = fluid_v;
+        spec.n_fluid = uint32_t(n_fluid);
+        sim->scene = sim->engine.add_scene(spec);
+        if (sim->scene < 0) {
+            delete sim;
+            return fail(EMERALD_ENOMEM, "scene does not fit");
+        }
+        sim->engine.set_active(sim->scene, true);
+        *out = sim;
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_destroy(emerald_sim* sim) {
+    delete sim;
+    return EMERALD_OK;
+}
+
+int emerald_sim_begin_frame(emerald_sim* sim, int32_t method) {
+    if (!sim || !valid_method(method)) return fail(EMERALD_EINVAL, "bad arguments");
+    return guarded([&] {
+        sim->engine.begin_frame(method);
+        sim->engine.check("begin_frame");
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_sub_step(emerald_sim* sim, int32_t method, float t, float dt,
+                         emerald_step_stats* stats) {
+    (void)t;
+    if (!sim || !valid_method(method)) return fail(EMERALD_EINVAL, "bad arguments");
+    return guarded([&] {
+        sim->engine.set_mode(sim->scene, kFixedDt, dt);
+        sim->engine.substep(method);
+        if (stats) fill_stats(sim->engine.scene_state(sim->scene), stats, 1);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_frame(emerald_sim* sim, int32_t method, emerald_step_stats* stats) {
+    if (!sim || !valid_method(method)) return fail(EMERALD_EINVAL, "bad arguments");
+    return guarded([&] {
+        sim->engine.set_mode(sim->scene, kFrame, 0.0f);
+        int n = 0;
+        SceneState s{};
+        do {
+            sim->engine.substep(method);
+            ++n;
+            s = sim->engine.scene_state(sim->scene);
+        } while (s.remaining > 0 && n < 100000);
+        fill_stats(s, stats, n);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_advance(emerald_sim* sim, int32_t method, int32_t n_substeps,
+                        emerald_step_stats* stats) {
+    if (!sim || !valid_method(method) || n_substeps < 0) return fail(EMERALD_EINVAL, "bad arguments");
+    return guarded([&] {
+        sim->engine.set_mode(sim->scene, kFrame, 0.0f);
+        for (int k = 0; k < n_substeps; ++k) sim->engine.substep(method);
+        if (stats) fill_stats(sim->engine.scene_state(sim->scene), stats, n_substeps);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_counts(emerald_sim const* sim, size_t* n_fluid, size_t* n_solid) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    if (n_fluid) *n_fluid = sim->engine.fluid_count(sim->scene);
+    if (n_solid) *n_solid = sim->engine.solid_count(sim->scene);
+    return EMERALD_OK;
+}
+
+int emerald_sim_time(emerald_sim const* sim, int64_t* flicks) {
+    if (!sim || !flicks) return fail(EMERALD_EINVAL, "bad arguments");
+    return guarded([&] {
+        SceneState const s = const_cast<emerald_sim*>(sim)->engine.scene_state(sim->scene);
+        *flicks = s.frame_time + s.elapsed;
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_get_state(emerald_sim* sim, float* x, float* v) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    return guarded([&] {
+        sim->engine.get_state(sim->scene, x, v);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_set_state(emerald_sim* sim, float const* x, float const* v) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    return guarded([&] {
+        sim->engine.set_state(sim->scene, x, v);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_get_solid(emerald_sim* sim, float* xy, float* volumes) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    return guarded([&] {
+        sim->engine.get_solid(sim->scene, xy, volumes);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_get_array(emerald_sim* sim, char const* name, float* out, int32_t* width) {
+    if (!sim || !name) return fail(EMERALD_EINVAL, "bad arguments");
+    return guarded([&] {
+        int w = 0;
+        if (!sim->engine.get_array(sim->scene, name, out, w)) {
+            return fail(EMERALD_ENOTFOUND, std::string("no array ") + name);
+        }
+        if (width) *width = w;
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_get_neighbors(emerald_sim* sim, int32_t solid, uint8_t* counts, uint32_t* idx,
+                              float* w, float* gw) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    return guarded([&] {
+        sim->engine.get_neighbors(sim->scene, solid != 0, counts, idx, w, gw);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_get_sort(emerald_sim* sim, int32_t solid, int32_t* grid_coords, uint64_t* z,
+                         uint64_t* pair_z, uint64_t* pair_index, uint32_t* block_indices,
+                         uint64_t* blocks, size_t* nblocks) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    return guarded([&] {
+        size_t const nb = sim->engine.get_sort(sim->scene, solid != 0, grid_coords, z, pair_z,
+                                               pair_index, block_indices, blocks);
+        if (nblocks) *nblocks = nb;
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_set_stream(emerald_sim* sim, void* cuda_stream) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    sim->engine.set_stream(static_cast<cudaStream_t>(cuda_stream));
+    return EMERALD_OK;
+}
+
+int emerald_sim_device_state(emerald_sim* sim, void** x, void** v) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    if (x) *x = sim->engine.device_x(sim->scene);
+    if (v) *v = sim->engine.device_v(sim->scene);
+    return EMERALD_OK;
+}
+
+int emerald_sim_enable_timing(emerald_sim* sim, int32_t enable) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    return guarded([&] {
+        sim->engine.reset_timing();
+        sim->engine.enable_timing(enable != 0);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_kernel_times(emerald_sim* sim, char* names, size_t names_len, double* ms,
+                             int32_t* launches, int32_t* count) {
+    if (!sim || !count) return fail(EMERALD_EINVAL, "bad arguments");
+    return guarded([&] {
+        KernelTimes const& t = sim->engine.kernel_times();
+        int const cap = *count;
+        int k = 0;
+        std::string joined;
+        for (auto const& kv : t.ms) {
+            if (k < cap) {
+                if (ms) ms[k] = kv.second;
+                if (launches) launches[k] = t.launches.at(kv.first);
+            }
+            if (!joined.empty()) joined += '\n';
+            joined += kv.first;
+            ++k;
+        }
+        if (names && names_len) {
+            std::strncpy(names, joined.c_str(), names_len - 1);
+            names[names_len - 1] = '\0';
+        }
+        *count = k;
+        return EMERALD_OK;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,751 @@
+// Engine: device arena management and the per-method launch sequence of one
+// sub-step (emerald/sph2d_box/{iisph,iisph_ap,iisph_pseudo_ap,dfsph_p,pcisph}.cpp).
+#include "engine.hpp"
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+namespace emerald {
+
+namespace {
+
+std::atomic<int64_t> g_launches{0};
+
+uint32_t ceil_log2(uint64_t v) {
+    uint32_t l = 0;
+    while ((uint64_t(1) << l) < v) ++l;
+    return l;
+}
+
+uint32_t tiles_for(uint32_t n) { return (n + kTile - 1) / kTile; }
+
+}  // namespace
+
+int64_t kernel_launch_count() { return g_launches.load(); }
+
+// ------------------------------------------------------------ allocator
+
+RangeAllocator::RangeAllocator(uint32_t capacity) : capacity_(capacity) {
+    if (capacity) free_[0] = capacity;
+}
+
+bool RangeAllocator::alloc(uint32_t size, uint32_t& begin) {
+    if (size == 0) {
+        begin = 0;
+        return true;
+    }
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+        if (it->second >= size) {
+            begin = it->first;
+            uint32_t const rest = it->second - size;
+            free_.erase(it);
+            if (rest) free_[begin + size] = rest;
+            return true;
+        }
+    }
+    return false;
+}
+
+void RangeAllocator::release(uint32_t begin, uint32_t size) {
+    if (!size) return;
+    auto it = free_.emplace(begin, size).first;
+    auto next = std::next(it);
+    if (next != free_.end() && it->first + it->second == next->first) {
+        it->second += next->second;
+        free_.erase(next);
+    }
+    if (it != free_.begin()) {
+        auto prev = std::prev(it);
+        if (prev->first + prev->second == it->first) {
+            prev->second += it->second;
+            free_.erase(it);
+        }
+    }
+}
+
+uint32_t RangeAllocator::largest_free() const {
+    uint32_t best = 0;
+    for (auto const& kv : free_) best = std::max(best, kv.second);
+    return best;
+}
+
+// --------------------------------------------------------------- engine
+
+void Engine::check(char const* what) {
+    cudaError_t const e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
+  : fluid_cap_(tiles_for(std::max<uint32_t>(fluid_capacity, 1)) * kTile),
+    solid_cap_(tiles_for(std::max<uint32_t>(solid_capacity, 1)) * kTile),
+    max_scenes_(std::max(max_scenes, 1)),
+    fluid_tiles_(fluid_cap_ / kTile),
+    solid_tiles_(solid_cap_ / kTile) {
+    // Cell tables: a scene of n particles takes 2^ceil_log2(max(64, 2n)) + 1
+    // slots, below 4n + 65.
+    uint64_t const ftab = 4ull * fluid_cap_ + 72ull * max_scenes_;
+    uint64_t const stab = 4ull * solid_cap_ + 72ull * max_scenes_;
+    if (ftab > 0xffffffffull || stab > 0xffffffffull) throw std::runtime_error("arena too large");
+    ftab_ = RangeAllocator(uint32_t(ftab));
+    stab_ = RangeAllocator(uint32_t(stab));
+
+    auto dev = [&](size_t bytes) -> void* {
+        void* p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(bytes, 16)) != cudaSuccess) {
+            cudaGetLastError();
+            throw std::bad_alloc();
+        }
+        allocations_.push_back(p);
+        return p;
+    };
+    size_t const N = fluid_cap_;
+    size_t const S = solid_cap_;
+    size_t const E = N * kMaxNeighbors;
+    d_sp_ = static_cast<SceneParams*>(dev(sizeof(SceneParams) * max_scenes_));
+    d_ss_ = static_cast<SceneState*>(dev(sizeof(SceneState) * max_scenes_));
+    d_tile_scene_ = static_cast<int32_t*>(dev(sizeof(int32_t) * (N / kTile)));
+    d_stile_scene_ = static_cast<int32_t*>(dev(sizeof(int32_t) * (S / kTile)));
+    a_.sp = d_sp_;
+    a_.ss = d_ss_;
+    a_.tile_scene = d_tile_scene_;
+    a_.stile_scene = d_stile_scene_;
+    a_.stride = uint32_t(N);
+    a_.sstride = uint32_t(S);
+    a_.x = static_cast<float2*>(dev(8 * N));
+    a_.v = static_cast<float2*>(dev(8 * N));
+    a_.rho = static_cast<float*>(dev(4 * N));
+    a_.rho_star = static_cast<float*>(dev(4 * N));
+    a_.pbuf0 = static_cast<float*>(dev(4 * N));
+    a_.pbuf1 = static_cast<float*>(dev(4 * N));
+    a_.alpha = static_cast<float*>(dev(4 * N));
+    a_.kdiv = static_cast<float*>(dev(4 * N));
+    a_.kdens = static_cast<float*>(dev(4 * N));
+    a_.qdiv = static_cast<float*>(dev(4 * N));
+    a_.qdens = static_cast<float*>(dev(4 * N));
+    a_.aii = static_cast<float*>(dev(4 * N));
+    a_.dii = static_cast<float2*>(dev(8 * N));
+    a_.sdp = static_cast<float2*>(dev(8 * N));
+    a_.acc = static_cast<float2*>(dev(8 * N));
+    a_.vext = static_cast<float2*>(dev(8 * N));
+    a_.xstar = static_cast<float2*>(dev(8 * N));
+    a_.vstar = static_cast<float2*>(dev(8 * N));
+    a_.fp = static_cast<float2*>(dev(8 * N));
+    a_.nf_cnt = static_cast<uint8_t*>(dev(N));
+    a_.nf_idx = static_cast<uint32_t*>(dev(4 * E));
+    a_.nf_w = static_cast<float*>(dev(4 * E));
+    a_.nf_gw = static_cast<float2*>(dev(8 * E));
+    a_.ns_cnt = static_cast<uint8_t*>(dev(N));
+    a_.ns_idx = static_cast<uint32_t*>(dev(4 * E));
+    a_.ns_w = static_cast<float*>(dev(4 * E));
+    a_.ns_gw = static_cast<float2*>(dev(8 * E));
+    a_.slot = static_cast<uint32_t*>(dev(4 * N));
+    a_.rank = static_cast<uint32_t*>(dev(4 * N));
+    a_.members = static_cast<uint32_t*>(dev(4 * N));
+    a_.zkey = static_cast<uint64_t*>(dev(8 * N));
+    a_.ftab_total = ftab_.capacity();
+    a_.fkeys = static_cast<uint64_t*>(dev(8ull * a_.ftab_total));
+    a_.fcount = static_cast<uint32_t*>(dev(4ull * a_.ftab_total));
+    a_.fstart = static_cast<uint32_t*>(dev(4ull * a_.ftab_total));
+    a_.xs = static_cast<float2*>(dev(8 * S));
+    a_.vs = static_cast<float2*>(dev(8 * S));
+    a_.vols = static_cast<float*>(dev(4 * S));
+    a_.sslot = static_cast<uint32_t*>(dev(4 * S));
+    a_.srank = static_cast<uint32_t*>(dev(4 * S));
+    a_.smembers = static_cast<uint32_t*>(dev(4 * S));
+    a_.szkey = static_cast<uint64_t*>(dev(8 * S));
+    a_.stab_total = stab_.capacity();
+    a_.skeys = static_cast<uint64_t*>(dev(8ull * a_.stab_total));
+    a_.scount = static_cast<uint32_t*>(dev(4ull * a_.stab_total));
+    a_.sstart = static_cast<uint32_t*>(dev(4ull * a_.stab_total));
+    uint32_t const scan_words =
+      std::max(scan_scratch_words(a_.ftab_total), scan_scratch_words(a_.stab_total)) + 64;
+    d_scan_ = static_cast<uint32_t*>(dev(4ull * scan_words));
+    d_running_ = static_cast<int*>(dev(sizeof(int)));
+    if (cudaMallocHost(reinterpret_cast<void**>(&h_running_), sizeof(int)) != cudaSuccess) {
+        throw std::bad_alloc();
+    }
+    cudaMemset(d_ss_, 0, sizeof(SceneState) * max_scenes_);
+    cudaMemset(a_.vs, 0, 8 * S);
+    cudaMemset(a_.nf_cnt, 0, N);
+    cudaMemset(a_.ns_cnt, 0, N);
+    cudaMemset(a_.kdiv, 0, 4 * N);
+    cudaMemset(a_.kdens, 0, 4 * N);
+    scenes_.resize(max_scenes_);
+    tile_scene_.assign(N / kTile, -1);
+    stile_scene_.assign(S / kTile, -1);
+    upload_tiles();
+    check("engine allocation");
+}
+
+Engine::~Engine() {
+    for (auto& p : pending_) {
+        cudaEventDestroy(p.start);
+        cudaEventDestroy(p.stop);
+    }
+    for (auto e : event_pool_) cudaEventDestroy(e);
+    if (sort_buf_) cudaFree(sort_buf_);
+    for (void* p : allocations_) cudaFree(p);
+    if (h_running_) cudaFreeHost(h_running_);
+}
+
+template <class F>
+void Engine::launch(char const* name, F&& f) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (!timing_) {
+        f();
+        return;
+    }
+    auto take = [&]() {
+        cudaEvent_t e;
+        if (!event_pool_.empty()) {
+            e = event_pool_.back();
+            event_pool_.pop_back();
+        } else {
+            cudaEventCreate(&e);
+        }
+        return e;
+    };
+    Pending p{name, take(), take()};
+    cudaEventRecord(p.start, st_);
+    f();
+    cudaEventRecord(p.stop, st_);
+    pending_.push_back(p);
+}
+
+void Engine::enable_timing(bool on) { timing_ = on; }
+
+void Engine::reset_timing() {
+    kernel_times();
+    times_ = KernelTimes{};
+}
+
+KernelTimes const& Engine::kernel_times() {
+    if (!pending_.empty()) {
+        cudaStreamSynchronize(st_);
+        for (auto& p : pending_) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, p.start, p.stop);
+            times_.ms[p.name] += ms;
+            times_.launches[p.name] += 1;
+            event_pool_.push_back(p.start);
+            event_pool_.push_back(p.stop);
+        }
+        pending_.clear();
+    }
+    return times_;
+}
+
+void Engine::upload_tiles() {
+    cudaMemcpyAsync(d_tile_scene_, tile_scene_.data(), sizeof(int32_t) * tile_scene_.size(),
+                    cudaMemcpyHostToDevice, st_);
+    cudaMemcpyAsync(d_stile_scene_, stile_scene_.data(), sizeof(int32_t) * stile_scene_.size(),
+                    cudaMemcpyHostToDevice, st_);
+    tiles_dirty_ = false;
+}
+
+void Engine::upload_params(int id) {
+    cudaMemcpyAsync(d_sp_ + id, &scenes_[id].p, sizeof(SceneParams), cudaMemcpyHostToDevice, st_);
+}
+
+int Engine::add_scene(SceneSpec const& spec) {
+    int id = -1;
+    for (int k = 0; k < max_scenes_; ++k) {
+        if (!scenes_[k].used) {
+            id = k;
+            break;
+        }
+    }
+    if (id < 0) return -1;
+    Scene sc;
+    sc.ftile_count = tiles_for(spec.n_fluid);
+    sc.stile_count = tiles_for(spec.n_solid);
+    uint32_t const flog = std::max<uint32_t>(6, ceil_log2(2ull * std::max<uint32_t>(spec.n_fluid, 1)));
+    uint32_t const slog = std::max<uint32_t>(6, ceil_log2(2ull * std::max<uint32_t>(spec.n_solid, 1)));
+    sc.ftab_size = (1u << flog) + 1;
+    sc.stab_size = (1u << slog) + 1;
+    uint32_t ft = 0, stl = 0, fb = 0, sb = 0;
+    if (!fluid_tiles_.alloc(sc.ftile_count, ft)) return -1;
+    if (!solid_tiles_.alloc(sc.stile_count, stl)) {
+        fluid_tiles_.release(ft, sc.ftile_count);
+        return -1;
+    }
+    if (!ftab_.alloc(sc.ftab_size, fb)) {
+        fluid_tiles_.release(ft, sc.ftile_count);
+        solid_tiles_.release(stl, sc.stile_count);
+        return -1;
+    }
+    if (!stab_.alloc(sc.stab_size, sb)) {
+        fluid_tiles_.release(ft, sc.ftile_count);
+        solid_tiles_.release(stl, sc.stile_count);
+        ftab_.release(fb, sc.ftab_size);
+        return -1;
+    }
+    sc.ftile_begin = ft;
+    sc.stile_begin = stl;
+    sc.used = true;
+    sc.active = false;
+
+    emerald_params const& ep = spec.params;
+    DerivedConfig const cfg = derive_config(ep);
+    SceneParams& P = sc.p;
+    P.fluid_begin = ft * kTile;
+    P.fluid_count = spec.n_fluid;
+    P.solid_begin = stl * kTile;
+    P.solid_count = spec.n_solid;
+    P.ftab_begin = fb;
+    P.ftab_log2 = flog;
+    P.stab_begin = sb;
+    P.stab_log2 = slog;
+    P.support = ep.support;
+    P.cell_size = ep.support * 2.0f;
+    P.rho0 = ep.target_density;
+    P.mass = cfg.mass_per_particle;
+    P.fluid_volume = cfg.mass_per_particle / ep.target_density;
+    P.gravity = ep.gravity;
+    P.viscosity = ep.viscosity;
+    P.w0 = kernel_w(0.0f, ep.support);
+    P.iisph_omega = ep.iisph_omega;
+    P.iisph_err_avg = ep.iisph_error_average_threshold;
+    P.iisph_err_max = ep.iisph_error_max_threshold;
+    P.iisph_max_iter = ep.iisph_max_pressure_iterations;
+    P.dfsph_max_iter = ep.dfsph_max_correction_iterations;
+    P.dfsph_dens_avg = ep.dfsph_density_error_average_threshold;
+    P.dfsph_dens_max = ep.dfsph_density_error_max_threshold;
+    P.dfsph_div_avg = ep.dfsph_divergence_error_average_threshold;
+    P.dfsph_div_max = ep.dfsph_divergence_error_max_threshold;
+    P.pcisph_denom = cfg.pressure_correction_denom;
+    P.method = spec.method;
+    P.mode = spec.mode;
+    P.time_per_step = ep.time_per_step_flicks;
+    P.sub_steps = ep.sub_steps;
+    P.min_denom = 60;
+    P.max_denom = spec.method == kIisph ? 6 : 4;
+    P.cfl_factor = spec.method == kIisph ? 0.2f : 0.4f;
+    P.seconds_per_sub_step = cfg.seconds_per_sub_step;
+    P.fixed_dt = spec.fixed_dt;
+    scenes_[id] = sc;
+
+    for (uint32_t t = 0; t < sc.ftile_count; ++t) tile_scene_[ft + t] = id;
+    for (uint32_t t = 0; t < sc.stile_count; ++t) stile_scene_[stl + t] = id;
+    upload_tiles();
+    upload_params(id);
+    SceneState s0{};
+    cudaMemcpyAsync(d_ss_ + id, &s0, sizeof(SceneState), cudaMemcpyHostToDevice, st_);
+    if (spec.n_fluid) {
+        cudaMemcpyAsync(a_.x + P.fluid_begin, spec.fluid_xy, 8ull * spec.n_fluid,
+                        cudaMemcpyHostToDevice, st_);
+        if (spec.fluid_v) {
+            cudaMemcpyAsync(a_.v + P.fluid_begin, spec.fluid_v, 8ull * spec.n_fluid,
+                            cudaMemcpyHostToDevice, st_);
+        } else {
+            cudaMemsetAsync(a_.v + P.fluid_begin, 0, 8ull * spec.n_fluid, st_);
+        }
+        cudaMemsetAsync(a_.kdiv + P.fluid_begin, 0, 4ull * spec.n_fluid, st_);
+        cudaMemsetAsync(a_.kdens + P.fluid_begin, 0, 4ull * spec.n_fluid, st_);
+        cudaMemsetAsync(a_.nf_cnt + P.fluid_begin, 0, spec.n_fluid, st_);
+        cudaMemsetAsync(a_.ns_cnt + P.fluid_begin, 0, spec.n_fluid, st_);
+    }
+    if (spec.n_solid) {
+        cudaMemcpyAsync(a_.xs + P.solid_begin, spec.solid_xy, 8ull * spec.n_solid,
+                        cudaMemcpyHostToDevice, st_);
+        cudaMemsetAsync(a_.vs + P.solid_begin, 0, 8ull * spec.n_solid, st_);
+    }
+    rebuild_solids();
+    if (spec.n_solid) {
+        if (spec.solid_volumes) {
+            cudaMemcpyAsync(a_.vols + P.solid_begin, spec.solid_volumes, 4ull * spec.n_solid,
+                            cudaMemcpyHostToDevice, st_);
+        } else {
+            launch("solid_volumes", [&] {
+                launch_solid_volumes(a_, solid_cap_ / kTile, 1.7f, id, st_);
+            });
+        }
+    }
+    check("add_scene");
+    return id;
+}
+
+void Engine::rebuild_solids() {
+    launch("build_cells_solid",
+           [&] { launch_build_cells(a_, true, solid_cap_ / kTile, d_scan_, st_); });
+}
+
+void Engine::remove_scene(int id) {
+    if (!scene_used(id)) return;
+    Scene& sc = scenes_[id];
+    SceneState s0{};
+    cudaMemcpyAsync(d_ss_ + id, &s0, sizeof(SceneState), cudaMemcpyHostToDevice, st_);
+    for (uint32_t t = 0; t < sc.ftile_count; ++t) tile_scene_[sc.ftile_begin + t] = -1;
+    for (uint32_t t = 0; t < sc.stile_count; ++t) stile_scene_[sc.stile_begin + t] = -1;
+    upload_tiles();
+    fluid_tiles_.release(sc.ftile_begin, sc.ftile_count);
+    solid_tiles_.release(sc.stile_begin, sc.stile_count);
+    ftab_.release(sc.p.ftab_begin, sc.ftab_size);
+    stab_.release(sc.p.stab_begin, sc.stab_size);
+    sc = Scene{};
+    rebuild_solids();
+}
+
+void Engine::set_active(int id, bool active) {
+    if (!scene_used(id)) return;
+    scenes_[id].active = active;
+    int32_t const v = active ? 1 : 0;
+    cudaMemcpyAsync(reinterpret_cast<char*>(d_ss_ + id) + offsetof(SceneState, active), &v,
+                    sizeof(int32_t), cudaMemcpyHostToDevice, st_);
+    cudaStreamSynchronize(st_);
+}
+
+void Engine::set_mode(int id, int32_t mode, float fixed_dt) {
+    if (!scene_used(id)) return;
+    SceneParams& P = scenes_[id].p;
+    if (P.mode != mode || P.fixed_dt != fixed_dt) {
+        P.mode = mode;
+        P.fixed_dt = fixed_dt;
+        upload_params(id);
+    }
+}
+
+int Engine::active_scenes() const {
+    int n = 0;
+    for (auto const& s : scenes_) n += (s.used && s.active) ? 1 : 0;
+    return n;
+}
+
+void Engine::begin_frame(int32_t method) {
+    if (method == kDfsph) {
+        launch("zero_kappas", [&] { launch_zero_kappas(a_, fluid_cap_ / kTile, st_); });
+    }
+}
+
+int Engine::max_iterations(int kind) const {
+    int m = 0;
+    for (auto const& s : scenes_) {
+        if (!s.used || !s.active) continue;
+        int const v = (kind == 0) ? s.p.iisph_max_iter : (kind == 3 ? 6 : s.p.dfsph_max_iter);
+        m = std::max(m, v);
+    }
+    return m;
+}
+
+void Engine::run_loop(int kind, int max_iter, int32_t method) {
+    uint32_t const tiles = fluid_cap_ / kTile;
+    launch("iter_reset", [&] { launch_iter_reset(a_, max_scenes_, st_); });
+    for (int it = 0; it < max_iter; ++it) {
+        switch (method) {
+        case kDfsph:
+            if (kind == 2) {
+                launch("dfsph_divergence", [&] { launch_dfsph_divergence(a_, tiles, st_); });
+                launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 1, st_); });
+            } else {
+                launch("dfsph_density", [&] { launch_dfsph_density(a_, tiles, st_); });
+                launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 1, 0, 1, st_); });
+            }
+            break;
+        case kIisph:
+            launch("iisph_sum_dij", [&] { launch_iisph_sum_dij(a_, tiles, st_); });
+            launch("iisph_beta_pressure", [&] { launch_iisph_beta_pressure(a_, tiles, st_); });
+            break;
+        case kIisphAp:
+        case kIisphPseudoAp: {
+            int const pseudo = method == kIisphPseudoAp ? 1 : 0;
+            launch("pressure_accel", [&] { launch_pressure_accel(a_, tiles, st_); });
+            launch("ap_iterate", [&] { launch_ap_iterate(a_, tiles, pseudo, st_); });
+            break;
+        }
+        case kPcisph:
+            launch("pc_predict", [&] { launch_pc_predict(a_, tiles, st_); });
+            launch("pc_density", [&] { launch_pc_density(a_, tiles, st_); });
+            launch("pc_forces", [&] { launch_pc_forces(a_, tiles, st_); });
+            break;
+        default: break;
+        }
+        launch("iter_check", [&] { launch_iter_check(a_, max_scenes_, kind, d_running_, st_); });
+        if (!unrolled_) {
+            cudaMemcpyAsync(h_running_, d_running_, sizeof(int), cudaMemcpyDeviceToHost, st_);
+            cudaStreamSynchronize(st_);
+            if (!*h_running_) break;
+        }
+    }
+}
+
+void Engine::substep(int32_t method) {
+    if (active_scenes() == 0) return;
+    uint32_t const tiles = fluid_cap_ / kTile;
+    for (int id = 0; id < max_scenes_; ++id) {
+        Scene& sc = scenes_[id];
+        if (!sc.used || !sc.active) continue;
+        if (sc.p.method != method) {
+            sc.p.method = method;
+            sc.p.max_denom = method == kIisph ? 6 : 4;
+            sc.p.cfl_factor = method == kIisph ? 0.2f : 0.4f;
+            upload_params(id);
+        }
+    }
+    launch("max_v2", [&] { launch_max_v2(a_, tiles, st_); });
+    launch("begin_substep", [&] { launch_begin_substep(a_, max_scenes_, st_); });
+    launch("build_cells", [&] { launch_build_cells(a_, false, tiles, d_scan_, st_); });
+    bool const kernels = method != kPcisph;
+    launch("neighbors_fluid", [&] { launch_neighbors(a_, tiles, false, kernels, st_); });
+    launch("neighbors_solid", [&] { launch_neighbors(a_, tiles, true, kernels, st_); });
+    switch (method) {
+    case kDfsph:
+        launch("dfsph_density_alpha", [&] { launch_dfsph_density_alpha(a_, tiles, st_); });
+        launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 0, st_); });
+        run_loop(2, max_iterations(2), method);
+        launch("apply_pressures_ext", [&] { launch_apply_pressures(a_, tiles, 1, 1, 0, st_); });
+        run_loop(1, max_iterations(1), method);
+        launch("integrate_positions", [&] { launch_integrate_positions(a_, tiles, st_); });
+        break;
+    case kIisph:
+        launch("iisph_density_dii", [&] { launch_iisph_density_dii(a_, tiles, st_); });
+        launch("iisph_aii", [&] { launch_iisph_aii(a_, tiles, st_); });
+        run_loop(0, max_iterations(0), method);
+        launch("make_q", [&] { launch_make_q(a_, tiles, st_); });
+        launch("apply_integrate", [&] { launch_apply_integrate(a_, tiles, st_); });
+        break;
+    case kIisphAp:
+    case kIisphPseudoAp: {
+        int const pseudo = method == kIisphPseudoAp ? 1 : 0;
+        launch("ap_density", [&] { launch_ap_density(a_, tiles, st_); });
+        launch("ap_diag", [&] { launch_ap_diag(a_, tiles, pseudo, st_); });
+        run_loop(0, max_iterations(0), method);
+        launch("ap_finish", [&] { launch_ap_finish(a_, tiles, pseudo, st_); });
+        break;
+    }
+    case kPcisph:
+        launch("pc_init", [&] { launch_pc_init(a_, tiles, st_); });
+        run_loop(3, 6, method);
+        launch("pc_final", [&] { launch_pc_final(a_, tiles, st_); });
+        break;
+    default: throw std::runtime_error("unknown method");
+    }
+    check("substep");
+}
+
+// ------------------------------------------------------------ accessors
+
+SceneState Engine::scene_state(int id) {
+    SceneState s{};
+    cudaMemcpyAsync(&s, d_ss_ + id, sizeof(SceneState), cudaMemcpyDeviceToHost, st_);
+    cudaStreamSynchronize(st_);
+    check("scene_state");
+    return s;
+}
+
+std::vector<SceneState> Engine::all_states() {
+    std::vector<SceneState> s(max_scenes_);
+    cudaMemcpyAsync(s.data(), d_ss_, sizeof(SceneState) * max_scenes_, cudaMemcpyDeviceToHost, st_);
+    cudaStreamSynchronize(st_);
+    check("all_states");
+    return s;
+}
+
+void Engine::get_state(int id, float* x, float* v) {
+    SceneParams const& P = scenes_[id].p;
+    if (x) cudaMemcpyAsync(x, a_.x + P.fluid_begin, 8ull * P.fluid_count, cudaMemcpyDeviceToHost, st_);
+    if (v) cudaMemcpyAsync(v, a_.v + P.fluid_begin, 8ull * P.fluid_count, cudaMemcpyDeviceToHost, st_);
+    cudaStreamSynchronize(st_);
+    check("get_state");
+}
+
+void Engine::set_state(int id, float const* x, float const* v) {
+    SceneParams const& P = scenes_[id].p;
+    if (x) cudaMemcpyAsync(a_.x + P.fluid_begin, x, 8ull * P.fluid_count, cudaMemcpyHostToDevice, st_);
+    if (v) cudaMemcpyAsync(a_.v + P.fluid_begin, v, 8ull * P.fluid_count, cudaMemcpyHostToDevice, st_);
+    cudaStreamSynchronize(st_);
+    check("set_state");
+}
+
+void Engine::get_solid(int id, float* xy, float* volumes) {
+    SceneParams const& P = scenes_[id].p;
+    if (xy) cudaMemcpyAsync(xy, a_.xs + P.solid_begin, 8ull * P.solid_count, cudaMemcpyDeviceToHost, st_);
+    if (volumes) {
+        cudaMemcpyAsync(volumes, a_.vols + P.solid_begin, 4ull * P.solid_count,
+                        cudaMemcpyDeviceToHost, st_);
+    }
+    cudaStreamSynchronize(st_);
+    check("get_solid");
+}
+
+bool Engine::get_array(int id, std::string const& name, float* out, int& width) {
+    SceneParams const& P = scenes_[id].p;
+    void const* src = nullptr;
+    width = 1;
+    if (name == "densities") {
+        src = a_.rho;
+    } else if (name == "pressures") {
+        if (P.method == kIisph) {
+            SceneState const s = scene_state(id);
+            src = (s.iter & 1) ? a_.pbuf1 : a_.pbuf0;
+        } else if (P.method == kDfsph) {
+            return false;
+        } else {
+            src = a_.pbuf0;
+        }
+    } else if (name == "density_stars") {
+        src = a_.rho_star;
+    } else if (name == "aiis") {
+        src = a_.aii;
+    } else if (name == "alphas") {
+        src = a_.alpha;
+    } else if (name == "divergence_kappas") {
+        src = a_.kdiv;
+    } else if (name == "density_kappas") {
+        src = a_.kdens;
+    } else if (name == "diis") {
+        src = a_.dii;
+        width = 2;
+    } else if (name == "sum_dij_pjs") {
+        src = a_.sdp;
+        width = 2;
+    } else if (name == "pressure_forces") {
+        src = a_.fp;
+        width = 2;
+    } else if (name == "pressure_accelerations") {
+        src = a_.acc;
+        width = 2;
+    } else if (name == "velocity_external_forces") {
+        src = a_.vext;
+        width = 2;
+    } else if (name == "position_stars") {
+        src = a_.xstar;
+        width = 2;
+    } else if (name == "velocity_stars") {
+        src = a_.vstar;
+        width = 2;
+    } else {
+        return false;
+    }
+    if (out) {
+        size_t const bytes = 4ull * width;
+        cudaMemcpyAsync(out, static_cast<char const*>(src) + bytes * P.fluid_begin,
+                        bytes * P.fluid_count, cudaMemcpyDeviceToHost, st_);
+        cudaStreamSynchronize(st_);
+        check("get_array");
+    }
+    return true;
+}
+
+void Engine::get_neighbors(int id, bool solid, uint8_t* counts, uint32_t* idx, float* w,
+                           float* gw) {
+    SceneParams const& P = scenes_[id].p;
+    uint32_t const n = P.fluid_count;
+    size_t const stride = a_.stride;
+    std::vector<uint8_t> cnt(n);
+    cudaMemcpyAsync(cnt.data(), (solid ? a_.ns_cnt : a_.nf_cnt) + P.fluid_begin, n,
+                    cudaMemcpyDeviceToHost, st_);
+    std::vector<uint32_t> ri(size_t(n) * kMaxNeighbors);
+    std::vector<float> rw(size_t(n) * kMaxNeighbors);
+    std::vector<float2> rg(size_t(n) * kMaxNeighbors);
+    for (int k = 0; k < kMaxNeighbors; ++k) {
+        size_t const off = size_t(k) * stride + P.fluid_begin;
+        if (idx) {
+            cudaMemcpyAsync(ri.data() + size_t(k) * n, (solid ? a_.ns_idx : a_.nf_idx) + off, 4ull * n,
+                            cudaMemcpyDeviceToHost, st_);
+        }
+        if (w) {
+            cudaMemcpyAsync(rw.data() + size_t(k) * n, (solid ? a_.ns_w : a_.nf_w) + off, 4ull * n,
+                            cudaMemcpyDeviceToHost, st_);
+        }
+        if (gw) {
+            cudaMemcpyAsync(rg.data() + size_t(k) * n, (solid ? a_.ns_gw : a_.nf_gw) + off, 8ull * n,
+                            cudaMemcpyDeviceToHost, st_);
+        }
+    }
+    cudaStreamSynchronize(st_);
+    check("get_neighbors");
+    uint32_t const base = solid ? P.solid_begin : P.fluid_begin;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (counts) counts[i] = cnt[i];
+        for (int k = 0; k < kMaxNeighbors; ++k) {
+            size_t const o = size_t(i) * kMaxNeighbors + k;
+            size_t const r = size_t(k) * n + i;
+            bool const live = k < cnt[i];
+            if (idx) idx[o] = live ? ri[r] - base : 0u;
+            if (w) w[o] = live ? rw[r] : 0.0f;
+            if (gw) {
+                gw[2 * o] = live ? rg[r].x : 0.0f;
+                gw[2 * o + 1] = live ? rg[r].y : 0.0f;
+            }
+        }
+    }
+}
+
+void Engine::ensure_sort_scratch(uint32_t n) {
+    if (sort_buf_ && sort_cap_ >= n) return;
+    if (sort_buf_) cudaFree(sort_buf_);
+    sort_buf_ = nullptr;
+    size_t const bytes = sort_scratch_bytes(n);
+    if (cudaMalloc(&sort_buf_, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        sort_buf_ = nullptr;
+        throw std::bad_alloc();
+    }
+    sort_cap_ = n;
+    sort_scratch_carve(sort_buf_, n, sort_);
+}
+
+size_t Engine::get_sort(int id, bool solid, int32_t* gc, uint64_t* z, uint64_t* pair_z,
+                        uint64_t* pair_index, uint32_t* block_indices, uint64_t* blocks) {
+    SceneParams const& P = scenes_[id].p;
+    Scene const& sc = scenes_[id];
+    uint32_t const n = solid ? P.solid_count : P.fluid_count;
+    if (n == 0) return 0;
+    ensure_sort_scratch(std::max(n, solid ? sc.stab_size : sc.ftab_size));
+    size_t const words = size_t(n);
+    void* out = nullptr;
+    size_t const bytes = words * (8 + 8 + 8 + 4 + 4 + 8) + 64;
+    if (cudaMalloc(&out, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        throw std::bad_alloc();
+    }
+    char* p = static_cast<char*>(out);
+    int2* d_gc = reinterpret_cast<int2*>(p);
+    p += 8 * words;
+    uint64_t* d_z = reinterpret_cast<uint64_t*>(p);
+    p += 8 * words;
+    uint64_t* d_pz = reinterpret_cast<uint64_t*>(p);
+    p += 8 * words;
+    uint32_t* d_pi = reinterpret_cast<uint32_t*>(p);
+    p += 4 * words;
+    uint32_t* d_bi = reinterpret_cast<uint32_t*>(p);
+    p += 4 * words;
+    uint32_t* d_bl = reinterpret_cast<uint32_t*>(p);
+    p += 8 * words;
+    uint32_t* d_nb = reinterpret_cast<uint32_t*>(p);
+    launch("sort_products", [&] {
+        launch_sort_products(a_, solid, id, solid ? P.solid_begin : P.fluid_begin, n,
+                             solid ? P.stab_begin : P.ftab_begin, solid ? sc.stab_size : sc.ftab_size,
+                             P.cell_size, sort_, d_gc, d_z, d_pz, d_pi, d_bi, d_bl, d_nb, st_);
+    });
+    uint32_t nb = 0;
+    std::vector<uint32_t> hpi(n), hbl(2 * size_t(n));
+    cudaMemcpyAsync(&nb, d_nb, 4, cudaMemcpyDeviceToHost, st_);
+    if (gc) cudaMemcpyAsync(gc, d_gc, 8 * words, cudaMemcpyDeviceToHost, st_);
+    if (z) cudaMemcpyAsync(z, d_z, 8 * words, cudaMemcpyDeviceToHost, st_);
+    if (pair_z) cudaMemcpyAsync(pair_z, d_pz, 8 * words, cudaMemcpyDeviceToHost, st_);
+    cudaMemcpyAsync(hpi.data(), d_pi, 4 * words, cudaMemcpyDeviceToHost, st_);
+    if (block_indices) cudaMemcpyAsync(block_indices, d_bi, 4 * words, cudaMemcpyDeviceToHost, st_);
+    cudaMemcpyAsync(hbl.data(), d_bl, 8 * words, cudaMemcpyDeviceToHost, st_);
+    cudaStreamSynchronize(st_);
+    cudaFree(out);
+    check("get_sort");
+    if (pair_index) {
+        for (uint32_t k = 0; k < n; ++k) pair_index[k] = hpi[k];
+    }
+    if (blocks) {
+        for (uint32_t b = 0; b < nb; ++b) {
+            blocks[2 * b] = hbl[2 * b];
+            blocks[2 * b + 1] = hbl[2 * b + 1];
+        }
+    }
+    return nb;
+}
+
+}  // namespace emerald

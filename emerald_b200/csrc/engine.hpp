@@ -1,0 +1,165 @@
+// Host-side engine: owns a device arena of scenes and launches the kernel
+// sequence of one solver sub-step for every active scene.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/emerald_sph.h"
+#include "engine_types.cuh"
+#include "kernels.cuh"
+#include "sph_math.cuh"
+
+namespace emerald {
+
+// First-fit allocator of [begin, begin + size) ranges in [0, capacity).
+class RangeAllocator {
+public:
+    explicit RangeAllocator(uint32_t capacity = 0);
+    bool alloc(uint32_t size, uint32_t& begin);
+    void release(uint32_t begin, uint32_t size);
+    uint32_t capacity() const { return capacity_; }
+    uint32_t largest_free() const;
+
+private:
+    uint32_t capacity_;
+    std::map<uint32_t, uint32_t> free_;  // begin -> size
+};
+
+struct SceneSpec {
+    emerald_params params;
+    int32_t method = kDfsph;
+    int32_t mode = kFrame;
+    float fixed_dt = 0.0f;
+    float const* solid_xy = nullptr;
+    float const* solid_volumes = nullptr;  // NULL: compute_volumes with numer 1.7
+    uint32_t n_solid = 0;
+    float const* fluid_xy = nullptr;
+    float const* fluid_v = nullptr;
+    uint32_t n_fluid = 0;
+};
+
+// Simulation_config derived from Parameters (emerald/sph2d_box/config.cpp:16-132).
+struct DerivedConfig {
+    float seconds_per_sub_step;
+    float mass_per_particle;
+    float draw_radius;
+    float pressure_correction_denom;
+};
+DerivedConfig derive_config(emerald_params const& p);
+void default_params(emerald_params& p);
+
+struct KernelTimes {
+    std::map<std::string, double> ms;
+    std::map<std::string, int> launches;
+};
+
+class Engine {
+public:
+    Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes);
+    ~Engine();
+    Engine(Engine const&) = delete;
+    Engine& operator=(Engine const&) = delete;
+
+    // Returns the scene id, or -1 when the arena has no room.
+    int add_scene(SceneSpec const& spec);
+    void remove_scene(int id);
+    void set_active(int id, bool active);
+    void set_mode(int id, int32_t mode, float fixed_dt);
+    bool scene_used(int id) const { return id >= 0 && id < (int)scenes_.size() && scenes_[id].used; }
+
+    void set_stream(cudaStream_t st) { st_ = st; }
+    cudaStream_t stream() const { return st_; }
+
+    // Zeroes the per-frame temporaries of the active scenes (fixed-dt runs).
+    void begin_frame(int32_t method);
+    // One sub-step of `method` for every active scene.
+    void substep(int32_t method);
+
+    // Synchronous accessors of one scene (original particle order).
+    void get_state(int id, float* x, float* v);
+    void set_state(int id, float const* x, float const* v);
+    void get_solid(int id, float* xy, float* volumes);
+    bool get_array(int id, std::string const& name, float* out, int& width);
+    void get_neighbors(int id, bool solid, uint8_t* counts, uint32_t* idx, float* w, float* gw);
+    size_t get_sort(int id, bool solid, int32_t* gc, uint64_t* z, uint64_t* pair_z,
+                    uint64_t* pair_index, uint32_t* block_indices, uint64_t* blocks);
+    SceneState scene_state(int id);
+    SceneParams const& scene_params(int id) const { return scenes_[id].p; }
+    std::vector<SceneState> all_states();
+    uint32_t fluid_count(int id) const { return scenes_[id].p.fluid_count; }
+    uint32_t solid_count(int id) const { return scenes_[id].p.solid_count; }
+    float2* device_x(int id) { return a_.x + scenes_[id].p.fluid_begin; }
+    float2* device_v(int id) { return a_.v + scenes_[id].p.fluid_begin; }
+    int active_scenes() const;
+    size_t free_fluid() const { return size_t(fluid_tiles_.largest_free()) * kTile; }
+
+    void enable_timing(bool on);
+    KernelTimes const& kernel_times();
+    void reset_timing();
+    // Loop control: false runs the exit test on the host after each solver
+    // iteration (one stream synchronisation per iteration, like the
+    // reference); true launches every iteration up to the cap and lets
+    // finished scenes' kernels return at once (no host round trips).
+    void set_unrolled_loops(bool on) { unrolled_ = on; }
+
+    void check(char const* what);
+
+private:
+    struct Scene {
+        bool used = false;
+        SceneParams p{};
+        uint32_t ftile_begin = 0, ftile_count = 0, stile_begin = 0, stile_count = 0;
+        uint32_t ftab_size = 0, stab_size = 0;
+        bool active = false;
+    };
+
+    template <class F>
+    void launch(char const* name, F&& f);
+    void upload_params(int id);
+    void upload_tiles();
+    void run_loop(int kind, int max_iter, int32_t method);
+    int max_iterations(int kind) const;
+    void rebuild_solids();
+    void ensure_sort_scratch(uint32_t n);
+
+    cudaStream_t st_ = nullptr;
+    uint32_t fluid_cap_, solid_cap_;
+    int max_scenes_;
+    Arena a_{};
+    std::vector<void*> allocations_;
+    SceneParams* d_sp_ = nullptr;
+    SceneState* d_ss_ = nullptr;
+    int32_t* d_tile_scene_ = nullptr;
+    int32_t* d_stile_scene_ = nullptr;
+    uint32_t* d_scan_ = nullptr;
+    int* d_running_ = nullptr;
+    int* h_running_ = nullptr;
+    std::vector<Scene> scenes_;
+    std::vector<int32_t> tile_scene_, stile_scene_;
+    RangeAllocator fluid_tiles_, solid_tiles_, ftab_, stab_;
+    bool tiles_dirty_ = true;
+    bool unrolled_ = false;
+    int32_t last_method_ = -1;
+
+    void* sort_buf_ = nullptr;
+    uint32_t sort_cap_ = 0;
+    SortScratch sort_{};
+
+    bool timing_ = false;
+    struct Pending {
+        std::string name;
+        cudaEvent_t start, stop;
+    };
+    std::vector<Pending> pending_;
+    std::vector<cudaEvent_t> event_pool_;
+    KernelTimes times_;
+};
+
+int64_t kernel_launch_count();
+
+}  // namespace emerald

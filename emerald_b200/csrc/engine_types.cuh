@@ -1,0 +1,143 @@
+// Device-side data layout of the SPH engine.
+//
+// Every simulation is a batch of scenes. A scene's fluid particles occupy a
+// contiguous range of the fluid arena that starts on a tile boundary (tiles
+// of kTile particles, one thread block per tile), so each block belongs to
+// exactly one scene and reads that scene's constants once. Boundary
+// (solid) particles live in a second arena laid out the same way.
+// Particles keep their original order inside a scene, as the reference's
+// State vectors do (emerald/sph2d_box/state.h:13-17).
+//
+// Neighbour lists are fixed-capacity (64, NEIGHBORHOOD_MAX_COUNT in
+// emerald/sph_common/neighborhood.h:38) and stored slot-major over the whole
+// arena: entry k of particle i lives at [k * stride + i], so the threads of a
+// warp (consecutive particles) read entry k of their lists in one coalesced
+// transaction. Indices are arena-global.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace emerald {
+
+constexpr int kTile = 128;
+constexpr int kMaxNeighbors = 64;
+constexpr uint64_t kEmptyKey = ~0ull;
+
+enum Method : int { kPcisph = 0, kIisph = 1, kIisphAp = 2, kIisphPseudoAp = 3, kDfsph = 4 };
+
+enum StepMode : int { kFixedDt = 0, kFrame = 1 };
+
+// Error bits reported through SceneState::error.
+enum ErrorBits : int { kErrTableFull = 1, kErrNonFinite = 2 };
+
+// Constants of one scene (mirrors Parameters + Simulation_config,
+// emerald/sph2d_box/parameters.h:12-41, config.h:7-18).
+struct SceneParams {
+    uint32_t fluid_begin, fluid_count;
+    uint32_t solid_begin, solid_count;
+    uint32_t ftab_begin, ftab_log2;  // fluid cell table region (size 2^log2 + 1)
+    uint32_t stab_begin, stab_log2;  // solid cell table region
+    float support, cell_size, rho0, mass, fluid_volume, gravity, viscosity, w0;
+    float iisph_omega, iisph_err_avg, iisph_err_max;
+    int32_t iisph_max_iter;
+    int32_t dfsph_max_iter;
+    float dfsph_dens_avg, dfsph_dens_max, dfsph_div_avg, dfsph_div_max;
+    float pcisph_denom;
+    int32_t method;
+    int32_t mode;
+    int64_t time_per_step;  // flicks
+    int32_t sub_steps;      // PCISPH sub-steps per frame
+    int32_t min_denom, max_denom;
+    float cfl_factor;
+    float seconds_per_sub_step;
+    float fixed_dt;
+};
+
+// Mutable per-scene state, device resident.
+struct SceneState {
+    int64_t frame_time;  // flicks at the start of the current frame
+    int64_t elapsed;     // flicks into the current frame
+    int32_t remaining;   // frame sub-step units left; 0: a new frame starts next
+    int32_t frame_substeps;
+    float dt, t;
+    int32_t active;
+    int32_t new_frame;
+    int32_t iter, done;
+    unsigned long long err_sum;
+    uint32_t err_max;  // bits of a non-negative float
+    uint32_t max_v2;   // bits of a non-negative float
+    float stat_avg, stat_max;
+    int32_t stat_iters;
+    float stat_div_avg, stat_div_max;
+    int32_t stat_div_iters;
+    int32_t error;
+    int32_t substeps_total;
+    int32_t pad;
+};
+
+// Raw device pointers of an arena, passed by value to every kernel.
+struct Arena {
+    SceneParams const* sp;
+    SceneState* ss;
+    int32_t const* tile_scene;   // fluid tile -> scene (-1: free)
+    int32_t const* stile_scene;  // solid tile -> scene
+    uint32_t stride;             // fluid arena capacity (multiple of kTile)
+    uint32_t sstride;            // solid arena capacity
+
+    // fluid state and solver temporaries (emerald/sph2d_box/state.h:34-69)
+    float2* x;
+    float2* v;
+    float* rho;
+    float* rho_star;
+    float* pbuf0;   // pressures / pseudo pressures (ping)
+    float* pbuf1;   // (pong)
+    float* alpha;
+    float* kdiv;
+    float* kdens;
+    float* qdiv;    // cached kdiv / rho^2
+    float* qdens;   // cached kdens / rho^2, also p / rho^2 for the AP solvers
+    float* aii;
+    float2* dii;
+    float2* sdp;    // sum_j d_ij p_j
+    float2* acc;    // pressure accelerations / displacements
+    float2* vext;
+    float2* xstar;
+    float2* vstar;
+    float2* fp;     // PCISPH pressure forces
+
+    // neighbour lists, slot-major
+    uint8_t* nf_cnt;
+    uint32_t* nf_idx;
+    float* nf_w;
+    float2* nf_gw;
+    uint8_t* ns_cnt;
+    uint32_t* ns_idx;
+    float* ns_w;
+    float2* ns_gw;
+
+    // neighbour build scratch
+    uint32_t* slot;
+    uint32_t* rank;
+    uint64_t* zkey;   // z key of each particle at the last build
+    uint32_t* members;
+    uint64_t* fkeys;
+    uint32_t* fcount;
+    uint32_t* fstart;
+    uint32_t ftab_total;
+
+    // boundary particles (static)
+    float2* xs;
+    float2* vs;
+    float* vols;
+    uint32_t* sslot;
+    uint32_t* srank;
+    uint64_t* szkey;
+    uint32_t* smembers;
+    uint64_t* skeys;
+    uint32_t* scount;
+    uint32_t* sstart;
+    uint32_t stab_total;
+};
+
+}  // namespace emerald

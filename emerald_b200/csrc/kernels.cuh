@@ -1,0 +1,76 @@
+// Host-side launchers of the engine's kernels (all stream ordered).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "engine_types.cuh"
+
+namespace emerald {
+
+// neighbour build (build_kernels.cu)
+uint32_t scan_scratch_words(uint32_t n);
+void launch_exclusive_scan(uint32_t const* in, uint32_t n, uint32_t* out, uint32_t* scratch,
+                           cudaStream_t st);
+void launch_build_cells(Arena const& a, bool solid, uint32_t tiles, uint32_t* scan_scratch,
+                        cudaStream_t st);
+void launch_neighbors(Arena const& a, uint32_t tiles, bool solid_other, bool write_kernels,
+                      cudaStream_t st);
+void launch_solid_volumes(Arena const& a, uint32_t solid_tiles, float numer, int scene,
+                          cudaStream_t st);
+
+// z-order sort products on request (sort_kernels.cu)
+struct SortScratch {
+    uint64_t* keys[2];
+    uint32_t* vals[2];
+    uint32_t* flags;
+    uint32_t* offsets;
+    uint32_t* hist;
+    uint32_t* scan;
+    uint32_t capacity;
+};
+size_t sort_scratch_bytes(uint32_t n);
+void sort_scratch_carve(void* base, uint32_t n, SortScratch& s);
+// Stable LSD radix sort of (key, value) pairs on the low `bits` key bits;
+// returns the buffer index (0 or 1) holding the result.
+int launch_radix_sort(SortScratch& s, uint32_t n, int bits, cudaStream_t st);
+// Reference sort products of one scene's fluid (solid=false) or boundary set:
+// per particle grid coords (int2) and z keys, the sorted (z, index) pairs
+// with scene-local indices, block indices and the [begin, end) block ranges.
+// Returns the number of blocks through *nblocks (device word).
+void launch_sort_products(Arena const& a, bool solid, int scene, uint32_t begin, uint32_t count,
+                          uint32_t tab_begin, uint32_t tab_size, float cell, SortScratch& s,
+                          int2* grid_coords, uint64_t* z, uint64_t* pair_z, uint32_t* pair_index,
+                          uint32_t* block_indices, uint32_t* blocks, uint32_t* nblocks,
+                          cudaStream_t st);
+
+// solver (solve_kernels.cu)
+void launch_max_v2(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_begin_substep(Arena const& a, int nscenes, cudaStream_t st);
+void launch_zero_kappas(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_iter_reset(Arena const& a, int nscenes, cudaStream_t st);
+void launch_iter_check(Arena const& a, int nscenes, int kind, int* running, cudaStream_t st);
+void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int external,
+                            int skip_done, cudaStream_t st);
+void launch_dfsph_divergence(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_dfsph_density(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_integrate_positions(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_iisph_density_dii(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_iisph_aii(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_make_q(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_apply_integrate(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_ap_density(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_ap_diag(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st);
+void launch_pressure_accel(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_ap_iterate(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st);
+void launch_ap_finish(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st);
+void launch_pc_init(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_pc_predict(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_pc_density(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_pc_forces(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_pc_final(Arena const& a, uint32_t tiles, cudaStream_t st);
+
+}  // namespace emerald

@@ -1,0 +1,1056 @@
+// Solver kernels of the 2D SPH sub-step: one thread per fluid particle,
+// neighbour lists streamed slot-major, neighbour state gathered by index.
+//
+// Each kernel fuses the reference's fluid pass and boundary pass of one
+// sph_common / sph2d_box function (they only read state the other pass does
+// not write) and, where the reference runs a per-particle step right after,
+// that step too. Sums run in neighbour-list order with the reference's
+// operator order, so every value is bit-identical to the CPU reference.
+//
+// Convergence loops stay on the device: iteration kernels accumulate the
+// reference's error reductions per scene (integer sum of error*1000 and the
+// maximum), and a one-block check kernel applies the reference's exit test
+// and marks finished scenes, whose later iteration launches return at once.
+#include "engine_types.cuh"
+#include "kernels.cuh"
+#include "sph_math.cuh"
+
+namespace emerald {
+
+namespace {
+
+constexpr double kFlicksPerSecond = 705600000.0;
+
+// Block-level setup shared by the per-particle kernels. A tile belongs to
+// one scene, so the scene checks are uniform across the block.
+struct Ctx {
+    int32_t s;
+    uint32_t i;
+    bool live;
+};
+
+__device__ __forceinline__ bool enter(Arena const& a, bool skip_done, Ctx& c) {
+    c.s = a.tile_scene[blockIdx.x];
+    if (c.s < 0) return false;
+    SceneState const& S = a.ss[c.s];
+    if (!S.active) return false;
+    if (skip_done && S.done) return false;
+    SceneParams const& P = a.sp[c.s];
+    c.i = blockIdx.x * kTile + threadIdx.x;
+    c.live = (c.i - P.fluid_begin) < P.fluid_count;
+    return true;
+}
+
+// Adds a per-thread error contribution to the scene's accumulators: the
+// integer sum and the maximum of non-negative floats (bit order equals value
+// order for them). NaN contributions are dropped, as std::max and the
+// compare-exchange loop of update_atomic_max drop them.
+__device__ void accumulate_error(SceneState* S, unsigned long long v, float m, bool live) {
+    uint32_t mb = (live && m == m && m > 0.0f) ? __float_as_uint(m) : 0u;
+    if (!live) v = 0ull;
+    for (int o = 16; o; o >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+        mb = max(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+    }
+    __shared__ unsigned long long ws[kTile / 32];
+    __shared__ uint32_t wm[kTile / 32];
+    int const lane = threadIdx.x & 31;
+    int const warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        ws[warp] = v;
+        wm[warp] = mb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        uint32_t tm = 0;
+        for (int w = 0; w < kTile / 32; ++w) {
+            t += ws[w];
+            tm = max(tm, wm[w]);
+        }
+        if (t) atomicAdd(&S->err_sum, t);
+        if (tm) atomicMax(&S->err_max, tm);
+    }
+}
+
+__device__ __forceinline__ float* pressures_cur(Arena const& a, SceneState const& S) {
+    return (S.iter & 1) ? a.pbuf1 : a.pbuf0;
+}
+__device__ __forceinline__ float* pressures_next(Arena const& a, SceneState const& S) {
+    return (S.iter & 1) ? a.pbuf0 : a.pbuf1;
+}
+
+// ------------------------------------------------------------ frame control
+
+// max_vector_squared_magnitude over the velocities (common.cpp:87-92), per scene.
+__global__ void k_max_v2(Arena a) {
+    Ctx c;
+    if (!enter(a, false, c)) return;
+    float d = 0.0f;
+    if (c.live) {
+        float2 const v = a.v[c.i];
+        d = v.x * v.x + v.y * v.y;
+    }
+    uint32_t mb = (c.live && d == d && d > 0.0f) ? __float_as_uint(d) : 0u;
+    for (int o = 16; o; o >>= 1) mb = max(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+    if ((threadIdx.x & 31) == 0 && mb) atomicMax(&a.ss[c.s].max_v2, mb);
+}
+
+__device__ int64_t to_flicks_x86(double s) {
+    double const f = s * kFlicksPerSecond;
+    if (!(f > -9.2233720368547758e18 && f < 9.2233720368547758e18)) return INT64_MIN;
+    return static_cast<int64_t>(f);
+}
+
+__device__ int to_int_x86(double d) {
+    if (!(d > -2147483649.0 && d < 2147483648.0)) return INT32_MIN;
+    return static_cast<int>(d);
+}
+
+// One thread per scene: picks the sub-step dt exactly as
+// std_adaptive_time_step (emerald/sph2d_box/adaptive_time_step.h:63-103) with
+// cfl_maximum_time_step (emerald/sph_common/cfl.cpp:12-21), or the fixed
+// PCISPH sub-step (emerald/sph2d_box/pcisph.cpp:166-204), or the caller's dt.
+__global__ void k_begin_substep(Arena a, int nscenes) {
+    int const s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nscenes) return;
+    SceneParams const& P = a.sp[s];
+    SceneState& S = a.ss[s];
+    if (!S.active) return;
+    S.error &= ~kErrNonFinite;
+    if (P.mode == kFixedDt) {
+        S.dt = P.fixed_dt;
+        S.t = static_cast<float>(static_cast<double>(S.substeps_total) *
+                                 static_cast<double>(P.fixed_dt));
+        S.new_frame = 0;
+        S.max_v2 = 0;
+        S.substeps_total += 1;
+        return;
+    }
+    if (S.remaining == 0) {
+        S.remaining = (P.method == kPcisph) ? P.sub_steps : P.min_denom;
+        S.elapsed = 0;
+        S.frame_substeps = 0;
+        S.new_frame = 1;
+    } else {
+        S.new_frame = 0;
+    }
+    int num;
+    int64_t sub;
+    float dt;
+    if (P.method == kPcisph) {
+        num = 1;
+        sub = P.time_per_step / P.sub_steps;
+        dt = P.seconds_per_sub_step;
+    } else {
+        double const numer = static_cast<double>(P.cfl_factor * P.support);
+        double const denom = sqrt(static_cast<double>(__uint_as_float(S.max_v2)));
+        double const r = safe_d(numer, denom) ? numer / denom : static_cast<double>(1.0f);
+        int64_t const cfl = to_flicks_x86(r);
+        int64_t const tpss = P.time_per_step / P.min_denom;
+        num = to_int_x86(ceil((static_cast<double>(cfl) / kFlicksPerSecond) /
+                              (static_cast<double>(tpss) / kFlicksPerSecond)));
+        int const divisor = P.min_denom / P.max_denom;
+        num = num < 1 ? 1 : (num > divisor ? divisor : num);
+        num = num < S.remaining ? num : S.remaining;
+        sub = static_cast<int64_t>(num) * tpss;
+        dt = static_cast<float>(static_cast<double>(sub) / kFlicksPerSecond);
+    }
+    S.t = static_cast<float>(static_cast<double>(S.frame_time + S.elapsed) / kFlicksPerSecond);
+    S.dt = dt;
+    S.elapsed += sub;
+    S.remaining -= num;
+    S.frame_substeps += 1;
+    S.substeps_total += 1;
+    if (S.remaining == 0) {
+        S.frame_time += P.time_per_step;
+        S.elapsed = 0;
+    }
+    S.max_v2 = 0;
+}
+
+// Per-frame reset of the DFSPH kappas (dfsph_p.cpp:214-229), fixed-dt mode.
+__global__ void k_zero_kappas(Arena a) {
+    Ctx c;
+    if (!enter(a, false, c) || !c.live) return;
+    a.kdiv[c.i] = 0.0f;
+    a.kdens[c.i] = 0.0f;
+}
+
+__global__ void k_iter_reset(Arena a, int nscenes) {
+    int const s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nscenes) return;
+    SceneState& S = a.ss[s];
+    S.iter = 0;
+    S.done = S.active ? 0 : 1;
+    S.err_sum = 0ull;
+    S.err_max = 0u;
+}
+
+// Exit test after one solver iteration. kind 0: IISPH family
+// (iisph.cpp:119-128), 1: DFSPH density (dfsph_p.cpp:113-133),
+// 2: DFSPH divergence (:187-211), 3: PCISPH (pcisph.cpp:144-148).
+// One block; *running is set when any scene still iterates.
+__global__ void k_iter_check(Arena a, int nscenes, int kind, int* running) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int s = threadIdx.x; s < nscenes; s += blockDim.x) {
+        SceneParams const& P = a.sp[s];
+        SceneState& S = a.ss[s];
+        if (!S.active || S.done) continue;
+        double const n = static_cast<double>(1000ull * P.fluid_count);
+        float const avg = P.fluid_count
+                            ? static_cast<float>(static_cast<double>(S.err_sum) / n)
+                            : 0.0f;
+        float const mx = __uint_as_float(S.err_max);
+        bool conv = false;
+        int max_iter = 0;
+        if (kind == 0) {
+            conv = S.iter > 1 && avg <= P.iisph_err_avg && mx <= P.iisph_err_max;
+            max_iter = P.iisph_max_iter;
+            S.stat_avg = avg;
+            S.stat_max = mx;
+        } else if (kind == 1) {
+            if (S.iter > 1) {
+                conv = avg <= P.dfsph_dens_avg && mx <= P.dfsph_dens_max;
+                S.stat_avg = avg;
+                S.stat_max = mx;
+            }
+            max_iter = P.dfsph_max_iter;
+        } else if (kind == 2) {
+            if (S.iter > 0) {
+                conv = avg <= P.dfsph_div_avg && mx <= P.dfsph_div_max;
+                S.stat_div_avg = avg;
+                S.stat_div_max = mx;
+            }
+            max_iter = P.dfsph_max_iter;
+        } else {
+            if (S.iter > 1) {
+                conv = (mx / P.rho0) <= 0.01f;
+                S.stat_max = mx / P.rho0;
+            }
+            max_iter = 6;
+        }
+        S.iter += 1;
+        S.err_sum = 0ull;
+        S.err_max = 0u;
+        if (conv || S.iter >= max_iter) {
+            S.done = 1;
+            if (kind == 2) {
+                S.stat_div_iters = S.iter;
+            } else {
+                S.stat_iters = S.iter;
+            }
+        } else {
+            any = 1;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *running = any;
+}
+
+// --------------------------------------------------------- shared SPH sums
+
+// compute_densities (emerald/sph_common/density.cpp:10-73).
+__device__ __forceinline__ float density_of(Arena const& a, SceneParams const& P, uint32_t i) {
+    size_t const stride = a.stride;
+    float const rho0 = P.rho0;
+    float const fmass = rho0 * P.fluid_volume;
+    float d = P.fluid_volume * rho0 * P.w0;
+    int const c = a.nf_cnt[i];
+    for (int k = 0; k < c; ++k) d += a.nf_w[k * stride + i] * fmass;
+    int const cs = a.ns_cnt[i];
+    if (cs) {
+        float db = 0.0f;
+        for (int k = 0; k < cs; ++k) {
+            size_t const e = k * stride + i;
+            db += a.ns_w[e] * (rho0 * a.vols[a.ns_idx[e]]);
+        }
+        d += db;
+    }
+    return d;
+}
+
+// compute_divergences (emerald/sph_common/divergence.cpp:5-74).
+__device__ __forceinline__ float divergence_of(Arena const& a, SceneParams const& P, uint32_t i) {
+    size_t const stride = a.stride;
+    float const rho0 = P.rho0;
+    float const fmass = rho0 * P.fluid_volume;
+    float2 const vi = a.v[i];
+    int const c = a.nf_cnt[i];
+    float d = 0.0f;
+    for (int k = 0; k < c; ++k) {
+        size_t const e = k * stride + i;
+        d += fmass * dot2(sub2(vi, a.v[a.nf_idx[e]]), a.nf_gw[e]);
+    }
+    int const cs = a.ns_cnt[i];
+    if (cs) {
+        float db = 0.0f;
+        for (int k = 0; k < cs; ++k) {
+            size_t const e = k * stride + i;
+            uint32_t const j = a.ns_idx[e];
+            db += (rho0 * a.vols[j]) * dot2(sub2(vi, a.vs[j]), a.ns_gw[e]);
+        }
+        d += db;
+    }
+    return d;
+}
+
+// apply_pressures_in_place (emerald/sph_common/pressure.cpp:9-80) for one
+// particle, with q = safe_divide(p, rho^2) precomputed per particle.
+__device__ __forceinline__ float2 apply_pressure_of(Arena const& a, SceneParams const& P, uint32_t i,
+                                                    float2 v, float const* q, float dt) {
+    size_t const stride = a.stride;
+    float const rho0 = P.rho0;
+    float const neg_fmass = -(rho0 * P.fluid_volume);
+    float const qi = q[i];
+    int const c = a.nf_cnt[i];
+    if (c) {
+        float2 acc = mk2(0.0f, 0.0f);
+        for (int k = 0; k < c; ++k) {
+            size_t const e = k * stride + i;
+            acc = add2(acc, scl2(neg_fmass * (qi + q[a.nf_idx[e]]), a.nf_gw[e]));
+        }
+        v = add2(v, scl2(dt, acc));
+    }
+    int const cs = a.ns_cnt[i];
+    if (cs) {
+        float2 acc = mk2(0.0f, 0.0f);
+        for (int k = 0; k < cs; ++k) {
+            size_t const e = k * stride + i;
+            acc = add2(acc, scl2(-(rho0 * a.vols[a.ns_idx[e]]) * qi, a.ns_gw[e]));
+        }
+        v = add2(v, scl2(dt, acc));
+    }
+    return v;
+}
+
+// compute_pressure_accelerations (emerald/sph_common/pressure.cpp:83-178).
+__device__ __forceinline__ float2 pressure_accel_of(Arena const& a, SceneParams const& P, uint32_t i,
+                                                    float const* q) {
+    size_t const stride = a.stride;
+    float const rho0 = P.rho0;
+    float const neg_fmass = -(rho0 * P.fluid_volume);
+    float const qi = q[i];
+    float2 out = mk2(0.0f, 0.0f);
+    int const c = a.nf_cnt[i];
+    if (c) {
+        float2 acc = mk2(0.0f, 0.0f);
+        for (int k = 0; k < c; ++k) {
+            size_t const e = k * stride + i;
+            acc = add2(acc, scl2(neg_fmass * (qi + q[a.nf_idx[e]]), a.nf_gw[e]));
+        }
+        out = acc;
+    }
+    int const cs = a.ns_cnt[i];
+    if (cs) {
+        float2 acc = mk2(0.0f, 0.0f);
+        for (int k = 0; k < cs; ++k) {
+            size_t const e = k * stride + i;
+            acc = add2(acc, scl2(-(rho0 * a.vols[a.ns_idx[e]]) * qi, a.ns_gw[e]));
+        }
+        out = add2(out, acc);
+    }
+    return out;
+}
+
+// integrate_velocities_in_place with the gravity force of
+// default_gravity_forces (dynamics.cpp:24-37, forces.cpp:63-83).
+__device__ __forceinline__ float2 integrate_external(SceneParams const& P, float2 v, float dt) {
+    float2 f = mk2(0.0f, 0.0f);
+    f.y -= P.mass * P.gravity;
+    float const denom = P.rho0 * P.fluid_volume;
+    float2 const numer = scl2(dt, f);
+    if (safe_v(numer, denom)) v = add2(v, div2(numer, denom));
+    return v;
+}
+
+// ------------------------------------------------------------------- DFSPH
+
+// compute_densities + dfsph_p_compute_shared_coeffs (dfsph_p_ops.cpp:19-72),
+// the per-frame kappa reset, and the p/rho^2 caches of both warm starts.
+__global__ void k_dfsph_density_alpha(Arena a) {
+    Ctx c;
+    if (!enter(a, false, c) || !c.live) return;
+    SceneParams const& P = a.sp[c.s];
+    uint32_t const i = c.i;
+    size_t const stride = a.stride;
+    float const rho0 = P.rho0;
+    float const fvol = P.fluid_volume;
+    float d = fvol * rho0 * P.w0;
+    float2 sum = mk2(0.0f, 0.0f);
+    float sdot = 0.0f;
+    int const cf = a.nf_cnt[i];
+    float const fmass = rho0 * fvol;
+    float const fmass_a = fvol * rho0;
+    for (int k = 0; k < cf; ++k) {
+        size_t const e = k * stride + i;
+        d += a.nf_w[e] * fmass;
+        float2 const m = scl2(fmass_a, a.nf_gw[e]);
+        sum = add2(sum, m);
+        sdot += dot2(m, m);
+    }
+    int const cs = a.ns_cnt[i];
+    if (cs) {
+        float db = 0.0f;
+        for (int k = 0; k < cs; ++k) {
+            size_t const e = k * stride + i;
+            float const vs = a.vols[a.ns_idx[e]];
+            db += a.ns_w[e] * (rho0 * vs);
+            sum = add2(sum, scl2(vs * rho0, a.ns_gw[e]));
+        }
+        d += db;
+    }
+    a.rho[i] = d;
+    float alpha = 0.0f;
+    if (cf + cs) {
+        float const numer = sqrf(d);
+        float const denom = dot2(sum, sum) + sdot;
+        alpha = safe_f(numer, denom) ? numer / denom : 0.0f;
+    }
+    a.alpha[i] = alpha;
+    float kd = a.kdiv[i];
+    float kn = a.kdens[i];
+    if (a.ss[c.s].new_frame) {
+        kd = 0.0f;
+        kn = 0.0f;
+        a.kdiv[i] = kd;
+        a.kdens[i] = kn;
+    }
+    a.qdiv[i] = p_over_rho2(kd, d);
+    a.qdens[i] = p_over_rho2(kn, d);
+}
+
+// apply_pressures_in_place over the cached q; with `external`, the velocity
+// first takes the external-force step (the DFSPH density warm start follows
+// integrate_velocities_in_place, dfsph_p.cpp:349-365).
+__global__ void k_apply_pressures(Arena a, int which_q, int external, int skip_done) {
+    Ctx c;
+    if (!enter(a, skip_done != 0, c) || !c.live) return;
+    SceneParams const& P = a.sp[c.s];
+    float const dt = a.ss[c.s].dt;
+    float2 v = a.v[c.i];
+    if (external) v = integrate_external(P, v, dt);
+    a.v[c.i] = apply_pressure_of(a, P, c.i, v, which_q ? a.qdens : a.qdiv, dt);
+}
+
+// compute_divergences + dfsph_p_compute_divergence_pseudo_pressures
+// (dfsph_p_ops.cpp:100-126) + the divergence error of dfsph_p.cpp:187-200.
+__global__ void k_dfsph_divergence(Arena a) {
+    Ctx c;
+    if (!enter(a, true, c)) return;
+    SceneParams const& P = a.sp[c.s];
+    SceneState* S = &a.ss[c.s];
+    float const dt = S->dt;
+    float err = 0.0f;
+    if (c.live) {
+        uint32_t const i = c.i;
+        float const d = divergence_of(a, P, i);
+        a.rho_star[i] = d;
+        float kappa = 0.0f;
+        if (!(d <= 0.0f)) {
+            float const numer = d * a.alpha[i];
+            kappa = safe_f(numer, dt) ? numer / dt : 0.0f;
+        }
+        a.kdiv[i] = kappa;
+        a.qdiv[i] = p_over_rho2(kappa, a.rho[i]);
+        err = d <= 0.0f ? 0.0f : (dt * d / P.rho0);
+    }
+    accumulate_error(S, static_cast<unsigned long long>(static_cast<long long>(err * 1000.0f)),
+                     err, c.live);
+}
+
+// predict_density_stars (density.cpp:75-109) +
+// dfsph_p_compute_density_pseudo_pressures (dfsph_p_ops.cpp:74-98) + the
+// density error of dfsph_p.cpp:134-148.
+__global__ void k_dfsph_density(Arena a) {
+    Ctx c;
+    if (!enter(a, true, c)) return;
+    SceneParams const& P = a.sp[c.s];
+    SceneState* S = &a.ss[c.s];
+    float const dt = S->dt;
+    float const rho0 = P.rho0;
+    float err = 0.0f;
+    if (c.live) {
+        uint32_t const i = c.i;
+        float const rho = a.rho[i];
+        float const star = max_0x(rho + (dt * divergence_of(a, P, i)));
+        a.rho_star[i] = star;
+        float const delta = star - rho0;
+        float kappa = 0.0f;
+        if (!(delta <= 0.0f)) {
+            float const numer = delta * a.alpha[i];
+            float const dd = sqrf(dt);
+            kappa = safe_f(numer, dd) ? numer / dd : 0.0f;
+        }
+        a.kdens[i] = kappa;
+        a.qdens[i] = p_over_rho2(kappa, rho);
+        err = delta <= 0.0f ? 0.0f : (delta / rho0);
+    }
+    accumulate_error(S, static_cast<unsigned long long>(static_cast<long long>(err * 1000.0f)),
+                     err, c.live);
+}
+
+// integrate_positions_in_place (dynamics.cpp:46-51).
+__global__ void k_integrate_positions(Arena a) {
+    Ctx c;
+    if (!enter(a, false, c) || !c.live) return;
+    float const dt = a.ss[c.s].dt;
+    a.x[c.i] = add2(a.x[c.i], scl2(dt, a.v[c.i]));
+}
+
+// -------------------------------------------------------------------- IISPH
+
+// compute_densities, integrate_velocities_in_place and iisph_compute_diis
+// (iisph_ops.cpp:20-90), plus the zero initial pressures (iisph.cpp:76).
+__global__ void k_iisph_density_dii(Arena a) {
+    Ctx c;
+    if (!enter(a, false, c) || !c.live) return;
+    SceneParams const& P = a.sp[c.s];
+    uint32_t const i = c.i;
+    size_t const stride = a.stride;
+    float const dt = a.ss[c.s].dt;
+    float const rho0 = P.rho0;
+    float const d = density_of(a, P, i);
+    a.rho[i] = d;
+    a.v[i] = integrate_external(P, a.v[i], dt);
+    float const neg_dt2 = -sqrf(dt);
+    float const denom = sqrf(d);
+    float2 dii = mk2(0.0f, 0.0f);
+    int const cf = a.nf_cnt[i];
+    if (cf) {
+        float const fmass = rho0 * P.fluid_volume;
+        float2 g = mk2(0.0f, 0.0f);
+        for (int k = 0; k < cf; ++k) g = add2(g, scl2(fmass, a.nf_gw[k * stride + i]));
+        float2 const numer = scl2(neg_dt2, g);
+        dii = safe_v(numer, denom) ? div2(numer, denom) : mk2(0.0f, 0.0f);
+    }
+    int const cs = a.ns_cnt[i];
+    if (cs) {
+        float2 g = mk2(0.0f, 0.0f);
+        for (int k = 0; k < cs; ++k) {
+            size_t const e = k * stride + i;
+            g = add2(g, scl2(rho0 * a.vols[a.ns_idx[e]], a.ns_gw[e]));
+        }
+        float2 const numer = scl2(neg_dt2, g);
+        dii = add2(dii, safe_v(numer, denom) ? div2(numer, denom) : mk2(0.0f, 0.0f));
+    }
+    a.dii[i] = dii;
+    a.pbuf0[i] = 0.0f;
+}
+
+// iisph_compute_aiis_and_density_stars (iisph_ops.cpp:92-200).
+__global__ void k_iisph_aii(Arena a) {
+    Ctx c;
+    if (!enter(a, false, c) || !c.live) return;
+    SceneParams const& P = a.sp[c.s];
+    uint32_t const i = c.i;
+    size_t const stride = a.stride;
+    float const dt = a.ss[c.s].dt;
+    float const rho0 = P.rho0;
+    float2 const dii = a.dii[i];
+    float2 const vi = a.v[i];
+    float const neg_dt2 = -sqrf(dt);
+    float aii = 0.0f;
+    float star = a.rho[i];
+    int const cf = a.nf_cnt[i];
+    if (cf) {
+        float const mass = P.fluid_volume * rho0;
+        float dd = 0.0f;
+        for (int k = 0; k < cf; ++k) {
+            size_t const e = k * stride + i;
+            uint32_t const j = a.nf_idx[e];
+            float2 const gw = a.nf_gw[e];
+            float2 const numer = scl2(neg_dt2 * mass, gw);
+            float const denom = sqrf(a.rho[j]);
+            if (safe_v(numer, denom)) {
+                float2 const dji = neg2(div2(numer, denom));
+                aii += mass * dot2(sub2(dii, dji), gw);
+            }
+            dd += dt * mass * dot2(sub2(vi, a.v[j]), gw);
+        }
+        star = a.rho[i] + dd;
+    }
+    int const cs = a.ns_cnt[i];
+    if (cs) {
+        float ab = 0.0f;
+        float dd = 0.0f;
+        for (int k = 0; k < cs; ++k) {
+            size_t const e = k * stride + i;
+            uint32_t const j = a.ns_idx[e];
+            float2 const gw = a.ns_gw[e];
+            float const mass = a.vols[j] * rho0;
+            ab += mass * dot2(dii, gw);
+            dd += dt * mass * dot2(sub2(vi, a.vs[j]), gw);
+        }
+        aii += ab;
+        star += dd;
+    }
+    a.aii[i] = aii;
+    a.rho_star[i] = star;
+}
+
+// iisph_compute_sum_dij_pjs (iisph_ops.cpp:202-235).
+__global__ void k_iisph_sum_dij(Arena a) {
+    Ctx c;
+    if (!enter(a, true, c) || !c.live) return;
+    SceneParams const& P = a.sp[c.s];
+    SceneState const& S = a.ss[c.s];
+    uint32_t const i = c.i;
+    size_t const stride = a.stride;
+    float const dt = S.dt;
+    float const* p = pressures_cur(a, S);
+    float const mass = P.fluid_volume * P.rho0;
+    float const neg_dt2 = -sqrf(dt);
+    float2 sum = mk2(0.0f, 0.0f);
+    int const cf = a.nf_cnt[i];
+    for (int k = 0; k < cf; ++k) {
+        size_t const e = k * stride + i;
+        uint32_t const j = a.nf_idx[e];
+        float2 const numer = scl2(neg_dt2 * mass * p[j], a.nf_gw[e]);
+        float const denom = sqrf(a.rho[j]);
+        if (safe_v(numer, denom)) sum = add2(sum, div2(numer, denom));
+    }
+    a.sdp[i] = sum;
+}
+
+// iisph_compute_betas (iisph_ops.cpp:237-330) followed by
+// iisph_compute_new_pressures for the same particle (iisph_ops.cpp:332-425).
+__global__ void k_iisph_beta_pressure(Arena a) {
+    Ctx c;
+    if (!enter(a, true, c)) return;
+    SceneParams const& P = a.sp[c.s];
+    SceneState* S = &a.ss[c.s];
+    float err = 0.0f;
+    bool counted = false;
+    if (c.live) {
+        uint32_t const i = c.i;
+        size_t const stride = a.stride;
+        float const dt = S->dt;
+        float const rho0 = P.rho0;
+        float const* p = pressures_cur(a, *S);
+        float* pn = pressures_next(a, *S);
+        float const pi = p[i];
+        float2 const si = a.sdp[i];
+        float const neg_dt2 = -sqrf(dt);
+        float beta = 0.0f;
+        int const cf = a.nf_cnt[i];
+        if (cf) {
+            float const mass = rho0 * P.fluid_volume;
+            for (int k = 0; k < cf; ++k) {
+                size_t const e = k * stride + i;
+                uint32_t const j = a.nf_idx[e];
+                float2 const gw = a.nf_gw[e];
+                float2 const numer = scl2(neg_dt2 * mass, gw);
+                float const denom = sqrf(a.rho[j]);
+                float2 const dij = safe_v(numer, denom) ? div2(numer, denom) : mk2(0.0f, 0.0f);
+                float2 const dji = neg2(dij);
+                float2 const skni = sub2(a.sdp[j], scl2(pi, dji));
+                float2 const t = sub2(sub2(si, scl2(p[j], a.dii[j])), skni);
+                beta += mass * dot2(t, gw);
+            }
+        }
+        int const cs = a.ns_cnt[i];
+        if (cs) {
+            float bb = 0.0f;
+            for (int k = 0; k < cs; ++k) {
+                size_t const e = k * stride + i;
+                bb += (rho0 * a.vols[a.ns_idx[e]]) * dot2(si, a.ns_gw[e]);
+            }
+            beta += bb;
+        }
+        float const alpha = a.aii[i];
+        float out = pi;
+        if (alpha != 0.0f) {
+            float const numer = rho0 - a.rho_star[i] - beta;
+            if (safe_f(numer, alpha)) {
+                err = max_0x(-(numer - (alpha * pi)) / rho0);
+                counted = true;
+                out = max_0x(mix1(pi, numer / alpha, P.iisph_omega));
+            } else {
+                atomicOr(&S->error, kErrNonFinite);
+            }
+        }
+        pn[i] = out;
+    }
+    accumulate_error(S, counted ? static_cast<unsigned long long>(err * 1000.0f) : 0ull, err,
+                     c.live && counted);
+}
+
+// q = safe_divide(p, rho^2) of the final pressures, for apply_pressures.
+__global__ void k_make_q(Arena a) {
+    Ctx c;
+    if (!enter(a, false, c) || !c.live) return;
+    SceneState const& S = a.ss[c.s];
+    a.qdens[c.i] = p_over_rho2(pressures_cur(a, S)[c.i], a.rho[c.i]);
+}
+
+// apply_pressures_in_place then integrate_positions_in_place
+// (iisph.cpp:138-150).
+__global__ void k_apply_integrate(Arena a) {
+    Ctx c;
+    if (!enter(a, false, c) || !c.live) return;
+    SceneParams const& P = a.sp[c.s];
+    float const dt = a.ss[c.s].dt;
+    float2 const v = apply_pressure_of(a, P, c.i, a.v[c.i], a.qdens, dt);
+    a.v[c.i] = v;
+    a.x[c.i] = add2(a.x[c.i], scl2(dt, v));
+}
+
+// ------------------------------------------------- IISPH_AP / PSEUDO_AP
+
+// compute_densities, integrate_velocities_in_place, zero pressures.
+__global__ void k_ap_density(Arena a) {
+    Ctx c;
+    if (!enter(a, false, c) || !c.live) return;
+    SceneParams const& P = a.sp[c.s];
+    float const dt = a.ss[c.s].dt;
+    a.rho[c.i] = density_of(a, P, c.i);
+    a.v[c.i] = integrate_external(P, a.v[c.i], dt);
+    a.pbuf0[c.i] = 0.0f;
+    a.qdens[c.i] = 0.0f;
+}
+
+// iisph_ap_density_stars_and_diagonals (iisph_ap_ops.cpp:19-103) and the
+// pseudo variant (iisph_pseudo_ap_ops.cpp:19-117).
+__global__ void k_ap_diag(Arena a, int pseudo) {
+    Ctx c;
+    if (!enter(a, false, c) || !c.live) return;
+    SceneParams const& P = a.sp[c.s];
+    uint32_t const i = c.i;
+    size_t const stride = a.stride;
+    float const dt = a.ss[c.s].dt;
+    float const rho0 = P.rho0;
+    int const cf = a.nf_cnt[i];
+    int const cs = a.ns_cnt[i];
+    float const rho = a.rho[i];
+    if (!(cf + cs)) {
+        a.rho_star[i] = rho;
+        a.aii[i] = 0.0f;
+        return;
+    }
+    float const self_mass = P.fluid_volume * rho0;
+    float2 const vi = a.v[i];
+    float2 sum = mk2(0.0f, 0.0f);
+    float sdot = 0.0f;
+    float div = 0.0f;
+    float const fmass = P.fluid_volume * rho0;
+    for (int k = 0; k < cf; ++k) {
+        size_t const e = k * stride + i;
+        float2 const gw = a.nf_gw[e];
+        sum = add2(sum, scl2(fmass, gw));
+        sdot += fmass * dot2(gw, gw);
+        div += fmass * dot2(sub2(vi, a.v[a.nf_idx[e]]), gw);
+    }
+    for (int k = 0; k < cs; ++k) {
+        size_t const e = k * stride + i;
+        uint32_t const j = a.ns_idx[e];
+        float2 const gw = a.ns_gw[e];
+        float const mass = a.vols[j] * rho0;
+        sum = add2(sum, scl2(mass, gw));
+        div += mass * dot2(sub2(vi, a.vs[j]), gw);
+    }
+    float const denom = sqrf(rho);
+    float const numer = pseudo ? -(dot2(sum, sum) + self_mass * sdot)
+                               : -sqrf(dt) * (dot2(sum, sum) + self_mass * sdot);
+    a.aii[i] = safe_f(numer, denom) ? numer / denom : 0.0f;
+    a.rho_star[i] = rho + dt * div;
+}
+
+// compute_pressure_accelerations over the cached p/rho^2 (also the pseudo
+// pressure displacements, iisph_pseudo_ap_ops.cpp:119-224).
+__global__ void k_pressure_accel(Arena a) {
+    Ctx c;
+    if (!enter(a, true, c) || !c.live) return;
+    SceneParams const& P = a.sp[c.s];
+    a.acc[c.i] = pressure_accel_of(a, P, c.i, a.qdens);
+}
+
+// iisph_ap_iterate_pressures_in_place (iisph_ap_ops.cpp:105-194) and the
+// pseudo variant (iisph_pseudo_ap_ops.cpp:226-323).
+__global__ void k_ap_iterate(Arena a, int pseudo) {
+    Ctx c;
+    if (!enter(a, true, c)) return;
+    SceneParams const& P = a.sp[c.s];
+    SceneState* S = &a.ss[c.s];
+    float err = 0.0f;
+    bool counted = false;
+    if (c.live) {
+        uint32_t const i = c.i;
+        size_t const stride = a.stride;
+        float const rho0 = P.rho0;
+        int const cf = a.nf_cnt[i];
+        int const cs = a.ns_cnt[i];
+        float const diag = a.aii[i];
+        float pnew;
+        if (!cf && !cs) {
+            pnew = 0.0f;
+        } else if (pseudo && diag == 0.0f) {
+            pnew = 0.0f;
+        } else {
+            float api = 0.0f;
+            float2 const ai = a.acc[i];
+            float const fmass = rho0 * P.fluid_volume;
+            for (int k = 0; k < cf; ++k) {
+                size_t const e = k * stride + i;
+                api += fmass * dot2(sub2(ai, a.acc[a.nf_idx[e]]), a.nf_gw[e]);
+            }
+            for (int k = 0; k < cs; ++k) {
+                size_t const e = k * stride + i;
+                api += (rho0 * a.vols[a.ns_idx[e]]) * dot2(ai, a.ns_gw[e]);
+            }
+            if (!pseudo) api *= sqrf(S->dt);
+            float const source = rho0 - a.rho_star[i];
+            float const r = api - source;
+            err = max_0x(safe_f(r, rho0) ? r / rho0 : 0.0f);
+            counted = true;
+            float const old = a.pbuf0[i];
+            float const numer = P.iisph_omega * (source - api);
+            pnew = max_0x(old + (safe_f(numer, diag) ? numer / diag : 0.0f));
+        }
+        a.pbuf0[i] = pnew;
+        a.qdens[i] = p_over_rho2(pnew, a.rho[i]);
+    }
+    accumulate_error(S, counted ? static_cast<unsigned long long>(err * 1000.0f) : 0ull, err,
+                     c.live && counted);
+}
+
+// Final pressure accelerations and the integration of iisph_ap.cpp:138-153
+// (integrate_velocities_and_positions_in_place, dynamics.cpp:53-63) or
+// iisph_pseudo_ap_integrate_velocities_and_positions_in_place
+// (iisph_pseudo_ap_ops.cpp:325-343).
+__global__ void k_ap_finish(Arena a, int pseudo) {
+    Ctx c;
+    if (!enter(a, false, c) || !c.live) return;
+    SceneParams const& P = a.sp[c.s];
+    float const dt = a.ss[c.s].dt;
+    uint32_t const i = c.i;
+    float2 const acc = pressure_accel_of(a, P, i, a.qdens);
+    a.acc[i] = acc;
+    if (!pseudo) {
+        float2 const v = add2(a.v[i], scl2(dt, acc));
+        a.v[i] = v;
+        a.x[i] = add2(a.x[i], scl2(dt, v));
+    } else {
+        float2 const vstar = a.v[i];
+        a.x[i] = add2(add2(a.x[i], scl2(dt, vstar)), acc);
+        if (safe_v(vstar, dt)) a.v[i] = add2(vstar, div2(acc, dt));
+    }
+}
+
+// ------------------------------------------------------------------- PCISPH
+
+// Velocity from external forces only (pcisph.cpp:54-65).
+__global__ void k_pc_init(Arena a) {
+    Ctx c;
+    if (!enter(a, false, c) || !c.live) return;
+    SceneParams const& P = a.sp[c.s];
+    float const dt = a.ss[c.s].dt;
+    float const mult = dt / P.mass;
+    float2 f = mk2(0.0f, 0.0f);
+    f.y -= P.mass * P.gravity;
+    a.vext[c.i] = add2(a.v[c.i], scl2(mult, f));
+    a.pbuf0[c.i] = 0.0f;
+}
+
+// Predicted velocity and position of one predictor pass (pcisph.cpp:72-88).
+__global__ void k_pc_predict(Arena a) {
+    Ctx c;
+    if (!enter(a, true, c) || !c.live) return;
+    SceneParams const& P = a.sp[c.s];
+    SceneState const& S = a.ss[c.s];
+    float const dt = S.dt;
+    float2 vs = a.vext[c.i];
+    if (S.iter > 0) vs = add2(vs, scl2(dt / P.mass, a.fp[c.i]));
+    a.vstar[c.i] = vs;
+    a.xstar[c.i] = add2(a.x[c.i], scl2(dt, vs));
+}
+
+// Densities at the predicted positions with the kernel values recomputed
+// (compute_neighbor_distances_and_vectors_to + compute_neighbor_kernels,
+// neighborhoods_from_state.cpp:103-128), pcisph_compute_densities,
+// pcisph_accumulate_density_from_solids and pcisph_update_pressures
+// (pcisph_ops.cpp:18-76), plus the max density error (common.cpp:78-85).
+__global__ void k_pc_density(Arena a) {
+    Ctx c;
+    if (!enter(a, true, c)) return;
+    SceneParams const& P = a.sp[c.s];
+    SceneState* S = &a.ss[c.s];
+    float err = 0.0f;
+    if (c.live) {
+        uint32_t const i = c.i;
+        size_t const stride = a.stride;
+        float const h = P.support;
+        float2 const pos = a.xstar[i];
+        int const cf = a.nf_cnt[i];
+        float ws = P.w0;
+        for (int k = 0; k < cf; ++k) {
+            uint32_t const j = a.nf_idx[k * stride + i];
+            ws += kernel_w(length2f(sub2(a.xstar[j], pos)), h);
+        }
+        float d = P.mass * ws;
+        int const cs = a.ns_cnt[i];
+        if (cs) {
+            float vf = 0.0f;
+            for (int k = 0; k < cs; ++k) {
+                uint32_t const j = a.ns_idx[k * stride + i];
+                vf += a.vols[j] * kernel_w(length2f(sub2(a.xs[j], pos)), h);
+            }
+            d += P.rho0 * vf;
+        }
+        a.rho[i] = d;
+        float const p = a.pbuf0[i] + max_x0(d - P.rho0) / P.pcisph_denom;
+        a.pbuf0[i] = p;
+        a.qdens[i] = p / sqrf(d);
+        err = max_0x(d - P.rho0);
+    }
+    accumulate_error(S, 0ull, err, c.live);
+}
+
+// pcisph_accumulate_pressure_forces and ..._from_solids (pcisph_ops.cpp:78-178)
+// on the fixed neighbour lists at the predicted positions.
+__global__ void k_pc_forces(Arena a) {
+    Ctx c;
+    if (!enter(a, true, c) || !c.live) return;
+    SceneParams const& P = a.sp[c.s];
+    uint32_t const i = c.i;
+    size_t const stride = a.stride;
+    float const h = P.support;
+    float const m = P.mass;
+    float const N2 = 0.01f * h * h;
+    float2 const pos = a.xstar[i];
+    float2 f = mk2(0.0f, 0.0f);
+    int const cf = a.nf_cnt[i];
+    if (cf) {
+        float2 const vi = a.vstar[i];
+        float const rho = a.rho[i];
+        float const pors = a.qdens[i];
+        float2 pf = mk2(0.0f, 0.0f);
+        for (int k = 0; k < cf; ++k) {
+            uint32_t const j = a.nf_idx[k * stride + i];
+            float2 const vto = sub2(a.xstar[j], pos);
+            float const dist = length2f(vto);
+            float2 const gw = kernel_grad_w(neg2(vto), h);
+            float const rho_j = a.rho[j];
+            pf = add2(pf, scl2(pors + a.qdens[j], gw));
+            float2 const dv = sub2(a.vstar[j], vi);
+            float const dvr = dot2(vto, dv);
+            if (dvr < 0.0f) {
+                float const mu = h * dvr / (dist + N2);
+                float const den = (rho + rho_j) / 2.0f;
+                pf = add2(pf, scl2(((-1.0f * P.viscosity * mu) + (2.0f * sqrf(mu))) / den, gw));
+            }
+        }
+        f = add2(f, scl2(-(m * m), pf));
+    }
+    int const cs = a.ns_cnt[i];
+    if (cs) {
+        float const pors = a.pbuf0[i] / sqrf(a.rho[i]);
+        float2 vg = mk2(0.0f, 0.0f);
+        for (int k = 0; k < cs; ++k) {
+            uint32_t const j = a.ns_idx[k * stride + i];
+            float2 const gw = kernel_grad_w(neg2(sub2(a.xs[j], pos)), h);
+            vg = add2(vg, scl2(a.vols[j], gw));
+        }
+        f = add2(f, scl2(-m * P.rho0 * pors, vg));
+    }
+    a.fp[i] = f;
+}
+
+// Final velocity and position update (pcisph.cpp:151-163).
+__global__ void k_pc_final(Arena a) {
+    Ctx c;
+    if (!enter(a, false, c) || !c.live) return;
+    SceneParams const& P = a.sp[c.s];
+    float const dt = a.ss[c.s].dt;
+    float2 const v = add2(a.vext[c.i], scl2(dt / P.mass, a.fp[c.i]));
+    a.v[c.i] = v;
+    a.x[c.i] = add2(a.x[c.i], scl2(dt, v));
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ launchers
+
+void launch_max_v2(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_max_v2<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_begin_substep(Arena const& a, int nscenes, cudaStream_t st) {
+    k_begin_substep<<<(nscenes + 127) / 128, 128, 0, st>>>(a, nscenes);
+}
+void launch_zero_kappas(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_zero_kappas<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_iter_reset(Arena const& a, int nscenes, cudaStream_t st) {
+    k_iter_reset<<<(nscenes + 127) / 128, 128, 0, st>>>(a, nscenes);
+}
+void launch_iter_check(Arena const& a, int nscenes, int kind, int* running, cudaStream_t st) {
+    k_iter_check<<<1, 256, 0, st>>>(a, nscenes, kind, running);
+}
+void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_dfsph_density_alpha<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int external,
+                            int skip_done, cudaStream_t st) {
+    k_apply_pressures<<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done);
+}
+void launch_dfsph_divergence(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_dfsph_divergence<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_dfsph_density(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_dfsph_density<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_integrate_positions(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_integrate_positions<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_iisph_density_dii(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_iisph_density_dii<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_iisph_aii(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_iisph_aii<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_iisph_sum_dij<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_iisph_beta_pressure<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_make_q(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_make_q<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_apply_integrate(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_apply_integrate<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_ap_density(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_ap_density<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_ap_diag(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st) {
+    k_ap_diag<<<tiles, kTile, 0, st>>>(a, pseudo);
+}
+void launch_pressure_accel(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_pressure_accel<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_ap_iterate(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st) {
+    k_ap_iterate<<<tiles, kTile, 0, st>>>(a, pseudo);
+}
+void launch_ap_finish(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st) {
+    k_ap_finish<<<tiles, kTile, 0, st>>>(a, pseudo);
+}
+void launch_pc_init(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_pc_init<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_pc_predict(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_pc_predict<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_pc_density(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_pc_density<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_pc_forces(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_pc_forces<<<tiles, kTile, 0, st>>>(a);
+}
+void launch_pc_final(Arena const& a, uint32_t tiles, cudaStream_t st) {
+    k_pc_final<<<tiles, kTile, 0, st>>>(a);
+}
+
+}  // namespace emerald

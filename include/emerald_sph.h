@@ -1,0 +1,207 @@
+/*
+ * emerald-b200: C ABI of the B200 implementation of the emerald 2D SPH step
+ * (emerald/sph2d_box + emerald/sph_common + emerald/z_index).
+ *
+ * The reference exposes C++ free functions and the EZ_EXAMPLE_SIM driver
+ * (emerald/sph2d_box/simulation.h:24-44); it has no C ABI. These entry points
+ * are the flat equivalents a foreign-function caller binds. Every function
+ * returns an emerald status code; buffers are caller-owned host arrays of
+ * interleaved (x, y) floats unless stated otherwise; particle indices are
+ * the caller's original order, as in the reference's State vectors.
+ */
+#ifndef EMERALD_SPH_H
+#define EMERALD_SPH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The reference aborts through EMLD_ASSERT/EMLD_FAIL
+ * (emerald/util/assert.h:14-26); here each failure is a return value and a
+ * message retrievable with emerald_last_error(). */
+#define EMERALD_OK 0
+#define EMERALD_EINVAL 22
+#define EMERALD_ENOMEM 12
+#define EMERALD_ENOSPC 28
+#define EMERALD_ENOTFOUND 2
+#define EMERALD_ETIMEOUT 110
+#define EMERALD_ECUDA 1000
+#define EMERALD_ESOLVER 1001
+
+/* Solver methods, numbered as EZ_EXAMPLE_SIM::Method
+ * (emerald/sph2d_box/simulation.h:25). */
+#define EMERALD_PCISPH 0
+#define EMERALD_IISPH 1
+#define EMERALD_IISPH_AP 2
+#define EMERALD_IISPH_PSEUDO_AP 3
+#define EMERALD_DFSPH_P 4
+
+/* Parameters (emerald/sph2d_box/parameters.h:12-41) plus the two derived
+ * Simulation_config values (emerald/sph2d_box/config.h:7-18). A zero
+ * mass_per_particle or pressure_correction_denom is derived from the
+ * reference's hex template (config.cpp:16-132). */
+typedef struct emerald_params {
+    uint64_t seed;
+    int64_t time_per_step_flicks;
+    int32_t sub_steps;
+    float length;
+    float support;
+    float gravity;
+    float viscosity;
+    float target_density;
+    int32_t iisph_max_pressure_iterations;
+    float iisph_error_average_threshold;
+    float iisph_error_max_threshold;
+    float iisph_omega;
+    int32_t dfsph_max_correction_iterations;
+    float dfsph_density_error_average_threshold;
+    float dfsph_density_error_max_threshold;
+    float dfsph_divergence_error_average_threshold;
+    float dfsph_divergence_error_max_threshold;
+    float mass_per_particle;
+    float pressure_correction_denom;
+} emerald_params;
+
+/* Statistics of the last sub-step (or of the last sub-step of a frame). The
+ * reference keeps these in local variables; they are returned here. */
+typedef struct emerald_step_stats {
+    int32_t sub_steps;
+    int32_t pressure_iterations;
+    float error_average;
+    float error_max;
+    int32_t divergence_iterations;
+    float divergence_error_average;
+    float divergence_error_max;
+    float dt;
+    double time_seconds;
+    int32_t error_flags;
+} emerald_step_stats;
+
+/* ---------------------------------------------------------------- setup */
+
+/* Parameters() defaults (emerald/sph2d_box/parameters.h:12-41). */
+int emerald_default_params(emerald_params* out);
+
+/* Simulation_config (emerald/sph2d_box/config.cpp:16-132): out[0]
+ * seconds_per_sub_step, out[1] mass_per_particle, out[2] draw_radius,
+ * out[3] pressure_correction_denom. Overrides in *params are honoured. */
+int emerald_config(emerald_params const* params, float* out);
+
+/* The same template sums over an unjittered square lattice of spacing dx
+ * (used by the block scenes): out[0] mass_per_particle, out[1] the PCISPH
+ * pressure-correction denominator for sub-step dt. */
+int emerald_lattice_config(emerald_params const* params, float dx, float dt, float* out);
+
+/* z_index(x, y) (emerald/z_index/z_index.cpp:8-10). */
+uint64_t emerald_z_index(uint32_t x, uint32_t y);
+
+/* Seeded block scene: nx*ny fluid particles at (i+0.5)dx, (j+0.5)dx offset
+ * by (x0, y0), each coordinate jittered by U(-jitter*dx, jitter*dx) from
+ * std::mt19937_64{seed}. Writes nx*ny points; returns the count. */
+size_t emerald_block_scene(uint32_t nx, uint32_t ny, float dx, float x0, float y0, float jitter,
+                           uint64_t seed, float* xy);
+
+/* Tank boundary: `layers` rows of particles at spacing dx below the floor
+ * and outside both side walls of [0, length]^2. xy may be NULL to count. */
+size_t emerald_wall_scene(float dx, float length, int32_t layers, float* xy);
+
+/* The reference's default scene generators: world_walls_initial_solid_state
+ * (emerald/sph2d_box/solids.cpp:139-213) and dam_break_initial_state
+ * (emerald/sph2d_box/initial_state.cpp:14-97). Pass NULL to count. */
+size_t emerald_world_walls(emerald_params const* params, float* xy);
+size_t emerald_dam_break(emerald_params const* params, float const* solid_xy, size_t n_solid,
+                         float* xy);
+
+/* ------------------------------------------------------------ simulation */
+
+typedef struct emerald_sim emerald_sim;
+
+/* Creates a single-scene simulation on the current CUDA device: the
+ * EZ_EXAMPLE_SIM state (emerald/sph2d_box/simulation.cpp:14-39) with the
+ * given boundary and fluid particles. solid_volumes may be NULL, in which
+ * case boundary volumes follow compute_volumes
+ * (emerald/sph2d_box/solids.cpp:52-74). fluid_v may be NULL (zero). */
+int emerald_sim_create(emerald_params const* params,
+                       float const* solid_xy,
+                       float const* solid_volumes,
+                       size_t n_solid,
+                       float const* fluid_xy,
+                       float const* fluid_v,
+                       size_t n_fluid,
+                       emerald_sim** out);
+int emerald_sim_destroy(emerald_sim* sim);
+
+/* Per-frame temporaries of a fixed-dt run: the resize/reset of the method's
+ * temporaries (e.g. emerald/sph2d_box/dfsph_p.cpp:214-229) and
+ * compute_constant_volumes (emerald/sph_common/volume.cpp:7-14). */
+int emerald_sim_begin_frame(emerald_sim* sim, int32_t method);
+
+/* One solver sub-step with a caller-chosen dt: iisph_sub_step
+ * (emerald/sph2d_box/iisph.cpp:23-151), iisph_ap_sub_step, iisph_pseudo_ap_sub_step,
+ * dfsph_p_sub_step (dfsph_p.cpp:265-374) or pcisph_sub_step (pcisph.cpp:36-164). */
+int emerald_sim_sub_step(emerald_sim* sim, int32_t method, float t, float dt,
+                         emerald_step_stats* stats);
+
+/* One frame, as X_simulation_step through EZ_EXAMPLE_SIM::step
+ * (emerald/sph2d_box/simulation.cpp:41-93): CFL-adaptive sub-steps
+ * (adaptive_time_step.h:35-122) or PCISPH's fixed sub-steps. */
+int emerald_sim_frame(emerald_sim* sim, int32_t method, emerald_step_stats* stats);
+
+/* Advances n adaptive sub-steps, continuing and starting frames exactly as
+ * successive emerald_sim_frame calls would. */
+int emerald_sim_advance(emerald_sim* sim, int32_t method, int32_t n_substeps,
+                        emerald_step_stats* stats);
+
+int emerald_sim_counts(emerald_sim const* sim, size_t* n_fluid, size_t* n_solid);
+int emerald_sim_time(emerald_sim const* sim, int64_t* flicks);
+int emerald_sim_get_state(emerald_sim* sim, float* x, float* v);
+int emerald_sim_set_state(emerald_sim* sim, float const* x, float const* v);
+int emerald_sim_get_solid(emerald_sim* sim, float* xy, float* volumes);
+
+/* Per-particle solver temporaries by their Temp_data name
+ * (emerald/sph2d_box/state.h:34-69): "densities", "pressures",
+ * "density_stars", "aiis", "alphas", "divergence_kappas", "density_kappas",
+ * "diis", "sum_dij_pjs", "pressure_forces", "pressure_accelerations",
+ * "velocity_external_forces", "position_stars", "velocity_stars".
+ * *width receives 1 or 2 floats per particle; out may be NULL to query. */
+int emerald_sim_get_array(emerald_sim* sim, char const* name, float* out, int32_t* width);
+
+/* Neighbour lists of the last sub-step in the reference layout
+ * (emerald/sph_common/neighborhood.h:126-160): counts[n], and n x 64 arrays
+ * of indices, kernel values and kernel gradients (x, y). Any may be NULL. */
+int emerald_sim_get_neighbors(emerald_sim* sim, int32_t solid, uint8_t* counts, uint32_t* idx,
+                              float* w, float* gw);
+
+/* Sort products of the last neighbour build (emerald/sph2d_box/state.h:34-40):
+ * grid coords (n x 2), z keys, the sorted (z, index) pairs, block indices
+ * and the [begin, end) blocks (nblocks x 2). Any output may be NULL. */
+int emerald_sim_get_sort(emerald_sim* sim, int32_t solid, int32_t* grid_coords, uint64_t* z,
+                         uint64_t* pair_z, uint64_t* pair_index, uint32_t* block_indices,
+                         uint64_t* blocks, size_t* nblocks);
+
+/* Device residency: the CUDA stream the simulation runs on (NULL keeps the
+ * legacy default stream) and device pointers to its float2 positions and
+ * velocities (original particle order). */
+int emerald_sim_set_stream(emerald_sim* sim, void* cuda_stream);
+int emerald_sim_device_state(emerald_sim* sim, void** x, void** v);
+
+/* Accumulated device time per kernel name since the last reset, measured
+ * with CUDA events around each launch when timing is enabled. */
+int emerald_sim_enable_timing(emerald_sim* sim, int32_t enable);
+int emerald_sim_kernel_times(emerald_sim* sim, char* names, size_t names_len, double* ms,
+                             int32_t* launches, int32_t* count);
+
+/* Number of kernels this library launched since the process started. */
+int64_t emerald_kernel_launches(void);
+
+/* Message of the last failed call on this thread. */
+char const* emerald_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

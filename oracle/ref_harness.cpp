@@ -236,6 +236,19 @@ void ref_block_scene(uint32_t nx,
     }
 }
 
+// n points with both coordinates drawn from
+// std::uniform_real_distribution<float>{lo, hi} over std::mt19937_64{seed}, x
+// then y per point: the fixture of emerald/sph_common/tests/test_common.cpp:18-31
+// and test_neighborhood.cpp:18-31 (7927 points, seed 17272, [-100, 100]).
+void ref_uniform_points(size_t n, uint64_t seed, float lo, float hi, float* xy) {
+    std::mt19937_64 gen{seed};
+    std::uniform_real_distribution<float> dist{lo, hi};
+    for (size_t i = 0; i < n; ++i) {
+        xy[2 * i] = dist(gen);
+        xy[2 * i + 1] = dist(gen);
+    }
+}
+
 void* ref_sim_create(ref_params const* p,
                      float const* solid_xy,
                      size_t n_solid,

@@ -254,6 +254,7 @@ class Reference:
         L.ref_vec2_length.argtypes = [c_f, c_f]
         L.ref_block_scene.argtypes = [ctypes.c_uint32, ctypes.c_uint32, c_f, c_f, c_f, c_f,
                                       c_u64, c_vp]
+        L.ref_uniform_points.argtypes = [c_sz, c_u64, c_f, c_f, c_vp]
         L.ref_sim_create.restype = c_vp
         L.ref_sim_create.argtypes = [ctypes.POINTER(RefParams), c_vp, c_sz, c_vp, c_vp, c_sz]
         L.ref_sim_destroy.argtypes = [c_vp]
@@ -311,6 +312,11 @@ class Reference:
     def block_scene(self, nx, ny, dx, x0=0.0, y0=0.0, jitter=0.01, seed=1):
         xy = np.zeros((nx * ny, 2), np.float32)
         self.L.ref_block_scene(nx, ny, dx, x0, y0, jitter, seed, ptr(xy))
+        return xy
+
+    def uniform_points(self, n, seed, lo, hi):
+        xy = np.zeros((n, 2), np.float32)
+        self.L.ref_uniform_points(n, seed, lo, hi, ptr(xy))
         return xy
 
     def self_neighborhoods(self, xy, cell_size):

@@ -1,0 +1,204 @@
+"""The CUDA path against the oracle and the reference's golden runs.
+
+Every comparison is bit-exact: positions, velocities, densities, neighbour
+lists and sort products of the GPU sub-step must equal the reference's."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import assert_bitwise
+from scenes import F
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+METHODS = ["pcisph", "iisph", "iisph_ap", "iisph_pseudo_ap", "dfsph_p"]
+
+
+@pytest.fixture(scope="module")
+def E():
+    import emerald_b200
+    return emerald_b200
+
+
+def golden_params(E, g):
+    return E.default_params(support=g["dx"], time_per_step_flicks=1411200, sub_steps=4,
+                            iisph_max_pressure_iterations=50,
+                            iisph_error_average_threshold=F(0.001),
+                            dfsph_divergence_error_average_threshold=F(0.001),
+                            dfsph_density_error_average_threshold=F(0.0005),
+                            mass_per_particle=g["mass"], pressure_correction_denom=g["denom"])
+
+
+def oracle_params(E, p):
+    d = p.as_dict()
+    cfg = E.config(p)
+    out = {k: d[k] for k in d if k not in ("seed", "length")}
+    out.update(mass_per_particle=cfg["mass_per_particle"],
+               pressure_correction_denom=cfg["pressure_correction_denom"],
+               seconds_per_sub_step=cfg["seconds_per_sub_step"])
+    return out
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_golden_runs(E, method):
+    """Six fixed-dt sub-steps of each solver equal the reference's run."""
+    g = dict(np.load(os.path.join(GOLDEN, "run_%s.npz" % method)))
+    sim = E.Simulation(golden_params(E, g), g["solid"], g["fluid"], None, g["solid_volumes"])
+    sim.begin_frame(method)
+    dt = g["dt"]
+    for s in range(len(g["x"])):
+        sim.sub_step(method, F(s * dt), dt)
+        x, v = sim.state()
+        assert_bitwise(x, g["x"][s], "%s x after sub-step %d" % (method, s))
+        assert_bitwise(v, g["v"][s], "%s v after sub-step %d" % (method, s))
+        assert_bitwise(sim.array("densities"), g["rho"][s], "%s densities %d" % (method, s))
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_substeps_match_oracle(E, oracle, method):
+    """Ten sub-steps of a jittered 48x48 block with every solver temporary,
+    the neighbour lists and the iteration counts compared."""
+    scene = E.BlockScene(48, dx=F(1 / 96), seed=5, dt=F(352800 / 705600000.0),
+                         iisph_max_pressure_iterations=50,
+                         iisph_error_average_threshold=F(0.001),
+                         time_per_step_flicks=1411200, sub_steps=4)
+    sim = E.Simulation.from_block_scene(scene)
+    osim = oracle.sim(oracle_params(E, scene.params), scene.solid, scene.solid_volumes,
+                      scene.fluid)
+    dt = F(352800 / 705600000.0) if method == "pcisph" else F(2e-4)
+    sim.begin_frame(method)
+    osim.begin_frame(method)
+    for s in range(10):
+        st = sim.sub_step(method, F(s * dt), dt)
+        ost = osim.sub_step(method, F(s * dt), dt)
+        assert st["pressure_iterations"] == ost["pressure_iterations"], (s, st, ost)
+        if method == "dfsph_p":
+            assert st["divergence_iterations"] == ost["divergence_iterations"], (s, st, ost)
+        x, v = sim.state()
+        ox, ov = osim.state()
+        assert_bitwise(x, ox, "%s x %d" % (method, s))
+        assert_bitwise(v, ov, "%s v %d" % (method, s))
+    names = {"pcisph": ["densities", "pressures", "pressure_forces", "position_stars",
+                        "velocity_stars", "velocity_external_forces"],
+             "iisph": ["densities", "pressures", "density_stars", "aiis", "diis", "sum_dij_pjs"],
+             "iisph_ap": ["densities", "pressures", "density_stars", "aiis",
+                          "pressure_accelerations"],
+             "iisph_pseudo_ap": ["densities", "pressures", "density_stars", "aiis",
+                                 "pressure_accelerations"],
+             "dfsph_p": ["densities", "density_stars", "alphas", "divergence_kappas",
+                         "density_kappas"]}[method]
+    for name in names:
+        assert_bitwise(sim.array(name), osim.array(name), "%s %s" % (method, name))
+    for solid in (False, True):
+        c1, i1, w1, g1 = sim.neighbors(solid)
+        c2, i2, w2, g2 = osim.neighbors(solid)
+        assert_bitwise(c1, c2, "counts")
+        assert_bitwise(i1, i2, "indices")
+        if method != "pcisph":
+            assert_bitwise(w1, w2, "W")
+            assert_bitwise(g1, g2, "grad W")
+
+
+@pytest.mark.parametrize("method", ["dfsph_p", "iisph", "pcisph", "iisph_pseudo_ap"])
+def test_adaptive_frames_match_oracle(E, oracle, method):
+    scene = E.BlockScene(40, dx=F(1 / 80), seed=2, dt=F(352800 / 705600000.0),
+                         time_per_step_flicks=1411200, sub_steps=4)
+    sim = E.Simulation.from_block_scene(scene)
+    osim = oracle.sim(oracle_params(E, scene.params), scene.solid, scene.solid_volumes,
+                      scene.fluid)
+    for f in range(3):
+        st = sim.frame(method)
+        k = osim.frame(method)
+        assert st["sub_steps"] == k
+        assert sim.time() == osim.time()
+        x, v = sim.state()
+        ox, ov = osim.state()
+        assert_bitwise(x, ox, "%s frame %d x" % (method, f))
+        assert_bitwise(v, ov, "%s frame %d v" % (method, f))
+
+
+def test_advance_equals_frames(E):
+    scene = E.BlockScene(32, dx=F(1 / 64), seed=4, time_per_step_flicks=1411200, sub_steps=4)
+    a = E.Simulation.from_block_scene(scene)
+    b = E.Simulation.from_block_scene(scene)
+    n = 0
+    for _ in range(3):
+        n += a.frame("dfsph_p")["sub_steps"]
+    b.advance("dfsph_p", n)
+    assert_bitwise(a.state()[0], b.state()[0], "x")
+    assert a.time() == b.time()
+
+
+def test_default_scene_frames(E):
+    """The reference's own dam break (hex lattice, world walls with 16 blocks,
+    boundary volumes 1.7/sum W computed on the GPU)."""
+    g = dict(np.load(os.path.join(GOLDEN, "frames_default.npz")))
+    p = E.default_params()
+    for m in ["dfsph_p", "iisph"]:
+        sim = E.Simulation(p, g["solid"], g["fluid"])
+        _, vol = sim.solid()
+        assert_bitwise(vol, g["solid_volumes"], "boundary volumes")
+        for f in range(2):
+            sim.frame(m)
+            x, v = sim.state()
+            assert_bitwise(x, g["%s_x%d" % (m, f)], "%s frame %d x" % (m, f))
+            assert_bitwise(v, g["%s_v%d" % (m, f)], "%s frame %d v" % (m, f))
+
+
+def test_fixture_neighbors_and_sort(E):
+    """The reference test fixture (7927 points in [-100, 100]^2, cell 2.1):
+    negative cells exercise the full 64-bit key range, including the key of
+    cell (-1, -1), which equals the table's empty marker."""
+    g = dict(np.load(os.path.join(GOLDEN, "uniform_7927.npz")))
+    p = E.default_params(support=F(1.05))
+    far = np.array([[1e4, 1e4]], np.float32)
+    sim = E.Simulation(p, far, g["xy"], None, np.ones(1, np.float32))
+    sim.sub_step("pcisph", 0.0, F(1e-6))
+    counts, idx, _, _ = sim.neighbors()
+    assert_bitwise(counts, g["counts"], "counts")
+    assert_bitwise(idx, g["idx"], "indices")
+    s = sim.sort()
+    assert_bitwise(s["grid_coords"], g["grid_coords"], "grid coords")
+    assert_bitwise(s["z_indices"], g["z_indices"], "z")
+    assert_bitwise(s["pair_index"], g["pair_index"], "pair index")
+    assert_bitwise(s["block_indices"], g["block_indices"], "block indices")
+    assert np.all(np.diff(s["pair_z"].astype(np.float64)) >= 0) or np.all(
+        s["pair_z"][1:] >= s["pair_z"][:-1])
+
+
+def test_sort_products_match_oracle(E, oracle):
+    scene = E.BlockScene(64, dx=F(1 / 128), seed=9)
+    sim = E.Simulation.from_block_scene(scene)
+    x0 = scene.fluid
+    sim.sub_step("dfsph_p", 0.0, F(1e-4))
+    for solid, pts in ((False, x0), (True, scene.solid)):
+        s = sim.sort(solid)
+        o = oracle.sort(pts, F(2 * scene.support))
+        for k in ("grid_coords", "z_indices", "pair_z", "pair_index", "block_indices", "blocks"):
+            assert_bitwise(s[k], o[k].astype(s[k].dtype), "%s %s" % ("solid" if solid else "fluid", k))
+
+
+def test_large_scene_matches_oracle(E, oracle):
+    """The 512x512 (262144-particle) dam break of the DFSPH benchmark, two
+    adaptive sub-steps against the oracle."""
+    scene = E.BlockScene(512, dx=F(1 / 1024), seed=1, time_per_step_flicks=1411200, sub_steps=4,
+                         dfsph_divergence_error_average_threshold=F(0.001),
+                         dfsph_density_error_average_threshold=F(0.0005))
+    sim = E.Simulation.from_block_scene(scene)
+    osim = oracle.sim(oracle_params(E, scene.params), scene.solid, scene.solid_volumes,
+                      scene.fluid)
+    oracle.set_threads(os.cpu_count() or 1)
+    try:
+        for s in range(2):
+            osim.sub_step("dfsph_p", F(s * 2e-4), F(2e-4))
+            sim.sub_step("dfsph_p", F(s * 2e-4), F(2e-4))
+    finally:
+        oracle.set_threads(1)
+    assert_bitwise(sim.state()[0], osim.state()[0], "x")
+    assert_bitwise(sim.state()[1], osim.state()[1], "v")
+    counts, idx, _, _ = sim.neighbors()
+    c2, i2, _, _ = osim.neighbors()
+    assert_bitwise(counts, c2, "counts")
+    assert_bitwise(idx, i2, "indices")

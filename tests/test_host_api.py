@@ -1,0 +1,104 @@
+"""Host-side parts of the product library that need no GPU: the C ABI
+exports, parameter validation, configuration and scene generators."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import emerald_b200 as E
+from conftest import assert_bitwise
+from scenes import F, lattice_template, walls
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "emerald_sph.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(emerald_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(E.LIB_PATH)
+    names = header_symbols()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_bindings_cover_header():
+    assert set(header_symbols()) == set(E.EXPORTS)
+
+
+@pytest.mark.parametrize("x,y,z", [(0b111, 0b111, 0b111111), (0xFFFF, 0xFFFF, 0xFFFFFFFF),
+                                   (0, 0xFFFF, 0xAAAAAAAA),
+                                   (0xFFFFFFFF, 0xFFFFFFFF, 0xFFFFFFFFFFFFFFFF)])
+def test_z_index(x, y, z):
+    assert E.z_index(x, y) == z
+
+
+def test_invalid_arguments_return_einval():
+    p = E.default_params(support=0.0)
+    h = ctypes.c_void_p()
+    rc = E.lib.emerald_sim_create(ctypes.byref(p), None, None, 0, None, None, 0, ctypes.byref(h))
+    assert rc == 22
+    assert b"support" in E.lib.emerald_last_error()
+    p = E.default_params()
+    rc = E.lib.emerald_sim_create(ctypes.byref(p), None, None, 5, None, None, 0, ctypes.byref(h))
+    assert rc == 22
+    assert E.lib.emerald_sim_sub_step(None, 1, 0.0, 1e-4, None) == 22
+    assert E.lib.emerald_sim_frame(None, 9, None) == 22
+
+
+def test_default_config_matches_reference_values():
+    c = E.config(E.default_params())
+    # emerald/sph2d_box/config.cpp for the default Parameters
+    assert c["seconds_per_sub_step"] == F(1.0 / 900.0)
+    assert c["draw_radius"] == F(0.99) * (F(0.025) * F(0.5))
+
+
+def test_config_matches_reference(reference):
+    for sup in (0.025, 0.01, 1 / 512, 1 / 2048):
+        p = E.default_params(support=F(sup))
+        rp = reference.default_params()
+        rp["support"] = F(sup)
+        a = E.config(p)
+        b = reference.config(rp)
+        for k in a:
+            assert F(a[k]) == F(b[k]), (sup, k)
+
+
+def test_lattice_config_matches_restatement(oracle):
+    for dx in (F(1 / 64), F(1 / 1024)):
+        p = E.default_params(support=dx)
+        got = E.lattice_config(p, dx, F(5e-4))
+        want = lattice_template(oracle.kernel_w, oracle.kernel_grad_w, oracle.L.oracle_vec2_length,
+                                dx, dx, 1000.0, F(5e-4))
+        assert F(got[0]) == F(want[0]) and F(got[1]) == F(want[1])
+
+
+def test_block_scene_and_walls_match_golden():
+    g = dict(np.load(os.path.join(GOLDEN, "run_iisph.npz")))
+    dx = F(1 / 48)
+    assert_bitwise(E.block_scene(24, 24, dx), g["fluid"], "block scene")
+    assert_bitwise(E.wall_scene(dx), g["solid"], "walls")
+    assert_bitwise(E.wall_scene(dx), walls(dx), "walls restated")
+    m, d = E.lattice_config(E.default_params(support=dx), dx, F(352800 / 705600000.0))
+    assert F(m) == F(g["mass"]) and F(d) == F(g["denom"])
+
+
+def test_reference_scene_generators_match_golden():
+    g = dict(np.load(os.path.join(GOLDEN, "frames_default.npz")))
+    p = E.default_params()
+    ww = E.world_walls(p)
+    assert_bitwise(ww, g["solid"], "world walls")
+    assert_bitwise(E.dam_break(p, ww), g["fluid"], "dam break")
+
+
+def test_block_scene_matches_reference_generator(reference):
+    a = E.block_scene(33, 17, F(1 / 100), 0.25, 0.5, 0.02, 11)
+    b = reference.block_scene(33, 17, F(1 / 100), 0.25, 0.5, 0.02, 11)
+    assert_bitwise(a, b, "block scene")
