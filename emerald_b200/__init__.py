@@ -92,6 +92,8 @@ EXPORTS = {
     "emerald_sim_enable_timing": (c_i32, [c_vp, c_i32]),
     "emerald_sim_kernel_times": (c_i32, [c_vp, ctypes.c_char_p, c_sz, c_vp, c_vp,
                                          ctypes.POINTER(c_i32)]),
+    "emerald_sim_set_graphs": (c_i32, [c_vp, c_i32]),
+    "emerald_sim_kernel_launches": (c_i32, [c_vp, ctypes.POINTER(c_i64)]),
     "emerald_kernel_launches": (c_i64, []),
     "emerald_last_error": (ctypes.c_char_p, []),
 }
@@ -333,6 +335,14 @@ class Simulation:
         _check(lib.emerald_sim_device_state(self._h, ctypes.byref(x), ctypes.byref(v)),
                "device_state")
         return x.value, v.value
+
+    def set_graphs(self, on=True):
+        _check(lib.emerald_sim_set_graphs(self._h, int(on)), "set_graphs")
+
+    def kernel_launches(self):
+        n = c_i64()
+        _check(lib.emerald_sim_kernel_launches(self._h, ctypes.byref(n)), "kernel_launches")
+        return n.value
 
     def enable_timing(self, on=True):
         _check(lib.emerald_sim_enable_timing(self._h, int(on)), "enable_timing")

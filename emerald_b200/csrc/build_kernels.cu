@@ -180,8 +180,67 @@ __global__ void k_sort_cells(uint32_t const* count,
     }
 }
 
+// Registers that hold a particle's sorted list on the common path.
+constexpr int kRegList = 16;
+
+// The search of find_neighbors with the sorted list in registers: every
+// accepted key bubbles through kRegList registers (min/max exchange, all
+// indices static, so nothing spills). Returns the accepted count; a count
+// above kRegList means the registers overflowed and the caller redoes the
+// particle with the 64-entry list.
+__device__ __forceinline__ int find_neighbors_reg(float2 pos,
+                                                  uint32_t self,
+                                                  bool same_set,
+                                                  float cell,
+                                                  float max_distance,
+                                                  OtherSet const& o,
+                                                  uint64_t (&r)[kRegList]) {
+#pragma unroll
+    for (int q = 0; q < kRegList; ++q) r[q] = ~0ull;
+    int32_t gx, gy;
+    grid_coord(pos, cell, gx, gy);
+    int cnt = 0;
+    for (int32_t j = gy - 1; cnt < kMaxNeighbors && j <= gy + 1; ++j) {
+        for (int32_t k = gx - 1; cnt < kMaxNeighbors && k <= gx + 1; ++k) {
+            uint32_t slot;
+            uint64_t const z = morton2(static_cast<uint32_t>(k), static_cast<uint32_t>(j));
+            if (!table_find(o.keys, o.log2cap, z, slot)) continue;
+            uint32_t const b = o.start[slot];
+            uint32_t const e = b + o.count[slot];
+            for (uint32_t m = b; cnt < kMaxNeighbors && m != e; ++m) {
+                uint32_t const other = o.members[m];
+                if (same_set && other == self) continue;
+                float2 const vec = sub2(o.x[other], pos);
+                float const dist = length2f(vec);
+                if (dist >= max_distance) continue;
+                uint64_t key = (static_cast<uint64_t>(__float_as_uint(dist)) << 32) |
+                               static_cast<uint64_t>(other - o.begin);
+#pragma unroll
+                for (int q = 0; q < kRegList; ++q) {
+                    uint64_t const lo = r[q] < key ? r[q] : key;
+                    key = r[q] < key ? key : r[q];
+                    r[q] = lo;
+                }
+                ++cnt;
+            }
+        }
+    }
+    return cnt;
+}
+
+// GradW (emerald/sph_common/kernels.h:57-64) of dp with |dp| = r already known
+// (the length of -v equals the length of v bit for bit).
+__device__ __forceinline__ float2 kernel_grad_w_r(float2 dp, float r, float h) {
+    if (safe_v(dp, r)) {
+        float const d = kernel_dw(r, h);
+        float2 const u = div2(dp, r);
+        return mk2(u.x * d, u.y * d);
+    }
+    return mk2(0.0f, 0.0f);
+}
+
 template <bool SOLID_OTHER>
-__global__ void k_neighbors(Arena a, int write_kernels) {
+__global__ void __launch_bounds__(kTile) k_neighbors(Arena a, int write_kernels) {
     int32_t const s = a.tile_scene[blockIdx.x];
     if (s < 0) return;
     SceneParams const& P = a.sp[s];
@@ -198,25 +257,46 @@ __global__ void k_neighbors(Arena a, int write_kernels) {
         o = OtherSet{a.x, a.fkeys + P.ftab_begin, a.fcount + P.ftab_begin, a.fstart + P.ftab_begin,
                      a.members, P.ftab_log2, P.fluid_begin};
     }
-    float2 const pos = a.x[i];
-    uint64_t list[kMaxNeighbors];
-    int const cnt = (SOLID_OTHER && P.solid_count == 0)
-                      ? 0
-                      : find_neighbors(pos, i, !SOLID_OTHER, cell, cell, o, list);
     uint8_t* cnt_out = SOLID_OTHER ? a.ns_cnt : a.nf_cnt;
     uint32_t* idx_out = SOLID_OTHER ? a.ns_idx : a.nf_idx;
     float* w_out = SOLID_OTHER ? a.ns_w : a.nf_w;
     float2* gw_out = SOLID_OTHER ? a.ns_gw : a.nf_gw;
-    cnt_out[i] = static_cast<uint8_t>(cnt);
     size_t const stride = a.stride;
-    for (int k = 0; k < cnt; ++k) {
+    float2 const pos = a.x[i];
+    if (SOLID_OTHER && P.solid_count == 0) {
+        cnt_out[i] = 0;
+        return;
+    }
+    uint64_t r[kRegList];
+    int const cnt = find_neighbors_reg(pos, i, !SOLID_OTHER, cell, cell, o, r);
+    cnt_out[i] = static_cast<uint8_t>(cnt);
+    if (cnt <= kRegList) {
+#pragma unroll
+        for (int k = 0; k < kRegList; ++k) {
+            if (k < cnt) {
+                uint32_t const j = o.begin + static_cast<uint32_t>(r[k] & 0xffffffffu);
+                size_t const e = static_cast<size_t>(k) * stride + i;
+                idx_out[e] = j;
+                if (write_kernels) {
+                    float const dist = __uint_as_float(static_cast<uint32_t>(r[k] >> 32));
+                    w_out[e] = kernel_w(dist, h);
+                    gw_out[e] = kernel_grad_w_r(neg2(sub2(o.x[j], pos)), dist, h);
+                }
+            }
+        }
+        return;
+    }
+    // more than kRegList neighbours: the full 64-entry list
+    uint64_t list[kMaxNeighbors];
+    int const n64 = find_neighbors(pos, i, !SOLID_OTHER, cell, cell, o, list);
+    for (int k = 0; k < n64; ++k) {
         uint32_t const j = o.begin + static_cast<uint32_t>(list[k] & 0xffffffffu);
         size_t const e = static_cast<size_t>(k) * stride + i;
         idx_out[e] = j;
         if (write_kernels) {
             float const dist = __uint_as_float(static_cast<uint32_t>(list[k] >> 32));
             w_out[e] = kernel_w(dist, h);
-            gw_out[e] = kernel_grad_w(neg2(sub2(o.x[j], pos)), h);
+            gw_out[e] = kernel_grad_w_r(neg2(sub2(o.x[j], pos)), dist, h);
         }
     }
 }

@@ -312,6 +312,20 @@ int emerald_sim_device_state(emerald_sim* sim, void** x, void** v) {
     return EMERALD_OK;
 }
 
+int emerald_sim_set_graphs(emerald_sim* sim, int32_t graphs) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    sim->engine.set_graphs(graphs != 0);
+    return EMERALD_OK;
+}
+
+int emerald_sim_kernel_launches(emerald_sim* sim, int64_t* count) {
+    if (!sim || !count) return fail(EMERALD_EINVAL, "bad arguments");
+    return guarded([&] {
+        *count = sim->engine.kernel_launches();
+        return EMERALD_OK;
+    });
+}
+
 int emerald_sim_enable_timing(emerald_sim* sim, int32_t enable) {
     if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
     return guarded([&] {

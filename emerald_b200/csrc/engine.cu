@@ -167,6 +167,13 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
       std::max(scan_scratch_words(a_.ftab_total), scan_scratch_words(a_.stab_total)) + 64;
     d_scan_ = static_cast<uint32_t*>(dev(4ull * scan_words));
     d_running_ = static_cast<int*>(dev(sizeof(int)));
+    d_loop_iters_ = static_cast<unsigned long long*>(dev(sizeof(unsigned long long) * 4));
+    a_.loop_iterations = d_loop_iters_;
+    cudaMemset(d_loop_iters_, 0, sizeof(unsigned long long) * 4);
+    if (cudaStreamCreateWithFlags(&cap_st_, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&body_st_, cudaStreamNonBlocking) != cudaSuccess) {
+        throw std::runtime_error("stream creation failed");
+    }
     if (cudaMallocHost(reinterpret_cast<void**>(&h_running_), sizeof(int)) != cudaSuccess) {
         throw std::bad_alloc();
     }
@@ -183,7 +190,16 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
     check("engine allocation");
 }
 
+void Engine::destroy_graphs() {
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+    graph_fixed_kernels_.clear();
+}
+
 Engine::~Engine() {
+    destroy_graphs();
+    if (cap_st_) cudaStreamDestroy(cap_st_);
+    if (body_st_) cudaStreamDestroy(body_st_);
     for (auto& p : pending_) {
         cudaEventDestroy(p.start);
         cudaEventDestroy(p.stop);
@@ -195,9 +211,16 @@ Engine::~Engine() {
 }
 
 template <class F>
-void Engine::launch(char const* name, F&& f) {
-    g_launches.fetch_add(1, std::memory_order_relaxed);
-    if (!timing_) {
+void Engine::launch(char const* name, F&& f, int kernels) {
+    if (count_host_) {
+        if (capturing_) {
+            capture_kernels_ += kernels;
+        } else {
+            g_launches.fetch_add(kernels, std::memory_order_relaxed);
+            host_launches_ += kernels;
+        }
+    }
+    if (!timing_ || capturing_) {
         f();
         return;
     }
@@ -373,7 +396,7 @@ int Engine::add_scene(SceneSpec const& spec) {
 
 void Engine::rebuild_solids() {
     launch("build_cells_solid",
-           [&] { launch_build_cells(a_, true, solid_cap_ / kTile, d_scan_, st_); });
+           [&] { launch_build_cells(a_, true, solid_cap_ / kTile, d_scan_, st_); }, 6);
 }
 
 void Engine::remove_scene(int id) {
@@ -433,50 +456,197 @@ int Engine::max_iterations(int kind) const {
     return m;
 }
 
-void Engine::run_loop(int kind, int max_iter, int32_t method) {
+// Solver iteration kernels of one loop kind (launched on cur_).
+void Engine::emit_loop_body(int kind, int32_t method, cudaGraphConditionalHandle cond,
+                            bool use_cond) {
     uint32_t const tiles = fluid_cap_ / kTile;
-    launch("iter_reset", [&] { launch_iter_reset(a_, max_scenes_, st_); });
+    cudaStream_t const st = cur_;
+    // loop kernels are counted on the device, once per executed iteration
+    bool const was_counting = count_host_;
+    count_host_ = false;
+    switch (method) {
+    case kDfsph:
+        if (kind == 2) {
+            launch("dfsph_divergence", [&] { launch_dfsph_divergence(a_, tiles, st); });
+            launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 1, st); });
+        } else {
+            launch("dfsph_density", [&] { launch_dfsph_density(a_, tiles, st); });
+            launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 1, 0, 1, st); });
+        }
+        break;
+    case kIisph:
+        launch("iisph_sum_dij", [&] { launch_iisph_sum_dij(a_, tiles, st); });
+        launch("iisph_beta_pressure", [&] { launch_iisph_beta_pressure(a_, tiles, st); });
+        break;
+    case kIisphAp:
+    case kIisphPseudoAp: {
+        int const pseudo = method == kIisphPseudoAp ? 1 : 0;
+        launch("pressure_accel", [&] { launch_pressure_accel(a_, tiles, st); });
+        launch("ap_iterate", [&] { launch_ap_iterate(a_, tiles, pseudo, st); });
+        break;
+    }
+    case kPcisph:
+        launch("pc_predict", [&] { launch_pc_predict(a_, tiles, st); });
+        launch("pc_density", [&] { launch_pc_density(a_, tiles, st); });
+        launch("pc_forces", [&] { launch_pc_forces(a_, tiles, st); });
+        break;
+    default: break;
+    }
+    launch("iter_check", [&] {
+        launch_iter_check(a_, max_scenes_, kind, d_running_, cond, use_cond ? 1 : 0, st);
+    });
+    count_host_ = was_counting;
+}
+
+// Kernels per executed iteration of each loop kind (body kernels + check).
+static int loop_body_kernels(int kind) { return kind == 3 ? 4 : 3; }
+
+int64_t Engine::kernel_launches() {
+    unsigned long long it[4] = {0, 0, 0, 0};
+    cudaMemcpyAsync(it, d_loop_iters_, sizeof(it), cudaMemcpyDeviceToHost, st_);
+    cudaStreamSynchronize(st_);
+    int64_t n = host_launches_;
+    for (int k = 0; k < 4; ++k) n += int64_t(it[k]) * loop_body_kernels(k);
+    return n;
+}
+
+void Engine::run_loop(int kind, int max_iter, int32_t method) {
+    launch("iter_reset", [&] { launch_iter_reset(a_, max_scenes_, kind, cur_); });
+    if (capturing_) {
+        // while (any scene iterates) { body; check } as a conditional node
+        cudaStreamCaptureStatus status;
+        cudaGraph_t g = nullptr;
+        cudaGraphNode_t const* deps = nullptr;
+        size_t ndeps = 0;
+        if (cudaStreamGetCaptureInfo(cur_, &status, nullptr, &g, &deps, &ndeps) != cudaSuccess ||
+            status != cudaStreamCaptureStatusActive) {
+            throw std::runtime_error("graph capture: no active capture");
+        }
+        cudaGraphConditionalHandle cond;
+        if (cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+            throw std::runtime_error("graph capture: conditional handle");
+        }
+        cudaGraphNodeParams params{};
+        params.type = cudaGraphNodeTypeConditional;
+        params.conditional.handle = cond;
+        params.conditional.type = cudaGraphCondTypeWhile;
+        params.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (cudaGraphAddNode(&node, g, deps, ndeps, &params) != cudaSuccess) {
+            throw std::runtime_error("graph capture: conditional node");
+        }
+        if (cudaStreamUpdateCaptureDependencies(cur_, &node, 1, cudaStreamSetCaptureDependencies) !=
+            cudaSuccess) {
+            throw std::runtime_error("graph capture: dependencies");
+        }
+        cudaGraph_t body = params.conditional.phGraph_out[0];
+        cudaStream_t const outer = cur_;
+        if (cudaStreamBeginCaptureToGraph(body_st_, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            throw std::runtime_error("graph capture: body");
+        }
+        cur_ = body_st_;
+        emit_loop_body(kind, method, cond, true);
+        cur_ = outer;
+        if (cudaStreamEndCapture(body_st_, &body) != cudaSuccess) {
+            throw std::runtime_error("graph capture: body end");
+        }
+        return;
+    }
     for (int it = 0; it < max_iter; ++it) {
-        switch (method) {
-        case kDfsph:
-            if (kind == 2) {
-                launch("dfsph_divergence", [&] { launch_dfsph_divergence(a_, tiles, st_); });
-                launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 1, st_); });
-            } else {
-                launch("dfsph_density", [&] { launch_dfsph_density(a_, tiles, st_); });
-                launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 1, 0, 1, st_); });
-            }
-            break;
-        case kIisph:
-            launch("iisph_sum_dij", [&] { launch_iisph_sum_dij(a_, tiles, st_); });
-            launch("iisph_beta_pressure", [&] { launch_iisph_beta_pressure(a_, tiles, st_); });
-            break;
-        case kIisphAp:
-        case kIisphPseudoAp: {
-            int const pseudo = method == kIisphPseudoAp ? 1 : 0;
-            launch("pressure_accel", [&] { launch_pressure_accel(a_, tiles, st_); });
-            launch("ap_iterate", [&] { launch_ap_iterate(a_, tiles, pseudo, st_); });
-            break;
-        }
-        case kPcisph:
-            launch("pc_predict", [&] { launch_pc_predict(a_, tiles, st_); });
-            launch("pc_density", [&] { launch_pc_density(a_, tiles, st_); });
-            launch("pc_forces", [&] { launch_pc_forces(a_, tiles, st_); });
-            break;
-        default: break;
-        }
-        launch("iter_check", [&] { launch_iter_check(a_, max_scenes_, kind, d_running_, st_); });
+        emit_loop_body(kind, method, 0, false);
         if (!unrolled_) {
-            cudaMemcpyAsync(h_running_, d_running_, sizeof(int), cudaMemcpyDeviceToHost, st_);
-            cudaStreamSynchronize(st_);
+            cudaMemcpyAsync(h_running_, d_running_, sizeof(int), cudaMemcpyDeviceToHost, cur_);
+            cudaStreamSynchronize(cur_);
             if (!*h_running_) break;
         }
     }
 }
 
+void Engine::emit_substep(int32_t method) {
+    uint32_t const tiles = fluid_cap_ / kTile;
+    cudaStream_t const st = cur_;
+    launch("max_v2", [&] { launch_max_v2(a_, tiles, st); });
+    launch("begin_substep", [&] { launch_begin_substep(a_, max_scenes_, st); });
+    // binning, three scan passes, scatter, per-cell ordering
+    launch("build_cells", [&] { launch_build_cells(a_, false, tiles, d_scan_, st); }, 6);
+    bool const kernels = method != kPcisph;
+    launch("neighbors_fluid", [&] { launch_neighbors(a_, tiles, false, kernels, st); });
+    launch("neighbors_solid", [&] { launch_neighbors(a_, tiles, true, kernels, st); });
+    switch (method) {
+    case kDfsph:
+        launch("dfsph_density_alpha", [&] { launch_dfsph_density_alpha(a_, tiles, st); });
+        launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 0, st); });
+        run_loop(2, max_iterations(2), method);
+        launch("apply_pressures_ext", [&] { launch_apply_pressures(a_, tiles, 1, 1, 0, st); });
+        run_loop(1, max_iterations(1), method);
+        launch("integrate_positions", [&] { launch_integrate_positions(a_, tiles, st); });
+        break;
+    case kIisph:
+        launch("iisph_density_dii", [&] { launch_iisph_density_dii(a_, tiles, st); });
+        launch("iisph_aii", [&] { launch_iisph_aii(a_, tiles, st); });
+        run_loop(0, max_iterations(0), method);
+        launch("make_q", [&] { launch_make_q(a_, tiles, st); });
+        launch("apply_integrate", [&] { launch_apply_integrate(a_, tiles, st); });
+        break;
+    case kIisphAp:
+    case kIisphPseudoAp: {
+        int const pseudo = method == kIisphPseudoAp ? 1 : 0;
+        launch("ap_density", [&] { launch_ap_density(a_, tiles, st); });
+        launch("ap_diag", [&] { launch_ap_diag(a_, tiles, pseudo, st); });
+        run_loop(0, max_iterations(0), method);
+        launch("ap_finish", [&] { launch_ap_finish(a_, tiles, pseudo, st); });
+        break;
+    }
+    case kPcisph:
+        launch("pc_init", [&] { launch_pc_init(a_, tiles, st); });
+        run_loop(3, 6, method);
+        launch("pc_final", [&] { launch_pc_final(a_, tiles, st); });
+        break;
+    default: throw std::runtime_error("unknown method");
+    }
+}
+
+// Records one sub-step of `method` into a graph. Kernel arguments are the
+// arena pointers and the tile count, which never change for an engine, and
+// every kernel reads scene membership and parameters from device memory, so
+// the graph stays valid as scenes are added, removed or (de)activated.
+void Engine::capture_substep(int32_t method) {
+    cudaStreamSynchronize(st_);
+    if (cudaStreamBeginCapture(cap_st_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        throw std::runtime_error("graph capture: begin");
+    }
+    capturing_ = true;
+    capture_kernels_ = 0;
+    cur_ = cap_st_;
+    try {
+        emit_substep(method);
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(cap_st_, &g);
+        if (g) cudaGraphDestroy(g);
+        capturing_ = false;
+        cur_ = st_;
+        throw;
+    }
+    capturing_ = false;
+    cur_ = st_;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamEndCapture(cap_st_, &g) != cudaSuccess) {
+        throw std::runtime_error("graph capture: end");
+    }
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t const e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        throw std::runtime_error(std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    graphs_[method] = exec;
+    graph_fixed_kernels_[method] = capture_kernels_;
+}
+
 void Engine::substep(int32_t method) {
     if (active_scenes() == 0) return;
-    uint32_t const tiles = fluid_cap_ / kTile;
     for (int id = 0; id < max_scenes_; ++id) {
         Scene& sc = scenes_[id];
         if (!sc.used || !sc.active) continue;
@@ -487,44 +657,24 @@ void Engine::substep(int32_t method) {
             upload_params(id);
         }
     }
-    launch("max_v2", [&] { launch_max_v2(a_, tiles, st_); });
-    launch("begin_substep", [&] { launch_begin_substep(a_, max_scenes_, st_); });
-    launch("build_cells", [&] { launch_build_cells(a_, false, tiles, d_scan_, st_); });
-    bool const kernels = method != kPcisph;
-    launch("neighbors_fluid", [&] { launch_neighbors(a_, tiles, false, kernels, st_); });
-    launch("neighbors_solid", [&] { launch_neighbors(a_, tiles, true, kernels, st_); });
-    switch (method) {
-    case kDfsph:
-        launch("dfsph_density_alpha", [&] { launch_dfsph_density_alpha(a_, tiles, st_); });
-        launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 0, st_); });
-        run_loop(2, max_iterations(2), method);
-        launch("apply_pressures_ext", [&] { launch_apply_pressures(a_, tiles, 1, 1, 0, st_); });
-        run_loop(1, max_iterations(1), method);
-        launch("integrate_positions", [&] { launch_integrate_positions(a_, tiles, st_); });
-        break;
-    case kIisph:
-        launch("iisph_density_dii", [&] { launch_iisph_density_dii(a_, tiles, st_); });
-        launch("iisph_aii", [&] { launch_iisph_aii(a_, tiles, st_); });
-        run_loop(0, max_iterations(0), method);
-        launch("make_q", [&] { launch_make_q(a_, tiles, st_); });
-        launch("apply_integrate", [&] { launch_apply_integrate(a_, tiles, st_); });
-        break;
-    case kIisphAp:
-    case kIisphPseudoAp: {
-        int const pseudo = method == kIisphPseudoAp ? 1 : 0;
-        launch("ap_density", [&] { launch_ap_density(a_, tiles, st_); });
-        launch("ap_diag", [&] { launch_ap_diag(a_, tiles, pseudo, st_); });
-        run_loop(0, max_iterations(0), method);
-        launch("ap_finish", [&] { launch_ap_finish(a_, tiles, pseudo, st_); });
-        break;
+    if (use_graphs_ && !timing_) {
+        auto it = graphs_.find(method);
+        if (it == graphs_.end()) {
+            capture_substep(method);
+            it = graphs_.find(method);
+        }
+        if (cudaGraphLaunch(it->second, st_) != cudaSuccess) {
+            check("graph launch");
+            throw std::runtime_error("graph launch failed");
+        }
+        int64_t const fixed = graph_fixed_kernels_[method];
+        host_launches_ += fixed;
+        g_launches.fetch_add(fixed, std::memory_order_relaxed);
+        check("substep graph");
+        return;
     }
-    case kPcisph:
-        launch("pc_init", [&] { launch_pc_init(a_, tiles, st_); });
-        run_loop(3, 6, method);
-        launch("pc_final", [&] { launch_pc_final(a_, tiles, st_); });
-        break;
-    default: throw std::runtime_error("unknown method");
-    }
+    cur_ = st_;
+    emit_substep(method);
     check("substep");
 }
 

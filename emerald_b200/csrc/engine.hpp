@@ -106,6 +106,12 @@ public:
     // reference); true launches every iteration up to the cap and lets
     // finished scenes' kernels return at once (no host round trips).
     void set_unrolled_loops(bool on) { unrolled_ = on; }
+    // Graph mode (default): each sub-step is one CUDA graph launch, with the
+    // solver loops as conditional while nodes (no host round trips).
+    void set_graphs(bool on) { use_graphs_ = on; }
+    // Kernels this engine launched (graph nodes included, loop bodies
+    // counted per executed iteration).
+    int64_t kernel_launches();
 
     void check(char const* what);
 
@@ -119,10 +125,14 @@ private:
     };
 
     template <class F>
-    void launch(char const* name, F&& f);
+    void launch(char const* name, F&& f, int kernels = 1);
     void upload_params(int id);
     void upload_tiles();
     void run_loop(int kind, int max_iter, int32_t method);
+    void emit_substep(int32_t method);
+    void emit_loop_body(int kind, int32_t method, cudaGraphConditionalHandle cond, bool use_cond);
+    void capture_substep(int32_t method);
+    void destroy_graphs();
     int max_iterations(int kind) const;
     void rebuild_solids();
     void ensure_sort_scratch(uint32_t n);
@@ -144,7 +154,17 @@ private:
     RangeAllocator fluid_tiles_, solid_tiles_, ftab_, stab_;
     bool tiles_dirty_ = true;
     bool unrolled_ = false;
-    int32_t last_method_ = -1;
+    bool use_graphs_ = true;
+    bool capturing_ = false;
+    cudaStream_t cur_ = nullptr;  // stream the emitted work goes to
+    cudaStream_t cap_st_ = nullptr;
+    cudaStream_t body_st_ = nullptr;
+    std::map<int32_t, cudaGraphExec_t> graphs_;
+    std::map<int32_t, int64_t> graph_fixed_kernels_;
+    int64_t host_launches_ = 0;
+    int64_t capture_kernels_ = 0;
+    bool count_host_ = true;
+    unsigned long long* d_loop_iters_ = nullptr;
 
     void* sort_buf_ = nullptr;
     uint32_t sort_cap_ = 0;

@@ -80,6 +80,7 @@ struct SceneState {
 struct Arena {
     SceneParams const* sp;
     SceneState* ss;
+    unsigned long long* loop_iterations;  // executed solver iterations per loop kind
     int32_t const* tile_scene;   // fluid tile -> scene (-1: free)
     int32_t const* stile_scene;  // solid tile -> scene
     uint32_t stride;             // fluid arena capacity (multiple of kTile)

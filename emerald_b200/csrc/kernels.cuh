@@ -48,8 +48,9 @@ void launch_sort_products(Arena const& a, bool solid, int scene, uint32_t begin,
 void launch_max_v2(Arena const& a, uint32_t tiles, cudaStream_t st);
 void launch_begin_substep(Arena const& a, int nscenes, cudaStream_t st);
 void launch_zero_kappas(Arena const& a, uint32_t tiles, cudaStream_t st);
-void launch_iter_reset(Arena const& a, int nscenes, cudaStream_t st);
-void launch_iter_check(Arena const& a, int nscenes, int kind, int* running, cudaStream_t st);
+void launch_iter_reset(Arena const& a, int nscenes, int kind, cudaStream_t st);
+void launch_iter_check(Arena const& a, int nscenes, int kind, int* running,
+                       cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st);
 void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, cudaStream_t st);
 void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int external,
                             int skip_done, cudaStream_t st);

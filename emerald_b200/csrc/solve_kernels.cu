@@ -177,12 +177,18 @@ __global__ void k_zero_kappas(Arena a) {
     a.kdens[c.i] = 0.0f;
 }
 
-__global__ void k_iter_reset(Arena a, int nscenes) {
+__device__ __forceinline__ int iteration_cap(SceneParams const& P, int kind) {
+    return kind == 0 ? P.iisph_max_iter : (kind == 3 ? 6 : P.dfsph_max_iter);
+}
+
+// Starts a solver loop; a scene whose cap is zero runs no iteration, as the
+// reference's for-loop would.
+__global__ void k_iter_reset(Arena a, int nscenes, int kind) {
     int const s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nscenes) return;
     SceneState& S = a.ss[s];
     S.iter = 0;
-    S.done = S.active ? 0 : 1;
+    S.done = (S.active && iteration_cap(a.sp[s], kind) > 0) ? 0 : 1;
     S.err_sum = 0ull;
     S.err_max = 0u;
 }
@@ -190,8 +196,10 @@ __global__ void k_iter_reset(Arena a, int nscenes) {
 // Exit test after one solver iteration. kind 0: IISPH family
 // (iisph.cpp:119-128), 1: DFSPH density (dfsph_p.cpp:113-133),
 // 2: DFSPH divergence (:187-211), 3: PCISPH (pcisph.cpp:144-148).
-// One block; *running is set when any scene still iterates.
-__global__ void k_iter_check(Arena a, int nscenes, int kind, int* running) {
+// One block; *running is set when any scene still iterates and, inside a
+// captured graph, the loop's while condition takes the same value.
+__global__ void k_iter_check(Arena a, int nscenes, int kind, int* running,
+                             cudaGraphConditionalHandle cond, int use_cond) {
     __shared__ int any;
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
@@ -205,10 +213,9 @@ __global__ void k_iter_check(Arena a, int nscenes, int kind, int* running) {
                             : 0.0f;
         float const mx = __uint_as_float(S.err_max);
         bool conv = false;
-        int max_iter = 0;
+        int const max_iter = iteration_cap(P, kind);
         if (kind == 0) {
             conv = S.iter > 1 && avg <= P.iisph_err_avg && mx <= P.iisph_err_max;
-            max_iter = P.iisph_max_iter;
             S.stat_avg = avg;
             S.stat_max = mx;
         } else if (kind == 1) {
@@ -217,20 +224,17 @@ __global__ void k_iter_check(Arena a, int nscenes, int kind, int* running) {
                 S.stat_avg = avg;
                 S.stat_max = mx;
             }
-            max_iter = P.dfsph_max_iter;
         } else if (kind == 2) {
             if (S.iter > 0) {
                 conv = avg <= P.dfsph_div_avg && mx <= P.dfsph_div_max;
                 S.stat_div_avg = avg;
                 S.stat_div_max = mx;
             }
-            max_iter = P.dfsph_max_iter;
         } else {
             if (S.iter > 1) {
                 conv = (mx / P.rho0) <= 0.01f;
                 S.stat_max = mx / P.rho0;
             }
-            max_iter = 6;
         }
         S.iter += 1;
         S.err_sum = 0ull;
@@ -247,7 +251,11 @@ __global__ void k_iter_check(Arena a, int nscenes, int kind, int* running) {
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0) *running = any;
+    if (threadIdx.x == 0) {
+        a.loop_iterations[kind] += 1ull;
+        *running = any;
+        if (use_cond) cudaGraphSetConditional(cond, any ? 1u : 0u);
+    }
 }
 
 // --------------------------------------------------------- shared SPH sums
@@ -259,10 +267,14 @@ __device__ __forceinline__ float density_of(Arena const& a, SceneParams const& P
     float const fmass = rho0 * P.fluid_volume;
     float d = P.fluid_volume * rho0 * P.w0;
     int const c = a.nf_cnt[i];
+    #pragma unroll 4
+
     for (int k = 0; k < c; ++k) d += a.nf_w[k * stride + i] * fmass;
     int const cs = a.ns_cnt[i];
     if (cs) {
         float db = 0.0f;
+        #pragma unroll 4
+
         for (int k = 0; k < cs; ++k) {
             size_t const e = k * stride + i;
             db += a.ns_w[e] * (rho0 * a.vols[a.ns_idx[e]]);
@@ -280,6 +292,8 @@ __device__ __forceinline__ float divergence_of(Arena const& a, SceneParams const
     float2 const vi = a.v[i];
     int const c = a.nf_cnt[i];
     float d = 0.0f;
+    #pragma unroll 4
+
     for (int k = 0; k < c; ++k) {
         size_t const e = k * stride + i;
         d += fmass * dot2(sub2(vi, a.v[a.nf_idx[e]]), a.nf_gw[e]);
@@ -287,6 +301,8 @@ __device__ __forceinline__ float divergence_of(Arena const& a, SceneParams const
     int const cs = a.ns_cnt[i];
     if (cs) {
         float db = 0.0f;
+        #pragma unroll 4
+
         for (int k = 0; k < cs; ++k) {
             size_t const e = k * stride + i;
             uint32_t const j = a.ns_idx[e];
@@ -308,6 +324,8 @@ __device__ __forceinline__ float2 apply_pressure_of(Arena const& a, SceneParams 
     int const c = a.nf_cnt[i];
     if (c) {
         float2 acc = mk2(0.0f, 0.0f);
+        #pragma unroll 4
+
         for (int k = 0; k < c; ++k) {
             size_t const e = k * stride + i;
             acc = add2(acc, scl2(neg_fmass * (qi + q[a.nf_idx[e]]), a.nf_gw[e]));
@@ -317,6 +335,8 @@ __device__ __forceinline__ float2 apply_pressure_of(Arena const& a, SceneParams 
     int const cs = a.ns_cnt[i];
     if (cs) {
         float2 acc = mk2(0.0f, 0.0f);
+        #pragma unroll 4
+
         for (int k = 0; k < cs; ++k) {
             size_t const e = k * stride + i;
             acc = add2(acc, scl2(-(rho0 * a.vols[a.ns_idx[e]]) * qi, a.ns_gw[e]));
@@ -337,6 +357,8 @@ __device__ __forceinline__ float2 pressure_accel_of(Arena const& a, SceneParams 
     int const c = a.nf_cnt[i];
     if (c) {
         float2 acc = mk2(0.0f, 0.0f);
+        #pragma unroll 4
+
         for (int k = 0; k < c; ++k) {
             size_t const e = k * stride + i;
             acc = add2(acc, scl2(neg_fmass * (qi + q[a.nf_idx[e]]), a.nf_gw[e]));
@@ -346,6 +368,8 @@ __device__ __forceinline__ float2 pressure_accel_of(Arena const& a, SceneParams 
     int const cs = a.ns_cnt[i];
     if (cs) {
         float2 acc = mk2(0.0f, 0.0f);
+        #pragma unroll 4
+
         for (int k = 0; k < cs; ++k) {
             size_t const e = k * stride + i;
             acc = add2(acc, scl2(-(rho0 * a.vols[a.ns_idx[e]]) * qi, a.ns_gw[e]));
@@ -384,6 +408,8 @@ __global__ void k_dfsph_density_alpha(Arena a) {
     int const cf = a.nf_cnt[i];
     float const fmass = rho0 * fvol;
     float const fmass_a = fvol * rho0;
+    #pragma unroll 4
+
     for (int k = 0; k < cf; ++k) {
         size_t const e = k * stride + i;
         d += a.nf_w[e] * fmass;
@@ -394,6 +420,8 @@ __global__ void k_dfsph_density_alpha(Arena a) {
     int const cs = a.ns_cnt[i];
     if (cs) {
         float db = 0.0f;
+        #pragma unroll 4
+
         for (int k = 0; k < cs; ++k) {
             size_t const e = k * stride + i;
             float const vs = a.vols[a.ns_idx[e]];
@@ -522,6 +550,8 @@ __global__ void k_iisph_density_dii(Arena a) {
     if (cf) {
         float const fmass = rho0 * P.fluid_volume;
         float2 g = mk2(0.0f, 0.0f);
+        #pragma unroll 4
+
         for (int k = 0; k < cf; ++k) g = add2(g, scl2(fmass, a.nf_gw[k * stride + i]));
         float2 const numer = scl2(neg_dt2, g);
         dii = safe_v(numer, denom) ? div2(numer, denom) : mk2(0.0f, 0.0f);
@@ -529,6 +559,8 @@ __global__ void k_iisph_density_dii(Arena a) {
     int const cs = a.ns_cnt[i];
     if (cs) {
         float2 g = mk2(0.0f, 0.0f);
+        #pragma unroll 4
+
         for (int k = 0; k < cs; ++k) {
             size_t const e = k * stride + i;
             g = add2(g, scl2(rho0 * a.vols[a.ns_idx[e]], a.ns_gw[e]));
@@ -558,6 +590,8 @@ __global__ void k_iisph_aii(Arena a) {
     if (cf) {
         float const mass = P.fluid_volume * rho0;
         float dd = 0.0f;
+        #pragma unroll 4
+
         for (int k = 0; k < cf; ++k) {
             size_t const e = k * stride + i;
             uint32_t const j = a.nf_idx[e];
@@ -576,6 +610,8 @@ __global__ void k_iisph_aii(Arena a) {
     if (cs) {
         float ab = 0.0f;
         float dd = 0.0f;
+        #pragma unroll 4
+
         for (int k = 0; k < cs; ++k) {
             size_t const e = k * stride + i;
             uint32_t const j = a.ns_idx[e];
@@ -605,6 +641,8 @@ __global__ void k_iisph_sum_dij(Arena a) {
     float const neg_dt2 = -sqrf(dt);
     float2 sum = mk2(0.0f, 0.0f);
     int const cf = a.nf_cnt[i];
+    #pragma unroll 4
+
     for (int k = 0; k < cf; ++k) {
         size_t const e = k * stride + i;
         uint32_t const j = a.nf_idx[e];
@@ -638,6 +676,8 @@ __global__ void k_iisph_beta_pressure(Arena a) {
         int const cf = a.nf_cnt[i];
         if (cf) {
             float const mass = rho0 * P.fluid_volume;
+            #pragma unroll 4
+
             for (int k = 0; k < cf; ++k) {
                 size_t const e = k * stride + i;
                 uint32_t const j = a.nf_idx[e];
@@ -654,6 +694,8 @@ __global__ void k_iisph_beta_pressure(Arena a) {
         int const cs = a.ns_cnt[i];
         if (cs) {
             float bb = 0.0f;
+            #pragma unroll 4
+
             for (int k = 0; k < cs; ++k) {
                 size_t const e = k * stride + i;
                 bb += (rho0 * a.vols[a.ns_idx[e]]) * dot2(si, a.ns_gw[e]);
@@ -736,6 +778,8 @@ __global__ void k_ap_diag(Arena a, int pseudo) {
     float sdot = 0.0f;
     float div = 0.0f;
     float const fmass = P.fluid_volume * rho0;
+    #pragma unroll 4
+
     for (int k = 0; k < cf; ++k) {
         size_t const e = k * stride + i;
         float2 const gw = a.nf_gw[e];
@@ -743,6 +787,8 @@ __global__ void k_ap_diag(Arena a, int pseudo) {
         sdot += fmass * dot2(gw, gw);
         div += fmass * dot2(sub2(vi, a.v[a.nf_idx[e]]), gw);
     }
+    #pragma unroll 4
+
     for (int k = 0; k < cs; ++k) {
         size_t const e = k * stride + i;
         uint32_t const j = a.ns_idx[e];
@@ -792,10 +838,14 @@ __global__ void k_ap_iterate(Arena a, int pseudo) {
             float api = 0.0f;
             float2 const ai = a.acc[i];
             float const fmass = rho0 * P.fluid_volume;
+            #pragma unroll 4
+
             for (int k = 0; k < cf; ++k) {
                 size_t const e = k * stride + i;
                 api += fmass * dot2(sub2(ai, a.acc[a.nf_idx[e]]), a.nf_gw[e]);
             }
+            #pragma unroll 4
+
             for (int k = 0; k < cs; ++k) {
                 size_t const e = k * stride + i;
                 api += (rho0 * a.vols[a.ns_idx[e]]) * dot2(ai, a.ns_gw[e]);
@@ -885,6 +935,8 @@ __global__ void k_pc_density(Arena a) {
         float2 const pos = a.xstar[i];
         int const cf = a.nf_cnt[i];
         float ws = P.w0;
+        #pragma unroll 4
+
         for (int k = 0; k < cf; ++k) {
             uint32_t const j = a.nf_idx[k * stride + i];
             ws += kernel_w(length2f(sub2(a.xstar[j], pos)), h);
@@ -893,6 +945,8 @@ __global__ void k_pc_density(Arena a) {
         int const cs = a.ns_cnt[i];
         if (cs) {
             float vf = 0.0f;
+            #pragma unroll 4
+
             for (int k = 0; k < cs; ++k) {
                 uint32_t const j = a.ns_idx[k * stride + i];
                 vf += a.vols[j] * kernel_w(length2f(sub2(a.xs[j], pos)), h);
@@ -927,6 +981,8 @@ __global__ void k_pc_forces(Arena a) {
         float const rho = a.rho[i];
         float const pors = a.qdens[i];
         float2 pf = mk2(0.0f, 0.0f);
+        #pragma unroll 4
+
         for (int k = 0; k < cf; ++k) {
             uint32_t const j = a.nf_idx[k * stride + i];
             float2 const vto = sub2(a.xstar[j], pos);
@@ -948,6 +1004,8 @@ __global__ void k_pc_forces(Arena a) {
     if (cs) {
         float const pors = a.pbuf0[i] / sqrf(a.rho[i]);
         float2 vg = mk2(0.0f, 0.0f);
+        #pragma unroll 4
+
         for (int k = 0; k < cs; ++k) {
             uint32_t const j = a.ns_idx[k * stride + i];
             float2 const gw = kernel_grad_w(neg2(sub2(a.xs[j], pos)), h);
@@ -982,11 +1040,12 @@ void launch_begin_substep(Arena const& a, int nscenes, cudaStream_t st) {
 void launch_zero_kappas(Arena const& a, uint32_t tiles, cudaStream_t st) {
     k_zero_kappas<<<tiles, kTile, 0, st>>>(a);
 }
-void launch_iter_reset(Arena const& a, int nscenes, cudaStream_t st) {
-    k_iter_reset<<<(nscenes + 127) / 128, 128, 0, st>>>(a, nscenes);
+void launch_iter_reset(Arena const& a, int nscenes, int kind, cudaStream_t st) {
+    k_iter_reset<<<(nscenes + 127) / 128, 128, 0, st>>>(a, nscenes, kind);
 }
-void launch_iter_check(Arena const& a, int nscenes, int kind, int* running, cudaStream_t st) {
-    k_iter_check<<<1, 256, 0, st>>>(a, nscenes, kind, running);
+void launch_iter_check(Arena const& a, int nscenes, int kind, int* running,
+                       cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st) {
+    k_iter_check<<<1, 256, 0, st>>>(a, nscenes, kind, running, cond, use_cond);
 }
 void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, cudaStream_t st) {
     k_dfsph_density_alpha<<<tiles, kTile, 0, st>>>(a);

@@ -194,7 +194,18 @@ int emerald_sim_enable_timing(emerald_sim* sim, int32_t enable);
 int emerald_sim_kernel_times(emerald_sim* sim, char* names, size_t names_len, double* ms,
                              int32_t* launches, int32_t* count);
 
-/* Number of kernels this library launched since the process started. */
+/* Execution mode: graphs != 0 (default) runs each sub-step as one CUDA graph
+ * launch with the solver loops as conditional nodes; graphs == 0 launches
+ * kernels one by one and tests the loop exit on the host after every
+ * iteration, as the reference does. */
+int emerald_sim_set_graphs(emerald_sim* sim, int32_t graphs);
+
+/* Kernels this simulation has launched (graph nodes included, loop bodies
+ * counted once per executed iteration). */
+int emerald_sim_kernel_launches(emerald_sim* sim, int64_t* count);
+
+/* Number of kernel launches this library issued from the host since the
+ * process started (a graph launch counts its kernels outside solver loops). */
 int64_t emerald_kernel_launches(void);
 
 /* Message of the last failed call on this thread. */

@@ -190,6 +190,8 @@ def test_large_scene_matches_oracle(E, oracle):
     osim = oracle.sim(oracle_params(E, scene.params), scene.solid, scene.solid_volumes,
                       scene.fluid)
     oracle.set_threads(os.cpu_count() or 1)
+    sim.begin_frame("dfsph_p")
+    osim.begin_frame("dfsph_p")
     try:
         for s in range(2):
             osim.sub_step("dfsph_p", F(s * 2e-4), F(2e-4))
@@ -202,3 +204,23 @@ def test_large_scene_matches_oracle(E, oracle):
     c2, i2, _, _ = osim.neighbors()
     assert_bitwise(counts, c2, "counts")
     assert_bitwise(idx, i2, "indices")
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_graph_and_eager_modes_agree(E, method):
+    """A sub-step as one CUDA graph (solver loops as conditional nodes) and
+    as host-driven kernel launches give the same bits and iteration counts."""
+    scene = E.BlockScene(32, dx=F(1 / 64), seed=8, time_per_step_flicks=1411200, sub_steps=4,
+                         iisph_max_pressure_iterations=50,
+                         iisph_error_average_threshold=F(0.001))
+    a = E.Simulation.from_block_scene(scene)
+    b = E.Simulation.from_block_scene(scene)
+    b.set_graphs(False)
+    for f in range(2):
+        sa = a.frame(method)
+        sb = b.frame(method)
+        assert sa["sub_steps"] == sb["sub_steps"]
+        assert sa["pressure_iterations"] == sb["pressure_iterations"]
+        assert_bitwise(a.state()[0], b.state()[0], "x")
+        assert_bitwise(a.state()[1], b.state()[1], "v")
+    assert a.kernel_launches() == b.kernel_launches()
