@@ -94,6 +94,7 @@ EXPORTS = {
                                          ctypes.POINTER(c_i32)]),
     "emerald_sim_set_graphs": (c_i32, [c_vp, c_i32]),
     "emerald_sim_kernel_launches": (c_i32, [c_vp, ctypes.POINTER(c_i64)]),
+    "emerald_neighbors_static": (c_i32, [c_vp, c_u32, c_f, c_vp, c_vp, c_vp, c_vp, c_u32, c_vp]),
     "emerald_kernel_launches": (c_i64, []),
     "emerald_last_error": (ctypes.c_char_p, []),
 }
@@ -192,6 +193,16 @@ def dam_break(params, solid_xy):
 
 def kernel_launches():
     return lib.emerald_kernel_launches()
+
+
+STATIC_MAX_POINTS = 65536
+
+
+def neighbors_static(d_xy, n, support, d_counts, d_idx, d_w, d_gw, stride, stream=None):
+    """emerald_neighbors_static on raw device pointers (integers): the
+    allocation-free neighbour build for callers that cannot allocate."""
+    _check(lib.emerald_neighbors_static(d_xy, n, support, d_counts, d_idx, d_w, d_gw, stride,
+                                        stream), "emerald_neighbors_static")
 
 
 class BlockScene:

@@ -1,0 +1,133 @@
+// emerald_neighbors_static: the neighbour build of one point set against
+// itself with every scratch buffer in a file-scope device array, for callers
+// that cannot allocate device memory themselves. Some hosts own all device
+// memory through their own allocator and do not allow a library to call
+// cudaMalloc behind their back; others run the build inside a per-frame loop
+// where cudaMalloc and cudaFree, which synchronise the device, would stall
+// the pipeline. This entry point allocates nothing: the caller passes the
+// positions and the output lists, and the cell table, particle slots, member
+// lists and scan scratch live in g_static_scratch below, sized for
+// EMERALD_STATIC_MAX_POINTS points (about 3.4 MB held by every device that
+// loads the library, until the process exits).
+#include <array>
+#include <cstdint>
+#include <mutex>
+
+#include "../../include/emerald_sph.h"
+#include "engine_types.cuh"
+#include "kernels.cuh"
+#include "sph_math.cuh"
+
+namespace emerald {
+
+namespace {
+
+constexpr uint32_t kMaxPoints = EMERALD_STATIC_MAX_POINTS;
+constexpr uint32_t kTableLog2 = 17;  // 2^17 slots >= 2 * kMaxPoints
+constexpr uint32_t kTableSize = (1u << kTableLog2) + 1;
+constexpr uint32_t kMaxTiles = kMaxPoints / kTile;
+constexpr uint32_t kScanWords = (kTableSize + 2047) / 2048 + 64;
+
+constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+// Byte offsets of the regions inside the static array.
+constexpr size_t kOffParams = 0;
+constexpr size_t kOffState = align256(kOffParams + sizeof(SceneParams));
+constexpr size_t kOffLoops = align256(kOffState + sizeof(SceneState));
+constexpr size_t kOffTiles = align256(kOffLoops + 4 * sizeof(unsigned long long));
+constexpr size_t kOffKeys = align256(kOffTiles + kMaxTiles * sizeof(int32_t));
+constexpr size_t kOffCount = align256(kOffKeys + size_t(kTableSize) * 8);
+constexpr size_t kOffStart = align256(kOffCount + size_t(kTableSize) * 4);
+constexpr size_t kOffSlot = align256(kOffStart + size_t(kTableSize) * 4);
+constexpr size_t kOffRank = align256(kOffSlot + size_t(kMaxPoints) * 4);
+constexpr size_t kOffMembers = align256(kOffRank + size_t(kMaxPoints) * 4);
+constexpr size_t kOffZkey = align256(kOffMembers + size_t(kMaxPoints) * 4);
+constexpr size_t kOffScan = align256(kOffZkey + size_t(kMaxPoints) * 8);
+constexpr size_t kScratchBytes = align256(kOffScan + size_t(kScanWords) * 4);
+
+static __device__ __align__(256) unsigned char g_static_scratch[kScratchBytes];
+
+// Writes the one-scene description the build kernels read.
+__global__ void k_static_setup(Arena a, uint32_t n, float support) {
+    uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < kMaxTiles) {
+        const_cast<int32_t*>(a.tile_scene)[t] = (t * kTile < n) ? 0 : -1;
+    }
+    if (t == 0) {
+        SceneParams p{};
+        p.fluid_begin = 0;
+        p.fluid_count = n;
+        p.ftab_begin = 0;
+        p.ftab_log2 = kTableLog2;
+        p.support = support;
+        p.cell_size = support * 2.0f;
+        *const_cast<SceneParams*>(a.sp) = p;
+        SceneState s{};
+        s.active = 1;
+        *a.ss = s;
+    }
+}
+
+// Device address of g_static_scratch per device, resolved on the first call
+// made with that device current.
+std::mutex g_mutex;
+std::array<unsigned char*, 64> g_addr{};
+
+}  // namespace
+
+}  // namespace emerald
+
+using namespace emerald;
+
+extern "C" int emerald_neighbors_static(void const* d_xy, uint32_t n, float support,
+                                        uint8_t* d_counts, uint32_t* d_idx, float* d_w,
+                                        void* d_gw, uint32_t stride, void* stream) {
+    if (n > kMaxPoints) return EMERALD_EINVAL;
+    if (!(support > 0.0f) || stride < n) return EMERALD_EINVAL;
+    if (n == 0) return EMERALD_OK;
+    if (!d_xy || !d_counts || !d_idx || !d_w || !d_gw) return EMERALD_EINVAL;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= int(g_addr.size())) {
+        cudaGetLastError();
+        return EMERALD_ECUDA;
+    }
+    unsigned char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_mutex);
+        if (!g_addr[dev]) {
+            void* ptr = nullptr;
+            if (cudaGetSymbolAddress(&ptr, g_static_scratch) != cudaSuccess || !ptr) {
+                cudaGetLastError();
+                return EMERALD_ECUDA;
+            }
+            g_addr[dev] = static_cast<unsigned char*>(ptr);
+        }
+        base = g_addr[dev];
+    }
+    cudaStream_t const st = static_cast<cudaStream_t>(stream);
+    Arena a{};
+    a.sp = reinterpret_cast<SceneParams const*>(base + kOffParams);
+    a.ss = reinterpret_cast<SceneState*>(base + kOffState);
+    a.loop_iterations = reinterpret_cast<unsigned long long*>(base + kOffLoops);
+    a.tile_scene = reinterpret_cast<int32_t const*>(base + kOffTiles);
+    a.stride = stride;
+    a.x = const_cast<float2*>(static_cast<float2 const*>(d_xy));
+    a.nf_cnt = d_counts;
+    a.nf_idx = d_idx;
+    a.nf_w = d_w;
+    a.nf_gw = static_cast<float2*>(d_gw);
+    a.fkeys = reinterpret_cast<uint64_t*>(base + kOffKeys);
+    a.fcount = reinterpret_cast<uint32_t*>(base + kOffCount);
+    a.fstart = reinterpret_cast<uint32_t*>(base + kOffStart);
+    a.slot = reinterpret_cast<uint32_t*>(base + kOffSlot);
+    a.rank = reinterpret_cast<uint32_t*>(base + kOffRank);
+    a.members = reinterpret_cast<uint32_t*>(base + kOffMembers);
+    a.zkey = reinterpret_cast<uint64_t*>(base + kOffZkey);
+    a.ftab_total = kTableSize;
+    uint32_t const tiles = (n + kTile - 1) / kTile;
+    k_static_setup<<<(kMaxTiles + 127) / 128, 128, 0, st>>>(a, n, support);
+    // The table is cleared by the build itself (keys to empty, counts to zero).
+    launch_build_cells(a, false, tiles, reinterpret_cast<uint32_t*>(base + kOffScan), st);
+    launch_neighbors(a, tiles, false, true, st);
+    return cudaGetLastError() == cudaSuccess ? EMERALD_OK : EMERALD_ECUDA;
+}

@@ -208,6 +208,28 @@ int emerald_sim_kernel_launches(emerald_sim* sim, int64_t* count);
  * process started (a graph launch counts its kernels outside solver loops). */
 int64_t emerald_kernel_launches(void);
 
+/* ---------------------------------------------------- allocation-free build */
+
+/* No counterpart in the reference (which always allocates its std::vector
+ * scratch). For callers that cannot allocate device memory: hosts that own
+ * all device memory through their own allocator and forbid a library's own
+ * cudaMalloc, and per-frame loops where cudaMalloc/cudaFree would synchronise
+ * the device. Builds the neighbour lists of n points (device float2
+ * positions) against themselves, cell size 2*support with the grid at the
+ * origin, exactly as the simulation's fluid build: counts[n] and, slot-major,
+ * idx/w/gw[k*stride + i] for the k-th neighbour of point i (gw holds float2).
+ * Allocates nothing: its scratch is a static device array sized for
+ * EMERALD_STATIC_MAX_POINTS points, held by every device that loads the
+ * library until exit. n above that limit returns EMERALD_EINVAL. The first
+ * call on each device resolves the array's device address with that device
+ * current; make that first call before any stream capture. All calls share
+ * the array, so calls whose work overlaps on the GPU race; order them on one
+ * stream. Work is enqueued on `stream` (NULL: the legacy default stream). */
+#define EMERALD_STATIC_MAX_POINTS 65536
+int emerald_neighbors_static(void const* d_xy, uint32_t n, float support, uint8_t* d_counts,
+                             uint32_t* d_idx, float* d_w, void* d_gw, uint32_t stride,
+                             void* stream);
+
 /* Message of the last failed call on this thread. */
 char const* emerald_last_error(void);
 
