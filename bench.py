@@ -93,14 +93,19 @@ def measured_peak():
 
 
 def traffic_from_profile(kernel):
-    """dram bytes per launch of `kernel` from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "ncu_summary.json")
-    try:
-        d = json.load(open(path))
-        k = d["kernels"][kernel]
-        return float(k["dram_bytes_per_launch"]) * float(d.get("scale_to_bench", 1.0))
-    except Exception:
-        return None
+    """DRAM bytes per launch of `kernel` (dram__bytes_read.sum +
+    dram__bytes_write.sum from one ncu capture of this workload), as recorded
+    in the committed summaries under profiles/ ("traffic_bytes_per_launch
+    k_<kernel> = N" lines); None when no capture covers the kernel."""
+    import glob
+    import re
+    pat = re.compile(r"^traffic_bytes_per_launch\s+k_%s\s*=\s*(\d+)" % re.escape(kernel))
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        for line in open(path):
+            m = pat.match(line.strip())
+            if m:
+                return float(m.group(1))
+    return None
 
 
 # Algorithmic bytes per launch (each element a kernel must touch, once, plus

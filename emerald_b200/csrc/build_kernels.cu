@@ -68,7 +68,16 @@ struct OtherSet {
     uint32_t const* members;
     uint32_t log2cap;
     uint32_t begin;
+    uint32_t const* oid;      // original index of a stored slot (nullptr: slot - begin)
+    uint32_t const* slot_of;  // stored slot of an original index (nullptr: begin + oid)
 };
+
+__device__ __forceinline__ uint32_t original_index(OtherSet const& o, uint32_t slot) {
+    return o.oid ? o.oid[slot] : slot - o.begin;
+}
+__device__ __forceinline__ uint32_t stored_slot(OtherSet const& o, uint32_t oid) {
+    return o.slot_of ? o.slot_of[o.begin + oid] : o.begin + oid;
+}
 
 // The neighbour search of create_neighborhoods
 // (emerald/sph_common/neighborhood.h:199-282). Accepted candidates are kept
@@ -99,7 +108,7 @@ __device__ int find_neighbors(float2 pos,
                 float const dist = length2f(vec);
                 if (dist >= max_distance) continue;
                 uint64_t const key = (static_cast<uint64_t>(__float_as_uint(dist)) << 32) |
-                                     static_cast<uint64_t>(other - o.begin);
+                                     static_cast<uint64_t>(original_index(o, other));
                 int p = cnt;
                 while (p > 0 && list[p - 1] > key) {
                     list[p] = list[p - 1];
@@ -158,11 +167,13 @@ __global__ void k_scatter(Arena a) {
     (SOLID ? a.smembers : a.members)[pos] = i;
 }
 
-// Orders every cell's members by index (the within-cell order of the
-// reference's sorted (z, index) pairs).
+// Orders every cell's members by original index (the within-cell order of
+// the reference's sorted (z, index) pairs). oid may be nullptr (storage order
+// is the original order).
 __global__ void k_sort_cells(uint32_t const* count,
                              uint32_t const* start,
                              uint32_t* members,
+                             uint32_t const* oid,
                              uint32_t total) {
     uint32_t const e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= total) return;
@@ -171,8 +182,9 @@ __global__ void k_sort_cells(uint32_t const* count,
     uint32_t* m = members + start[e];
     for (uint32_t q = 1; q < c; ++q) {
         uint32_t const v = m[q];
+        uint32_t const kv = oid ? oid[v] : v;
         uint32_t p = q;
-        while (p > 0 && m[p - 1] > v) {
+        while (p > 0 && (oid ? oid[m[p - 1]] : m[p - 1]) > kv) {
             m[p] = m[p - 1];
             --p;
         }
@@ -184,37 +196,47 @@ __global__ void k_sort_cells(uint32_t const* count,
 constexpr int kRegList = 16;
 
 // The search of find_neighbors with the sorted list in registers: every
-// accepted key bubbles through kRegList registers (min/max exchange, all
-// indices static, so nothing spills). Returns the accepted count; a count
-// above kRegList means the registers overflowed and the caller redoes the
-// particle with the 64-entry list.
-__device__ __forceinline__ int find_neighbors_reg(float2 pos,
-                                                  uint32_t self,
-                                                  bool same_set,
-                                                  float cell,
-                                                  float max_distance,
-                                                  OtherSet const& o,
-                                                  uint64_t (&r)[kRegList]) {
+// accepted key bubbles through kRegList registers (min/max exchange, static
+// indices, so nothing spills). A candidate is rejected before its square root
+// when x*x + y*y >= reject_l2: sqrtf is correctly rounded and monotone, so
+// that test equals the reference's length() >= max_distance for every
+// non-tiny vector, and tiny vectors (dot < 2*FLT_MIN) are far below it.
+// Returns the accepted count; above kRegList the registers overflowed and the
+// caller redoes the particle with the 64-entry list.
+__device__ __forceinline__ int find_neighbors_reg(float2 pos, uint32_t self, bool same_set,
+                                                  float cell, float max_distance, float reject_l2,
+                                                  OtherSet const& o, uint64_t (&r)[kRegList]) {
 #pragma unroll
     for (int q = 0; q < kRegList; ++q) r[q] = ~0ull;
     int32_t gx, gy;
     grid_coord(pos, cell, gx, gy);
+    uint64_t const sx0 = spread_bits(static_cast<uint32_t>(gx - 1));
+    uint64_t const sx1 = spread_bits(static_cast<uint32_t>(gx));
+    uint64_t const sx2 = spread_bits(static_cast<uint32_t>(gx + 1));
+    uint64_t const sy0 = spread_bits(static_cast<uint32_t>(gy - 1)) << 1;
+    uint64_t const sy1 = spread_bits(static_cast<uint32_t>(gy)) << 1;
+    uint64_t const sy2 = spread_bits(static_cast<uint32_t>(gy + 1)) << 1;
     int cnt = 0;
-    for (int32_t j = gy - 1; cnt < kMaxNeighbors && j <= gy + 1; ++j) {
-        for (int32_t k = gx - 1; cnt < kMaxNeighbors && k <= gx + 1; ++k) {
+#pragma unroll 1
+    for (int jj = 0; jj < 3 && cnt < kMaxNeighbors; ++jj) {
+        uint64_t const zy = jj == 0 ? sy0 : (jj == 1 ? sy1 : sy2);
+#pragma unroll 1
+        for (int kk = 0; kk < 3 && cnt < kMaxNeighbors; ++kk) {
+            uint64_t const zx = kk == 0 ? sx0 : (kk == 1 ? sx1 : sx2);
             uint32_t slot;
-            uint64_t const z = morton2(static_cast<uint32_t>(k), static_cast<uint32_t>(j));
-            if (!table_find(o.keys, o.log2cap, z, slot)) continue;
+            if (!table_find(o.keys, o.log2cap, zx | zy, slot)) continue;
             uint32_t const b = o.start[slot];
             uint32_t const e = b + o.count[slot];
+#pragma unroll 1
             for (uint32_t m = b; cnt < kMaxNeighbors && m != e; ++m) {
                 uint32_t const other = o.members[m];
                 if (same_set && other == self) continue;
                 float2 const vec = sub2(o.x[other], pos);
+                if (vec.x * vec.x + vec.y * vec.y >= reject_l2) continue;
                 float const dist = length2f(vec);
                 if (dist >= max_distance) continue;
                 uint64_t key = (static_cast<uint64_t>(__float_as_uint(dist)) << 32) |
-                               static_cast<uint64_t>(other - o.begin);
+                               static_cast<uint64_t>(original_index(o, other));
 #pragma unroll
                 for (int q = 0; q < kRegList; ++q) {
                     uint64_t const lo = r[q] < key ? r[q] : key;
@@ -228,15 +250,25 @@ __device__ __forceinline__ int find_neighbors_reg(float2 pos,
     return cnt;
 }
 
-// GradW (emerald/sph_common/kernels.h:57-64) of dp with |dp| = r already known
-// (the length of -v equals the length of v bit for bit).
-__device__ __forceinline__ float2 kernel_grad_w_r(float2 dp, float r, float h) {
-    if (safe_v(dp, r)) {
-        float const d = kernel_dw(r, h);
-        float2 const u = div2(dp, r);
-        return mk2(u.x * d, u.y * d);
+// Writes list entry k of particle i: index, W and GradW(-vector_to)
+// (compute_neighbor_kernels / compute_neighbor_kernel_gradients,
+// emerald/sph_common/neighborhood.cpp:178-210), the vector recomputed from
+// positions bit for bit and its length taken from the search.
+__device__ __forceinline__ void write_entry(uint32_t* idx_out, float* w_out, float2* gw_out,
+                                            size_t e, uint32_t j, float dist, float2 pos,
+                                            float2 const* xo, float h, bool kernels) {
+    idx_out[e] = j;
+    if (!kernels) return;
+    float w, dw;
+    kernel_w_dw(dist, h, w, dw);
+    w_out[e] = w;
+    float2 const dp = neg2(sub2(xo[j], pos));
+    float2 g = mk2(0.0f, 0.0f);
+    if (safe_v(dp, dist)) {
+        float2 const u = div2(dp, dist);
+        g = mk2(u.x * dw, u.y * dw);
     }
-    return mk2(0.0f, 0.0f);
+    gw_out[e] = g;
 }
 
 template <bool SOLID_OTHER>
@@ -252,52 +284,47 @@ __global__ void __launch_bounds__(kTile) k_neighbors(Arena a, int write_kernels)
     OtherSet o;
     if (SOLID_OTHER) {
         o = OtherSet{a.xs, a.skeys + P.stab_begin, a.scount + P.stab_begin, a.sstart + P.stab_begin,
-                     a.smembers, P.stab_log2, P.solid_begin};
+                     a.smembers, P.stab_log2, P.solid_begin, nullptr, nullptr};
     } else {
         o = OtherSet{a.x, a.fkeys + P.ftab_begin, a.fcount + P.ftab_begin, a.fstart + P.ftab_begin,
-                     a.members, P.ftab_log2, P.fluid_begin};
+                     a.members, P.ftab_log2, P.fluid_begin, a.oid, a.slot_of};
     }
     uint8_t* cnt_out = SOLID_OTHER ? a.ns_cnt : a.nf_cnt;
     uint32_t* idx_out = SOLID_OTHER ? a.ns_idx : a.nf_idx;
     float* w_out = SOLID_OTHER ? a.ns_w : a.nf_w;
     float2* gw_out = SOLID_OTHER ? a.ns_gw : a.nf_gw;
     size_t const stride = a.stride;
-    float2 const pos = a.x[i];
     if (SOLID_OTHER && P.solid_count == 0) {
         cnt_out[i] = 0;
         return;
     }
+    bool const kernels = write_kernels != 0;
+    float2 const pos = a.x[i];
     uint64_t r[kRegList];
-    int const cnt = find_neighbors_reg(pos, i, !SOLID_OTHER, cell, cell, o, r);
+    int const cnt = find_neighbors_reg(pos, i, !SOLID_OTHER, cell, cell, P.reject_l2, o, r);
     cnt_out[i] = static_cast<uint8_t>(cnt);
     if (cnt <= kRegList) {
+        // drain the sorted registers from the front: one copy of the entry
+        // code, register moves instead of dynamic indexing
+#pragma unroll 1
+        for (int k = 0; k < cnt; ++k) {
+            uint64_t const key = r[0];
 #pragma unroll
-        for (int k = 0; k < kRegList; ++k) {
-            if (k < cnt) {
-                uint32_t const j = o.begin + static_cast<uint32_t>(r[k] & 0xffffffffu);
-                size_t const e = static_cast<size_t>(k) * stride + i;
-                idx_out[e] = j;
-                if (write_kernels) {
-                    float const dist = __uint_as_float(static_cast<uint32_t>(r[k] >> 32));
-                    w_out[e] = kernel_w(dist, h);
-                    gw_out[e] = kernel_grad_w_r(neg2(sub2(o.x[j], pos)), dist, h);
-                }
-            }
+            for (int q = 0; q + 1 < kRegList; ++q) r[q] = r[q + 1];
+            write_entry(idx_out, w_out, gw_out, static_cast<size_t>(k) * stride + i,
+                        stored_slot(o, static_cast<uint32_t>(key & 0xffffffffu)),
+                        __uint_as_float(static_cast<uint32_t>(key >> 32)), pos, o.x, h, kernels);
         }
         return;
     }
     // more than kRegList neighbours: the full 64-entry list
-    uint64_t list[kMaxNeighbors];
-    int const n64 = find_neighbors(pos, i, !SOLID_OTHER, cell, cell, o, list);
+    uint64_t full[kMaxNeighbors];
+    int const n64 = find_neighbors(pos, i, !SOLID_OTHER, cell, cell, o, full);
+#pragma unroll 1
     for (int k = 0; k < n64; ++k) {
-        uint32_t const j = o.begin + static_cast<uint32_t>(list[k] & 0xffffffffu);
-        size_t const e = static_cast<size_t>(k) * stride + i;
-        idx_out[e] = j;
-        if (write_kernels) {
-            float const dist = __uint_as_float(static_cast<uint32_t>(list[k] >> 32));
-            w_out[e] = kernel_w(dist, h);
-            gw_out[e] = kernel_grad_w_r(neg2(sub2(o.x[j], pos)), dist, h);
-        }
+        write_entry(idx_out, w_out, gw_out, static_cast<size_t>(k) * stride + i,
+                    stored_slot(o, static_cast<uint32_t>(full[k] & 0xffffffffu)),
+                    __uint_as_float(static_cast<uint32_t>(full[k] >> 32)), pos, o.x, h, kernels);
     }
 }
 
@@ -311,7 +338,7 @@ __global__ void k_solid_volumes(Arena a, float numer, int only_scene) {
     uint32_t const i = blockIdx.x * kTile + threadIdx.x;
     if (i - P.solid_begin >= P.solid_count) return;
     OtherSet const o{a.xs, a.skeys + P.stab_begin, a.scount + P.stab_begin, a.sstart + P.stab_begin,
-                     a.smembers, P.stab_log2, P.solid_begin};
+                     a.smembers, P.stab_log2, P.solid_begin, nullptr, nullptr};
     uint64_t list[kMaxNeighbors];
     int const cnt = find_neighbors(a.xs[i], i, true, P.cell_size, P.cell_size, o, list);
     float const w0 = kernel_w(0.0f, P.support);
@@ -427,7 +454,7 @@ void launch_build_cells(Arena const& a, bool solid, uint32_t tiles, uint32_t* sc
         launch_exclusive_scan(a.scount, a.stab_total, a.sstart, scan_scratch, st);
         k_scatter<true><<<tiles, kTile, 0, st>>>(a);
         k_sort_cells<<<(a.stab_total + 255) / 256, 256, 0, st>>>(a.scount, a.sstart, a.smembers,
-                                                                 a.stab_total);
+                                                                 nullptr, a.stab_total);
     } else {
         cudaMemsetAsync(a.fkeys, 0xff, sizeof(uint64_t) * a.ftab_total, st);
         cudaMemsetAsync(a.fcount, 0, sizeof(uint32_t) * a.ftab_total, st);
@@ -435,7 +462,7 @@ void launch_build_cells(Arena const& a, bool solid, uint32_t tiles, uint32_t* sc
         launch_exclusive_scan(a.fcount, a.ftab_total, a.fstart, scan_scratch, st);
         k_scatter<false><<<tiles, kTile, 0, st>>>(a);
         k_sort_cells<<<(a.ftab_total + 255) / 256, 256, 0, st>>>(a.fcount, a.fstart, a.members,
-                                                                 a.ftab_total);
+                                                                 a.oid, a.ftab_total);
     }
 }
 

@@ -136,6 +136,15 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
     a_.xstar = static_cast<float2*>(dev(8 * N));
     a_.vstar = static_cast<float2*>(dev(8 * N));
     a_.fp = static_cast<float2*>(dev(8 * N));
+    a_.oid = static_cast<uint32_t*>(dev(4 * N));
+    a_.slot_of = static_cast<uint32_t*>(dev(4 * N));
+    a_.tx = static_cast<float2*>(dev(8 * N));
+    a_.tv = static_cast<float2*>(dev(8 * N));
+    a_.tkdiv = static_cast<float*>(dev(4 * N));
+    a_.tkdens = static_cast<float*>(dev(4 * N));
+    a_.toid = static_cast<uint32_t*>(dev(4 * N));
+    order_buf_ = dev(sort_scratch_bytes(uint32_t(N)));
+    sort_scratch_carve(order_buf_, uint32_t(N), order_sort_);
     a_.nf_cnt = static_cast<uint8_t*>(dev(N));
     a_.nf_idx = static_cast<uint32_t*>(dev(4 * E));
     a_.nf_w = static_cast<float*>(dev(4 * E));
@@ -264,6 +273,32 @@ KernelTimes const& Engine::kernel_times() {
     return times_;
 }
 
+// Leading key of the storage-order sort: the scene's first tile above a
+// 24-bit cell key (see reorder_kernels.cu), rounded up to whole 8-bit passes.
+int Engine::order_key_bits() const {
+    int bits = 24;
+    if (max_scenes_ > 1) bits += int(ceil_log2(uint64_t(fluid_cap_ / kTile) + 1));
+    return (bits + 7) / 8 * 8;
+}
+
+// sort_base of each scene: the real particles of all scenes stored before it.
+void Engine::update_sort_bases() {
+    std::vector<std::pair<uint32_t, int>> order;
+    for (int id = 0; id < max_scenes_; ++id) {
+        if (scenes_[id].used) order.push_back({scenes_[id].p.fluid_begin, id});
+    }
+    std::sort(order.begin(), order.end());
+    uint32_t base = 0;
+    for (auto const& kv : order) {
+        Scene& sc = scenes_[kv.second];
+        if (sc.p.sort_base != base) {
+            sc.p.sort_base = base;
+            upload_params(kv.second);
+        }
+        base += sc.p.fluid_count;
+    }
+}
+
 void Engine::upload_tiles() {
     cudaMemcpyAsync(d_tile_scene_, tile_scene_.data(), sizeof(int32_t) * tile_scene_.size(),
                     cudaMemcpyHostToDevice, st_);
@@ -352,6 +387,8 @@ int Engine::add_scene(SceneSpec const& spec) {
     P.cfl_factor = spec.method == kIisph ? 0.2f : 0.4f;
     P.seconds_per_sub_step = cfg.seconds_per_sub_step;
     P.fixed_dt = spec.fixed_dt;
+    P.sort_base = 0;
+    P.reject_l2 = reject_threshold(P.cell_size);
     scenes_[id] = sc;
 
     for (uint32_t t = 0; t < sc.ftile_count; ++t) tile_scene_[ft + t] = id;
@@ -372,6 +409,7 @@ int Engine::add_scene(SceneSpec const& spec) {
         cudaMemsetAsync(a_.kdiv + P.fluid_begin, 0, 4ull * spec.n_fluid, st_);
         cudaMemsetAsync(a_.kdens + P.fluid_begin, 0, 4ull * spec.n_fluid, st_);
         cudaMemsetAsync(a_.nf_cnt + P.fluid_begin, 0, spec.n_fluid, st_);
+        launch_identity_order(a_, P.fluid_begin, spec.n_fluid, st_);
         cudaMemsetAsync(a_.ns_cnt + P.fluid_begin, 0, spec.n_fluid, st_);
     }
     if (spec.n_solid) {
@@ -379,6 +417,7 @@ int Engine::add_scene(SceneSpec const& spec) {
                         cudaMemcpyHostToDevice, st_);
         cudaMemsetAsync(a_.vs + P.solid_begin, 0, 8ull * spec.n_solid, st_);
     }
+    update_sort_bases();
     rebuild_solids();
     if (spec.n_solid) {
         if (spec.solid_volumes) {
@@ -412,6 +451,7 @@ void Engine::remove_scene(int id) {
     ftab_.release(sc.p.ftab_begin, sc.ftab_size);
     stab_.release(sc.p.stab_begin, sc.stab_size);
     sc = Scene{};
+    update_sort_bases();
     rebuild_solids();
 }
 
@@ -563,9 +603,15 @@ void Engine::run_loop(int kind, int max_iter, int32_t method) {
     }
 }
 
-void Engine::emit_substep(int32_t method) {
+void Engine::emit_substep(int32_t method, bool reorder) {
     uint32_t const tiles = fluid_cap_ / kTile;
     cudaStream_t const st = cur_;
+    if (reorder) {
+        // keys, three to five radix passes of three kernels, permute, commit
+        int const bits = order_key_bits();
+        launch("reorder", [&] { launch_reorder(a_, order_sort_, fluid_cap_, bits, st); },
+               3 + 3 * (bits / 8));
+    }
     launch("max_v2", [&] { launch_max_v2(a_, tiles, st); });
     launch("begin_substep", [&] { launch_begin_substep(a_, max_scenes_, st); });
     // binning, three scan passes, scatter, per-cell ordering
@@ -611,7 +657,7 @@ void Engine::emit_substep(int32_t method) {
 // arena pointers and the tile count, which never change for an engine, and
 // every kernel reads scene membership and parameters from device memory, so
 // the graph stays valid as scenes are added, removed or (de)activated.
-void Engine::capture_substep(int32_t method) {
+void Engine::capture_substep(int32_t method, bool reorder) {
     cudaStreamSynchronize(st_);
     if (cudaStreamBeginCapture(cap_st_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         throw std::runtime_error("graph capture: begin");
@@ -620,7 +666,7 @@ void Engine::capture_substep(int32_t method) {
     capture_kernels_ = 0;
     cur_ = cap_st_;
     try {
-        emit_substep(method);
+        emit_substep(method, reorder);
     } catch (...) {
         cudaGraph_t g = nullptr;
         cudaStreamEndCapture(cap_st_, &g);
@@ -641,8 +687,8 @@ void Engine::capture_substep(int32_t method) {
     if (e != cudaSuccess) {
         throw std::runtime_error(std::string("graph instantiate: ") + cudaGetErrorString(e));
     }
-    graphs_[method] = exec;
-    graph_fixed_kernels_[method] = capture_kernels_;
+    graphs_[method * 2 + (reorder ? 1 : 0)] = exec;
+    graph_fixed_kernels_[method * 2 + (reorder ? 1 : 0)] = capture_kernels_;
 }
 
 void Engine::substep(int32_t method) {
@@ -657,24 +703,27 @@ void Engine::substep(int32_t method) {
             upload_params(id);
         }
     }
+    bool const reorder = reorder_every_ > 0 && (substeps_launched_ % reorder_every_) == 0;
+    ++substeps_launched_;
     if (use_graphs_ && !timing_) {
-        auto it = graphs_.find(method);
+        int const key = method * 2 + (reorder ? 1 : 0);
+        auto it = graphs_.find(key);
         if (it == graphs_.end()) {
-            capture_substep(method);
-            it = graphs_.find(method);
+            capture_substep(method, reorder);
+            it = graphs_.find(key);
         }
         if (cudaGraphLaunch(it->second, st_) != cudaSuccess) {
             check("graph launch");
             throw std::runtime_error("graph launch failed");
         }
-        int64_t const fixed = graph_fixed_kernels_[method];
+        int64_t const fixed = graph_fixed_kernels_[key];
         host_launches_ += fixed;
         g_launches.fetch_add(fixed, std::memory_order_relaxed);
         check("substep graph");
         return;
     }
     cur_ = st_;
-    emit_substep(method);
+    emit_substep(method, reorder);
     check("substep");
 }
 
@@ -696,18 +745,34 @@ std::vector<SceneState> Engine::all_states() {
     return s;
 }
 
+// Positions and velocities in original particle order: gathered through
+// slot_of into the reorder staging buffers, then copied out.
 void Engine::get_state(int id, float* x, float* v) {
     SceneParams const& P = scenes_[id].p;
-    if (x) cudaMemcpyAsync(x, a_.x + P.fluid_begin, 8ull * P.fluid_count, cudaMemcpyDeviceToHost, st_);
-    if (v) cudaMemcpyAsync(v, a_.v + P.fluid_begin, 8ull * P.fluid_count, cudaMemcpyDeviceToHost, st_);
+    uint32_t const b = P.fluid_begin, n = P.fluid_count;
+    if (x) {
+        launch_gather_f2(a_, b, n, a_.x, a_.tx + b, st_);
+        cudaMemcpyAsync(x, a_.tx + b, 8ull * n, cudaMemcpyDeviceToHost, st_);
+    }
+    if (v) {
+        launch_gather_f2(a_, b, n, a_.v, a_.tv + b, st_);
+        cudaMemcpyAsync(v, a_.tv + b, 8ull * n, cudaMemcpyDeviceToHost, st_);
+    }
     cudaStreamSynchronize(st_);
     check("get_state");
 }
 
 void Engine::set_state(int id, float const* x, float const* v) {
     SceneParams const& P = scenes_[id].p;
-    if (x) cudaMemcpyAsync(a_.x + P.fluid_begin, x, 8ull * P.fluid_count, cudaMemcpyHostToDevice, st_);
-    if (v) cudaMemcpyAsync(a_.v + P.fluid_begin, v, 8ull * P.fluid_count, cudaMemcpyHostToDevice, st_);
+    uint32_t const b = P.fluid_begin, n = P.fluid_count;
+    if (x) {
+        cudaMemcpyAsync(a_.tx + b, x, 8ull * n, cudaMemcpyHostToDevice, st_);
+        launch_scatter_f2(a_, b, n, a_.tx + b, a_.x, st_);
+    }
+    if (v) {
+        cudaMemcpyAsync(a_.tv + b, v, 8ull * n, cudaMemcpyHostToDevice, st_);
+        launch_scatter_f2(a_, b, n, a_.tv + b, a_.v, st_);
+    }
     cudaStreamSynchronize(st_);
     check("set_state");
 }
@@ -773,9 +838,14 @@ bool Engine::get_array(int id, std::string const& name, float* out, int& width) 
         return false;
     }
     if (out) {
-        size_t const bytes = 4ull * width;
-        cudaMemcpyAsync(out, static_cast<char const*>(src) + bytes * P.fluid_begin,
-                        bytes * P.fluid_count, cudaMemcpyDeviceToHost, st_);
+        uint32_t const b = P.fluid_begin, n = P.fluid_count;
+        if (width == 2) {
+            launch_gather_f2(a_, b, n, static_cast<float2 const*>(src), a_.tx + b, st_);
+            cudaMemcpyAsync(out, a_.tx + b, 8ull * n, cudaMemcpyDeviceToHost, st_);
+        } else {
+            launch_gather_f(a_, b, n, static_cast<float const*>(src), a_.tkdiv + b, st_);
+            cudaMemcpyAsync(out, a_.tkdiv + b, 4ull * n, cudaMemcpyDeviceToHost, st_);
+        }
         cudaStreamSynchronize(st_);
         check("get_array");
     }
@@ -808,16 +878,21 @@ void Engine::get_neighbors(int id, bool solid, uint8_t* counts, uint32_t* idx, f
                             cudaMemcpyDeviceToHost, st_);
         }
     }
+    std::vector<uint32_t> oid(n), slot_of(n);
+    cudaMemcpyAsync(oid.data(), a_.oid + P.fluid_begin, 4ull * n, cudaMemcpyDeviceToHost, st_);
+    cudaMemcpyAsync(slot_of.data(), a_.slot_of + P.fluid_begin, 4ull * n, cudaMemcpyDeviceToHost, st_);
     cudaStreamSynchronize(st_);
     check("get_neighbors");
     uint32_t const base = solid ? P.solid_begin : P.fluid_begin;
     for (uint32_t i = 0; i < n; ++i) {
-        if (counts) counts[i] = cnt[i];
+        uint32_t const row = slot_of[i] - P.fluid_begin;  // storage column of particle i
+        if (counts) counts[i] = cnt[row];
         for (int k = 0; k < kMaxNeighbors; ++k) {
             size_t const o = size_t(i) * kMaxNeighbors + k;
-            size_t const r = size_t(k) * n + i;
-            bool const live = k < cnt[i];
-            if (idx) idx[o] = live ? ri[r] - base : 0u;
+            size_t const r = size_t(k) * n + row;
+            bool const live = k < cnt[row];
+            uint32_t const j = live ? ri[r] - base : 0u;
+            if (idx) idx[o] = live ? (solid ? j : oid[j]) : 0u;
             if (w) w[o] = live ? rw[r] : 0.0f;
             if (gw) {
                 gw[2 * o] = live ? rg[r].x : 0.0f;

@@ -109,6 +109,8 @@ public:
     // Graph mode (default): each sub-step is one CUDA graph launch, with the
     // solver loops as conditional while nodes (no host round trips).
     void set_graphs(bool on) { use_graphs_ = on; }
+    // Sub-steps between re-sorts of the particle storage order (0: never).
+    void set_reorder_every(int k) { reorder_every_ = k; }
     // Kernels this engine launched (graph nodes included, loop bodies
     // counted per executed iteration).
     int64_t kernel_launches();
@@ -129,9 +131,11 @@ private:
     void upload_params(int id);
     void upload_tiles();
     void run_loop(int kind, int max_iter, int32_t method);
-    void emit_substep(int32_t method);
+    void emit_substep(int32_t method, bool reorder);
     void emit_loop_body(int kind, int32_t method, cudaGraphConditionalHandle cond, bool use_cond);
-    void capture_substep(int32_t method);
+    void capture_substep(int32_t method, bool reorder);
+    void update_sort_bases();
+    int order_key_bits() const;
     void destroy_graphs();
     int max_iterations(int kind) const;
     void rebuild_solids();
@@ -159,8 +163,12 @@ private:
     cudaStream_t cur_ = nullptr;  // stream the emitted work goes to
     cudaStream_t cap_st_ = nullptr;
     cudaStream_t body_st_ = nullptr;
-    std::map<int32_t, cudaGraphExec_t> graphs_;
+    std::map<int32_t, cudaGraphExec_t> graphs_;        // key: method * 2 + reorder
     std::map<int32_t, int64_t> graph_fixed_kernels_;
+    int reorder_every_ = 16;
+    int64_t substeps_launched_ = 0;
+    void* order_buf_ = nullptr;
+    SortScratch order_sort_{};
     int64_t host_launches_ = 0;
     int64_t capture_kernels_ = 0;
     bool count_host_ = true;

@@ -52,6 +52,8 @@ struct SceneParams {
     float cfl_factor;
     float seconds_per_sub_step;
     float fixed_dt;
+    uint32_t sort_base;  // real particles of scenes stored before this one
+    float reject_l2;     // smallest float whose sqrtf is >= cell_size
 };
 
 // Mutable per-scene state, device resident.
@@ -106,6 +108,17 @@ struct Arena {
     float2* xstar;
     float2* vstar;
     float2* fp;     // PCISPH pressure forces
+
+    // storage order: oid[slot] = original (scene-local) index of the particle
+    // stored at `slot`; slot_of[fluid_begin + oid] = its slot. nullptr means
+    // storage order is the original order.
+    uint32_t* oid;
+    uint32_t* slot_of;
+    float2* tx;  // reorder staging
+    float2* tv;
+    float* tkdiv;
+    float* tkdens;
+    uint32_t* toid;
 
     // neighbour lists, slot-major
     uint8_t* nf_cnt;

@@ -44,6 +44,16 @@ void launch_sort_products(Arena const& a, bool solid, int scene, uint32_t begin,
                           uint32_t* block_indices, uint32_t* blocks, uint32_t* nblocks,
                           cudaStream_t st);
 
+// storage order (reorder_kernels.cu)
+void launch_reorder(Arena const& a, SortScratch& s, uint32_t n, int key_bits, cudaStream_t st);
+void launch_gather_f(Arena const& a, uint32_t begin, uint32_t count, float const* src, float* out,
+                     cudaStream_t st);
+void launch_gather_f2(Arena const& a, uint32_t begin, uint32_t count, float2 const* src, float2* out,
+                      cudaStream_t st);
+void launch_scatter_f2(Arena const& a, uint32_t begin, uint32_t count, float2 const* in, float2* dst,
+                       cudaStream_t st);
+void launch_identity_order(Arena const& a, uint32_t begin, uint32_t count, cudaStream_t st);
+
 // solver (solve_kernels.cu)
 void launch_max_v2(Arena const& a, uint32_t tiles, cudaStream_t st);
 void launch_begin_substep(Arena const& a, int nscenes, cudaStream_t st);

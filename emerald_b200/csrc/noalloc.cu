@@ -48,7 +48,7 @@ constexpr size_t kScratchBytes = align256(kOffScan + size_t(kScanWords) * 4);
 static __device__ __align__(256) unsigned char g_static_scratch[kScratchBytes];
 
 // Writes the one-scene description the build kernels read.
-__global__ void k_static_setup(Arena a, uint32_t n, float support) {
+__global__ void k_static_setup(Arena a, uint32_t n, float support, float reject_l2) {
     uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < kMaxTiles) {
         const_cast<int32_t*>(a.tile_scene)[t] = (t * kTile < n) ? 0 : -1;
@@ -61,6 +61,7 @@ __global__ void k_static_setup(Arena a, uint32_t n, float support) {
         p.ftab_log2 = kTableLog2;
         p.support = support;
         p.cell_size = support * 2.0f;
+        p.reject_l2 = reject_l2;
         *const_cast<SceneParams*>(a.sp) = p;
         SceneState s{};
         s.active = 1;
@@ -125,7 +126,8 @@ extern "C" int emerald_neighbors_static(void const* d_xy, uint32_t n, float supp
     a.zkey = reinterpret_cast<uint64_t*>(base + kOffZkey);
     a.ftab_total = kTableSize;
     uint32_t const tiles = (n + kTile - 1) / kTile;
-    k_static_setup<<<(kMaxTiles + 127) / 128, 128, 0, st>>>(a, n, support);
+    k_static_setup<<<(kMaxTiles + 127) / 128, 128, 0, st>>>(a, n, support,
+                                                             reject_threshold(support * 2.0f));
     // The table is cleared by the build itself (keys to empty, counts to zero).
     launch_build_cells(a, false, tiles, reinterpret_cast<uint32_t*>(base + kOffScan), st);
     launch_neighbors(a, tiles, false, true, st);

@@ -105,9 +105,9 @@ __global__ void k_cell_counts(uint32_t const* sorted_slots, uint32_t const* coun
 __global__ void k_expand_pairs(uint64_t const* sorted_z, uint32_t const* sorted_slots,
                                uint32_t const* cell_start, uint32_t const* count,
                                uint32_t const* start, uint32_t const* members,
-                               uint32_t const* ncells, uint32_t limit, uint32_t first,
-                               uint64_t* pair_z, uint32_t* pair_index, uint32_t* block_indices,
-                               uint32_t* blocks) {
+                               uint32_t const* oid, uint32_t const* ncells, uint32_t limit,
+                               uint32_t first, uint64_t* pair_z, uint32_t* pair_index,
+                               uint32_t* block_indices, uint32_t* blocks) {
     uint32_t const c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= limit || c >= *ncells) return;
     uint32_t const slot = sorted_slots[c];
@@ -116,7 +116,7 @@ __global__ void k_expand_pairs(uint64_t const* sorted_z, uint32_t const* sorted_
     uint32_t const* m = members + start[slot];
     for (uint32_t k = 0; k < n; ++k) {
         pair_z[b + k] = sorted_z[c];
-        pair_index[b + k] = m[k] - first;
+        pair_index[b + k] = oid ? oid[m[k]] : m[k] - first;
         block_indices[b + k] = c;
     }
     blocks[2 * c] = b;
@@ -133,12 +133,13 @@ __device__ __forceinline__ uint32_t compact_bits(uint64_t x) {
     return static_cast<uint32_t>(x);
 }
 
-// Grid coords and z keys of the last build, recovered from the stored keys.
-__global__ void k_keys_of(uint64_t const* zkey, uint32_t begin, uint32_t count, int2* gc,
-                          uint64_t* z) {
+// Grid coords and z keys of the last build per original index, recovered
+// from the stored keys.
+__global__ void k_keys_of(uint64_t const* zkey, uint32_t const* slot_of, uint32_t begin,
+                          uint32_t count, int2* gc, uint64_t* z) {
     uint32_t const k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= count) return;
-    uint64_t const key = zkey[begin + k];
+    uint64_t const key = zkey[slot_of ? slot_of[begin + k] : begin + k];
     gc[k] = make_int2(static_cast<int32_t>(compact_bits(key)),
                       static_cast<int32_t>(compact_bits(key >> 1)));
     z[k] = key;
@@ -212,7 +213,8 @@ void launch_sort_products(Arena const& a, bool solid, int scene, uint32_t begin,
     uint32_t const* members = solid ? a.smembers : a.members;
     (void)cell;
     if (count) {
-        k_keys_of<<<(count + 255) / 256, 256, 0, st>>>(solid ? a.szkey : a.zkey, begin, count,
+        k_keys_of<<<(count + 255) / 256, 256, 0, st>>>(solid ? a.szkey : a.zkey,
+                                                      solid ? nullptr : a.slot_of, begin, count,
                                                       grid_coords, z);
     }
     uint32_t const total = tab_size;
@@ -232,8 +234,9 @@ void launch_sort_products(Arena const& a, bool solid, int scene, uint32_t begin,
     k_cell_counts<<<(limit + 255) / 256, 256, 0, st>>>(s.vals[cur], cnt, nblocks, limit, cell_count);
     launch_exclusive_scan(cell_count, limit, cell_start, s.scan, st);
     k_expand_pairs<<<(limit + 255) / 256, 256, 0, st>>>(s.keys[cur], s.vals[cur], cell_start, cnt,
-                                                       start, members, nblocks, limit, begin,
-                                                       pair_z, pair_index, block_indices, blocks);
+                                                       start, members, solid ? nullptr : a.oid,
+                                                       nblocks, limit, begin, pair_z, pair_index,
+                                                       block_indices, blocks);
 }
 
 }  // namespace emerald

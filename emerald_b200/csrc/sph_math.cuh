@@ -7,7 +7,10 @@
 // reference's CPU results for the same inputs.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
+#include <limits>
+
 #include <cuda_runtime.h>
 
 namespace emerald {
@@ -91,6 +94,24 @@ EMLD_HD float kernel_dw(float r, float h) {
     return 0.0f;
 }
 
+// W and dW of the same r, sharing q = r / h (the same value either function
+// computes on its own).
+EMLD_HD void kernel_w_dw(float r, float h, float& w, float& dw) {
+    float const q = r / h;
+    float const k = h * h * h * kPi;
+    if (q <= 1.0f) {
+        w = (1.0f + q * q * (q * 0.75f - 1.5f)) / k;
+        dw = (-3.0f * r / (h * h) + 2.25f * r * r / (h * h * h)) / k;
+    } else if (q <= 2.0f) {
+        float const t = 2.0f - q;
+        w = ((t * t * t) / 4.0f) / k;
+        dw = (-3.0f * sqrf(2.0f - q) / (4.0f * h)) / k;
+    } else {
+        w = 0.0f;
+        dw = 0.0f;
+    }
+}
+
 EMLD_HD float2 kernel_grad_w(float2 dp, float h) {
     float const r = length2f(dp);
     if (safe_v(dp, r)) {
@@ -126,6 +147,18 @@ EMLD_HD void grid_coord(float2 p, float cell, int32_t& gx, int32_t& gy) {
     float2 const q = div2(sub2(p, mk2(0.0f, 0.0f)), cell);
     gx = static_cast<int32_t>(floorf(q.x));
     gy = static_cast<int32_t>(floorf(q.y));
+}
+
+// Smallest float t with sqrtf(t) >= d (host side): x*x + y*y >= t holds
+// exactly when the correctly rounded length of (x, y) is >= d.
+inline float reject_threshold(float d) {
+    float const inf = std::numeric_limits<float>::infinity();
+    if (!(d > 0.0f)) return 0.0f;
+    if (!(d < 1.8e19f)) return inf;
+    float t = d * d;
+    while (t > 0.0f && std::sqrt(std::nextafter(t, 0.0f)) >= d) t = std::nextafter(t, 0.0f);
+    while (std::sqrt(t) < d) t = std::nextafter(t, inf);
+    return t;
 }
 
 }  // namespace emerald
