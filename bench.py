@@ -28,12 +28,18 @@ METRIC = "2D SPH particle-steps/s at 0.1% density error; batched scenes/s, p50/p
 N_SIDE = 512
 DX = np.float32(1.0 / 1024)
 TPS_FLICKS = 1411200  # 2e-3 s: DFSPH sub-steps between tps/60 and tps/4 = 5e-4 s
+DFSPH_CAP = 100
 WORKLOAD = ("DFSPH_P dam break, 512x512=262144 fluid particles, dx=1/1024, support=dx, "
-            "3 boundary rows, CFL dt<=5e-4 s, div tol 0.1%/s, density tol 0.05%")
+            "3 boundary rows, CFL dt<=5e-4 s, div tol 0.1%/s, density tol 0.05%, "
+            "100 correction iterations at most")
 
 
 def scene_kwargs():
+    # 100 correction iterations: with the reference's default cap of 15 the
+    # density solve stops above 0.1% average error on most sub-steps of this
+    # scene, and the metric is quoted at 0.1%.
     return dict(dx=DX, seed=1, time_per_step_flicks=TPS_FLICKS, sub_steps=4,
+                dfsph_max_correction_iterations=DFSPH_CAP,
                 dfsph_divergence_error_average_threshold=np.float32(0.001),
                 dfsph_density_error_average_threshold=np.float32(0.0005))
 
@@ -208,9 +214,10 @@ def run_gpu(args):
     # per-kernel device times (events around every launch) for the roofline
     sim.enable_timing(True)
     rsteps = max(3, min(args.steps, 50))
+    errs = []
     for _ in range(rsteps):
         flush.zero_()
-        sim.advance("dfsph_p", 1, stats=False)
+        errs.append(sim.advance("dfsph_p", 1)["error_average"])
     times = sim.kernel_times()
     sim.enable_timing(False)
     counts_f, _, _, _ = sim.neighbors(False)
@@ -250,7 +257,10 @@ def run_gpu(args):
                        "p99_step_ms": round(float(np.percentile(step_ms, 99)), 4),
                        "last_step": {k: last[k] for k in ("dt", "pressure_iterations",
                                                           "divergence_iterations",
-                                                          "error_average", "error_max")}},
+                                                          "error_average", "error_max")},
+                       "density_error_after_timing": {
+                           "steps": len(errs), "max_avg_error": max(errs),
+                           "steps_above_0.1%": int(sum(e > 0.001 for e in errs))}},
             "roofline": roofline,
             "kernels": kernel_table,
             "e2e": {"value": round(e2e_value, 1), "unit": "particle-steps/s",
@@ -261,11 +271,164 @@ def run_gpu(args):
         }
         if world == 1 and not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline(args, sample_seconds=args.cpu_seconds)
+    sim.close()
+    if args.batched_scenes > 0:
+        batched = run_batched(args, torch, E, rank, world, barrier)
+        if rank == 0:
+            result["batched"] = batched
+    if args.serving_requests > 0 and world == 1:
+        result["serving"] = run_serving(args, torch, E)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
     return result
+
+
+def run_batched(args, torch, E, rank, world, barrier):
+    """The batched workload: independent IISPH dam breaks of uneven sizes
+    (fluid count log-uniform in [1024, 65536], aspect ratio uniform in
+    [0.25, 4]) advanced together, every kernel of a sub-step launched once
+    over all scenes (one CUDA graph launch per sub-step). With N GPUs each
+    rank takes its greedy bin-pack share of N * `count` scenes. Compared, on
+    one GPU, with the same scenes advanced one at a time by the single-scene
+    API over the same sub-steps."""
+    from emerald_b200 import workloads as W
+    count = args.batched_scenes
+    specs = W.batched_specs(count * world)
+    sizes = [s["nx"] * s["ny"] for s in specs]
+    mine = W.assign_scenes(sizes, world)[rank]
+    scenes = [W.scene_for(specs[k]["nx"], specs[k]["ny"], specs[k]["seed"],
+                          specs[k]["viscosity"]) for k in mine]
+    nf = sum(len(s.fluid) for s in scenes)
+    ns = sum(len(s.solid) for s in scenes)
+    b = E.Batch(nf + 128 * len(scenes), ns + 128 * len(scenes), len(scenes))
+    ids = [b.add_block_scene(s) for s in scenes]
+    warm = 3
+    steps = args.batched_steps
+    b.step("iisph", warm)
+    barrier()
+    l0 = b.kernel_launches()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    for k in range(steps):
+        ev[k][0].record()
+        b.step("iisph", 1)
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    launches = b.kernel_launches() - l0
+    step_ms = [a.elapsed_time(c) for a, c in ev]
+    t = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_s = float(t.item()) / 1000.0
+    stats = [b.stats(i) for i in ids]
+    err = max(st["error_average"] for st in stats)
+    iters = [st["pressure_iterations"] for st in stats]
+    b.close()
+    out = {"workload": "%d IISPH dam breaks per GPU, fluid count log-uniform in [1024, 65536], "
+                       "aspect U[0.25,4], viscosity U[0.001,0.05] (unused by IISPH), "
+                       "support=dx, CFL dt<=5e-4 s, 50-iteration cap, 0.1%% tolerance" % count,
+           "scenes": len(scenes) * world, "fluid_particles": nf, "boundary_particles": ns,
+           "steps": steps, "warmup": warm,
+           "scene_steps_per_s": round(len(scenes) * world * steps / total_s, 1),
+           "scenes_per_s_at_200_steps": round(len(scenes) * world * steps / total_s / 200.0, 3),
+           "particle_steps_per_s": round(world * nf * steps / total_s, 1),
+           "p50_step_ms": round(float(np.percentile(step_ms, 50)), 3),
+           "p99_step_ms": round(float(np.percentile(step_ms, 99)), 3),
+           "max_avg_density_error": err,
+           "scenes_above_0.1%": int(sum(st["error_average"] > 0.001 for st in stats)),
+           "iterations_last_step": [min(iters), max(iters)],
+           "gpu_launches": int(launches)}
+    if world == 1:
+        # the same scenes one at a time through the single-scene API
+        plain_s = 0.0
+        plain_launches = 0
+        for s in scenes:
+            sim = E.Simulation.from_block_scene(s)
+            sim.advance("iisph", warm, stats=False)
+            l1 = sim.kernel_launches()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(steps):
+                sim.advance("iisph", 1, stats=False)
+            e1.record()
+            torch.cuda.synchronize()
+            plain_s += e0.elapsed_time(e1) / 1000.0
+            plain_launches += sim.kernel_launches() - l1
+            sim.close()
+        plain_rate = len(scenes) * steps / plain_s
+        out["plain_one_scene_at_a_time"] = {
+            "scene_steps_per_s": round(plain_rate, 1),
+            "particle_steps_per_s": round(nf * steps / plain_s, 1),
+            "gpu_launches": int(plain_launches)}
+        out["speedup_vs_plain"] = round(out["scene_steps_per_s"] / plain_rate, 3)
+    return out
+
+
+def run_serving(args, torch, E):
+    """The served workload: a Poisson stream (200 requests/s) of DFSPH dam
+    breaks, fluid count log-uniform in [2048, 262144], sub-step count uniform
+    in [50, 500], admitted under a 120 GB device-memory budget and stepped
+    by continuous batching. Compared with the same requests served one at a
+    time by the single-scene API (scene set-up, sub-steps and result copy of
+    each, back to back)."""
+    import threading
+    from emerald_b200 import workloads as W
+    reqs = W.serving_requests(args.serving_requests)
+    scenes = [W.scene_for(r["nx"], r["ny"], r["seed"]) for r in reqs]
+    srv = E.Server(120 * 10**9, "dfsph_p", max_scenes=max(64, len(reqs)),
+                   max_substeps_per_launch=8)
+    ids = [None] * len(reqs)
+    t_start = time.perf_counter()
+
+    def client():
+        for k, (r, sc) in enumerate(zip(reqs, scenes)):
+            delay = t_start + r["arrival"] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            ids[k] = srv.submit_block_scene(sc, r["substeps"])
+
+    th = threading.Thread(target=client)
+    th.start()
+    th.join()
+    done = [srv.wait(rid, -1) for rid in ids]
+    wall = time.perf_counter() - t_start
+    st = srv.stats()
+    srv.close()
+    total_ms = [d[3]["total_ms"] for d in done]
+    particle_steps = sum(len(sc.fluid) * r["substeps"] for r, sc in zip(reqs, scenes))
+    out = {"workload": "%d DFSPH dam-break requests, Poisson 200/s, fluid count log-uniform in "
+                       "[2048, 262144], sub-steps uniform in [50, 500], 120 GB budget, "
+                       "continuous batching (admission every <= 8 sub-steps)" % len(reqs),
+           "requests": len(reqs), "wall_s": round(wall, 3),
+           "scenes_per_s": round(len(reqs) / wall, 3),
+           "particle_steps_per_s": round(particle_steps / wall, 1),
+           "step_ms_p50": round(st["step_ms_p50"], 3), "step_ms_p99": round(st["step_ms_p99"], 3),
+           "request_ms_p50": round(float(np.percentile(total_ms, 50)), 1),
+           "request_ms_p99": round(float(np.percentile(total_ms, 99)), 1),
+           "queue_ms_p99": round(st["queue_ms_p99"], 1),
+           "resident_peak": st["resident_peak"], "arena_bytes": st["device_bytes"],
+           "max_avg_density_error": max(d[2]["error_average"] for d in done),
+           "requests_above_0.1%": int(sum(d[2]["error_average"] > 0.001 for d in done))}
+    # the same requests one at a time, bounded in time
+    t0 = time.perf_counter()
+    served = 0
+    for r, sc in zip(reqs, scenes):
+        sim = E.Simulation.from_block_scene(sc)
+        sim.advance("dfsph_p", r["substeps"], stats=False)
+        sim.state()
+        sim.close()
+        served += 1
+        if time.perf_counter() - t0 > args.serving_plain_seconds:
+            break
+    plain_wall = time.perf_counter() - t0
+    out["plain_one_request_at_a_time"] = {"requests": served, "wall_s": round(plain_wall, 3),
+                                          "scenes_per_s": round(served / plain_wall, 3)}
+    out["speedup_vs_plain"] = round(out["scenes_per_s"] / (served / plain_wall), 3)
+    return out
 
 
 def reference_sim(threads):
@@ -365,6 +528,12 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batched-scenes", type=int, default=512,
+                    help="scenes per GPU of the batched workload (0: skip it)")
+    ap.add_argument("--batched-steps", type=int, default=40)
+    ap.add_argument("--serving-requests", type=int, default=96,
+                    help="requests of the served workload (0: skip it)")
+    ap.add_argument("--serving-plain-seconds", type=float, default=30.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

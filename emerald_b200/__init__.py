@@ -62,6 +62,31 @@ class StepStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", c_sz), ("method", c_i32), ("max_scenes", c_i32),
+                ("max_substeps_per_launch", c_i32), ("reserved", c_i32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", c_i64), ("completed", c_i64), ("rejected", c_i64), ("queued", c_i64),
+        ("resident", c_i64), ("batch_substeps", c_i64), ("scene_substeps", c_i64),
+        ("particle_substeps", ctypes.c_double), ("busy_seconds", ctypes.c_double),
+        ("step_ms_p50", c_f), ("step_ms_p99", c_f), ("request_ms_p50", c_f),
+        ("request_ms_p99", c_f), ("queue_ms_p50", c_f), ("queue_ms_p99", c_f),
+        ("fluid_capacity", c_sz), ("solid_capacity", c_sz), ("device_bytes", c_sz),
+        ("resident_peak", c_i32), ("status", c_i32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class RequestTiming(ctypes.Structure):
+    _fields_ = [("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double),
+                ("total_ms", ctypes.c_double)]
+
+
 EXPORTS = {
     "emerald_default_params": (c_i32, [ctypes.POINTER(Params)]),
     "emerald_config": (c_i32, [ctypes.POINTER(Params), c_vp]),
@@ -94,6 +119,27 @@ EXPORTS = {
                                          ctypes.POINTER(c_i32)]),
     "emerald_sim_set_graphs": (c_i32, [c_vp, c_i32]),
     "emerald_sim_kernel_launches": (c_i32, [c_vp, ctypes.POINTER(c_i64)]),
+    "emerald_batch_create": (c_i32, [c_sz, c_sz, c_i32, ctypes.POINTER(c_vp)]),
+    "emerald_batch_destroy": (c_i32, [c_vp]),
+    "emerald_batch_add_scene": (c_i32, [c_vp, ctypes.POINTER(Params), c_vp, c_vp, c_sz, c_vp, c_vp,
+                                        c_sz, ctypes.POINTER(c_i32)]),
+    "emerald_batch_remove_scene": (c_i32, [c_vp, c_i32]),
+    "emerald_batch_set_active": (c_i32, [c_vp, c_i32, c_i32]),
+    "emerald_batch_step": (c_i32, [c_vp, c_i32, c_i32]),
+    "emerald_batch_scene_stats": (c_i32, [c_vp, c_i32, ctypes.POINTER(StepStats)]),
+    "emerald_batch_get_state": (c_i32, [c_vp, c_i32, c_vp, c_vp]),
+    "emerald_batch_set_state": (c_i32, [c_vp, c_i32, c_vp, c_vp]),
+    "emerald_batch_free": (c_i32, [c_vp, ctypes.POINTER(c_sz), ctypes.POINTER(c_i32)]),
+    "emerald_batch_set_stream": (c_i32, [c_vp, c_vp]),
+    "emerald_batch_synchronize": (c_i32, [c_vp]),
+    "emerald_batch_kernel_launches": (c_i32, [c_vp, ctypes.POINTER(c_i64)]),
+    "emerald_server_create": (c_i32, [ctypes.POINTER(ServerConfig), ctypes.POINTER(c_vp)]),
+    "emerald_server_destroy": (c_i32, [c_vp]),
+    "emerald_server_submit": (c_i32, [c_vp, ctypes.POINTER(Params), c_vp, c_vp, c_sz, c_vp, c_vp,
+                                      c_sz, c_i32, ctypes.POINTER(c_i64)]),
+    "emerald_server_wait": (c_i32, [c_vp, c_i64, c_i32, c_vp, c_vp, ctypes.POINTER(StepStats),
+                                    ctypes.POINTER(RequestTiming)]),
+    "emerald_server_get_stats": (c_i32, [c_vp, ctypes.POINTER(ServerStats)]),
     "emerald_neighbors_static": (c_i32, [c_vp, c_u32, c_f, c_vp, c_vp, c_vp, c_vp, c_u32, c_vp]),
     "emerald_kernel_launches": (c_i64, []),
     "emerald_last_error": (ctypes.c_char_p, []),
@@ -367,3 +413,163 @@ class Simulation:
                                             ctypes.byref(count)), "kernel_times")
         keys = names.value.decode().split("\n") if names.value else []
         return {k: (float(ms[i]), int(launches[i])) for i, k in enumerate(keys[:count.value])}
+
+
+class Batch:
+    """Many independent scenes advanced together on one GPU: each kernel of a
+    sub-step runs once over every active scene. A scene's results are the
+    bits it gives when run alone."""
+
+    def __init__(self, fluid_capacity, solid_capacity, max_scenes):
+        h = c_vp()
+        _check(lib.emerald_batch_create(fluid_capacity, solid_capacity, max_scenes,
+                                        ctypes.byref(h)), "emerald_batch_create")
+        self._h = h
+        self._sizes = {}
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib.emerald_batch_destroy(self._h)
+            self._h = c_vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_scene(self, params, solid_xy, fluid_xy, fluid_v=None, solid_volumes=None,
+                  active=True):
+        """Returns the scene id, or None when the batch has no room."""
+        s = _f32(solid_xy).reshape(-1, 2)
+        f = _f32(fluid_xy).reshape(-1, 2)
+        v = None if fluid_v is None else _f32(fluid_v).reshape(-1, 2)
+        vol = None if solid_volumes is None else _f32(solid_volumes)
+        sid = c_i32()
+        rc = lib.emerald_batch_add_scene(self._h, ctypes.byref(params), _ptr(s), _ptr(vol), len(s),
+                                         _ptr(f), _ptr(v), len(f), ctypes.byref(sid))
+        if rc == 28:
+            return None
+        _check(rc, "emerald_batch_add_scene")
+        self._sizes[sid.value] = len(f)
+        if active:
+            self.set_active(sid.value, True)
+        return sid.value
+
+    def add_block_scene(self, scene, active=True):
+        return self.add_scene(scene.params, scene.solid, scene.fluid, None, scene.solid_volumes,
+                              active)
+
+    def remove_scene(self, sid):
+        _check(lib.emerald_batch_remove_scene(self._h, sid), "remove_scene")
+        self._sizes.pop(sid, None)
+
+    def set_active(self, sid, on=True):
+        _check(lib.emerald_batch_set_active(self._h, sid, int(on)), "set_active")
+
+    def step(self, method, n_substeps=1):
+        _check(lib.emerald_batch_step(self._h, method_id(method), n_substeps), "batch_step")
+
+    def stats(self, sid):
+        st = StepStats()
+        _check(lib.emerald_batch_scene_stats(self._h, sid, ctypes.byref(st)), "scene_stats")
+        return st.as_dict()
+
+    def state(self, sid):
+        n = self._sizes[sid]
+        x = np.zeros((n, 2), np.float32)
+        v = np.zeros((n, 2), np.float32)
+        _check(lib.emerald_batch_get_state(self._h, sid, _ptr(x), _ptr(v)), "get_state")
+        return x, v
+
+    def set_state(self, sid, x=None, v=None):
+        x = None if x is None else _f32(x)
+        v = None if v is None else _f32(v)
+        _check(lib.emerald_batch_set_state(self._h, sid, _ptr(x), _ptr(v)), "set_state")
+
+    def free(self):
+        n = c_sz()
+        k = c_i32()
+        _check(lib.emerald_batch_free(self._h, ctypes.byref(n), ctypes.byref(k)), "batch_free")
+        return n.value, k.value
+
+    def set_stream(self, stream_ptr):
+        _check(lib.emerald_batch_set_stream(self._h, stream_ptr), "set_stream")
+
+    def synchronize(self):
+        _check(lib.emerald_batch_synchronize(self._h), "synchronize")
+
+    def kernel_launches(self):
+        n = c_i64()
+        _check(lib.emerald_batch_kernel_launches(self._h, ctypes.byref(n)), "kernel_launches")
+        return n.value
+
+
+class Server:
+    """Request loop over one batch arena sized from a device-memory budget:
+    submitted scenes are admitted as room frees up, stepped together with
+    every resident scene, and retired when their sub-steps are done."""
+
+    ENOSPC = 28
+    ETIMEOUT = 110
+
+    def __init__(self, hbm_budget_bytes, method="dfsph_p", max_scenes=256,
+                 max_substeps_per_launch=8):
+        cfg = ServerConfig(int(hbm_budget_bytes), method_id(method), int(max_scenes),
+                           int(max_substeps_per_launch), 0)
+        h = c_vp()
+        _check(lib.emerald_server_create(ctypes.byref(cfg), ctypes.byref(h)),
+               "emerald_server_create")
+        self._h = h
+        self._sizes = {}
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib.emerald_server_destroy(self._h)
+            self._h = c_vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, params, solid_xy, fluid_xy, n_substeps, fluid_v=None, solid_volumes=None):
+        """Queues a request and returns its id (None if it can never fit)."""
+        s = _f32(solid_xy).reshape(-1, 2)
+        f = _f32(fluid_xy).reshape(-1, 2)
+        v = None if fluid_v is None else _f32(fluid_v).reshape(-1, 2)
+        vol = None if solid_volumes is None else _f32(solid_volumes)
+        rid = c_i64()
+        rc = lib.emerald_server_submit(self._h, ctypes.byref(params), _ptr(s), _ptr(vol), len(s),
+                                       _ptr(f), _ptr(v), len(f), int(n_substeps),
+                                       ctypes.byref(rid))
+        if rc == self.ENOSPC:
+            return None
+        _check(rc, "emerald_server_submit")
+        self._sizes[rid.value] = len(f)
+        return rid.value
+
+    def submit_block_scene(self, scene, n_substeps):
+        return self.submit(scene.params, scene.solid, scene.fluid, n_substeps,
+                           solid_volumes=scene.solid_volumes)
+
+    def wait(self, rid, timeout_ms=-1):
+        """(x, v, stats, timing) of a finished request, or None on timeout."""
+        n = self._sizes.get(rid, 0)
+        x = np.zeros((n, 2), np.float32)
+        v = np.zeros((n, 2), np.float32)
+        st = StepStats()
+        tm = RequestTiming()
+        rc = lib.emerald_server_wait(self._h, rid, int(timeout_ms), _ptr(x), _ptr(v),
+                                     ctypes.byref(st), ctypes.byref(tm))
+        if rc == self.ETIMEOUT:
+            return None
+        _check(rc, "emerald_server_wait")
+        self._sizes.pop(rid, None)
+        return x, v, st.as_dict(), {k: getattr(tm, k) for k, _ in tm._fields_}
+
+    def stats(self):
+        out = ServerStats()
+        _check(lib.emerald_server_get_stats(self._h, ctypes.byref(out)), "server_stats")
+        return out.as_dict()

@@ -7,6 +7,7 @@
 
 #include "../../include/emerald_sph.h"
 #include "engine.hpp"
+#include "server.hpp"
 
 namespace emerald {
 void lattice_config(emerald_params const& p, float dx, float dt, float& mass, float& denom);
@@ -18,6 +19,16 @@ std::vector<float2> dam_break(emerald_params const& p, float2 const* solid, size
 }  // namespace emerald
 
 using namespace emerald;
+
+struct emerald_batch {
+    Engine engine;
+    emerald_batch(uint32_t n, uint32_t ns, int scenes) : engine(n, ns, scenes) {}
+};
+
+struct emerald_server {
+    Server server;
+    explicit emerald_server(emerald_server_config const& c) : server(c) {}
+};
 
 struct emerald_sim {
     Engine engine;
@@ -310,6 +321,191 @@ int emerald_sim_device_state(emerald_sim* sim, void** x, void** v) {
     if (x) *x = sim->engine.device_x(sim->scene);
     if (v) *v = sim->engine.device_v(sim->scene);
     return EMERALD_OK;
+}
+
+int emerald_batch_create(size_t fluid_capacity, size_t solid_capacity, int32_t max_scenes,
+                         emerald_batch** out) {
+    if (!out || max_scenes < 1 || fluid_capacity > (size_t(1) << 30) ||
+        solid_capacity > (size_t(1) << 30)) {
+        return fail(EMERALD_EINVAL, "bad batch capacity");
+    }
+    return guarded([&] {
+        *out = new emerald_batch(uint32_t(fluid_capacity), uint32_t(solid_capacity), max_scenes);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_batch_destroy(emerald_batch* batch) {
+    delete batch;
+    return EMERALD_OK;
+}
+
+int emerald_batch_add_scene(emerald_batch* batch, emerald_params const* params,
+                            float const* solid_xy, float const* solid_volumes, size_t n_solid,
+                            float const* fluid_xy, float const* fluid_v, size_t n_fluid,
+                            int32_t* scene) {
+    if (!batch || !scene) return fail(EMERALD_EINVAL, "bad arguments");
+    if (int rc = check_params(params)) return rc;
+    if ((n_fluid && !fluid_xy) || (n_solid && !solid_xy)) {
+        return fail(EMERALD_EINVAL, "particle arrays are NULL");
+    }
+    return guarded([&] {
+        SceneSpec spec;
+        spec.params = *params;
+        spec.method = kDfsph;
+        spec.mode = kFrame;
+        spec.solid_xy = solid_xy;
+        spec.solid_volumes = solid_volumes;
+        spec.n_solid = uint32_t(n_solid);
+        spec.fluid_xy = fluid_xy;
+        spec.fluid_v = fluid_v;
+        spec.n_fluid = uint32_t(n_fluid);
+        int const id = batch->engine.add_scene(spec);
+        if (id < 0) return fail(EMERALD_ENOSPC, "no room in the batch for this scene");
+        *scene = id;
+        return EMERALD_OK;
+    });
+}
+
+int emerald_batch_remove_scene(emerald_batch* batch, int32_t scene) {
+    if (!batch || !batch->engine.scene_used(scene)) return fail(EMERALD_EINVAL, "bad scene");
+    return guarded([&] {
+        batch->engine.remove_scene(scene);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_batch_set_active(emerald_batch* batch, int32_t scene, int32_t active) {
+    if (!batch || !batch->engine.scene_used(scene)) return fail(EMERALD_EINVAL, "bad scene");
+    return guarded([&] {
+        batch->engine.set_active(scene, active != 0);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_batch_step(emerald_batch* batch, int32_t method, int32_t n_substeps) {
+    if (!batch || !valid_method(method) || n_substeps < 0) return fail(EMERALD_EINVAL, "bad arguments");
+    return guarded([&] {
+        for (int k = 0; k < n_substeps; ++k) batch->engine.substep(method);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_batch_scene_stats(emerald_batch* batch, int32_t scene, emerald_step_stats* stats) {
+    if (!batch || !stats || !batch->engine.scene_used(scene)) return fail(EMERALD_EINVAL, "bad scene");
+    return guarded([&] {
+        SceneState const s = batch->engine.scene_state(scene);
+        fill_stats(s, stats, s.substeps_total);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_batch_get_state(emerald_batch* batch, int32_t scene, float* x, float* v) {
+    if (!batch || !batch->engine.scene_used(scene)) return fail(EMERALD_EINVAL, "bad scene");
+    return guarded([&] {
+        batch->engine.get_state(scene, x, v);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_batch_set_state(emerald_batch* batch, int32_t scene, float const* x, float const* v) {
+    if (!batch || !batch->engine.scene_used(scene)) return fail(EMERALD_EINVAL, "bad scene");
+    return guarded([&] {
+        batch->engine.set_state(scene, x, v);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_batch_free(emerald_batch* batch, size_t* fluid, int32_t* scenes) {
+    if (!batch) return fail(EMERALD_EINVAL, "batch is NULL");
+    if (fluid) *fluid = batch->engine.free_fluid();
+    if (scenes) *scenes = batch->engine.free_scene_slots();
+    return EMERALD_OK;
+}
+
+int emerald_batch_set_stream(emerald_batch* batch, void* cuda_stream) {
+    if (!batch) return fail(EMERALD_EINVAL, "batch is NULL");
+    batch->engine.set_stream(static_cast<cudaStream_t>(cuda_stream));
+    return EMERALD_OK;
+}
+
+int emerald_batch_synchronize(emerald_batch* batch) {
+    if (!batch) return fail(EMERALD_EINVAL, "batch is NULL");
+    return guarded([&] {
+        cudaStreamSynchronize(batch->engine.stream());
+        batch->engine.check("synchronize");
+        return EMERALD_OK;
+    });
+}
+
+int emerald_batch_kernel_launches(emerald_batch* batch, int64_t* count) {
+    if (!batch || !count) return fail(EMERALD_EINVAL, "bad arguments");
+    return guarded([&] {
+        *count = batch->engine.kernel_launches();
+        return EMERALD_OK;
+    });
+}
+
+int emerald_server_create(emerald_server_config const* config, emerald_server** out) {
+    if (!config || !out || !valid_method(config->method) || config->hbm_budget_bytes == 0) {
+        return fail(EMERALD_EINVAL, "bad server configuration");
+    }
+    return guarded([&] {
+        *out = new emerald_server(*config);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_server_destroy(emerald_server* server) {
+    delete server;
+    return EMERALD_OK;
+}
+
+int emerald_server_submit(emerald_server* server, emerald_params const* params,
+                          float const* solid_xy, float const* solid_volumes, size_t n_solid,
+                          float const* fluid_xy, float const* fluid_v, size_t n_fluid,
+                          int32_t n_substeps, int64_t* request) {
+    if (!server || !request || n_substeps < 0) return fail(EMERALD_EINVAL, "bad arguments");
+    if (int rc = check_params(params)) return rc;
+    if ((n_fluid && !fluid_xy) || (n_solid && !solid_xy) || n_fluid > (size_t(1) << 30) ||
+        n_solid > (size_t(1) << 30)) {
+        return fail(EMERALD_EINVAL, "bad particle arrays");
+    }
+    return guarded([&] {
+        std::unique_ptr<ServerRequest> r(new ServerRequest);
+        r->params = *params;
+        r->n_fluid = uint32_t(n_fluid);
+        r->n_solid = uint32_t(n_solid);
+        r->substeps = n_substeps;
+        r->fluid_xy.assign(fluid_xy, fluid_xy + 2 * n_fluid);
+        if (fluid_v) r->fluid_v.assign(fluid_v, fluid_v + 2 * n_fluid);
+        if (n_solid) r->solid_xy.assign(solid_xy, solid_xy + 2 * n_solid);
+        if (solid_volumes) r->solid_volumes.assign(solid_volumes, solid_volumes + n_solid);
+        int const rc = server->server.submit(std::move(r), *request);
+        if (rc == EMERALD_ENOSPC) return fail(rc, "scene larger than the server's arena");
+        if (rc != EMERALD_OK) return fail(rc, "server loop failed");
+        return EMERALD_OK;
+    });
+}
+
+int emerald_server_wait(emerald_server* server, int64_t request, int32_t timeout_ms, float* x,
+                        float* v, emerald_step_stats* stats, emerald_request_timing* timing) {
+    if (!server) return fail(EMERALD_EINVAL, "server is NULL");
+    return guarded([&] {
+        int const rc = server->server.wait(request, timeout_ms, x, v, stats, timing);
+        if (rc == EMERALD_ETIMEOUT) return fail(rc, "request not done yet");
+        if (rc == EMERALD_ENOTFOUND) return fail(rc, "unknown request");
+        if (rc != EMERALD_OK) return fail(rc, "request failed");
+        return EMERALD_OK;
+    });
+}
+
+int emerald_server_get_stats(emerald_server* server, emerald_server_stats* out) {
+    if (!server || !out) return fail(EMERALD_EINVAL, "bad arguments");
+    return guarded([&] {
+        server->server.stats(*out);
+        return EMERALD_OK;
+    });
 }
 
 int emerald_sim_set_graphs(emerald_sim* sim, int32_t graphs) {

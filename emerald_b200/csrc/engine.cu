@@ -81,6 +81,29 @@ void Engine::check(char const* what) {
     }
 }
 
+// The sum of the constructor's allocations below, region by region.
+size_t Engine::footprint(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes) {
+    size_t const N = size_t(tiles_for(std::max<uint32_t>(fluid_capacity, 1))) * kTile;
+    size_t const S = size_t(tiles_for(std::max<uint32_t>(solid_capacity, 1))) * kTile;
+    size_t const M = size_t(std::max(max_scenes, 1));
+    size_t const E = N * kMaxNeighbors;
+    size_t const ftab = 4 * N + 72 * M;
+    size_t const stab = 4 * S + 72 * M;
+    auto r = [](size_t b) { return std::max<size_t>(b, 16); };
+    size_t bytes = r(sizeof(SceneParams) * M) + r(sizeof(SceneState) * M) + r(4 * (N / kTile)) +
+                   r(4 * (S / kTile));
+    bytes += 12 * r(8 * N) + 18 * r(4 * N) + 2 * r(N);   // per-particle state and scratch
+    bytes += r(sort_scratch_bytes(uint32_t(N)));            // storage-order sort
+    bytes += 2 * (2 * r(4 * E) + r(8 * E));                 // fluid and solid neighbour lists
+    bytes += r(8 * ftab) + 2 * r(4 * ftab);                 // fluid cell table
+    bytes += 3 * r(8 * S) + 4 * r(4 * S);                   // solid particles
+    bytes += r(8 * stab) + 2 * r(4 * stab);                 // solid cell table
+    size_t const scan_words = std::max(scan_scratch_words(uint32_t(ftab)),
+                                       scan_scratch_words(uint32_t(stab))) + 64;
+    bytes += r(4 * scan_words) + r(sizeof(int)) + r(sizeof(unsigned long long) * 4);
+    return bytes;
+}
+
 Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
   : fluid_cap_(tiles_for(std::max<uint32_t>(fluid_capacity, 1)) * kTile),
     solid_cap_(tiles_for(std::max<uint32_t>(solid_capacity, 1)) * kTile),
@@ -102,6 +125,7 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
             throw std::bad_alloc();
         }
         allocations_.push_back(p);
+        device_bytes_ += std::max<size_t>(bytes, 16);
         return p;
     };
     size_t const N = fluid_cap_;
@@ -196,6 +220,7 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
     tile_scene_.assign(N / kTile, -1);
     stile_scene_.assign(S / kTile, -1);
     upload_tiles();
+    update_extent();
     check("engine allocation");
 }
 
@@ -418,6 +443,7 @@ int Engine::add_scene(SceneSpec const& spec) {
         cudaMemsetAsync(a_.vs + P.solid_begin, 0, 8ull * spec.n_solid, st_);
     }
     update_sort_bases();
+    update_extent();
     rebuild_solids();
     if (spec.n_solid) {
         if (spec.solid_volumes) {
@@ -425,7 +451,7 @@ int Engine::add_scene(SceneSpec const& spec) {
                             cudaMemcpyHostToDevice, st_);
         } else {
             launch("solid_volumes", [&] {
-                launch_solid_volumes(a_, solid_cap_ / kTile, 1.7f, id, st_);
+                launch_solid_volumes(a_, ext_stiles_, 1.7f, id, st_);
             });
         }
     }
@@ -434,8 +460,43 @@ int Engine::add_scene(SceneSpec const& spec) {
 }
 
 void Engine::rebuild_solids() {
-    launch("build_cells_solid",
-           [&] { launch_build_cells(a_, true, solid_cap_ / kTile, d_scan_, st_); }, 6);
+    Arena const e = extent_arena();
+    launch("build_cells_solid", [&] { launch_build_cells(e, true, ext_stiles_, d_scan_, st_); }, 6);
+}
+
+namespace {
+uint32_t round_extent(uint64_t used, uint32_t capacity, uint32_t min_quantum) {
+    uint64_t const q = std::max<uint64_t>(min_quantum, capacity / 32);
+    uint64_t const r = (used + q - 1) / q * q;
+    return uint32_t(std::min<uint64_t>(std::max<uint64_t>(r, 1), capacity));
+}
+}  // namespace
+
+void Engine::update_extent() {
+    uint64_t t = 0, st = 0, ft = 0, sb = 0;
+    for (auto const& sc : scenes_) {
+        if (!sc.used) continue;
+        t = std::max<uint64_t>(t, sc.ftile_begin + sc.ftile_count);
+        st = std::max<uint64_t>(st, sc.stile_begin + sc.stile_count);
+        ft = std::max<uint64_t>(ft, uint64_t(sc.p.ftab_begin) + sc.ftab_size);
+        sb = std::max<uint64_t>(sb, uint64_t(sc.p.stab_begin) + sc.stab_size);
+    }
+    uint32_t const nt = round_extent(t, fluid_cap_ / kTile, 16);
+    uint32_t const ns = round_extent(st, solid_cap_ / kTile, 16);
+    uint32_t const nf = round_extent(ft, ftab_.capacity(), 8192);
+    uint32_t const nsb = round_extent(sb, stab_.capacity(), 8192);
+    if (nt != ext_tiles_ || nf != ext_ftab_) destroy_graphs();
+    ext_tiles_ = nt;
+    ext_stiles_ = ns;
+    ext_ftab_ = nf;
+    ext_stab_ = nsb;
+}
+
+Arena Engine::extent_arena() const {
+    Arena e = a_;
+    e.ftab_total = ext_ftab_;
+    e.stab_total = ext_stab_;
+    return e;
 }
 
 void Engine::remove_scene(int id) {
@@ -452,6 +513,7 @@ void Engine::remove_scene(int id) {
     stab_.release(sc.p.stab_begin, sc.stab_size);
     sc = Scene{};
     update_sort_bases();
+    update_extent();
     rebuild_solids();
 }
 
@@ -482,7 +544,7 @@ int Engine::active_scenes() const {
 
 void Engine::begin_frame(int32_t method) {
     if (method == kDfsph) {
-        launch("zero_kappas", [&] { launch_zero_kappas(a_, fluid_cap_ / kTile, st_); });
+        launch("zero_kappas", [&] { launch_zero_kappas(a_, ext_tiles_, st_); });
     }
 }
 
@@ -499,7 +561,7 @@ int Engine::max_iterations(int kind) const {
 // Solver iteration kernels of one loop kind (launched on cur_).
 void Engine::emit_loop_body(int kind, int32_t method, cudaGraphConditionalHandle cond,
                             bool use_cond) {
-    uint32_t const tiles = fluid_cap_ / kTile;
+    uint32_t const tiles = ext_tiles_;
     cudaStream_t const st = cur_;
     // loop kernels are counted on the device, once per executed iteration
     bool const was_counting = count_host_;
@@ -604,18 +666,19 @@ void Engine::run_loop(int kind, int max_iter, int32_t method) {
 }
 
 void Engine::emit_substep(int32_t method, bool reorder) {
-    uint32_t const tiles = fluid_cap_ / kTile;
+    uint32_t const tiles = ext_tiles_;
     cudaStream_t const st = cur_;
     if (reorder) {
         // keys, three to five radix passes of three kernels, permute, commit
         int const bits = order_key_bits();
-        launch("reorder", [&] { launch_reorder(a_, order_sort_, fluid_cap_, bits, st); },
+        launch("reorder", [&] { launch_reorder(a_, order_sort_, tiles * kTile, bits, st); },
                3 + 3 * (bits / 8));
     }
     launch("max_v2", [&] { launch_max_v2(a_, tiles, st); });
     launch("begin_substep", [&] { launch_begin_substep(a_, max_scenes_, st); });
     // binning, three scan passes, scatter, per-cell ordering
-    launch("build_cells", [&] { launch_build_cells(a_, false, tiles, d_scan_, st); }, 6);
+    Arena const ext = extent_arena();
+    launch("build_cells", [&] { launch_build_cells(ext, false, tiles, d_scan_, st); }, 6);
     bool const kernels = method != kPcisph;
     launch("neighbors_fluid", [&] { launch_neighbors(a_, tiles, false, kernels, st); });
     launch("neighbors_solid", [&] { launch_neighbors(a_, tiles, true, kernels, st); });

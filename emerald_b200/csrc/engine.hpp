@@ -62,6 +62,11 @@ class Engine {
 public:
     Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes);
     ~Engine();
+    // Device bytes the constructor allocates for these capacities.
+    static size_t footprint(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes);
+    size_t device_bytes() const { return device_bytes_; }
+    uint32_t fluid_capacity() const { return fluid_cap_; }
+    uint32_t solid_capacity() const { return solid_cap_; }
     Engine(Engine const&) = delete;
     Engine& operator=(Engine const&) = delete;
 
@@ -97,6 +102,11 @@ public:
     float2* device_v(int id) { return a_.v + scenes_[id].p.fluid_begin; }
     int active_scenes() const;
     size_t free_fluid() const { return size_t(fluid_tiles_.largest_free()) * kTile; }
+    int free_scene_slots() const {
+        int n = 0;
+        for (auto const& s : scenes_) n += s.used ? 0 : 1;
+        return n;
+    }
 
     void enable_timing(bool on);
     KernelTimes const& kernel_times();
@@ -139,6 +149,11 @@ private:
     void destroy_graphs();
     int max_iterations(int kind) const;
     void rebuild_solids();
+    // Extent of the arena the per-sub-step launches cover: the highest tile
+    // and cell-table slot any resident scene uses, rounded up to 1/32 of the
+    // capacity so that graphs are re-captured only when it moves by that much.
+    void update_extent();
+    Arena extent_arena() const;
     void ensure_sort_scratch(uint32_t n);
 
     cudaStream_t st_ = nullptr;
@@ -146,6 +161,8 @@ private:
     int max_scenes_;
     Arena a_{};
     std::vector<void*> allocations_;
+    size_t device_bytes_ = 0;
+    uint32_t ext_tiles_ = 0, ext_stiles_ = 0, ext_ftab_ = 0, ext_stab_ = 0;
     SceneParams* d_sp_ = nullptr;
     SceneState* d_ss_ = nullptr;
     int32_t* d_tile_scene_ = nullptr;

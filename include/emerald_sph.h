@@ -208,6 +208,92 @@ int emerald_sim_kernel_launches(emerald_sim* sim, int64_t* count);
  * process started (a graph launch counts its kernels outside solver loops). */
 int64_t emerald_kernel_launches(void);
 
+/* ----------------------------------------------------------------- batches */
+
+/* Many independent scenes advanced together: every kernel of a sub-step runs
+ * once over all active scenes' particles (one CUDA graph launch per
+ * sub-step), each scene with its own parameters, time step and convergence
+ * state. The reference runs one scene per EZ_EXAMPLE_SIM; a scene here gives
+ * the same bits as that scene run alone. */
+typedef struct emerald_batch emerald_batch;
+
+int emerald_batch_create(size_t fluid_capacity, size_t solid_capacity, int32_t max_scenes,
+                         emerald_batch** out);
+int emerald_batch_destroy(emerald_batch* batch);
+/* Adds a scene (inactive until emerald_batch_set_active); *scene receives its
+ * id. EMERALD_ENOSPC when the batch has no room for it. */
+int emerald_batch_add_scene(emerald_batch* batch, emerald_params const* params,
+                            float const* solid_xy, float const* solid_volumes, size_t n_solid,
+                            float const* fluid_xy, float const* fluid_v, size_t n_fluid,
+                            int32_t* scene);
+int emerald_batch_remove_scene(emerald_batch* batch, int32_t scene);
+int emerald_batch_set_active(emerald_batch* batch, int32_t scene, int32_t active);
+/* n adaptive sub-steps (frames continue across calls) of `method` for every
+ * active scene. Asynchronous on the batch's stream. */
+int emerald_batch_step(emerald_batch* batch, int32_t method, int32_t n_substeps);
+int emerald_batch_scene_stats(emerald_batch* batch, int32_t scene, emerald_step_stats* stats);
+int emerald_batch_get_state(emerald_batch* batch, int32_t scene, float* x, float* v);
+int emerald_batch_set_state(emerald_batch* batch, int32_t scene, float const* x, float const* v);
+/* Largest fluid range and scene slots still free. */
+int emerald_batch_free(emerald_batch* batch, size_t* fluid, int32_t* scenes);
+int emerald_batch_set_stream(emerald_batch* batch, void* cuda_stream);
+int emerald_batch_synchronize(emerald_batch* batch);
+int emerald_batch_kernel_launches(emerald_batch* batch, int64_t* count);
+
+/* ----------------------------------------------------------------- serving */
+
+/* A request loop over one batch: requests (a scene and a sub-step count) are
+ * queued by any host thread, admitted in arrival order as soon as the arena
+ * has room for them (first fit: a large request waiting for room does not
+ * hold back smaller ones behind it), stepped together with every other
+ * resident scene, and retired as soon as their sub-steps are done, which
+ * frees their room for the queue. The arena is sized once from the device
+ * memory budget. No counterpart in the reference (one scene per process). */
+typedef struct emerald_server emerald_server;
+
+typedef struct emerald_server_config {
+    size_t hbm_budget_bytes;         /* device bytes the arena may take */
+    int32_t method;                  /* EMERALD_METHOD_* every request runs */
+    int32_t max_scenes;              /* scenes resident at once */
+    int32_t max_substeps_per_launch; /* sub-steps between admission points (0: 8) */
+    int32_t reserved;
+} emerald_server_config;
+
+typedef struct emerald_server_stats {
+    int64_t submitted, completed, rejected, queued, resident;
+    int64_t batch_substeps;    /* batched sub-step launches */
+    int64_t scene_substeps;    /* sum over scenes of their sub-steps */
+    double particle_substeps;  /* sum over scenes of fluid count x sub-steps */
+    double busy_seconds;       /* wall time with at least one scene resident */
+    float step_ms_p50, step_ms_p99;       /* device time of one batched sub-step */
+    float request_ms_p50, request_ms_p99; /* submit to result ready */
+    float queue_ms_p50, queue_ms_p99;     /* submit to admission */
+    size_t fluid_capacity, solid_capacity, device_bytes;
+    int32_t resident_peak;
+    int32_t status; /* first error of the loop, EMERALD_OK while healthy */
+} emerald_server_stats;
+
+typedef struct emerald_request_timing {
+    double queue_ms, run_ms, total_ms;
+} emerald_request_timing;
+
+int emerald_server_create(emerald_server_config const* config, emerald_server** out);
+/* Stops the loop; requests not yet waited for are dropped. */
+int emerald_server_destroy(emerald_server* server);
+/* Copies the inputs and queues the request; *request receives its id.
+ * EMERALD_ENOSPC when the scene is larger than the whole arena. */
+int emerald_server_submit(emerald_server* server, emerald_params const* params,
+                          float const* solid_xy, float const* solid_volumes, size_t n_solid,
+                          float const* fluid_xy, float const* fluid_v, size_t n_fluid,
+                          int32_t n_substeps, int64_t* request);
+/* Waits for a request (timeout_ms < 0: without limit), copies out its final
+ * positions and velocities (original order; NULL skips) and statistics, and
+ * forgets it. EMERALD_ETIMEOUT when it is not done within the limit,
+ * EMERALD_ENOTFOUND for an unknown or already collected id. */
+int emerald_server_wait(emerald_server* server, int64_t request, int32_t timeout_ms, float* x,
+                        float* v, emerald_step_stats* stats, emerald_request_timing* timing);
+int emerald_server_get_stats(emerald_server* server, emerald_server_stats* out);
+
 /* ---------------------------------------------------- allocation-free build */
 
 /* No counterpart in the reference (which always allocates its std::vector
