@@ -1,0 +1,245 @@
+// C++ drop-in for the reference's step functions over the C ABI.
+//
+// emerald/sph2d_box declares, per solver (e.g. emerald/sph2d_box/iisph.h),
+//
+//     State iisph_simulation_step(flicks global_time, Simulation_config const& config,
+//                                 State&& state, Solid_state const& solid_state,
+//                                 Temp_data& temp, User_forces_function const& user_forces,
+//                                 User_colors_function const& user_colors);
+//
+// and EZ_EXAMPLE_SIM::step (emerald/sph2d_box/simulation.cpp:41-93) calls one of
+// them per frame. The templates below take the caller's own types with the
+// same argument list, so that code written against the reference compiles
+// unchanged after `using namespace emerald_b200::sph2d_box;`:
+//
+//   * State / Solid_state: anything with `positions` and `velocities`
+//     (std::vector of a two-float vector type such as Imath::V2f) and, for
+//     State, `colors` (a vector of a four-float colour type);
+//   * Simulation_config: anything with `params` (the reference's Parameters
+//     member names) and `mass_per_particle`, `pressure_correction_denom`,
+//     `draw_radius`;
+//   * Temp_data: any object; its address keys the device simulation that
+//     stands for it (release it with emerald_b200::release(temp) before the
+//     object goes away);
+//   * flicks: anything with `.count()` (std::chrono::duration) or an integer.
+//
+// Each call uploads the state, runs one frame on the GPU, downloads the new
+// state and, if user_colors is callable, calls it on the host with the
+// frame's densities, as compute_colors does (emerald/sph2d_box/colors.cpp:22-38).
+// user_forces is not called: the device applies gravity, which is what the
+// reference's default_gravity_forces (emerald/sph2d_box/forces.cpp:63-83)
+// computes; callers with other forces stay on the reference path.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+#include "emerald_sph.h"
+
+namespace emerald_b200 {
+
+class Error : public std::runtime_error {
+public:
+    Error(int code, std::string const& what)
+      : std::runtime_error(what + " (" + std::to_string(code) + "): " + emerald_last_error()),
+        code_(code) {}
+    int code() const { return code_; }
+
+private:
+    int code_;
+};
+
+inline void check(int rc, char const* what) {
+    if (rc != EMERALD_OK) throw Error(rc, what);
+}
+
+namespace detail {
+
+template <class T, class = void>
+struct has_volumes : std::false_type {};
+template <class T>
+struct has_volumes<T, std::void_t<decltype(std::declval<T const&>().volumes)>>
+  : std::is_same<typename std::decay<decltype(std::declval<T const&>().volumes)>::type,
+                 std::vector<float>> {};
+
+template <class V>
+float const* floats(std::vector<V> const& v) {
+    static_assert(sizeof(V) == 2 * sizeof(float) && std::is_standard_layout<V>::value,
+                  "positions and velocities must be vectors of two packed floats");
+    return reinterpret_cast<float const*>(v.data());
+}
+
+template <class V>
+float* floats(std::vector<V>& v) {
+    static_assert(sizeof(V) == 2 * sizeof(float) && std::is_standard_layout<V>::value,
+                  "positions and velocities must be vectors of two packed floats");
+    return reinterpret_cast<float*>(v.data());
+}
+
+template <class T>
+auto ticks(T const& t, int) -> decltype(int64_t(t.count())) {
+    return int64_t(t.count());
+}
+template <class T>
+int64_t ticks(T const& t, long) {
+    return int64_t(t);
+}
+
+template <class F>
+auto callable(F const& f, int) -> decltype(bool(f)) {
+    return bool(f);
+}
+template <class F>
+bool callable(F const&, long) {
+    return false;
+}
+
+// Parameters + Simulation_config (emerald/sph2d_box/parameters.h:12-41,
+// emerald/sph2d_box/config.h:7-18) to emerald_params.
+template <class Config>
+emerald_params to_params(Config const& config) {
+    emerald_params p{};
+    check(emerald_default_params(&p), "emerald_default_params");
+    auto const& in = config.params;
+    p.seed = uint64_t(in.seed);
+    p.time_per_step_flicks = ticks(in.time_per_step, 0);
+    p.sub_steps = int32_t(in.sub_steps);
+    p.length = float(in.length);
+    p.support = float(in.support);
+    p.gravity = float(in.gravity);
+    p.viscosity = float(in.viscosity);
+    p.target_density = float(in.target_density);
+    p.iisph_max_pressure_iterations = int32_t(in.iisph.max_pressure_iterations);
+    p.iisph_error_average_threshold = float(in.iisph.error_average_threshold);
+    p.iisph_error_max_threshold = float(in.iisph.error_max_threshold);
+    p.iisph_omega = float(in.iisph.omega);
+    p.dfsph_max_correction_iterations = int32_t(in.dfsph.max_correction_iterations);
+    p.dfsph_density_error_average_threshold = float(in.dfsph.density_error_average_threshold);
+    p.dfsph_density_error_max_threshold = float(in.dfsph.density_error_max_threshold);
+    p.dfsph_divergence_error_average_threshold = float(in.dfsph.divergence_error_average_threshold);
+    p.dfsph_divergence_error_max_threshold = float(in.dfsph.divergence_error_max_threshold);
+    p.mass_per_particle = float(config.mass_per_particle);
+    p.pressure_correction_denom = float(config.pressure_correction_denom);
+    return p;
+}
+
+// The device simulation standing for one Temp_data object.
+struct Context {
+    emerald_sim* sim = nullptr;
+    size_t n_fluid = 0;
+    int64_t time = 0;
+    std::vector<float> densities;
+    ~Context() {
+        if (sim) emerald_sim_destroy(sim);
+    }
+};
+
+inline std::map<void const*, std::unique_ptr<Context>>& registry() {
+    static std::map<void const*, std::unique_ptr<Context>> r;
+    return r;
+}
+inline std::mutex& registry_mutex() {
+    static std::mutex m;
+    return m;
+}
+
+template <class Config, class Solid_state>
+Context& context(void const* key, Config const& config, Solid_state const& solid, size_t n_fluid,
+                 float const* x, float const* v, int64_t time) {
+    std::lock_guard<std::mutex> lock(registry_mutex());
+    auto& slot = registry()[key];
+    if (slot && slot->n_fluid == n_fluid) return *slot;
+    slot.reset(new Context);
+    emerald_params const p = to_params(config);
+    float const* vols = nullptr;
+    if constexpr (has_volumes<typename std::decay<Solid_state>::type>::value) {
+        // the reference's compute_neighbor_data_and_volumes results, if filled
+        if (solid.volumes.size() == solid.positions.size()) vols = solid.volumes.data();
+    }
+    check(emerald_sim_create(&p, floats(solid.positions), vols, solid.positions.size(), x, v,
+                             n_fluid, &slot->sim),
+          "emerald_sim_create");
+    slot->n_fluid = n_fluid;
+    slot->time = time;
+    return *slot;
+}
+
+template <class State, class Config, class Solid_state, class Colors>
+State step(int32_t method, int64_t global_time, Config const& config, State&& state,
+           Solid_state const& solid, void const* temp_key, Colors const& user_colors) {
+    size_t const n = state.positions.size();
+    if (state.velocities.size() != n) {
+        throw std::invalid_argument("positions and velocities differ in size");
+    }
+    Context& ctx = context(temp_key, config, solid, n, floats(state.positions),
+                           floats(state.velocities), global_time);
+    if (ctx.time != global_time) {
+        throw std::invalid_argument("global_time does not continue the device simulation's clock");
+    }
+    check(emerald_sim_set_state(ctx.sim, floats(state.positions), floats(state.velocities)),
+          "emerald_sim_set_state");
+    emerald_step_stats stats{};
+    check(emerald_sim_frame(ctx.sim, method, &stats), "emerald_sim_frame");
+    check(emerald_sim_get_state(ctx.sim, floats(state.positions), floats(state.velocities)),
+          "emerald_sim_get_state");
+    ctx.time += to_params(config).time_per_step_flicks;
+    if (callable(user_colors, 0)) {
+        ctx.densities.resize(n);
+        int32_t width = 0;
+        check(emerald_sim_get_array(ctx.sim, "densities", ctx.densities.data(), &width),
+              "emerald_sim_get_array");
+        state.colors.resize(n);
+        user_colors(n, float(double(global_time) / 705600000.0), config.mass_per_particle,
+                    config.draw_radius, state.colors.data(), state.positions.data(),
+                    state.velocities.data(), ctx.densities.data());
+    }
+    return std::move(state);
+}
+
+}  // namespace detail
+
+// Destroys the device simulation that stands for `temp`.
+template <class Temp>
+void release(Temp const& temp) {
+    std::lock_guard<std::mutex> lock(detail::registry_mutex());
+    detail::registry().erase(static_cast<void const*>(&temp));
+}
+
+namespace sph2d_box {
+
+#define EMERALD_B200_STEP(name, method)                                                        \
+    template <class Flicks, class Config, class State, class Solid_state, class Temp,          \
+              class Forces, class Colors>                                                      \
+    typename std::decay<State>::type name(Flicks const global_time, Config const& config,      \
+                                          State&& state, Solid_state const& solid_state,       \
+                                          Temp& temp, Forces const& user_forces,               \
+                                          Colors const& user_colors) {                         \
+        (void)user_forces;                                                                     \
+        return detail::step(method, detail::ticks(global_time, 0), config,                     \
+                            std::forward<State>(state), solid_state,                           \
+                            static_cast<void const*>(&temp), user_colors);                     \
+    }
+
+// emerald/sph2d_box/pcisph.cpp:166-204
+EMERALD_B200_STEP(pcisph_simulation_step, EMERALD_PCISPH)
+// emerald/sph2d_box/iisph.cpp:168-188
+EMERALD_B200_STEP(iisph_simulation_step, EMERALD_IISPH)
+// emerald/sph2d_box/iisph_ap.cpp
+EMERALD_B200_STEP(iisph_ap_simulation_step, EMERALD_IISPH_AP)
+// emerald/sph2d_box/iisph_pseudo_ap.cpp
+EMERALD_B200_STEP(iisph_pseudo_ap_simulation_step, EMERALD_IISPH_PSEUDO_AP)
+// emerald/sph2d_box/dfsph_p.cpp:376-396
+EMERALD_B200_STEP(dfsph_p_simulation_step, EMERALD_DFSPH_P)
+
+#undef EMERALD_B200_STEP
+
+}  // namespace sph2d_box
+
+}  // namespace emerald_b200

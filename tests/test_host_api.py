@@ -102,3 +102,23 @@ def test_block_scene_matches_reference_generator(reference):
     a = E.block_scene(33, 17, F(1 / 100), 0.25, 0.5, 0.02, 11)
     b = reference.block_scene(33, 17, F(1 / 100), 0.25, 0.5, 0.02, 11)
     assert_bitwise(a, b, "block scene")
+
+
+def test_dropin_header_compiles():
+    """include/emerald_sph.hpp compiles against a caller spelled like the
+    reference's EZ_EXAMPLE_SIM::step and links against the library."""
+    import shutil
+    import subprocess
+    import tempfile
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no g++")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib = os.path.join(root, "emerald_b200")
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "step_dropin")
+        r = subprocess.run([gxx, "-std=c++17", "-O1", "-Wall", "-Werror", "-I",
+                            os.path.join(root, "include"),
+                            os.path.join(root, "tests", "cpp", "step_dropin.cpp"), "-L", lib,
+                            "-lemerald_b200", "-o", out], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
