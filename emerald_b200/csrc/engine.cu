@@ -81,6 +81,20 @@ void Engine::check(char const* what) {
     }
 }
 
+Engine::Room Engine::room() const {
+    return Room{fluid_tiles_.largest_free(), solid_tiles_.largest_free(), ftab_.largest_free(),
+                stab_.largest_free(), free_scene_slots()};
+}
+
+// The same sizes add_scene allocates.
+bool Engine::Room::fits(uint32_t n_fluid, uint32_t n_solid) const {
+    uint32_t const flog = std::max<uint32_t>(6, ceil_log2(2ull * std::max<uint32_t>(n_fluid, 1)));
+    uint32_t const slog = std::max<uint32_t>(6, ceil_log2(2ull * std::max<uint32_t>(n_solid, 1)));
+    return scene_slots > 0 && tiles_for(n_fluid) <= fluid_tiles &&
+           tiles_for(n_solid) <= solid_tiles && (1u << flog) + 1 <= fluid_table &&
+           (1u << slog) + 1 <= solid_table;
+}
+
 // The sum of the constructor's allocations below, region by region.
 size_t Engine::footprint(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes) {
     size_t const N = size_t(tiles_for(std::max<uint32_t>(fluid_capacity, 1))) * kTile;

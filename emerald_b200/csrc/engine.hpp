@@ -102,6 +102,14 @@ public:
     float2* device_v(int id) { return a_.v + scenes_[id].p.fluid_begin; }
     int active_scenes() const;
     size_t free_fluid() const { return size_t(fluid_tiles_.largest_free()) * kTile; }
+    // Largest free runs of each arena region, for admission decisions made
+    // away from the thread that owns the engine.
+    struct Room {
+        uint32_t fluid_tiles, solid_tiles, fluid_table, solid_table;
+        int scene_slots;
+        bool fits(uint32_t n_fluid, uint32_t n_solid) const;
+    };
+    Room room() const;
     int free_scene_slots() const {
         int n = 0;
         for (auto const& s : scenes_) n += s.used ? 0 : 1;

@@ -1,4 +1,4 @@
-// Request loop over one batch arena (see server.hpp).
+// Request loop over batch arenas (see server.hpp).
 #include "server.hpp"
 
 #include <algorithm>
@@ -49,22 +49,31 @@ double ms_between(std::chrono::steady_clock::time_point a, std::chrono::steady_c
 Server::Server(emerald_server_config const& cfg) : cfg_(cfg) {
     if (cfg_.max_scenes < 1) cfg_.max_scenes = 1;
     if (cfg_.max_substeps_per_launch < 1) cfg_.max_substeps_per_launch = 8;
-    uint32_t fluid = 0, solid = 0;
-    capacities(cfg_.hbm_budget_bytes, cfg_.max_scenes, fluid, solid);
+    if (cfg_.lanes < 1) cfg_.lanes = 4;
     if (cudaGetDevice(&device_) != cudaSuccess) {
         cudaGetLastError();
         throw std::runtime_error("no current CUDA device");
     }
-    engine_.reset(new Engine(fluid, solid, cfg_.max_scenes));
-    cudaStream_t st = nullptr;
-    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
-        throw std::runtime_error("stream creation failed");
+    int const per_lane_scenes = (cfg_.max_scenes + cfg_.lanes - 1) / cfg_.lanes;
+    size_t const per_lane_budget = cfg_.hbm_budget_bytes / size_t(cfg_.lanes);
+    for (int k = 0; k < cfg_.lanes; ++k) {
+        std::unique_ptr<Lane> lane(new Lane);
+        lane->index = k;
+        uint32_t fluid = 0, solid = 0;
+        capacities(per_lane_budget, per_lane_scenes, fluid, solid);
+        lane->engine.reset(new Engine(fluid, solid, per_lane_scenes));
+        if (cudaStreamCreateWithFlags(&lane->stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreate(&lane->ev0) != cudaSuccess || cudaEventCreate(&lane->ev1) != cudaSuccess) {
+            throw std::runtime_error("stream or event creation failed");
+        }
+        lane->engine->set_stream(lane->stream);
+        lane->room = lane->engine->room();
+        lanes_.push_back(std::move(lane));
     }
-    engine_->set_stream(st);
-    if (cudaEventCreate(&ev0_) != cudaSuccess || cudaEventCreate(&ev1_) != cudaSuccess) {
-        throw std::runtime_error("event creation failed");
+    for (auto& lane : lanes_) {
+        Lane* l = lane.get();
+        l->worker = std::thread([this, l] { loop(*l); });
     }
-    worker_ = std::thread([this] { loop(); });
 }
 
 Server::~Server() {
@@ -73,18 +82,27 @@ Server::~Server() {
         stop_ = true;
     }
     work_cv_.notify_all();
-    if (worker_.joinable()) worker_.join();
-    cudaStream_t const st = engine_ ? engine_->stream() : nullptr;
-    engine_.reset();
-    if (st) cudaStreamDestroy(st);
-    if (ev0_) cudaEventDestroy(ev0_);
-    if (ev1_) cudaEventDestroy(ev1_);
+    for (auto& lane : lanes_) {
+        if (lane->worker.joinable()) lane->worker.join();
+    }
+    for (auto& lane : lanes_) {
+        lane->engine.reset();
+        if (lane->stream) cudaStreamDestroy(lane->stream);
+        if (lane->ev0) cudaEventDestroy(lane->ev0);
+        if (lane->ev1) cudaEventDestroy(lane->ev1);
+    }
 }
 
 int Server::submit(std::unique_ptr<ServerRequest> r, int64_t& id) {
     std::lock_guard<std::mutex> lock(mu_);
     if (loop_status_ != EMERALD_OK) return loop_status_;
-    if (r->n_fluid > engine_->fluid_capacity() || r->n_solid > engine_->solid_capacity()) {
+    bool fits_empty = false;
+    for (auto const& lane : lanes_) {
+        fits_empty = fits_empty ||
+                     (r->n_fluid <= lane->engine->fluid_capacity() &&
+                      r->n_solid <= lane->engine->solid_capacity());
+    }
+    if (!fits_empty) {
         ++rejected_;
         return EMERALD_ENOSPC;
     }
@@ -94,17 +112,40 @@ int Server::submit(std::unique_ptr<ServerRequest> r, int64_t& id) {
     id = r->id;
     queue_.push_back(std::move(r));
     ++submitted_;
+    ++version_;
     work_cv_.notify_all();
     return EMERALD_OK;
 }
 
-// First fit in arrival order: every queued request that the arena has room
-// for now joins the batch; a large request that does not fit yet keeps its
-// place while smaller ones behind it start.
-void Server::admit_locked(std::unique_lock<std::mutex>& lock) {
-    (void)lock;
+int Server::preferred_lane(ServerRequest const& r) const {
+    int best = -1;
+    for (auto const& lane : lanes_) {
+        if (!lane->room.fits(r.n_fluid, r.n_solid)) continue;
+        if (best < 0 || lane->resident_particles < lanes_[size_t(best)]->resident_particles) {
+            best = lane->index;
+        }
+    }
+    return best;
+}
+
+void Server::resident_changed_locked(int delta) {
+    auto const now = std::chrono::steady_clock::now();
+    if (resident_ == 0 && delta > 0) busy_since_ = now;
+    resident_ += delta;
+    if (resident_ == 0 && delta < 0) busy_seconds_ += ms_between(busy_since_, now) / 1000.0;
+    resident_peak_ = std::max<int32_t>(resident_peak_, resident_);
+}
+
+// First fit in arrival order: every queued request for which this lane is
+// the least-loaded lane with room joins this lane's batch; a large request
+// that fits nowhere yet keeps its place while smaller ones behind it start.
+void Server::admit_locked(Lane& lane) {
     for (auto it = queue_.begin(); it != queue_.end();) {
         ServerRequest& r = **it;
+        if (preferred_lane(r) != lane.index) {
+            ++it;
+            continue;
+        }
         SceneSpec spec;
         spec.params = r.params;
         spec.method = cfg_.method;
@@ -115,12 +156,14 @@ void Server::admit_locked(std::unique_lock<std::mutex>& lock) {
         spec.fluid_xy = r.fluid_xy.data();
         spec.fluid_v = r.fluid_v.empty() ? nullptr : r.fluid_v.data();
         spec.n_fluid = r.n_fluid;
-        int const scene = engine_->add_scene(spec);
+        int const scene = lane.engine->add_scene(spec);
+        lane.room = lane.engine->room();
         if (scene < 0) {
             ++it;
             continue;
         }
-        engine_->set_active(scene, true);
+        lane.engine->set_active(scene, true);
+        r.lane = lane.index;
         r.scene = scene;
         r.admitted = std::chrono::steady_clock::now();
         queue_ms_.push_back(float(ms_between(r.submitted, r.admitted)));
@@ -129,137 +172,137 @@ void Server::admit_locked(std::unique_lock<std::mutex>& lock) {
         std::vector<float>().swap(r.solid_volumes);
         std::vector<float>().swap(r.fluid_xy);
         std::vector<float>().swap(r.fluid_v);
-        running_.push_back(std::move(*it));
+        lane.resident_particles += double(r.n_fluid);
+        lane.running.push_back(std::move(*it));
         it = queue_.erase(it);
-    }
-    resident_peak_ = std::max<int32_t>(resident_peak_, int32_t(running_.size()));
-}
-
-void Server::retire(std::vector<ServerRequest*> const& finished) {
-    for (ServerRequest* r : finished) {
-        r->x.resize(2ull * r->n_fluid);
-        r->v.resize(2ull * r->n_fluid);
-        engine_->get_state(r->scene, r->x.data(), r->v.data());
-        r->final_state = engine_->scene_state(r->scene);
-        engine_->remove_scene(r->scene);
+        resident_changed_locked(+1);
+        ++version_;
     }
 }
 
-void Server::loop() {
+void Server::loop(Lane& lane) {
     cudaSetDevice(device_);
-    auto busy_since = std::chrono::steady_clock::now();
-    bool busy = false;
+    Engine& engine = *lane.engine;
     std::unique_lock<std::mutex> lock(mu_);
     while (true) {
-        try {
-            admit_locked(lock);
-        } catch (std::exception const&) {
-            loop_status_ = EMERALD_ECUDA;
-        }
-        if (running_.empty()) {
-            if (busy) {
-                busy_seconds_ += ms_between(busy_since, std::chrono::steady_clock::now()) / 1000.0;
-                busy = false;
+        uint64_t const seen = version_;
+        if (!stop_ && loop_status_ == EMERALD_OK) {
+            try {
+                admit_locked(lane);
+            } catch (std::exception const&) {
+                loop_status_ = EMERALD_ECUDA;
             }
-            if (stop_ || loop_status_ != EMERALD_OK) break;
-            work_cv_.wait(lock, [this] { return stop_ || !queue_.empty(); });
-            continue;
         }
-        if (!busy) {
-            busy = true;
-            busy_since = std::chrono::steady_clock::now();
-        }
+        if (version_ != seen) work_cv_.notify_all();
         if (stop_ || loop_status_ != EMERALD_OK) {
             // drop what is resident: results of a stopped server are not read
-            for (auto& r : running_) engine_->remove_scene(r->scene);
-            running_.clear();
+            for (auto& r : lane.running) {
+                try {
+                    engine.remove_scene(r->scene);
+                } catch (std::exception const&) {
+                }
+                resident_changed_locked(-1);
+            }
+            lane.running.clear();
+            lane.resident_particles = 0.0;
+            done_cv_.notify_all();
+            break;
+        }
+        if (lane.running.empty()) {
+            uint64_t const now_seen = version_;
+            work_cv_.wait(lock, [&] { return stop_ || version_ != now_seen; });
             continue;
         }
         int32_t k = cfg_.max_substeps_per_launch;
         double particles = 0.0;
-        for (auto const& r : running_) {
+        for (auto const& r : lane.running) {
             k = std::min(k, r->remaining);
             particles += double(r->n_fluid);
         }
-        size_t const resident = running_.size();
+        size_t const resident = lane.running.size();
         lock.unlock();
         std::vector<float> step_ms(size_t(std::max(k, 0)));
         int status = EMERALD_OK;
         try {
             for (int32_t s = 0; s < k; ++s) {
-                cudaEventRecord(ev0_, engine_->stream());
-                engine_->substep(cfg_.method);
-                cudaEventRecord(ev1_, engine_->stream());
-                cudaEventSynchronize(ev1_);
-                cudaEventElapsedTime(&step_ms[size_t(s)], ev0_, ev1_);
+                cudaEventRecord(lane.ev0, lane.stream);
+                engine.substep(cfg_.method);
+                cudaEventRecord(lane.ev1, lane.stream);
+                cudaEventSynchronize(lane.ev1);
+                cudaEventElapsedTime(&step_ms[size_t(s)], lane.ev0, lane.ev1);
             }
-            engine_->check("server sub-step");
+            engine.check("server sub-step");
         } catch (std::exception const&) {
             status = EMERALD_ECUDA;
         }
-        lock.lock();
-        if (status != EMERALD_OK) {
-            loop_status_ = status;
-            for (auto& r : running_) {
-                r->done = true;
-                r->status = status;
-                r->finished = std::chrono::steady_clock::now();
-                finished_[r->id] = std::move(r);
-            }
-            running_.clear();
-            done_cv_.notify_all();
-            continue;
+        std::vector<ServerRequest*> fin;
+        for (auto& r : lane.running) {
+            r->remaining -= k;
+            if (r->remaining <= 0) fin.push_back(r.get());
         }
+        if (status == EMERALD_OK) {
+            try {
+                for (ServerRequest* r : fin) {
+                    r->x.resize(2ull * r->n_fluid);
+                    r->v.resize(2ull * r->n_fluid);
+                    engine.get_state(r->scene, r->x.data(), r->v.data());
+                    r->final_state = engine.scene_state(r->scene);
+                    engine.remove_scene(r->scene);
+                }
+            } catch (std::exception const&) {
+                status = EMERALD_ECUDA;
+            }
+        }
+        lock.lock();
         step_ms_.insert(step_ms_.end(), step_ms.begin(), step_ms.end());
         batch_substeps_ += k;
         scene_substeps_ += int64_t(k) * int64_t(resident);
         particle_substeps_ += double(k) * particles;
-        std::vector<ServerRequest*> fin;
-        for (auto& r : running_) {
-            r->remaining -= k;
-            if (r->remaining <= 0) fin.push_back(r.get());
+        lane.room = engine.room();
+        auto const now = std::chrono::steady_clock::now();
+        for (auto it = lane.running.begin(); it != lane.running.end();) {
+            ServerRequest& r = **it;
+            if (status == EMERALD_OK && r.remaining > 0) {
+                ++it;
+                continue;
+            }
+            r.status = status;
+            r.finished = now;
+            if (status == EMERALD_OK) {
+                request_ms_.push_back(float(ms_between(r.submitted, r.finished)));
+                ++completed_;
+            }
+            lane.resident_particles -= double(r.n_fluid);
+            resident_changed_locked(-1);
+            finished_[r.id] = std::move(*it);
+            it = lane.running.erase(it);
         }
-        if (!fin.empty()) {
-            lock.unlock();
-            try {
-                retire(fin);
-            } catch (std::exception const&) {
-                status = EMERALD_ECUDA;
-            }
-            lock.lock();
-            auto const now = std::chrono::steady_clock::now();
-            for (auto it = running_.begin(); it != running_.end();) {
-                if ((*it)->remaining <= 0) {
-                    ServerRequest& r = **it;
-                    r.done = true;
-                    r.status = status;
-                    r.finished = now;
-                    request_ms_.push_back(float(ms_between(r.submitted, r.finished)));
-                    ++completed_;
-                    finished_[r.id] = std::move(*it);
-                    it = running_.erase(it);
-                } else {
-                    ++it;
-                }
-            }
-            if (status != EMERALD_OK) loop_status_ = status;
+        if (status != EMERALD_OK) loop_status_ = status;
+        if (!fin.empty() || status != EMERALD_OK) {
+            ++version_;
+            work_cv_.notify_all();
             done_cv_.notify_all();
         }
     }
-    lock.unlock();
-    done_cv_.notify_all();
 }
 
 int Server::wait(int64_t id, int32_t timeout_ms, float* x, float* v, emerald_step_stats* stats,
                  emerald_request_timing* timing) {
     std::unique_lock<std::mutex> lock(mu_);
-    auto ready = [&] { return finished_.count(id) != 0 || loop_status_ != EMERALD_OK; };
-    bool known = finished_.count(id) != 0;
-    if (!known) {
-        for (auto const& r : queue_) known = known || r->id == id;
-        for (auto const& r : running_) known = known || r->id == id;
-    }
-    if (!known) return EMERALD_ENOTFOUND;
+    auto known = [&] {
+        if (finished_.count(id)) return true;
+        for (auto const& r : queue_) {
+            if (r->id == id) return true;
+        }
+        for (auto const& lane : lanes_) {
+            for (auto const& r : lane->running) {
+                if (r->id == id) return true;
+            }
+        }
+        return false;
+    };
+    if (!known()) return EMERALD_ENOTFOUND;
+    auto ready = [&] { return finished_.count(id) != 0 || loop_status_ != EMERALD_OK || stop_; };
     if (timeout_ms < 0) {
         done_cv_.wait(lock, ready);
     } else if (!done_cv_.wait_for(lock, std::chrono::milliseconds(timeout_ms), ready)) {
@@ -301,7 +344,7 @@ void Server::stats(emerald_server_stats& out) {
     out.completed = completed_;
     out.rejected = rejected_;
     out.queued = int64_t(queue_.size());
-    out.resident = int64_t(running_.size());
+    out.resident = int64_t(resident_);
     out.batch_substeps = batch_substeps_;
     out.scene_substeps = scene_substeps_;
     out.particle_substeps = particle_substeps_;
@@ -312,9 +355,11 @@ void Server::stats(emerald_server_stats& out) {
     out.request_ms_p99 = percentile(request_ms_, 0.99);
     out.queue_ms_p50 = percentile(queue_ms_, 0.50);
     out.queue_ms_p99 = percentile(queue_ms_, 0.99);
-    out.fluid_capacity = engine_->fluid_capacity();
-    out.solid_capacity = engine_->solid_capacity();
-    out.device_bytes = engine_->device_bytes();
+    for (auto const& lane : lanes_) {
+        out.fluid_capacity = std::max<size_t>(out.fluid_capacity, lane->engine->fluid_capacity());
+        out.solid_capacity = std::max<size_t>(out.solid_capacity, lane->engine->solid_capacity());
+        out.device_bytes += lane->engine->device_bytes();
+    }
     out.resident_peak = resident_peak_;
     out.status = loop_status_;
 }

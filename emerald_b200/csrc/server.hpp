@@ -1,9 +1,15 @@
-// Request loop over one batch arena: scene-simulation requests are admitted
-// while the arena (sized from a device-memory budget) has room, stay
-// resident on the device until their sub-steps are done, and are stepped
-// together with every other resident scene (continuous batching: a request
-// that arrives while others run joins at the next admission point, and a
-// finished one leaves and frees its room at once).
+// Request loop over batch arenas: scene-simulation requests are admitted
+// while an arena (sized from a device-memory budget) has room, stay resident
+// on the device until their sub-steps are done, and are stepped together
+// with every other scene of their arena (continuous batching: a request that
+// arrives while others run joins at the next admission point, and a finished
+// one leaves and frees its room at once).
+//
+// The budget is split over a few lanes, each an arena with its own stream
+// and worker thread. The scenes of one arena advance in lock step, so a
+// sub-step lasts as long as its slowest scene's solver loop; while one lane
+// runs the last iterations of a few unconverged scenes (small launches),
+// the other lanes' sub-steps fill the GPU.
 #pragma once
 
 #include <chrono>
@@ -28,10 +34,10 @@ struct ServerRequest {
     uint32_t n_fluid = 0, n_solid = 0;
     int32_t substeps = 0;
     // filled by the loop
+    int lane = -1;
     int scene = -1;
     int32_t remaining = 0;
     std::chrono::steady_clock::time_point submitted, admitted, finished;
-    bool done = false;
     int status = EMERALD_OK;
     std::vector<float> x, v;
     SceneState final_state{};
@@ -45,7 +51,7 @@ public:
     Server& operator=(Server const&) = delete;
 
     // Queues a request (inputs are copied). Returns EMERALD_ENOSPC when the
-    // scene can never fit the arena.
+    // scene can never fit an arena.
     int submit(std::unique_ptr<ServerRequest> r, int64_t& id);
     // Waits up to timeout_ms (negative: for ever) for the request's result,
     // copies it out and forgets the request. EMERALD_ETIMEOUT when not done.
@@ -54,20 +60,33 @@ public:
     void stats(emerald_server_stats& out);
 
 private:
-    void loop();
-    void admit_locked(std::unique_lock<std::mutex>& lock);
-    void retire(std::vector<ServerRequest*> const& finished);
+    struct Lane {
+        int index = 0;
+        std::unique_ptr<Engine> engine;
+        cudaStream_t stream = nullptr;
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        std::thread worker;
+        std::vector<std::unique_ptr<ServerRequest>> running;
+        // guarded by mu_
+        Engine::Room room{};
+        double resident_particles = 0.0;
+    };
+
+    void loop(Lane& lane);
+    // Lane that request r should join now: the least-loaded one with room.
+    int preferred_lane(ServerRequest const& r) const;
+    void admit_locked(Lane& lane);
+    void resident_changed_locked(int delta);
 
     emerald_server_config cfg_;
     int device_ = 0;
-    std::unique_ptr<Engine> engine_;
-    std::thread worker_;
-    std::mutex mu_;
+    std::vector<std::unique_ptr<Lane>> lanes_;
+    mutable std::mutex mu_;
     std::condition_variable work_cv_, done_cv_;
     bool stop_ = false;
+    uint64_t version_ = 0;  // bumped on every submit, admission and retirement
     int64_t next_id_ = 1;
     std::deque<std::unique_ptr<ServerRequest>> queue_;
-    std::vector<std::unique_ptr<ServerRequest>> running_;
     std::map<int64_t, std::unique_ptr<ServerRequest>> finished_;
     int loop_status_ = EMERALD_OK;
 
@@ -76,9 +95,10 @@ private:
     int64_t batch_substeps_ = 0, scene_substeps_ = 0;
     double particle_substeps_ = 0.0;
     double busy_seconds_ = 0.0;
+    int resident_ = 0;
+    std::chrono::steady_clock::time_point busy_since_;
     int32_t resident_peak_ = 0;
     std::vector<float> step_ms_, request_ms_, queue_ms_;
-    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
 };
 
 }  // namespace emerald

@@ -242,13 +242,15 @@ int emerald_batch_kernel_launches(emerald_batch* batch, int64_t* count);
 
 /* ----------------------------------------------------------------- serving */
 
-/* A request loop over one batch: requests (a scene and a sub-step count) are
- * queued by any host thread, admitted in arrival order as soon as the arena
+/* A request loop over batches: requests (a scene and a sub-step count) are
+ * queued by any host thread, admitted in arrival order as soon as an arena
  * has room for them (first fit: a large request waiting for room does not
- * hold back smaller ones behind it), stepped together with every other
- * resident scene, and retired as soon as their sub-steps are done, which
- * frees their room for the queue. The arena is sized once from the device
- * memory budget. No counterpart in the reference (one scene per process). */
+ * hold back smaller ones behind it; each goes to the least-loaded lane with
+ * room), stepped together with every other scene of its arena, and retired
+ * as soon as their sub-steps are done, which frees their room for the
+ * queue. The device memory budget is split evenly over `lanes` arenas, each
+ * with its own stream and host thread, sized once at creation. No
+ * counterpart in the reference (one scene per process). */
 typedef struct emerald_server emerald_server;
 
 typedef struct emerald_server_config {
@@ -256,7 +258,7 @@ typedef struct emerald_server_config {
     int32_t method;                  /* EMERALD_METHOD_* every request runs */
     int32_t max_scenes;              /* scenes resident at once */
     int32_t max_substeps_per_launch; /* sub-steps between admission points (0: 8) */
-    int32_t reserved;
+    int32_t lanes;                   /* arenas stepped concurrently (0: 4) */
 } emerald_server_config;
 
 typedef struct emerald_server_stats {
@@ -268,7 +270,8 @@ typedef struct emerald_server_stats {
     float step_ms_p50, step_ms_p99;       /* device time of one batched sub-step */
     float request_ms_p50, request_ms_p99; /* submit to result ready */
     float queue_ms_p50, queue_ms_p99;     /* submit to admission */
-    size_t fluid_capacity, solid_capacity, device_bytes;
+    size_t fluid_capacity, solid_capacity; /* of one lane */
+    size_t device_bytes;                   /* all lanes */
     int32_t resident_peak;
     int32_t status; /* first error of the loop, EMERALD_OK while healthy */
 } emerald_server_stats;

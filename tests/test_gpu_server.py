@@ -39,14 +39,14 @@ def alone(E, sc, n):
 
 
 def test_requests_equal_alone_under_continuous_batching(E):
-    srv = E.Server(3 << 20, "dfsph_p", max_scenes=8, max_substeps_per_launch=3)
-    cap = srv.stats()["fluid_capacity"]
-    assert cap >= 1000, cap
+    srv = E.Server(3 << 20, "dfsph_p", max_scenes=8, max_substeps_per_launch=3, lanes=2)
+    cap = srv.stats()["fluid_capacity"]  # of one lane
+    assert cap >= 512, cap
     jobs = [(12, None, 3, 7), (16, None, 4, 11), (20, 10, 5, 4), (14, None, 6, 9),
-            (10, 18, 7, 5), (16, None, 8, 6), (12, 12, 9, 10)]
+            (10, 18, 7, 5), (16, None, 8, 6), (12, 12, 9, 10), (18, None, 10, 5)]
     scenes = [scene(E, n, seed, ny) for n, ny, seed, _ in jobs]
     assert max(len(s.fluid) for s in scenes) <= cap
-    assert sum(len(s.fluid) for s in scenes) > cap  # not all fit at once
+    assert sum(len(s.fluid) for s in scenes) > 2 * cap  # not all fit at once
     ids = [None] * len(jobs)
 
     def client():
@@ -75,7 +75,7 @@ def test_requests_equal_alone_under_continuous_batching(E):
 
 
 def test_server_rejects_and_times_out(E):
-    srv = E.Server(4 << 20, "iisph", max_scenes=4)
+    srv = E.Server(4 << 20, "iisph", max_scenes=4, lanes=1)
     cap = srv.stats()["fluid_capacity"]
     big = scene(E, int(np.ceil(np.sqrt(cap))) + 8, 1)
     assert len(big.fluid) > cap
