@@ -15,6 +15,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libemerald_b200.so")
 
 METHODS = {"pcisph": 0, "iisph": 1, "iisph_ap": 2, "iisph_pseudo_ap": 3, "dfsph_p": 4}
+PRECISION_REFERENCE = 0
+PRECISION_COMPENSATED = 1
 FLICKS_PER_SECOND = 705600000
 
 c_f = ctypes.c_float
@@ -44,6 +46,7 @@ class Params(ctypes.Structure):
         ("dfsph_divergence_error_average_threshold", c_f),
         ("dfsph_divergence_error_max_threshold", c_f),
         ("mass_per_particle", c_f), ("pressure_correction_denom", c_f),
+        ("precision", c_i32),
     ]
 
     def as_dict(self):
@@ -55,7 +58,8 @@ class StepStats(ctypes.Structure):
         ("sub_steps", c_i32), ("pressure_iterations", c_i32), ("error_average", c_f),
         ("error_max", c_f), ("divergence_iterations", c_i32), ("divergence_error_average", c_f),
         ("divergence_error_max", c_f), ("dt", c_f), ("time_seconds", ctypes.c_double),
-        ("error_flags", c_i32),
+        ("error_flags", c_i32), ("error_average_exact", ctypes.c_double),
+        ("divergence_error_average_exact", ctypes.c_double),
     ]
 
     def as_dict(self):

@@ -271,6 +271,29 @@ __device__ __forceinline__ void write_entry(uint32_t* idx_out, float* w_out, flo
     gw_out[e] = g;
 }
 
+// Compensated mode: the entry's vector and distance come from the double
+// positions (x_i - x_j in double, rounded once), so that the rounding of
+// large coordinates does not enter the kernel values.
+__device__ __noinline__ void write_entry_precise(uint32_t* idx_out, float* w_out, float2* gw_out,
+                                                 size_t e, uint32_t j, double2 pos64,
+                                                 double2 const* x64o, float2 const* xo, float h) {
+    idx_out[e] = j;
+    double2 const xj = x64o ? x64o[j] : make_double2(double(xo[j].x), double(xo[j].y));
+    double const ddx = pos64.x - xj.x;
+    double const ddy = pos64.y - xj.y;
+    float2 const dp = mk2(static_cast<float>(ddx), static_cast<float>(ddy));
+    float const dist = static_cast<float>(sqrt(ddx * ddx + ddy * ddy));
+    float w, dw;
+    kernel_w_dw(dist, h, w, dw);
+    w_out[e] = w;
+    float2 g = mk2(0.0f, 0.0f);
+    if (safe_v(dp, dist)) {
+        float2 const u = div2(dp, dist);
+        g = mk2(u.x * dw, u.y * dw);
+    }
+    gw_out[e] = g;
+}
+
 template <bool SOLID_OTHER>
 __global__ void __launch_bounds__(kTile) k_neighbors(Arena a, int write_kernels) {
     int32_t const s = a.tile_scene[blockIdx.x];
@@ -303,6 +326,27 @@ __global__ void __launch_bounds__(kTile) k_neighbors(Arena a, int write_kernels)
     uint64_t r[kRegList];
     int const cnt = find_neighbors_reg(pos, i, !SOLID_OTHER, cell, cell, P.reject_l2, o, r);
     cnt_out[i] = static_cast<uint8_t>(cnt);
+    if (P.precision && kernels) {
+        double2 const pos64 = a.x64[i];
+        double2 const* x64o = SOLID_OTHER ? nullptr : a.x64;
+        uint64_t full[kMaxNeighbors];
+        int const n64 = cnt <= kRegList ? cnt : find_neighbors(pos, i, !SOLID_OTHER, cell, cell, o, full);
+#pragma unroll 1
+        for (int k = 0; k < n64; ++k) {
+            uint64_t key;
+            if (cnt <= kRegList) {
+                key = r[0];
+#pragma unroll
+                for (int q = 0; q + 1 < kRegList; ++q) r[q] = r[q + 1];
+            } else {
+                key = full[k];
+            }
+            write_entry_precise(idx_out, w_out, gw_out, static_cast<size_t>(k) * stride + i,
+                                stored_slot(o, static_cast<uint32_t>(key & 0xffffffffu)), pos64,
+                                x64o, o.x, h);
+        }
+        return;
+    }
     if (cnt <= kRegList) {
         // drain the sorted registers from the front: one copy of the entry
         // code, register moves instead of dynamic indexing

@@ -65,6 +65,9 @@ int check_params(emerald_params const* p) {
     if (!(p->target_density > 0.0f)) return fail(EMERALD_EINVAL, "target_density must be positive");
     if (p->time_per_step_flicks <= 0) return fail(EMERALD_EINVAL, "time_per_step must be positive");
     if (p->sub_steps <= 0) return fail(EMERALD_EINVAL, "sub_steps must be positive");
+    if (p->precision != EMERALD_PRECISION_REFERENCE && p->precision != EMERALD_PRECISION_COMPENSATED) {
+        return fail(EMERALD_EINVAL, "unknown precision mode");
+    }
     return EMERALD_OK;
 }
 
@@ -80,6 +83,8 @@ void fill_stats(SceneState const& s, emerald_step_stats* out, int substeps) {
     out->dt = s.dt;
     out->time_seconds = double(s.frame_time + s.elapsed) / 705600000.0;
     out->error_flags = s.error;
+    out->error_average_exact = s.stat_avg_exact;
+    out->divergence_error_average_exact = s.stat_div_avg_exact;
 }
 
 }  // namespace

@@ -107,6 +107,7 @@ size_t Engine::footprint(uint32_t fluid_capacity, uint32_t solid_capacity, int m
     size_t bytes = r(sizeof(SceneParams) * M) + r(sizeof(SceneState) * M) + r(4 * (N / kTile)) +
                    r(4 * (S / kTile));
     bytes += 12 * r(8 * N) + 18 * r(4 * N) + 2 * r(N);   // per-particle state and scratch
+    bytes += 2 * r(16 * N);                                 // double positions and their staging
     bytes += r(sort_scratch_bytes(uint32_t(N)));            // storage-order sort
     bytes += 2 * (2 * r(4 * E) + r(8 * E));                 // fluid and solid neighbour lists
     bytes += r(8 * ftab) + 2 * r(4 * ftab);                 // fluid cell table
@@ -181,6 +182,8 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
     a_.tkdiv = static_cast<float*>(dev(4 * N));
     a_.tkdens = static_cast<float*>(dev(4 * N));
     a_.toid = static_cast<uint32_t*>(dev(4 * N));
+    a_.x64 = static_cast<double2*>(dev(16 * N));
+    a_.tx64 = static_cast<double2*>(dev(16 * N));
     order_buf_ = dev(sort_scratch_bytes(uint32_t(N)));
     sort_scratch_carve(order_buf_, uint32_t(N), order_sort_);
     a_.nf_cnt = static_cast<uint8_t*>(dev(N));
@@ -428,6 +431,7 @@ int Engine::add_scene(SceneSpec const& spec) {
     P.fixed_dt = spec.fixed_dt;
     P.sort_base = 0;
     P.reject_l2 = reject_threshold(P.cell_size);
+    P.precision = ep.precision;
     scenes_[id] = sc;
 
     for (uint32_t t = 0; t < sc.ftile_count; ++t) tile_scene_[ft + t] = id;
@@ -449,6 +453,7 @@ int Engine::add_scene(SceneSpec const& spec) {
         cudaMemsetAsync(a_.kdens + P.fluid_begin, 0, 4ull * spec.n_fluid, st_);
         cudaMemsetAsync(a_.nf_cnt + P.fluid_begin, 0, spec.n_fluid, st_);
         launch_identity_order(a_, P.fluid_begin, spec.n_fluid, st_);
+        launch_positions_to_double(a_, P.fluid_begin, spec.n_fluid, st_);
         cudaMemsetAsync(a_.ns_cnt + P.fluid_begin, 0, spec.n_fluid, st_);
     }
     if (spec.n_solid) {
@@ -845,6 +850,7 @@ void Engine::set_state(int id, float const* x, float const* v) {
     if (x) {
         cudaMemcpyAsync(a_.tx + b, x, 8ull * n, cudaMemcpyHostToDevice, st_);
         launch_scatter_f2(a_, b, n, a_.tx + b, a_.x, st_);
+        launch_positions_to_double(a_, b, n, st_);
     }
     if (v) {
         cudaMemcpyAsync(a_.tv + b, v, 8ull * n, cudaMemcpyHostToDevice, st_);

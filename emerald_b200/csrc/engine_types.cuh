@@ -54,6 +54,7 @@ struct SceneParams {
     float fixed_dt;
     uint32_t sort_base;  // real particles of scenes stored before this one
     float reject_l2;     // smallest float whose sqrtf is >= cell_size
+    int32_t precision;   // 0: the reference's FP32 arithmetic; 1: compensated (DFSPH_P)
 };
 
 // Mutable per-scene state, device resident.
@@ -76,6 +77,8 @@ struct SceneState {
     int32_t error;
     int32_t substeps_total;
     int32_t pad;
+    double err_sum_d;  // exact sum of the errors (DFSPH loops)
+    double stat_avg_exact, stat_div_avg_exact;
 };
 
 // Raw device pointers of an arena, passed by value to every kernel.
@@ -119,6 +122,8 @@ struct Arena {
     float* tkdiv;
     float* tkdens;
     uint32_t* toid;
+    double2* x64;   // positions accumulated in double (compensated mode)
+    double2* tx64;
 
     // neighbour lists, slot-major
     uint8_t* nf_cnt;

@@ -52,6 +52,7 @@ void launch_gather_f2(Arena const& a, uint32_t begin, uint32_t count, float2 con
                       cudaStream_t st);
 void launch_scatter_f2(Arena const& a, uint32_t begin, uint32_t count, float2 const* in, float2* dst,
                        cudaStream_t st);
+void launch_positions_to_double(Arena const& a, uint32_t begin, uint32_t count, cudaStream_t st);
 void launch_identity_order(Arena const& a, uint32_t begin, uint32_t count, cudaStream_t st);
 
 // solver (solve_kernels.cu)

@@ -58,6 +58,7 @@ __global__ void k_permute(Arena a, uint64_t const* keys, uint32_t const* vals, u
     a.tkdiv[dst] = a.kdiv[old];
     a.tkdens[dst] = a.kdens[old];
     a.toid[dst] = a.oid[old];
+    a.tx64[dst] = a.x64[old];
 }
 
 __global__ void k_commit_order(Arena a, uint32_t n) {
@@ -71,6 +72,7 @@ __global__ void k_commit_order(Arena a, uint32_t n) {
     a.v[t] = a.tv[t];
     a.kdiv[t] = a.tkdiv[t];
     a.kdens[t] = a.tkdens[t];
+    a.x64[t] = a.tx64[t];
     uint32_t const o = a.toid[t];
     a.oid[t] = o;
     a.slot_of[P.fluid_begin + o] = t;
@@ -89,6 +91,15 @@ __global__ void k_gather_f2(Arena a, uint32_t begin, uint32_t count, float2 cons
 __global__ void k_scatter_f2(Arena a, uint32_t begin, uint32_t count, float2 const* in, float2* dst) {
     uint32_t const k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < count) dst[a.slot_of[begin + k]] = in[k];
+}
+
+// Double positions of a scene's particles from their float positions (at
+// creation and whenever the caller sets positions).
+__global__ void k_positions_to_double(Arena a, uint32_t begin, uint32_t count) {
+    uint32_t const k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    float2 const p = a.x[begin + k];
+    a.x64[begin + k] = make_double2(double(p.x), double(p.y));
 }
 
 __global__ void k_identity_order(Arena a, uint32_t begin, uint32_t count) {
@@ -118,6 +129,9 @@ void launch_gather_f2(Arena const& a, uint32_t begin, uint32_t count, float2 con
 void launch_scatter_f2(Arena const& a, uint32_t begin, uint32_t count, float2 const* in, float2* dst,
                        cudaStream_t st) {
     if (count) k_scatter_f2<<<(count + 255) / 256, 256, 0, st>>>(a, begin, count, in, dst);
+}
+void launch_positions_to_double(Arena const& a, uint32_t begin, uint32_t count, cudaStream_t st) {
+    if (count) k_positions_to_double<<<(count + 255) / 256, 256, 0, st>>>(a, begin, count);
 }
 void launch_identity_order(Arena const& a, uint32_t begin, uint32_t count, cudaStream_t st) {
     if (count) k_identity_order<<<(count + 255) / 256, 256, 0, st>>>(a, begin, count);

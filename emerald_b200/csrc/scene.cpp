@@ -82,6 +82,7 @@ void default_params(emerald_params& p) {
     p.dfsph_divergence_error_max_threshold = 0.03f;
     p.mass_per_particle = 0.0f;
     p.pressure_correction_denom = 0.0f;
+    p.precision = EMERALD_PRECISION_REFERENCE;
 }
 
 // Simulation_config::Simulation_config (emerald/sph2d_box/config.cpp:16-132):

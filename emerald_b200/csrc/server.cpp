@@ -328,6 +328,8 @@ int Server::wait(int64_t id, int32_t timeout_ms, float* x, float* v, emerald_ste
         stats->dt = s.dt;
         stats->time_seconds = double(s.frame_time + s.elapsed) / 705600000.0;
         stats->error_flags = s.error;
+        stats->error_average_exact = s.stat_avg_exact;
+        stats->divergence_error_average_exact = s.stat_div_avg_exact;
     }
     if (timing) {
         timing->queue_ms = ms_between(r->submitted, r->admitted);

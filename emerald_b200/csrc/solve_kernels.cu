@@ -45,31 +45,39 @@ __device__ __forceinline__ bool enter(Arena const& a, bool skip_done, Ctx& c) {
 // integer sum and the maximum of non-negative floats (bit order equals value
 // order for them). NaN contributions are dropped, as std::max and the
 // compare-exchange loop of update_atomic_max drop them.
-__device__ void accumulate_error(SceneState* S, unsigned long long v, float m, bool live) {
+__device__ void accumulate_error(SceneState* S, unsigned long long v, float m, bool live,
+                                 bool exact = false) {
     uint32_t mb = (live && m == m && m > 0.0f) ? __float_as_uint(m) : 0u;
     if (!live) v = 0ull;
+    double ed = (exact && live && m == m && m > 0.0f) ? static_cast<double>(m) : 0.0;
     for (int o = 16; o; o >>= 1) {
         v += __shfl_xor_sync(0xffffffffu, v, o);
         mb = max(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+        if (exact) ed += __shfl_xor_sync(0xffffffffu, ed, o);
     }
     __shared__ unsigned long long ws[kTile / 32];
     __shared__ uint32_t wm[kTile / 32];
+    __shared__ double wd[kTile / 32];
     int const lane = threadIdx.x & 31;
     int const warp = threadIdx.x >> 5;
     if (lane == 0) {
         ws[warp] = v;
         wm[warp] = mb;
+        wd[warp] = ed;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long t = 0;
         uint32_t tm = 0;
+        double td = 0.0;
         for (int w = 0; w < kTile / 32; ++w) {
             t += ws[w];
             tm = max(tm, wm[w]);
+            td += wd[w];
         }
         if (t) atomicAdd(&S->err_sum, t);
         if (tm) atomicMax(&S->err_max, tm);
+        if (exact && td != 0.0) atomicAdd(&S->err_sum_d, td);
     }
 }
 
@@ -191,6 +199,7 @@ __global__ void k_iter_reset(Arena a, int nscenes, int kind) {
     S.done = (S.active && iteration_cap(a.sp[s], kind) > 0) ? 0 : 1;
     S.err_sum = 0ull;
     S.err_max = 0u;
+    S.err_sum_d = 0.0;
 }
 
 // Exit test after one solver iteration. kind 0: IISPH family
@@ -211,6 +220,9 @@ __global__ void k_iter_check(Arena a, int nscenes, int kind, int* running,
         float const avg = P.fluid_count
                             ? static_cast<float>(static_cast<double>(S.err_sum) / n)
                             : 0.0f;
+        // the exact mean of the errors, reported beside the reference's
+        // metric (which drops each particle's error below 0.1%)
+        double const exact = P.fluid_count ? S.err_sum_d / static_cast<double>(P.fluid_count) : 0.0;
         float const mx = __uint_as_float(S.err_max);
         bool conv = false;
         int const max_iter = iteration_cap(P, kind);
@@ -223,12 +235,14 @@ __global__ void k_iter_check(Arena a, int nscenes, int kind, int* running,
                 conv = avg <= P.dfsph_dens_avg && mx <= P.dfsph_dens_max;
                 S.stat_avg = avg;
                 S.stat_max = mx;
+                S.stat_avg_exact = exact;
             }
         } else if (kind == 2) {
             if (S.iter > 0) {
                 conv = avg <= P.dfsph_div_avg && mx <= P.dfsph_div_max;
                 S.stat_div_avg = avg;
                 S.stat_div_max = mx;
+                S.stat_div_avg_exact = exact;
             }
         } else {
             if (S.iter > 1) {
@@ -239,6 +253,7 @@ __global__ void k_iter_check(Arena a, int nscenes, int kind, int* running,
         S.iter += 1;
         S.err_sum = 0ull;
         S.err_max = 0u;
+        S.err_sum_d = 0.0;
         if (conv || S.iter >= max_iter) {
             S.done = 1;
             if (kind == 2) {
@@ -285,12 +300,28 @@ __device__ __forceinline__ float density_of(Arena const& a, SceneParams const& P
 }
 
 // compute_divergences (emerald/sph_common/divergence.cpp:5-74).
+// With K, the fluid and boundary terms go into one Kahan-compensated sum.
+template <bool K = false>
 __device__ __forceinline__ float divergence_of(Arena const& a, SceneParams const& P, uint32_t i) {
     size_t const stride = a.stride;
     float const rho0 = P.rho0;
     float const fmass = rho0 * P.fluid_volume;
     float2 const vi = a.v[i];
     int const c = a.nf_cnt[i];
+    if (K) {
+        KahanF acc{0.0f, 0.0f};
+        for (int k = 0; k < c; ++k) {
+            size_t const e = k * stride + i;
+            kahan_add(acc, fmass * dot2(sub2(vi, a.v[a.nf_idx[e]]), a.nf_gw[e]));
+        }
+        int const cs = a.ns_cnt[i];
+        for (int k = 0; k < cs; ++k) {
+            size_t const e = k * stride + i;
+            uint32_t const j = a.ns_idx[e];
+            kahan_add(acc, (rho0 * a.vols[j]) * dot2(sub2(vi, a.vs[j]), a.ns_gw[e]));
+        }
+        return acc.s;
+    }
     float d = 0.0f;
     #pragma unroll 4
 
@@ -314,7 +345,9 @@ __device__ __forceinline__ float divergence_of(Arena const& a, SceneParams const
 }
 
 // apply_pressures_in_place (emerald/sph_common/pressure.cpp:9-80) for one
-// particle, with q = safe_divide(p, rho^2) precomputed per particle.
+// particle, with q = safe_divide(p, rho^2) precomputed per particle. With K,
+// each sum is Kahan-compensated.
+template <bool K = false>
 __device__ __forceinline__ float2 apply_pressure_of(Arena const& a, SceneParams const& P, uint32_t i,
                                                     float2 v, float const* q, float dt) {
     size_t const stride = a.stride;
@@ -322,6 +355,26 @@ __device__ __forceinline__ float2 apply_pressure_of(Arena const& a, SceneParams 
     float const neg_fmass = -(rho0 * P.fluid_volume);
     float const qi = q[i];
     int const c = a.nf_cnt[i];
+    if (K) {
+        if (c) {
+            KahanF2 acc{{0.0f, 0.0f}, {0.0f, 0.0f}};
+            for (int k = 0; k < c; ++k) {
+                size_t const e = k * stride + i;
+                kahan_add(acc, scl2(neg_fmass * (qi + q[a.nf_idx[e]]), a.nf_gw[e]));
+            }
+            v = add2(v, scl2(dt, mk2(acc.x.s, acc.y.s)));
+        }
+        int const cs = a.ns_cnt[i];
+        if (cs) {
+            KahanF2 acc{{0.0f, 0.0f}, {0.0f, 0.0f}};
+            for (int k = 0; k < cs; ++k) {
+                size_t const e = k * stride + i;
+                kahan_add(acc, scl2(-(rho0 * a.vols[a.ns_idx[e]]) * qi, a.ns_gw[e]));
+            }
+            v = add2(v, scl2(dt, mk2(acc.x.s, acc.y.s)));
+        }
+        return v;
+    }
     if (c) {
         float2 acc = mk2(0.0f, 0.0f);
         #pragma unroll 4
@@ -394,9 +447,9 @@ __device__ __forceinline__ float2 integrate_external(SceneParams const& P, float
 
 // compute_densities + dfsph_p_compute_shared_coeffs (dfsph_p_ops.cpp:19-72),
 // the per-frame kappa reset, and the p/rho^2 caches of both warm starts.
-__global__ void k_dfsph_density_alpha(Arena a) {
-    Ctx c;
-    if (!enter(a, false, c) || !c.live) return;
+// With K, the density and the two alpha sums are Kahan-compensated.
+template <bool K>
+__device__ __forceinline__ void dfsph_density_alpha(Arena const& a, Ctx const& c) {
     SceneParams const& P = a.sp[c.s];
     uint32_t const i = c.i;
     size_t const stride = a.stride;
@@ -405,6 +458,8 @@ __global__ void k_dfsph_density_alpha(Arena a) {
     float d = fvol * rho0 * P.w0;
     float2 sum = mk2(0.0f, 0.0f);
     float sdot = 0.0f;
+    KahanF kd{d, 0.0f}, ksdot{0.0f, 0.0f};
+    KahanF2 ksum{{0.0f, 0.0f}, {0.0f, 0.0f}};
     int const cf = a.nf_cnt[i];
     float const fmass = rho0 * fvol;
     float const fmass_a = fvol * rho0;
@@ -412,10 +467,16 @@ __global__ void k_dfsph_density_alpha(Arena a) {
 
     for (int k = 0; k < cf; ++k) {
         size_t const e = k * stride + i;
-        d += a.nf_w[e] * fmass;
         float2 const m = scl2(fmass_a, a.nf_gw[e]);
-        sum = add2(sum, m);
-        sdot += dot2(m, m);
+        if (K) {
+            kahan_add(kd, a.nf_w[e] * fmass);
+            kahan_add(ksum, m);
+            kahan_add(ksdot, dot2(m, m));
+        } else {
+            d += a.nf_w[e] * fmass;
+            sum = add2(sum, m);
+            sdot += dot2(m, m);
+        }
     }
     int const cs = a.ns_cnt[i];
     if (cs) {
@@ -425,10 +486,20 @@ __global__ void k_dfsph_density_alpha(Arena a) {
         for (int k = 0; k < cs; ++k) {
             size_t const e = k * stride + i;
             float const vs = a.vols[a.ns_idx[e]];
-            db += a.ns_w[e] * (rho0 * vs);
-            sum = add2(sum, scl2(vs * rho0, a.ns_gw[e]));
+            if (K) {
+                kahan_add(kd, a.ns_w[e] * (rho0 * vs));
+                kahan_add(ksum, scl2(vs * rho0, a.ns_gw[e]));
+            } else {
+                db += a.ns_w[e] * (rho0 * vs);
+                sum = add2(sum, scl2(vs * rho0, a.ns_gw[e]));
+            }
         }
-        d += db;
+        if (!K) d += db;
+    }
+    if (K) {
+        d = kd.s;
+        sum = mk2(ksum.x.s, ksum.y.s);
+        sdot = ksdot.s;
     }
     a.rho[i] = d;
     float alpha = 0.0f;
@@ -438,16 +509,26 @@ __global__ void k_dfsph_density_alpha(Arena a) {
         alpha = safe_f(numer, denom) ? numer / denom : 0.0f;
     }
     a.alpha[i] = alpha;
-    float kd = a.kdiv[i];
+    float kd0 = a.kdiv[i];
     float kn = a.kdens[i];
     if (a.ss[c.s].new_frame) {
-        kd = 0.0f;
+        kd0 = 0.0f;
         kn = 0.0f;
-        a.kdiv[i] = kd;
+        a.kdiv[i] = kd0;
         a.kdens[i] = kn;
     }
-    a.qdiv[i] = p_over_rho2(kd, d);
+    a.qdiv[i] = p_over_rho2(kd0, d);
     a.qdens[i] = p_over_rho2(kn, d);
+}
+
+__global__ void k_dfsph_density_alpha(Arena a) {
+    Ctx c;
+    if (!enter(a, false, c) || !c.live) return;
+    if (a.sp[c.s].precision) {
+        dfsph_density_alpha<true>(a, c);
+    } else {
+        dfsph_density_alpha<false>(a, c);
+    }
 }
 
 // apply_pressures_in_place over the cached q; with `external`, the velocity
@@ -460,7 +541,9 @@ __global__ void k_apply_pressures(Arena a, int which_q, int external, int skip_d
     float const dt = a.ss[c.s].dt;
     float2 v = a.v[c.i];
     if (external) v = integrate_external(P, v, dt);
-    a.v[c.i] = apply_pressure_of(a, P, c.i, v, which_q ? a.qdens : a.qdiv, dt);
+    float const* q = which_q ? a.qdens : a.qdiv;
+    a.v[c.i] = P.precision ? apply_pressure_of<true>(a, P, c.i, v, q, dt)
+                           : apply_pressure_of<false>(a, P, c.i, v, q, dt);
 }
 
 // compute_divergences + dfsph_p_compute_divergence_pseudo_pressures
@@ -474,7 +557,7 @@ __global__ void k_dfsph_divergence(Arena a) {
     float err = 0.0f;
     if (c.live) {
         uint32_t const i = c.i;
-        float const d = divergence_of(a, P, i);
+        float const d = P.precision ? divergence_of<true>(a, P, i) : divergence_of<false>(a, P, i);
         a.rho_star[i] = d;
         float kappa = 0.0f;
         if (!(d <= 0.0f)) {
@@ -486,7 +569,7 @@ __global__ void k_dfsph_divergence(Arena a) {
         err = d <= 0.0f ? 0.0f : (dt * d / P.rho0);
     }
     accumulate_error(S, static_cast<unsigned long long>(static_cast<long long>(err * 1000.0f)),
-                     err, c.live);
+                     err, c.live, true);
 }
 
 // predict_density_stars (density.cpp:75-109) +
@@ -503,7 +586,8 @@ __global__ void k_dfsph_density(Arena a) {
     if (c.live) {
         uint32_t const i = c.i;
         float const rho = a.rho[i];
-        float const star = max_0x(rho + (dt * divergence_of(a, P, i)));
+        float const div = P.precision ? divergence_of<true>(a, P, i) : divergence_of<false>(a, P, i);
+        float const star = max_0x(rho + (dt * div));
         a.rho_star[i] = star;
         float const delta = star - rho0;
         float kappa = 0.0f;
@@ -517,14 +601,24 @@ __global__ void k_dfsph_density(Arena a) {
         err = delta <= 0.0f ? 0.0f : (delta / rho0);
     }
     accumulate_error(S, static_cast<unsigned long long>(static_cast<long long>(err * 1000.0f)),
-                     err, c.live);
+                     err, c.live, true);
 }
 
-// integrate_positions_in_place (dynamics.cpp:46-51).
+// integrate_positions_in_place (dynamics.cpp:46-51). Compensated mode
+// accumulates the positions in double and stores their float rounding.
 __global__ void k_integrate_positions(Arena a) {
     Ctx c;
     if (!enter(a, false, c) || !c.live) return;
     float const dt = a.ss[c.s].dt;
+    if (a.sp[c.s].precision) {
+        float2 const v = a.v[c.i];
+        double2 x = a.x64[c.i];
+        x.x += static_cast<double>(dt) * static_cast<double>(v.x);
+        x.y += static_cast<double>(dt) * static_cast<double>(v.y);
+        a.x64[c.i] = x;
+        a.x[c.i] = mk2(static_cast<float>(x.x), static_cast<float>(x.y));
+        return;
+    }
     a.x[c.i] = add2(a.x[c.i], scl2(dt, a.v[c.i]));
 }
 

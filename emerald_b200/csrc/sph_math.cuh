@@ -71,6 +71,26 @@ EMLD_HD float length2f(float2 a) {
     return sqrtf(l2);
 }
 
+// Kahan-compensated running sums (Kahan 1965): s holds the sum, c the
+// low-order part lost by the last addition. Exact under IEEE arithmetic
+// without contraction, which these sources are compiled for.
+struct KahanF {
+    float s, c;
+};
+struct KahanF2 {
+    KahanF x, y;
+};
+EMLD_HD void kahan_add(KahanF& k, float v) {
+    float const y = v - k.c;
+    float const t = k.s + y;
+    k.c = (t - k.s) - y;
+    k.s = t;
+}
+EMLD_HD void kahan_add(KahanF2& k, float2 v) {
+    kahan_add(k.x, v.x);
+    kahan_add(k.y, v.y);
+}
+
 // Cubic spline with the reference's 3D normalisation 1/(pi h^3), support 2h
 // (emerald/sph_common/kernels.h:12-64).
 constexpr float kPi = 3.14159274101257324218750f;

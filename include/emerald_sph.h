@@ -63,7 +63,18 @@ typedef struct emerald_params {
     float dfsph_divergence_error_max_threshold;
     float mass_per_particle;
     float pressure_correction_denom;
+    int32_t precision; /* EMERALD_PRECISION_*; not in the reference */
 } emerald_params;
+
+/* Arithmetic of a scene. REFERENCE (default): the reference's FP32
+ * operations in its order, bit-identical results. COMPENSATED (DFSPH_P
+ * only; other methods keep REFERENCE): neighbour sums in FP32 with Kahan
+ * compensation, positions accumulated in FP64 and the neighbour vectors
+ * x_i - x_j taken from them. The solver's exit test is the reference's in
+ * both modes (an exact int64 sum and an FP64 division); the exact FP64 mean
+ * of the errors is reported in emerald_step_stats. */
+#define EMERALD_PRECISION_REFERENCE 0
+#define EMERALD_PRECISION_COMPENSATED 1
 
 /* Statistics of the last sub-step (or of the last sub-step of a frame). The
  * reference keeps these in local variables; they are returned here. */
@@ -78,6 +89,11 @@ typedef struct emerald_step_stats {
     float dt;
     double time_seconds;
     int32_t error_flags;
+    /* DFSPH_P: the exact mean of the per-particle errors (FP64 sum), beside
+     * the reference's metric above, sum(int64(err * 1000)) / (1000 n), which
+     * drops every particle's error below 0.1%. */
+    double error_average_exact;
+    double divergence_error_average_exact;
 } emerald_step_stats;
 
 /* ---------------------------------------------------------------- setup */

@@ -1,4 +1,4 @@
-"""Test infrastructure: builds the two CPU checkers used by tests and bench.
+"""Test infrastructure: builds the checkers used by tests and bench.
 
 1. ``oracle/liboracle_sph.so`` — the project's own C restatement of the
    reference SPH path (``oracle/sph_oracle.c``).
@@ -8,9 +8,13 @@
    Built only where ``/root/reference`` exists; the built file is git-ignored
    but travels with the working tree.
 
-Both are compiled ``-O2 -ffp-contract=off`` (IEEE single-precision operations
-in source order, as the reference's own CMake build with CXX_EXTENSIONS OFF
-gives on x86-64).
+3. ``oracle/libfp64_oracle.so`` — the FP64 GPU oracle of the DFSPH_P
+   sub-step (``oracle/fp64/dfsph_fp64.cu``), which states the error of the
+   FP32 results; used by tests only.
+
+The first two are compiled ``-O2 -ffp-contract=off`` (IEEE single-precision
+operations in source order, as the reference's own CMake build with
+CXX_EXTENSIONS OFF gives on x86-64).
 """
 import os
 import subprocess
@@ -22,6 +26,7 @@ REF_ROOT = "/root/reference"
 REF_OUT = os.path.join(HERE, "_ref")
 ORACLE_SO = os.path.join(HERE, "liboracle_sph.so")
 REF_SO = os.path.join(REF_OUT, "libemerald_ref.so")
+FP64_SO = os.path.join(HERE, "libfp64_oracle.so")
 
 REF_SOURCES = [
     "emerald/z_index/z_index.cpp",
@@ -72,6 +77,16 @@ def build_oracle(force=False):
     return ORACLE_SO
 
 
+def build_fp64(force=False):
+    src = os.path.join(HERE, "fp64", "dfsph_fp64.cu")
+    if not force and _newer(FP64_SO, [src, __file__]):
+        return FP64_SO
+    nvcc = "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else "nvcc"
+    _run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-shared",
+          "-Xcompiler", "-fPIC", "-cudart", "static", "-o", FP64_SO, src])
+    return FP64_SO
+
+
 def build_reference(force=False):
     if not os.path.isdir(REF_ROOT):
         return REF_SO if os.path.exists(REF_SO) else None
@@ -102,6 +117,7 @@ def main():
     force = "--force" in sys.argv
     if os.path.exists(os.path.join(HERE, "sph_oracle.c")):
         print(build_oracle(force))
+    print(build_fp64(force))
     print(build_reference(force))
 
 

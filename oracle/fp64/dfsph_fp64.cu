@@ -1,0 +1,416 @@
+// FP64 GPU oracle of the DFSPH_P sub-step: test infrastructure only.
+//
+// The same formulas and neighbour-list order as the reference's sph_common
+// and dfsph_p code (cubic spline W/GradW, emerald/sph_common/kernels.h:12-64;
+// densities, emerald/sph_common/density.cpp:10-73; divergences,
+// emerald/sph_common/divergence.cpp:5-74; apply_pressures_in_place,
+// emerald/sph_common/pressure.cpp:9-80; DFSPH_P coefficients and pseudo
+// pressures, emerald/sph2d_box/dfsph_p_ops.cpp:19-126; the sub-step order of
+// emerald/sph2d_box/dfsph_p.cpp:325-373), evaluated in double. It states the
+// error of the FP32 results: the caller passes each sub-step's dt and the
+// iteration counts the FP32 run took, so the two runs differ only in
+// arithmetic precision.
+//
+// Independent of the product's kernels: neighbours come from a sort of
+// (cell key, index) pairs and a binary search per cell, lists are built by
+// sorted insertion on (distance, index), and every loop is a plain
+// one-thread-per-particle kernel driven from the host.
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include <cuda_runtime.h>
+#include <thrust/device_ptr.h>
+#include <thrust/sort.h>
+
+namespace {
+
+constexpr int kMax = 64;
+constexpr double kPi = 3.14159274101257324218750;  // the reference's float pi, widened
+
+struct Params {
+    double support, rho0, mass, fluid_volume, gravity;
+};
+
+struct Sim {
+    Params p;
+    size_t n = 0, ns = 0;
+    double2 *x = nullptr, *v = nullptr, *xs = nullptr;
+    double* vols = nullptr;
+    double *rho = nullptr, *alpha = nullptr, *kdiv = nullptr, *kdens = nullptr, *qdiv = nullptr,
+           *qdens = nullptr, *rho_star = nullptr, *div = nullptr;
+    // neighbour lists, slot-major: entry k of particle i at k * n + i
+    int *fcnt = nullptr, *scnt = nullptr, *fidx = nullptr, *sidx = nullptr;
+    double *fw = nullptr, *sw = nullptr;
+    double2 *fgw = nullptr, *sgw = nullptr;
+    // cell sort of fluid and solid particles
+    unsigned long long *fkeys = nullptr, *skeys = nullptr;
+    int *fvals = nullptr, *svals = nullptr;
+};
+
+__host__ __device__ double kernel_w(double r, double h) {
+    double const q = r / h;
+    double const k = h * h * h * kPi;
+    if (q <= 1.0) return (1.0 + q * q * (q * 0.75 - 1.5)) / k;
+    if (q <= 2.0) {
+        double const t = 2.0 - q;
+        return ((t * t * t) / 4.0) / k;
+    }
+    return 0.0;
+}
+
+__host__ __device__ double kernel_dw(double r, double h) {
+    double const q = r / h;
+    double const k = h * h * h * kPi;
+    if (q <= 1.0) return (-3.0 * r / (h * h) + 2.25 * r * r / (h * h * h)) / k;
+    if (q <= 2.0) {
+        double const t = 2.0 - q;
+        return (-3.0 * t * t / (4.0 * h)) / k;
+    }
+    return 0.0;
+}
+
+__device__ unsigned long long cell_key(double2 p, double cell) {
+    long long const gx = static_cast<long long>(floor(p.x / cell)) + (1ll << 30);
+    long long const gy = static_cast<long long>(floor(p.y / cell)) + (1ll << 30);
+    return (static_cast<unsigned long long>(gy) << 32) | static_cast<unsigned long long>(gx);
+}
+
+__global__ void k_keys(double2 const* x, size_t n, double cell, unsigned long long* keys, int* vals) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    keys[i] = cell_key(x[i], cell);
+    vals[i] = int(i);
+}
+
+__device__ size_t lower_bound(unsigned long long const* keys, size_t n, unsigned long long key) {
+    size_t lo = 0, hi = n;
+    while (lo < hi) {
+        size_t const mid = (lo + hi) / 2;
+        if (keys[mid] < key) {
+            lo = mid + 1;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
+// Neighbours of fluid particle i among `other` (fluid or solid) within
+// 2 * support, self excluded, ordered by (distance, index), at most kMax.
+__global__ void k_neighbors(Sim s, double2 const* other, size_t n_other,
+                            unsigned long long const* keys, int const* vals, bool self_set,
+                            int* cnt, int* idx, double* w, double2* gw) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const h = s.p.support;
+    double const cell = 2.0 * h;
+    double2 const xi = s.x[i];
+    unsigned long long const k0 = cell_key(xi, cell);
+    double ld[kMax];
+    int lj[kMax];
+    int m = 0;
+    for (int dy = -1; dy <= 1; ++dy) {
+        for (int dx = -1; dx <= 1; ++dx) {
+            unsigned long long const key =
+              k0 + (static_cast<unsigned long long>(static_cast<long long>(dy)) << 32) +
+              static_cast<unsigned long long>(static_cast<long long>(dx));
+            for (size_t q = lower_bound(keys, n_other, key); q < n_other && keys[q] == key; ++q) {
+                int const j = vals[q];
+                if (self_set && size_t(j) == i) continue;
+                double const ddx = other[j].x - xi.x;
+                double const ddy = other[j].y - xi.y;
+                double const d = sqrt(ddx * ddx + ddy * ddy);
+                if (!(d < cell)) continue;
+                // sorted insertion on (d, j), keeping the first kMax
+                int pos = m;
+                while (pos > 0 && (ld[pos - 1] > d || (ld[pos - 1] == d && lj[pos - 1] > j))) --pos;
+                if (pos >= kMax) continue;
+                int const last = m < kMax ? m : kMax - 1;
+                for (int t = last; t > pos; --t) {
+                    ld[t] = ld[t - 1];
+                    lj[t] = lj[t - 1];
+                }
+                ld[pos] = d;
+                lj[pos] = j;
+                if (m < kMax) ++m;
+            }
+        }
+    }
+    cnt[i] = m;
+    for (int k = 0; k < m; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        int const j = lj[k];
+        double const d = ld[k];
+        idx[e] = j;
+        w[e] = kernel_w(d, h);
+        double2 g = make_double2(0.0, 0.0);
+        if (d > 0.0) {
+            double const dw = kernel_dw(d, h);
+            g = make_double2((xi.x - other[j].x) / d * dw, (xi.y - other[j].y) / d * dw);
+        }
+        gw[e] = g;
+    }
+}
+
+__device__ double q_of(double p, double rho) {
+    double const d = rho * rho;
+    return d != 0.0 ? p / d : 0.0;
+}
+
+__global__ void k_density_alpha(Sim s, int new_frame) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const rho0 = s.p.rho0, fvol = s.p.fluid_volume;
+    double const fmass = rho0 * fvol;
+    double d = fvol * rho0 * kernel_w(0.0, s.p.support);
+    double2 sum = make_double2(0.0, 0.0);
+    double sdot = 0.0;
+    int const cf = s.fcnt[i];
+    for (int k = 0; k < cf; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        d += s.fw[e] * fmass;
+        double2 const m = make_double2(fmass * s.fgw[e].x, fmass * s.fgw[e].y);
+        sum.x += m.x;
+        sum.y += m.y;
+        sdot += m.x * m.x + m.y * m.y;
+    }
+    int const cs = s.scnt[i];
+    double db = 0.0;
+    for (int k = 0; k < cs; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        double const vs = s.vols[s.sidx[e]];
+        db += s.sw[e] * (rho0 * vs);
+        sum.x += vs * rho0 * s.sgw[e].x;
+        sum.y += vs * rho0 * s.sgw[e].y;
+    }
+    d += db;
+    s.rho[i] = d;
+    double alpha = 0.0;
+    if (cf + cs) {
+        double const denom = sum.x * sum.x + sum.y * sum.y + sdot;
+        alpha = denom != 0.0 ? d * d / denom : 0.0;
+    }
+    s.alpha[i] = alpha;
+    if (new_frame) {
+        s.kdiv[i] = 0.0;
+        s.kdens[i] = 0.0;
+    }
+    s.qdiv[i] = q_of(s.kdiv[i], d);
+    s.qdens[i] = q_of(s.kdens[i], d);
+}
+
+__global__ void k_apply(Sim s, double const* q, double dt, int external) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const rho0 = s.p.rho0;
+    double const neg_fmass = -(rho0 * s.p.fluid_volume);
+    double2 v = s.v[i];
+    if (external) {
+        double const denom = rho0 * s.p.fluid_volume;
+        v.y += dt * (-(s.p.mass * s.p.gravity)) / denom;
+    }
+    double const qi = q[i];
+    double2 acc = make_double2(0.0, 0.0);
+    int const c = s.fcnt[i];
+    for (int k = 0; k < c; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        double const f = neg_fmass * (qi + q[s.fidx[e]]);
+        acc.x += f * s.fgw[e].x;
+        acc.y += f * s.fgw[e].y;
+    }
+    v.x += dt * acc.x;
+    v.y += dt * acc.y;
+    acc = make_double2(0.0, 0.0);
+    int const cs = s.scnt[i];
+    for (int k = 0; k < cs; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        double const f = -(rho0 * s.vols[s.sidx[e]]) * qi;
+        acc.x += f * s.sgw[e].x;
+        acc.y += f * s.sgw[e].y;
+    }
+    v.x += dt * acc.x;
+    v.y += dt * acc.y;
+    s.v[i] = v;
+}
+
+__device__ double divergence(Sim const& s, size_t i) {
+    double const rho0 = s.p.rho0;
+    double const fmass = rho0 * s.p.fluid_volume;
+    double2 const vi = s.v[i];
+    double d = 0.0;
+    int const c = s.fcnt[i];
+    for (int k = 0; k < c; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        double2 const vj = s.v[s.fidx[e]];
+        d += fmass * ((vi.x - vj.x) * s.fgw[e].x + (vi.y - vj.y) * s.fgw[e].y);
+    }
+    double db = 0.0;
+    int const cs = s.scnt[i];
+    for (int k = 0; k < cs; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        int const j = s.sidx[e];
+        db += (rho0 * s.vols[j]) * (vi.x * s.sgw[e].x + vi.y * s.sgw[e].y);  // solids at rest
+    }
+    return d + db;
+}
+
+// Divergence step (kind 0) or density step (kind 1) of one solver iteration.
+__global__ void k_kappa(Sim s, double dt, int kind) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const d = divergence(s, i);
+    s.div[i] = d;
+    if (kind == 0) {
+        double const kappa = d > 0.0 ? d * s.alpha[i] / dt : 0.0;
+        s.kdiv[i] = kappa;
+        s.qdiv[i] = q_of(kappa, s.rho[i]);
+    } else {
+        double star = s.rho[i] + dt * d;
+        if (star < 0.0) star = 0.0;
+        s.rho_star[i] = star;
+        double const delta = star - s.p.rho0;
+        double const kappa = delta > 0.0 ? delta * s.alpha[i] / (dt * dt) : 0.0;
+        s.kdens[i] = kappa;
+        s.qdens[i] = q_of(kappa, s.rho[i]);
+    }
+}
+
+__global__ void k_positions(Sim s, double dt) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    s.x[i].x += dt * s.v[i].x;
+    s.x[i].y += dt * s.v[i].y;
+}
+
+template <class T>
+T* dalloc(size_t count) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, count * sizeof(T) + 16) != cudaSuccess) return nullptr;
+    return static_cast<T*>(p);
+}
+
+unsigned grid(size_t n) { return unsigned((n + 127) / 128); }
+
+void sort_cells(double2 const* x, size_t n, double cell, unsigned long long* keys, int* vals) {
+    if (!n) return;
+    k_keys<<<grid(n), 128>>>(x, n, cell, keys, vals);
+    thrust::sort_by_key(thrust::device_ptr<unsigned long long>(keys),
+                        thrust::device_ptr<unsigned long long>(keys + n),
+                        thrust::device_ptr<int>(vals));
+}
+
+}  // namespace
+
+extern "C" {
+
+typedef struct fp64_params {
+    double support, rho0, mass, fluid_volume, gravity;
+} fp64_params;
+
+int fp64_create(fp64_params const* p, double const* solid_xy, double const* solid_vols, size_t ns,
+                double const* fluid_xy, double const* fluid_v, size_t n, void** out) {
+    Sim* s = new Sim;
+    s->p = Params{p->support, p->rho0, p->mass, p->fluid_volume, p->gravity};
+    s->n = n;
+    s->ns = ns;
+    size_t const E = n * kMax;
+    s->x = dalloc<double2>(n);
+    s->v = dalloc<double2>(n);
+    s->xs = dalloc<double2>(ns);
+    s->vols = dalloc<double>(ns);
+    s->rho = dalloc<double>(n);
+    s->alpha = dalloc<double>(n);
+    s->kdiv = dalloc<double>(n);
+    s->kdens = dalloc<double>(n);
+    s->qdiv = dalloc<double>(n);
+    s->qdens = dalloc<double>(n);
+    s->rho_star = dalloc<double>(n);
+    s->div = dalloc<double>(n);
+    s->fcnt = dalloc<int>(n);
+    s->scnt = dalloc<int>(n);
+    s->fidx = dalloc<int>(E);
+    s->sidx = dalloc<int>(E);
+    s->fw = dalloc<double>(E);
+    s->sw = dalloc<double>(E);
+    s->fgw = dalloc<double2>(E);
+    s->sgw = dalloc<double2>(E);
+    s->fkeys = dalloc<unsigned long long>(n);
+    s->skeys = dalloc<unsigned long long>(ns);
+    s->fvals = dalloc<int>(n);
+    s->svals = dalloc<int>(ns);
+    if (!s->sgw || !s->svals || !s->fvals) return 12;
+    cudaMemcpy(s->x, fluid_xy, 16 * n, cudaMemcpyHostToDevice);
+    if (fluid_v) {
+        cudaMemcpy(s->v, fluid_v, 16 * n, cudaMemcpyHostToDevice);
+    } else {
+        cudaMemset(s->v, 0, 16 * n);
+    }
+    cudaMemcpy(s->xs, solid_xy, 16 * ns, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->vols, solid_vols, 8 * ns, cudaMemcpyHostToDevice);
+    cudaMemset(s->kdiv, 0, 8 * n);
+    cudaMemset(s->kdens, 0, 8 * n);
+    sort_cells(s->xs, ns, 2.0 * s->p.support, s->skeys, s->svals);
+    *out = s;
+    return cudaGetLastError() == cudaSuccess ? 0 : 1000;
+}
+
+int fp64_destroy(void* h) {
+    Sim* s = static_cast<Sim*>(h);
+    void* ptrs[] = {s->x,    s->v,    s->xs,    s->vols,  s->rho,   s->alpha, s->kdiv,
+                    s->kdens, s->qdiv, s->qdens, s->rho_star, s->div, s->fcnt,  s->scnt,
+                    s->fidx, s->sidx, s->fw,    s->sw,    s->fgw,   s->sgw,   s->fkeys,
+                    s->skeys, s->fvals, s->svals};
+    for (void* p : ptrs) cudaFree(p);
+    delete s;
+    return 0;
+}
+
+// One DFSPH_P sub-step of length dt with the given iteration counts.
+int fp64_sub_step(void* h, double dt, int new_frame, int div_iters, int dens_iters) {
+    Sim& s = *static_cast<Sim*>(h);
+    size_t const n = s.n;
+    double const cell = 2.0 * s.p.support;
+    sort_cells(s.x, n, cell, s.fkeys, s.fvals);
+    k_neighbors<<<grid(n), 128>>>(s, s.x, n, s.fkeys, s.fvals, true, s.fcnt, s.fidx, s.fw, s.fgw);
+    k_neighbors<<<grid(n), 128>>>(s, s.xs, s.ns, s.skeys, s.svals, false, s.scnt, s.sidx, s.sw,
+                                  s.sgw);
+    k_density_alpha<<<grid(n), 128>>>(s, new_frame);
+    k_apply<<<grid(n), 128>>>(s, s.qdiv, dt, 0);
+    for (int it = 0; it < div_iters; ++it) {
+        k_kappa<<<grid(n), 128>>>(s, dt, 0);
+        k_apply<<<grid(n), 128>>>(s, s.qdiv, dt, 0);
+    }
+    k_apply<<<grid(n), 128>>>(s, s.qdens, dt, 1);
+    for (int it = 0; it < dens_iters; ++it) {
+        k_kappa<<<grid(n), 128>>>(s, dt, 1);
+        k_apply<<<grid(n), 128>>>(s, s.qdens, dt, 0);
+    }
+    k_positions<<<grid(n), 128>>>(s, dt);
+    cudaError_t const e = cudaDeviceSynchronize();
+    return e == cudaSuccess ? 0 : 1000;
+}
+
+// "x", "v" (2 doubles per particle), "densities", "alphas", "counts".
+int fp64_get(void* h, char const* name, double* out) {
+    Sim& s = *static_cast<Sim*>(h);
+    size_t const n = s.n;
+    if (!std::strcmp(name, "x")) return cudaMemcpy(out, s.x, 16 * n, cudaMemcpyDeviceToHost) ? 1000 : 0;
+    if (!std::strcmp(name, "v")) return cudaMemcpy(out, s.v, 16 * n, cudaMemcpyDeviceToHost) ? 1000 : 0;
+    if (!std::strcmp(name, "densities")) {
+        return cudaMemcpy(out, s.rho, 8 * n, cudaMemcpyDeviceToHost) ? 1000 : 0;
+    }
+    if (!std::strcmp(name, "alphas")) {
+        return cudaMemcpy(out, s.alpha, 8 * n, cudaMemcpyDeviceToHost) ? 1000 : 0;
+    }
+    if (!std::strcmp(name, "counts")) {
+        std::vector<int> c(n);
+        if (cudaMemcpy(c.data(), s.fcnt, 4 * n, cudaMemcpyDeviceToHost)) return 1000;
+        for (size_t i = 0; i < n; ++i) out[i] = c[i];
+        return 0;
+    }
+    return 22;
+}
+
+}  // extern "C"

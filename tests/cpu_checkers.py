@@ -424,3 +424,65 @@ class RefSim:
                                          ptr(bi), ptr(blocks))
         return dict(grid_coords=gc, z_indices=z, pair_z=pz, pair_index=pi, block_indices=bi,
                     blocks=blocks[:nb])
+
+
+class FP64Oracle:
+    """The FP64 GPU oracle of the DFSPH_P sub-step (oracle/fp64/dfsph_fp64.cu):
+    the same formulas and list order in double, driven with each FP32
+    sub-step's dt and iteration counts."""
+
+    path = os.path.join(ORACLE_DIR, "libfp64_oracle.so")
+
+    class Params(ctypes.Structure):
+        _fields_ = [("support", ctypes.c_double), ("rho0", ctypes.c_double),
+                    ("mass", ctypes.c_double), ("fluid_volume", ctypes.c_double),
+                    ("gravity", ctypes.c_double)]
+
+    def __init__(self):
+        lib = ctypes.CDLL(self.path)
+        vp = ctypes.c_void_p
+        lib.fp64_create.argtypes = [ctypes.POINTER(FP64Oracle.Params), vp, vp, ctypes.c_size_t,
+                                    vp, vp, ctypes.c_size_t, ctypes.POINTER(vp)]
+        lib.fp64_destroy.argtypes = [vp]
+        lib.fp64_sub_step.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int]
+        lib.fp64_get.argtypes = [vp, ctypes.c_char_p, vp]
+        self.lib = lib
+
+    def sim(self, support, rho0, mass, gravity, solid_xy, solid_vols, fluid_xy, fluid_v=None):
+        return FP64Sim(self, support, rho0, mass, gravity, solid_xy, solid_vols, fluid_xy, fluid_v)
+
+
+class FP64Sim:
+    def __init__(self, o, support, rho0, mass, gravity, solid_xy, solid_vols, fluid_xy, fluid_v):
+        self.o = o
+        p = FP64Oracle.Params(float(support), float(rho0), float(mass),
+                              float(mass) / float(rho0), float(gravity))
+        s = np.ascontiguousarray(solid_xy, np.float64).reshape(-1, 2)
+        sv = np.ascontiguousarray(solid_vols, np.float64)
+        f = np.ascontiguousarray(fluid_xy, np.float64).reshape(-1, 2)
+        v = None if fluid_v is None else np.ascontiguousarray(fluid_v, np.float64).reshape(-1, 2)
+        h = ctypes.c_void_p()
+        rc = o.lib.fp64_create(ctypes.byref(p), s.ctypes.data, sv.ctypes.data, len(s),
+                               f.ctypes.data, None if v is None else v.ctypes.data, len(f),
+                               ctypes.byref(h))
+        assert rc == 0, rc
+        self.h = h
+        self.n = len(f)
+
+    def sub_step(self, dt, new_frame, div_iters, dens_iters):
+        rc = self.o.lib.fp64_sub_step(self.h, float(dt), int(new_frame), int(div_iters),
+                                      int(dens_iters))
+        assert rc == 0, rc
+
+    def get(self, name):
+        w = 2 if name in ("x", "v") else 1
+        out = np.zeros((self.n, w) if w > 1 else self.n, np.float64)
+        rc = self.o.lib.fp64_get(self.h, name.encode(), out.ctypes.data)
+        assert rc == 0, rc
+        return out
+
+    def close(self):
+        if self.h:
+            self.o.lib.fp64_destroy(self.h)
+            self.h = None

@@ -1,0 +1,63 @@
+"""Error of the FP32 DFSPH_P results against the FP64 GPU oracle.
+
+The FP32 run (the CUDA path, in either precision mode) advances CFL-adaptive
+sub-steps; the FP64 oracle repeats each sub-step with the same dt, frame
+boundaries and iteration counts, so the two differ only in arithmetic
+precision. Reported per checkpoint: per-particle density error (relative,
+L_inf and RMS), position error (in units of the particle spacing, max and
+RMS) and the kinetic-energy difference."""
+import numpy as np
+
+from cpu_checkers import FP64Oracle
+
+
+def dfsph_scene(E, n_side, precision, seed=1):
+    return E.BlockScene(n_side, dx=np.float32(1.0 / (2 * n_side)), seed=seed,
+                        time_per_step_flicks=1411200, sub_steps=4,
+                        dfsph_max_correction_iterations=100,
+                        dfsph_divergence_error_average_threshold=np.float32(0.001),
+                        dfsph_density_error_average_threshold=np.float32(0.0005),
+                        precision=precision)
+
+
+def compare(E, n_side, steps, checkpoints, precision, seed=1, offset=0.0):
+    """Rows of error statistics at the given sub-steps. `offset` moves the
+    whole scene (fluid and walls) by (offset, offset) metres, rounded to
+    float, before either run starts."""
+    scene = dfsph_scene(E, n_side, precision, seed)
+    p = scene.params
+    off = np.float32(offset)
+    fluid = (scene.fluid + off).astype(np.float32)
+    solid = (scene.solid + off).astype(np.float32)
+    sim = E.Simulation(p, solid, fluid, None, scene.solid_volumes)
+    ref = FP64Oracle().sim(p.support, p.target_density, p.mass_per_particle, p.gravity,
+                           solid, scene.solid_volumes, fluid)
+    mass = float(p.mass_per_particle)
+    dx = float(scene.dx)
+    tps = int(p.time_per_step_flicks)
+    rows = []
+    for step in range(1, steps + 1):
+        new_frame = sim.time() % tps == 0
+        st = sim.advance("dfsph_p", 1)
+        ref.sub_step(float(np.float32(st["dt"])), new_frame, st["divergence_iterations"],
+                     st["pressure_iterations"])
+        if step in checkpoints:
+            x, v = sim.state()
+            rho = sim.array("densities").astype(np.float64)
+            x64 = ref.get("x")
+            v64 = ref.get("v")
+            rho64 = ref.get("densities")
+            drel = np.abs(rho - rho64) / np.abs(rho64)
+            dpos = np.hypot(*(x.astype(np.float64) - x64).T) / dx
+            ke = 0.5 * mass * float(np.sum(v.astype(np.float64) ** 2))
+            ke64 = 0.5 * mass * float(np.sum(v64 ** 2))
+            rows.append(dict(step=step, density_linf=float(drel.max()),
+                             density_rms=float(np.sqrt(np.mean(drel ** 2))),
+                             position_max_dx=float(dpos.max()),
+                             position_rms_dx=float(np.sqrt(np.mean(dpos ** 2))),
+                             kinetic_energy=ke, kinetic_energy_fp64=ke64,
+                             energy_rel_diff=abs(ke - ke64) / ke64 if ke64 else 0.0,
+                             iterations=st["pressure_iterations"]))
+    ref.close()
+    sim.close()
+    return rows
