@@ -160,7 +160,8 @@ def run_gpu(args):
     # device-resident timing: one event pair per sub-step, L2 flushed between
     clocks_path = "/tmp/emerald_clocks_%d.csv" % rank
     smi, smi_file = clock_sampler(local, clocks_path)
-    launches0 = E.kernel_launches()
+    # kernels of this simulation, loop bodies counted per executed iteration
+    launches0 = sim.kernel_launches()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
     for k in range(args.steps):
@@ -169,7 +170,7 @@ def run_gpu(args):
         sim.advance("dfsph_p", 1, stats=False)
         ev[k][1].record()
     torch.cuda.synchronize()
-    launches = E.kernel_launches() - launches0
+    launches = sim.kernel_launches() - launches0
     total_ms = sum(a.elapsed_time(b) for a, b in ev)
     step_ms = [a.elapsed_time(b) for a, b in ev]
     if smi is not None:

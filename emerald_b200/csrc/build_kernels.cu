@@ -294,7 +294,7 @@ __device__ __noinline__ void write_entry_precise(uint32_t* idx_out, float* w_out
     gw_out[e] = g;
 }
 
-template <bool SOLID_OTHER>
+template <bool SOLID_OTHER, bool COMP>
 __global__ void __launch_bounds__(kTile) k_neighbors(Arena a, int write_kernels) {
     int32_t const s = a.tile_scene[blockIdx.x];
     if (s < 0) return;
@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(kTile) k_neighbors(Arena a, int write_kernels)
     uint64_t r[kRegList];
     int const cnt = find_neighbors_reg(pos, i, !SOLID_OTHER, cell, cell, P.reject_l2, o, r);
     cnt_out[i] = static_cast<uint8_t>(cnt);
-    if (P.precision && kernels) {
+    if (COMP && P.precision && kernels) {
         double2 const pos64 = a.x64[i];
         double2 const* x64o = SOLID_OTHER ? nullptr : a.x64;
         uint64_t full[kMaxNeighbors];
@@ -511,11 +511,20 @@ void launch_build_cells(Arena const& a, bool solid, uint32_t tiles, uint32_t* sc
 }
 
 void launch_neighbors(Arena const& a, uint32_t tiles, bool solid_other, bool write_kernels,
-                      cudaStream_t st) {
+                      cudaStream_t st, bool comp) {
+    int const wk = write_kernels ? 1 : 0;
     if (solid_other) {
-        k_neighbors<true><<<tiles, kTile, 0, st>>>(a, write_kernels ? 1 : 0);
+        if (comp) {
+            k_neighbors<true, true><<<tiles, kTile, 0, st>>>(a, wk);
+        } else {
+            k_neighbors<true, false><<<tiles, kTile, 0, st>>>(a, wk);
+        }
     } else {
-        k_neighbors<false><<<tiles, kTile, 0, st>>>(a, write_kernels ? 1 : 0);
+        if (comp) {
+            k_neighbors<false, true><<<tiles, kTile, 0, st>>>(a, wk);
+        } else {
+            k_neighbors<false, false><<<tiles, kTile, 0, st>>>(a, wk);
+        }
     }
 }
 

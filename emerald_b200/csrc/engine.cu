@@ -504,7 +504,10 @@ void Engine::update_extent() {
     uint32_t const ns = round_extent(st, solid_cap_ / kTile, 16);
     uint32_t const nf = round_extent(ft, ftab_.capacity(), 8192);
     uint32_t const nsb = round_extent(sb, stab_.capacity(), 8192);
-    if (nt != ext_tiles_ || nf != ext_ftab_) destroy_graphs();
+    bool comp = false;
+    for (auto const& sc : scenes_) comp = comp || (sc.used && sc.p.precision != 0);
+    if (nt != ext_tiles_ || nf != ext_ftab_ || comp != compensated_) destroy_graphs();
+    compensated_ = comp;
     ext_tiles_ = nt;
     ext_stiles_ = ns;
     ext_ftab_ = nf;
@@ -588,11 +591,11 @@ void Engine::emit_loop_body(int kind, int32_t method, cudaGraphConditionalHandle
     switch (method) {
     case kDfsph:
         if (kind == 2) {
-            launch("dfsph_divergence", [&] { launch_dfsph_divergence(a_, tiles, st); });
-            launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 1, st); });
+            launch("dfsph_divergence", [&] { launch_dfsph_divergence(a_, tiles, compensated_, st); });
+            launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 1, compensated_, st); });
         } else {
-            launch("dfsph_density", [&] { launch_dfsph_density(a_, tiles, st); });
-            launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 1, 0, 1, st); });
+            launch("dfsph_density", [&] { launch_dfsph_density(a_, tiles, compensated_, st); });
+            launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 1, 0, 1, compensated_, st); });
         }
         break;
     case kIisph:
@@ -699,16 +702,16 @@ void Engine::emit_substep(int32_t method, bool reorder) {
     Arena const ext = extent_arena();
     launch("build_cells", [&] { launch_build_cells(ext, false, tiles, d_scan_, st); }, 6);
     bool const kernels = method != kPcisph;
-    launch("neighbors_fluid", [&] { launch_neighbors(a_, tiles, false, kernels, st); });
-    launch("neighbors_solid", [&] { launch_neighbors(a_, tiles, true, kernels, st); });
+    launch("neighbors_fluid", [&] { launch_neighbors(a_, tiles, false, kernels, st, compensated_); });
+    launch("neighbors_solid", [&] { launch_neighbors(a_, tiles, true, kernels, st, compensated_); });
     switch (method) {
     case kDfsph:
-        launch("dfsph_density_alpha", [&] { launch_dfsph_density_alpha(a_, tiles, st); });
-        launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 0, st); });
+        launch("dfsph_density_alpha", [&] { launch_dfsph_density_alpha(a_, tiles, compensated_, st); });
+        launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 0, compensated_, st); });
         run_loop(2, max_iterations(2), method);
-        launch("apply_pressures_ext", [&] { launch_apply_pressures(a_, tiles, 1, 1, 0, st); });
+        launch("apply_pressures_ext", [&] { launch_apply_pressures(a_, tiles, 1, 1, 0, compensated_, st); });
         run_loop(1, max_iterations(1), method);
-        launch("integrate_positions", [&] { launch_integrate_positions(a_, tiles, st); });
+        launch("integrate_positions", [&] { launch_integrate_positions(a_, tiles, compensated_, st); });
         break;
     case kIisph:
         launch("iisph_density_dii", [&] { launch_iisph_density_dii(a_, tiles, st); });

@@ -171,6 +171,7 @@ private:
     std::vector<void*> allocations_;
     size_t device_bytes_ = 0;
     uint32_t ext_tiles_ = 0, ext_stiles_ = 0, ext_ftab_ = 0, ext_stab_ = 0;
+    bool compensated_ = false;  // some resident scene is in compensated mode
     SceneParams* d_sp_ = nullptr;
     SceneState* d_ss_ = nullptr;
     int32_t* d_tile_scene_ = nullptr;

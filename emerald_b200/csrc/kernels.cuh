@@ -15,7 +15,7 @@ void launch_exclusive_scan(uint32_t const* in, uint32_t n, uint32_t* out, uint32
 void launch_build_cells(Arena const& a, bool solid, uint32_t tiles, uint32_t* scan_scratch,
                         cudaStream_t st);
 void launch_neighbors(Arena const& a, uint32_t tiles, bool solid_other, bool write_kernels,
-                      cudaStream_t st);
+                      cudaStream_t st, bool comp = false);
 void launch_solid_volumes(Arena const& a, uint32_t solid_tiles, float numer, int scene,
                           cudaStream_t st);
 
@@ -62,12 +62,13 @@ void launch_zero_kappas(Arena const& a, uint32_t tiles, cudaStream_t st);
 void launch_iter_reset(Arena const& a, int nscenes, int kind, cudaStream_t st);
 void launch_iter_check(Arena const& a, int nscenes, int kind, int* running,
                        cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st);
-void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, cudaStream_t st);
+// comp: some resident scene is in compensated mode (selects the kernel variant)
+void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st);
 void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int external,
-                            int skip_done, cudaStream_t st);
-void launch_dfsph_divergence(Arena const& a, uint32_t tiles, cudaStream_t st);
-void launch_dfsph_density(Arena const& a, uint32_t tiles, cudaStream_t st);
-void launch_integrate_positions(Arena const& a, uint32_t tiles, cudaStream_t st);
+                            int skip_done, bool comp, cudaStream_t st);
+void launch_dfsph_divergence(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st);
+void launch_dfsph_density(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st);
+void launch_integrate_positions(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st);
 void launch_iisph_density_dii(Arena const& a, uint32_t tiles, cudaStream_t st);
 void launch_iisph_aii(Arena const& a, uint32_t tiles, cudaStream_t st);
 void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st);
