@@ -224,3 +224,35 @@ def test_graph_and_eager_modes_agree(E, method):
         assert_bitwise(a.state()[0], b.state()[0], "x")
         assert_bitwise(a.state()[1], b.state()[1], "v")
     assert a.kernel_launches() == b.kernel_launches()
+
+
+def test_dense_cells_take_the_fallback_path(E, oracle):
+    """A lattice with dense clusters: a cell with 50 members (more than a
+    warp), a 3x3 block with more than 128 candidates, and a particle with
+    more than 64 neighbours inside the radius (the reference keeps the first
+    64 in scan order). Fluid and boundary lists equal the oracle's."""
+    rng = np.random.Generator(np.random.PCG64(4))
+    dx = F(1 / 80)
+    g = (np.arange(40, dtype=np.float32) + F(0.5)) * dx
+    lattice = np.stack(np.meshgrid(g, g), -1).reshape(-1, 2).astype(np.float32)
+    cell = F(2 * dx)
+    c1 = (F(0.2) + rng.uniform(0.0, 0.9, (50, 2)).astype(np.float32) * cell).astype(np.float32)
+    c2 = (F(0.6) + rng.uniform(-1.4, 1.4, (150, 2)).astype(np.float32) * cell).astype(np.float32)
+    c3 = (F(0.35) + rng.uniform(-0.3, 0.3, (80, 2)).astype(np.float32) * cell).astype(np.float32)
+    fluid = np.concatenate([lattice, c1, c2, c3]).astype(np.float32)
+    solid = np.concatenate([
+        np.stack([g, np.full_like(g, -dx / 2)], -1),
+        (F(0.5) + rng.uniform(-1.2, 1.2, (140, 2)).astype(np.float32) * cell) * np.float32([1, 0]) +
+        np.float32([0, -dx]),
+    ]).astype(np.float32)
+    p = E.default_params(support=dx)
+    sim = E.Simulation(p, solid, fluid, None, np.full(len(solid), F(1e-4), np.float32))
+    sim.sub_step("dfsph_p", 0.0, F(1e-6))
+    for is_solid, other in ((False, fluid), (True, solid)):
+        counts, idx, _, _ = sim.neighbors(is_solid)
+        oc, oi, _, _ = oracle.neighborhoods(fluid, other, not is_solid, cell)
+        assert counts.max() == 64 or is_solid
+        assert_bitwise(counts, oc, "%s counts" % ("solid" if is_solid else "fluid"))
+        mask = np.arange(64)[None, :] < oc[:, None]
+        assert_bitwise(np.where(mask, idx, 0), np.where(mask, oi, 0),
+                       "%s indices" % ("solid" if is_solid else "fluid"))
