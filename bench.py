@@ -155,6 +155,7 @@ def run_gpu(args):
 
     for _ in range(args.warmup):
         sim.advance("dfsph_p", 1, stats=False)
+    tuning = sim.autotune("dfsph_p")  # gather-kernel chunks, same bits either way
     barrier()
 
     # device-resident timing: one event pair per sub-step, L2 flushed between
@@ -256,6 +257,7 @@ def run_gpu(args):
                        "neighbours_per_particle": round(nnz_f / n, 2),
                        "parallelism": "replicas" if world > 1 else "single scene",
                        "l2": "flushed between timed steps (256 MiB write)",
+                       "autotuned_chunks": tuning["chunks"],
                        "p50_step_ms": round(float(np.percentile(step_ms, 50)), 4),
                        "p99_step_ms": round(float(np.percentile(step_ms, 99)), 4),
                        "last_step": {k: last[k] for k in ("dt", "pressure_iterations",
@@ -314,6 +316,7 @@ def run_batched(args, torch, E, rank, world, barrier):
     warm = 3
     steps = args.batched_steps
     b.step("iisph", warm)
+    tuning = b.autotune("iisph")
     barrier()
     l0 = b.kernel_launches()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -347,6 +350,7 @@ def run_batched(args, torch, E, rank, world, barrier):
            "max_avg_density_error": err,
            "scenes_above_0.1%": int(sum(st["error_average"] > 0.001 for st in stats)),
            "iterations_last_step": [min(iters), max(iters)],
+           "autotuned": tuning,
            "gpu_launches": int(launches)}
     if world == 1:
         # the same scenes one at a time through the single-scene API

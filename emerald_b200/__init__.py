@@ -91,6 +91,19 @@ class RequestTiming(ctypes.Structure):
                 ("total_ms", ctypes.c_double)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("apply_chunk", c_i32), ("divergence_chunk", c_i32), ("iisph_sum_chunk", c_i32),
+                ("iisph_beta_chunk", c_i32), ("candidates", c_i32),
+                ("candidate_chunks", (c_i32 * 4) * 8), ("candidate_ms", c_f * 8)]
+
+    def as_dict(self):
+        fams = ("apply", "divergence", "iisph_sum", "iisph_beta")
+        return {"chunks": {f: getattr(self, f + "_chunk") for f in fams},
+                "candidates": [{"chunks": dict(zip(fams, list(self.candidate_chunks[k]))),
+                                "ms_per_substep": round(self.candidate_ms[k], 4)}
+                               for k in range(self.candidates)]}
+
+
 EXPORTS = {
     "emerald_default_params": (c_i32, [ctypes.POINTER(Params)]),
     "emerald_config": (c_i32, [ctypes.POINTER(Params), c_vp]),
@@ -144,6 +157,8 @@ EXPORTS = {
     "emerald_server_wait": (c_i32, [c_vp, c_i64, c_i32, c_vp, c_vp, ctypes.POINTER(StepStats),
                                     ctypes.POINTER(RequestTiming)]),
     "emerald_server_get_stats": (c_i32, [c_vp, ctypes.POINTER(ServerStats)]),
+    "emerald_sim_autotune": (c_i32, [c_vp, c_i32, ctypes.POINTER(Tuning)]),
+    "emerald_batch_autotune": (c_i32, [c_vp, c_i32, ctypes.POINTER(Tuning)]),
     "emerald_neighbors_static": (c_i32, [c_vp, c_u32, c_f, c_vp, c_vp, c_vp, c_vp, c_u32, c_vp]),
     "emerald_kernel_launches": (c_i64, []),
     "emerald_last_error": (ctypes.c_char_p, []),
@@ -405,6 +420,11 @@ class Simulation:
         _check(lib.emerald_sim_kernel_launches(self._h, ctypes.byref(n)), "kernel_launches")
         return n.value
 
+    def autotune(self, method):
+        t = Tuning()
+        _check(lib.emerald_sim_autotune(self._h, method_id(method), ctypes.byref(t)), "autotune")
+        return t.as_dict()
+
     def enable_timing(self, on=True):
         _check(lib.emerald_sim_enable_timing(self._h, int(on)), "enable_timing")
 
@@ -507,6 +527,11 @@ class Batch:
         n = c_i64()
         _check(lib.emerald_batch_kernel_launches(self._h, ctypes.byref(n)), "kernel_launches")
         return n.value
+
+    def autotune(self, method):
+        t = Tuning()
+        _check(lib.emerald_batch_autotune(self._h, method_id(method), ctypes.byref(t)), "autotune")
+        return t.as_dict()
 
 
 class Server:

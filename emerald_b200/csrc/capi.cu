@@ -2,6 +2,7 @@
 #include <cstring>
 #include <exception>
 #include <new>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -449,6 +450,46 @@ int emerald_batch_kernel_launches(emerald_batch* batch, int64_t* count) {
         *count = batch->engine.kernel_launches();
         return EMERALD_OK;
     });
+}
+
+namespace {
+int autotune_into(Engine& engine, int32_t method, emerald_tuning* out) {
+    if (!valid_method(method)) return fail(EMERALD_EINVAL, "bad method");
+    return guarded([&] {
+        try {
+            Engine::TuneReport const r = engine.autotune(method);
+            if (out) {
+                *out = emerald_tuning{};
+                out->apply_chunk = r.chosen.apply;
+                out->divergence_chunk = r.chosen.divergence;
+                out->iisph_sum_chunk = r.chosen.iisph_sum;
+                out->iisph_beta_chunk = r.chosen.iisph_beta;
+                out->candidates = r.count;
+                for (int k = 0; k < r.count && k < 8; ++k) {
+                    Engine::Tuning const& t = r.candidates[k];
+                    out->candidate_chunks[k][0] = t.apply;
+                    out->candidate_chunks[k][1] = t.divergence;
+                    out->candidate_chunks[k][2] = t.iisph_sum;
+                    out->candidate_chunks[k][3] = t.iisph_beta;
+                    out->candidate_ms[k] = r.ms[k];
+                }
+            }
+        } catch (std::invalid_argument const& e) {
+            return fail(EMERALD_EINVAL, e.what());
+        }
+        return EMERALD_OK;
+    });
+}
+}  // namespace
+
+int emerald_sim_autotune(emerald_sim* sim, int32_t method, emerald_tuning* out) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    return autotune_into(sim->engine, method, out);
+}
+
+int emerald_batch_autotune(emerald_batch* batch, int32_t method, emerald_tuning* out) {
+    if (!batch) return fail(EMERALD_EINVAL, "batch is NULL");
+    return autotune_into(batch->engine, method, out);
 }
 
 int emerald_server_create(emerald_server_config const* config, emerald_server** out) {

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -591,16 +592,16 @@ void Engine::emit_loop_body(int kind, int32_t method, cudaGraphConditionalHandle
     switch (method) {
     case kDfsph:
         if (kind == 2) {
-            launch("dfsph_divergence", [&] { launch_dfsph_divergence(a_, tiles, compensated_, st); });
-            launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 1, compensated_, st); });
+            launch("dfsph_divergence", [&] { launch_dfsph_divergence(a_, tiles, compensated_, st, tuning_.divergence); });
+            launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 1, compensated_, st, tuning_.apply); });
         } else {
-            launch("dfsph_density", [&] { launch_dfsph_density(a_, tiles, compensated_, st); });
-            launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 1, 0, 1, compensated_, st); });
+            launch("dfsph_density", [&] { launch_dfsph_density(a_, tiles, compensated_, st, tuning_.divergence); });
+            launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 1, 0, 1, compensated_, st, tuning_.apply); });
         }
         break;
     case kIisph:
-        launch("iisph_sum_dij", [&] { launch_iisph_sum_dij(a_, tiles, st); });
-        launch("iisph_beta_pressure", [&] { launch_iisph_beta_pressure(a_, tiles, st); });
+        launch("iisph_sum_dij", [&] { launch_iisph_sum_dij(a_, tiles, st, tuning_.iisph_sum); });
+        launch("iisph_beta_pressure", [&] { launch_iisph_beta_pressure(a_, tiles, st, tuning_.iisph_beta); });
         break;
     case kIisphAp:
     case kIisphPseudoAp: {
@@ -707,9 +708,9 @@ void Engine::emit_substep(int32_t method, bool reorder) {
     switch (method) {
     case kDfsph:
         launch("dfsph_density_alpha", [&] { launch_dfsph_density_alpha(a_, tiles, compensated_, st); });
-        launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 0, compensated_, st); });
+        launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 0, compensated_, st, tuning_.apply); });
         run_loop(2, max_iterations(2), method);
-        launch("apply_pressures_ext", [&] { launch_apply_pressures(a_, tiles, 1, 1, 0, compensated_, st); });
+        launch("apply_pressures_ext", [&] { launch_apply_pressures(a_, tiles, 1, 1, 0, compensated_, st, tuning_.apply); });
         run_loop(1, max_iterations(1), method);
         launch("integrate_positions", [&] { launch_integrate_positions(a_, tiles, compensated_, st); });
         break;
@@ -776,8 +777,32 @@ void Engine::capture_substep(int32_t method, bool reorder) {
     graph_fixed_kernels_[method * 2 + (reorder ? 1 : 0)] = capture_kernels_;
 }
 
+// Tunings chosen by autotune, per (method, log2 of the active particle
+// count); engines of the same size class start from them.
+namespace {
+std::mutex g_tuning_mutex;
+std::map<uint64_t, Engine::Tuning> g_tuning_cache;
+}  // namespace
+
+uint64_t Engine::tuning_key(int32_t method) const {
+    uint64_t n = 0;
+    for (auto const& sc : scenes_) {
+        if (sc.used && sc.active) n += sc.p.fluid_count;
+    }
+    return uint64_t(method) * 64u + ceil_log2(std::max<uint64_t>(n, 1));
+}
+
 void Engine::substep(int32_t method) {
     if (active_scenes() == 0) return;
+    if (!tuning_locked_) {
+        std::lock_guard<std::mutex> lock(g_tuning_mutex);
+        auto const it = g_tuning_cache.find(tuning_key(method));
+        if (it != g_tuning_cache.end() && !(it->second == tuning_)) {
+            tuning_ = it->second;
+            destroy_graphs();
+        }
+    }
+    last_method_ = method;
     for (int id = 0; id < max_scenes_; ++id) {
         Scene& sc = scenes_[id];
         if (!sc.used || !sc.active) continue;
@@ -810,6 +835,121 @@ void Engine::substep(int32_t method) {
     cur_ = st_;
     emit_substep(method, reorder);
     check("substep");
+}
+
+// Times whole sub-steps of `method` with each candidate tuning, every
+// candidate from the same state (positions, velocities, kappas, storage
+// order, frame clocks and launch counters are snapshotted and restored), and
+// keeps the fastest. The candidates give the same bits, so the choice
+// changes speed only.
+Engine::TuneReport Engine::autotune(int32_t method, int substeps) {
+    if (last_method_ != method) {
+        throw std::invalid_argument("autotune: run a sub-step of this method first");
+    }
+    if (method != kDfsph && method != kIisph) {
+        throw std::invalid_argument("autotune: DFSPH_P and IISPH have tunable kernels");
+    }
+    size_t const N = fluid_cap_;
+    struct Region {
+        void* dev;
+        size_t size;
+    };
+    Region const regions[] = {{a_.x, 8 * N},      {a_.v, 8 * N},         {a_.kdiv, 4 * N},
+                              {a_.kdens, 4 * N},  {a_.x64, 16 * N},      {a_.oid, 4 * N},
+                              {a_.slot_of, 4 * N}, {d_ss_, sizeof(SceneState) * size_t(max_scenes_)},
+                              {d_loop_iters_, sizeof(unsigned long long) * 4}};
+    size_t bytes = 0;
+    for (auto const& r : regions) bytes += r.size;
+    char* snap = nullptr;
+    if (cudaMalloc(&snap, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        throw std::bad_alloc();
+    }
+    auto copy = [&](bool save) {
+        size_t off = 0;
+        for (auto const& r : regions) {
+            if (save) {
+                cudaMemcpyAsync(snap + off, r.dev, r.size, cudaMemcpyDeviceToDevice, st_);
+            } else {
+                cudaMemcpyAsync(r.dev, snap + off, r.size, cudaMemcpyDeviceToDevice, st_);
+            }
+            off += r.size;
+        }
+    };
+    copy(true);
+    int64_t const launched0 = substeps_launched_;
+    int64_t const host0 = host_launches_;
+    int64_t const global0 = g_launches.load();
+    std::vector<Tuning> cand;
+    if (method == kDfsph) {
+        int const opts[][2] = {{4, 8}, {1, 4}, {4, 4}, {1, 8}, {8, 8}};
+        for (auto const& o : opts) {
+            Tuning t = tuning_;
+            t.apply = o[0];
+            t.divergence = o[1];
+            cand.push_back(t);
+        }
+    } else {
+        int const opts[][2] = {{4, 4}, {1, 1}, {1, 4}, {4, 1}, {8, 4}};
+        for (auto const& o : opts) {
+            Tuning t = tuning_;
+            t.iisph_sum = o[0];
+            t.iisph_beta = o[1];
+            cand.push_back(t);
+        }
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    TuneReport rep{};
+    tuning_locked_ = true;
+    float best = 0.0f;
+    Tuning best_t = cand[0];
+    try {
+        for (size_t k = 0; k < cand.size(); ++k) {
+            tuning_ = cand[k];
+            destroy_graphs();
+            // the same sub-steps once untimed: captures every graph they use
+            for (int q = 0; q < substeps; ++q) substep(method);
+            copy(false);
+            substeps_launched_ = launched0;
+            cudaEventRecord(e0, st_);
+            for (int q = 0; q < substeps; ++q) substep(method);
+            cudaEventRecord(e1, st_);
+            cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            rep.candidates[k] = cand[k];
+            rep.ms[k] = ms / float(substeps);
+            if (k == 0 || rep.ms[k] < best) {
+                best = rep.ms[k];
+                best_t = cand[k];
+            }
+            copy(false);
+            substeps_launched_ = launched0;
+        }
+    } catch (...) {
+        tuning_locked_ = false;
+        cudaFree(snap);
+        throw;
+    }
+    rep.count = int(cand.size());
+    tuning_locked_ = false;
+    cudaStreamSynchronize(st_);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(snap);
+    host_launches_ = host0;
+    g_launches.fetch_sub(g_launches.load() - global0);
+    check("autotune");
+    tuning_ = best_t;
+    destroy_graphs();
+    {
+        std::lock_guard<std::mutex> lock(g_tuning_mutex);
+        g_tuning_cache[tuning_key(method)] = tuning_;
+    }
+    rep.chosen = tuning_;
+    return rep;
 }
 
 // ------------------------------------------------------------ accessors

@@ -60,6 +60,21 @@ struct KernelTimes {
 
 class Engine {
 public:
+    // Neighbour entries loaded together by each gather-sum kernel (1, 4 or
+    // 8); every choice gives the same bits.
+    struct Tuning {
+        int apply = 4, divergence = 8, iisph_sum = 4, iisph_beta = 4;
+        bool operator==(Tuning const& o) const {
+            return apply == o.apply && divergence == o.divergence && iisph_sum == o.iisph_sum &&
+                   iisph_beta == o.iisph_beta;
+        }
+    };
+    struct TuneReport {
+        Tuning chosen;
+        int count;               // candidates timed
+        Tuning candidates[8];
+        float ms[8];             // mean sub-step time of each candidate
+    };
     Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes);
     ~Engine();
     // Device bytes the constructor allocates for these capacities.
@@ -135,7 +150,18 @@ public:
 
     void check(char const* what);
 
+    // Picks the fastest chunk settings of `method`'s gather kernels by timing
+    // whole sub-steps on the resident scenes (after at least one sub-step of
+    // it), restoring the state after each; the choice is kept for engines of
+    // the same method and size class.
+    TuneReport autotune(int32_t method, int substeps = 4);
+    Tuning const& tuning() const { return tuning_; }
+
 private:
+    uint64_t tuning_key(int32_t method) const;
+    Tuning tuning_{};
+    bool tuning_locked_ = false;
+    int32_t last_method_ = -1;
     struct Scene {
         bool used = false;
         SceneParams p{};

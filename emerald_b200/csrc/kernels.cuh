@@ -64,15 +64,20 @@ void launch_iter_check(Arena const& a, int nscenes, int kind, int* running,
                        cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st);
 // comp: some resident scene is in compensated mode (selects the kernel variant)
 void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st);
+// chunk: neighbour entries loaded together in the gather sums (1, 4 or 8;
+// every choice gives the same bits)
 void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int external,
-                            int skip_done, bool comp, cudaStream_t st);
-void launch_dfsph_divergence(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st);
-void launch_dfsph_density(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st);
+                            int skip_done, bool comp, cudaStream_t st, int chunk = 4);
+void launch_dfsph_divergence(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st,
+                             int chunk = 8);
+void launch_dfsph_density(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st,
+                          int chunk = 8);
 void launch_integrate_positions(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st);
 void launch_iisph_density_dii(Arena const& a, uint32_t tiles, cudaStream_t st);
 void launch_iisph_aii(Arena const& a, uint32_t tiles, cudaStream_t st);
-void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st);
-void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk = 4);
+void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st,
+                                int chunk = 4);
 void launch_make_q(Arena const& a, uint32_t tiles, cudaStream_t st);
 void launch_apply_integrate(Arena const& a, uint32_t tiles, cudaStream_t st);
 void launch_ap_density(Arena const& a, uint32_t tiles, cudaStream_t st);

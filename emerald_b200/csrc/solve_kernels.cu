@@ -279,10 +279,17 @@ __global__ void k_iter_check(Arena a, int nscenes, int kind, int* running,
 // chunk first loads its indices and kernel gradients, then every gathered
 // neighbour value, then folds them into the sum in order. The loads of a
 // chunk are independent, so they are in flight together; the sum is the
-// same sequence of operations as a plain loop. (Chunks measured on B200 at
-// 262,144 particles: 8 for the divergence sums, 4 for apply_pressures.)
+// same sequence of operations as a plain loop. The chunk of each kernel is
+// a launch-time choice among 1, 4 and 8 (Tuning, set by the autotuner);
+// defaults measured on B200 at 262,144 particles.
 constexpr int kDivergenceChunk = 8;
 constexpr int kPressureChunk = 4;
+
+// Neighbour values the IISPH beta sum gathers.
+struct IisphNeighbor {
+    float rho, p;
+    float2 sdp, dii;
+};
 
 template <int CH, class Gather, class Fold>
 __device__ __forceinline__ void fold_fluid_list(Arena const& a, uint32_t i, int c, Gather gather,
@@ -338,7 +345,7 @@ __device__ __forceinline__ float density_of(Arena const& a, SceneParams const& P
 
 // compute_divergences (emerald/sph_common/divergence.cpp:5-74).
 // With K, the fluid and boundary terms go into one Kahan-compensated sum.
-template <bool K = false>
+template <bool K = false, int CH = kDivergenceChunk>
 __device__ __forceinline__ float divergence_of(Arena const& a, SceneParams const& P, uint32_t i) {
     size_t const stride = a.stride;
     float const rho0 = P.rho0;
@@ -360,7 +367,7 @@ __device__ __forceinline__ float divergence_of(Arena const& a, SceneParams const
         return acc.s;
     }
     float d = 0.0f;
-    fold_fluid_list<kDivergenceChunk>(
+    fold_fluid_list<CH>(
       a, i, c, [&](uint32_t j) { return a.v[j]; },
       [&](float2 vj, float2 g) { d += fmass * dot2(sub2(vi, vj), g); });
     int const cs = a.ns_cnt[i];
@@ -381,7 +388,7 @@ __device__ __forceinline__ float divergence_of(Arena const& a, SceneParams const
 // apply_pressures_in_place (emerald/sph_common/pressure.cpp:9-80) for one
 // particle, with q = safe_divide(p, rho^2) precomputed per particle. With K,
 // each sum is Kahan-compensated.
-template <bool K = false>
+template <bool K = false, int CH = kPressureChunk>
 __device__ __forceinline__ float2 apply_pressure_of(Arena const& a, SceneParams const& P, uint32_t i,
                                                     float2 v, float const* q, float dt) {
     size_t const stride = a.stride;
@@ -411,7 +418,7 @@ __device__ __forceinline__ float2 apply_pressure_of(Arena const& a, SceneParams 
     }
     if (c) {
         float2 acc = mk2(0.0f, 0.0f);
-        fold_fluid_list<kPressureChunk>(
+        fold_fluid_list<CH>(
           a, i, c, [&](uint32_t j) { return q[j]; },
           [&](float qj, float2 g) { acc = add2(acc, scl2(neg_fmass * (qi + qj), g)); });
         v = add2(v, scl2(dt, acc));
@@ -568,7 +575,7 @@ __global__ void k_dfsph_density_alpha(Arena a) {
 // apply_pressures_in_place over the cached q; with `external`, the velocity
 // first takes the external-force step (the DFSPH density warm start follows
 // integrate_velocities_in_place, dfsph_p.cpp:349-365).
-template <int MODE>
+template <int MODE, int CH>
 __global__ void k_apply_pressures(Arena a, int which_q, int external, int skip_done) {
     Ctx c;
     if (!enter(a, skip_done != 0, c) || !c.live) return;
@@ -577,13 +584,13 @@ __global__ void k_apply_pressures(Arena a, int which_q, int external, int skip_d
     float2 v = a.v[c.i];
     if (external) v = integrate_external(P, v, dt);
     float const* q = which_q ? a.qdens : a.qdiv;
-    a.v[c.i] = (MODE && P.precision) ? apply_pressure_of<true>(a, P, c.i, v, q, dt)
-                                     : apply_pressure_of<false>(a, P, c.i, v, q, dt);
+    a.v[c.i] = (MODE && P.precision) ? apply_pressure_of<true, CH>(a, P, c.i, v, q, dt)
+                                     : apply_pressure_of<false, CH>(a, P, c.i, v, q, dt);
 }
 
 // compute_divergences + dfsph_p_compute_divergence_pseudo_pressures
 // (dfsph_p_ops.cpp:100-126) + the divergence error of dfsph_p.cpp:187-200.
-template <int MODE>
+template <int MODE, int CH>
 __global__ void k_dfsph_divergence(Arena a) {
     Ctx c;
     if (!enter(a, true, c)) return;
@@ -593,8 +600,8 @@ __global__ void k_dfsph_divergence(Arena a) {
     float err = 0.0f;
     if (c.live) {
         uint32_t const i = c.i;
-        float const d = (MODE && P.precision) ? divergence_of<true>(a, P, i)
-                                              : divergence_of<false>(a, P, i);
+        float const d = (MODE && P.precision) ? divergence_of<true, CH>(a, P, i)
+                                              : divergence_of<false, CH>(a, P, i);
         a.rho_star[i] = d;
         float kappa = 0.0f;
         if (!(d <= 0.0f)) {
@@ -612,7 +619,7 @@ __global__ void k_dfsph_divergence(Arena a) {
 // predict_density_stars (density.cpp:75-109) +
 // dfsph_p_compute_density_pseudo_pressures (dfsph_p_ops.cpp:74-98) + the
 // density error of dfsph_p.cpp:134-148.
-template <int MODE>
+template <int MODE, int CH>
 __global__ void k_dfsph_density(Arena a) {
     Ctx c;
     if (!enter(a, true, c)) return;
@@ -624,8 +631,8 @@ __global__ void k_dfsph_density(Arena a) {
     if (c.live) {
         uint32_t const i = c.i;
         float const rho = a.rho[i];
-        float const div = (MODE && P.precision) ? divergence_of<true>(a, P, i)
-                                                : divergence_of<false>(a, P, i);
+        float const div = (MODE && P.precision) ? divergence_of<true, CH>(a, P, i)
+                                                : divergence_of<false, CH>(a, P, i);
         float const star = max_0x(rho + (dt * div));
         a.rho_star[i] = star;
         float const delta = star - rho0;
@@ -762,6 +769,7 @@ __global__ void k_iisph_aii(Arena a) {
 }
 
 // iisph_compute_sum_dij_pjs (iisph_ops.cpp:202-235).
+template <int CH>
 __global__ void k_iisph_sum_dij(Arena a) {
     Ctx c;
     if (!enter(a, true, c) || !c.live) return;
@@ -775,20 +783,20 @@ __global__ void k_iisph_sum_dij(Arena a) {
     float const neg_dt2 = -sqrf(dt);
     float2 sum = mk2(0.0f, 0.0f);
     int const cf = a.nf_cnt[i];
-    #pragma unroll 4
-
-    for (int k = 0; k < cf; ++k) {
-        size_t const e = k * stride + i;
-        uint32_t const j = a.nf_idx[e];
-        float2 const numer = scl2(neg_dt2 * mass * p[j], a.nf_gw[e]);
-        float const denom = sqrf(a.rho[j]);
-        if (safe_v(numer, denom)) sum = add2(sum, div2(numer, denom));
-    }
+    (void)stride;
+    fold_fluid_list<CH>(
+      a, i, cf, [&](uint32_t j) { return mk2(p[j], a.rho[j]); },
+      [&](float2 prho, float2 g) {
+          float2 const numer = scl2(neg_dt2 * mass * prho.x, g);
+          float const denom = sqrf(prho.y);
+          if (safe_v(numer, denom)) sum = add2(sum, div2(numer, denom));
+      });
     a.sdp[i] = sum;
 }
 
 // iisph_compute_betas (iisph_ops.cpp:237-330) followed by
 // iisph_compute_new_pressures for the same particle (iisph_ops.cpp:332-425).
+template <int CH>
 __global__ void k_iisph_beta_pressure(Arena a) {
     Ctx c;
     if (!enter(a, true, c)) return;
@@ -810,20 +818,18 @@ __global__ void k_iisph_beta_pressure(Arena a) {
         int const cf = a.nf_cnt[i];
         if (cf) {
             float const mass = rho0 * P.fluid_volume;
-            #pragma unroll 4
-
-            for (int k = 0; k < cf; ++k) {
-                size_t const e = k * stride + i;
-                uint32_t const j = a.nf_idx[e];
-                float2 const gw = a.nf_gw[e];
-                float2 const numer = scl2(neg_dt2 * mass, gw);
-                float const denom = sqrf(a.rho[j]);
-                float2 const dij = safe_v(numer, denom) ? div2(numer, denom) : mk2(0.0f, 0.0f);
-                float2 const dji = neg2(dij);
-                float2 const skni = sub2(a.sdp[j], scl2(pi, dji));
-                float2 const t = sub2(sub2(si, scl2(p[j], a.dii[j])), skni);
-                beta += mass * dot2(t, gw);
-            }
+            fold_fluid_list<CH>(
+              a, i, cf,
+              [&](uint32_t j) { return IisphNeighbor{a.rho[j], p[j], a.sdp[j], a.dii[j]}; },
+              [&](IisphNeighbor const& nb, float2 gw) {
+                  float2 const numer = scl2(neg_dt2 * mass, gw);
+                  float const denom = sqrf(nb.rho);
+                  float2 const dij = safe_v(numer, denom) ? div2(numer, denom) : mk2(0.0f, 0.0f);
+                  float2 const dji = neg2(dij);
+                  float2 const skni = sub2(nb.sdp, scl2(pi, dji));
+                  float2 const t = sub2(sub2(si, scl2(nb.p, nb.dii)), skni);
+                  beta += mass * dot2(t, gw);
+              });
         }
         int const cs = a.ns_cnt[i];
         if (cs) {
@@ -1189,25 +1195,49 @@ void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, bool comp, cudaS
     }
 }
 void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int external,
-                            int skip_done, bool comp, cudaStream_t st) {
+                            int skip_done, bool comp, cudaStream_t st, int chunk) {
     if (comp) {
-        k_apply_pressures<1><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done);
+    switch (chunk) {
+        case 1: k_apply_pressures<1, 1><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done); break;
+        case 4: k_apply_pressures<1, 4><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done); break;
+        default: k_apply_pressures<1, 8><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done); break;
+        }
     } else {
-        k_apply_pressures<0><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done);
+    switch (chunk) {
+        case 1: k_apply_pressures<0, 1><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done); break;
+        case 4: k_apply_pressures<0, 4><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done); break;
+        default: k_apply_pressures<0, 8><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done); break;
+        }
     }
 }
-void launch_dfsph_divergence(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st) {
+void launch_dfsph_divergence(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st, int chunk) {
     if (comp) {
-        k_dfsph_divergence<1><<<tiles, kTile, 0, st>>>(a);
+    switch (chunk) {
+        case 1: k_dfsph_divergence<1, 1><<<tiles, kTile, 0, st>>>(a); break;
+        case 4: k_dfsph_divergence<1, 4><<<tiles, kTile, 0, st>>>(a); break;
+        default: k_dfsph_divergence<1, 8><<<tiles, kTile, 0, st>>>(a); break;
+        }
     } else {
-        k_dfsph_divergence<0><<<tiles, kTile, 0, st>>>(a);
+    switch (chunk) {
+        case 1: k_dfsph_divergence<0, 1><<<tiles, kTile, 0, st>>>(a); break;
+        case 4: k_dfsph_divergence<0, 4><<<tiles, kTile, 0, st>>>(a); break;
+        default: k_dfsph_divergence<0, 8><<<tiles, kTile, 0, st>>>(a); break;
+        }
     }
 }
-void launch_dfsph_density(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st) {
+void launch_dfsph_density(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st, int chunk) {
     if (comp) {
-        k_dfsph_density<1><<<tiles, kTile, 0, st>>>(a);
+    switch (chunk) {
+        case 1: k_dfsph_density<1, 1><<<tiles, kTile, 0, st>>>(a); break;
+        case 4: k_dfsph_density<1, 4><<<tiles, kTile, 0, st>>>(a); break;
+        default: k_dfsph_density<1, 8><<<tiles, kTile, 0, st>>>(a); break;
+        }
     } else {
-        k_dfsph_density<0><<<tiles, kTile, 0, st>>>(a);
+    switch (chunk) {
+        case 1: k_dfsph_density<0, 1><<<tiles, kTile, 0, st>>>(a); break;
+        case 4: k_dfsph_density<0, 4><<<tiles, kTile, 0, st>>>(a); break;
+        default: k_dfsph_density<0, 8><<<tiles, kTile, 0, st>>>(a); break;
+        }
     }
 }
 void launch_integrate_positions(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st) {
@@ -1223,11 +1253,19 @@ void launch_iisph_density_dii(Arena const& a, uint32_t tiles, cudaStream_t st) {
 void launch_iisph_aii(Arena const& a, uint32_t tiles, cudaStream_t st) {
     k_iisph_aii<<<tiles, kTile, 0, st>>>(a);
 }
-void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st) {
-    k_iisph_sum_dij<<<tiles, kTile, 0, st>>>(a);
+void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk) {
+    switch (chunk) {
+    case 1: k_iisph_sum_dij<1><<<tiles, kTile, 0, st>>>(a); break;
+    case 4: k_iisph_sum_dij<4><<<tiles, kTile, 0, st>>>(a); break;
+    default: k_iisph_sum_dij<8><<<tiles, kTile, 0, st>>>(a); break;
+    }
 }
-void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st) {
-    k_iisph_beta_pressure<<<tiles, kTile, 0, st>>>(a);
+void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk) {
+    switch (chunk) {
+    case 1: k_iisph_beta_pressure<1><<<tiles, kTile, 0, st>>>(a); break;
+    case 4: k_iisph_beta_pressure<4><<<tiles, kTile, 0, st>>>(a); break;
+    default: k_iisph_beta_pressure<8><<<tiles, kTile, 0, st>>>(a); break;
+    }
 }
 void launch_make_q(Arena const& a, uint32_t tiles, cudaStream_t st) {
     k_make_q<<<tiles, kTile, 0, st>>>(a);

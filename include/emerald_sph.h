@@ -256,6 +256,27 @@ int emerald_batch_set_stream(emerald_batch* batch, void* cuda_stream);
 int emerald_batch_synchronize(emerald_batch* batch);
 int emerald_batch_kernel_launches(emerald_batch* batch, int64_t* count);
 
+/* -------------------------------------------------------------- autotuning */
+
+/* Neighbour entries each gather-sum kernel loads together (1, 4 or 8). Every
+ * choice gives the same bits. Autotuning (DFSPH_P and IISPH) times a few
+ * whole sub-steps of `method` with each candidate setting, every candidate
+ * from the same state (restored afterwards, so the simulation is left as it
+ * was), after at least one sub-step of that method, and keeps the fastest,
+ * also for later simulations and batches of the same method and size class
+ * (log2 of the active particle count). candidate_ms[k]: mean sub-step time
+ * of candidate k, whose chunks are candidate_chunks[k] (apply, divergence,
+ * iisph_sum, iisph_beta). No counterpart in the reference. */
+typedef struct emerald_tuning {
+    int32_t apply_chunk, divergence_chunk, iisph_sum_chunk, iisph_beta_chunk;
+    int32_t candidates;
+    int32_t candidate_chunks[8][4];
+    float candidate_ms[8];
+} emerald_tuning;
+
+int emerald_sim_autotune(emerald_sim* sim, int32_t method, emerald_tuning* out);
+int emerald_batch_autotune(emerald_batch* batch, int32_t method, emerald_tuning* out);
+
 /* ----------------------------------------------------------------- serving */
 
 /* A request loop over batches: requests (a scene and a sub-step count) are
