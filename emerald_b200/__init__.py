@@ -168,7 +168,7 @@ EXPORTS = {
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            "emerald_b200: %s is missing; build it with `python -m emerald_b200.build` "
+            "emerald_b200: %s is missing; build it with `python emerald_b200/build.py` "
             "(there is no CPU fallback)" % LIB_PATH)
     lib = ctypes.CDLL(LIB_PATH)
     for name, (res, args) in EXPORTS.items():
