@@ -196,6 +196,14 @@ def _f32(a, shape_tail=None):
     return a
 
 
+def _out_array(a, n):
+    if a is None:
+        return np.zeros((n, 2), np.float32)
+    if a.dtype != np.float32 or a.shape != (n, 2) or not a.flags.c_contiguous:
+        raise ValueError("output array must be C-contiguous float32 of shape (%d, 2)" % n)
+    return a
+
+
 def method_id(method):
     return METHODS[method] if isinstance(method, str) else int(method)
 
@@ -353,9 +361,12 @@ class Simulation:
         _check(lib.emerald_sim_time(self._h, ctypes.byref(t)), "time")
         return t.value
 
-    def state(self):
-        x = np.zeros((self.n, 2), np.float32)
-        v = np.zeros((self.n, 2), np.float32)
+    def state(self, x=None, v=None):
+        """Positions and velocities (original order). Given x / v (C-contiguous
+        float32 arrays of shape (n, 2), e.g. pinned host memory) are filled in
+        place instead of new arrays."""
+        x = _out_array(x, self.n)
+        v = _out_array(v, self.n)
         _check(lib.emerald_sim_get_state(self._h, _ptr(x), _ptr(v)), "get_state")
         return x, v
 

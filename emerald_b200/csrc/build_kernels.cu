@@ -250,6 +250,60 @@ __device__ __forceinline__ int find_neighbors_reg(float2 pos, uint32_t self, boo
     return cnt;
 }
 
+// The search of find_neighbors_reg with the sorted list in shared memory:
+// entry k of this thread at list[k * kTile], an accepted key shifts only the
+// entries above it (fewer instructions than the register bubble, measured
+// 6% faster on B200). Above kRegList entries the caller redoes the particle
+// with the 64-entry list.
+__device__ __forceinline__ int find_neighbors_smem(float2 pos, uint32_t self, bool same_set,
+                                                   float cell, float max_distance, float reject_l2,
+                                                   OtherSet const& o, uint64_t* list) {
+    int32_t gx, gy;
+    grid_coord(pos, cell, gx, gy);
+    uint64_t const sx0 = spread_bits(static_cast<uint32_t>(gx - 1));
+    uint64_t const sx1 = spread_bits(static_cast<uint32_t>(gx));
+    uint64_t const sx2 = spread_bits(static_cast<uint32_t>(gx + 1));
+    uint64_t const sy0 = spread_bits(static_cast<uint32_t>(gy - 1)) << 1;
+    uint64_t const sy1 = spread_bits(static_cast<uint32_t>(gy)) << 1;
+    uint64_t const sy2 = spread_bits(static_cast<uint32_t>(gy + 1)) << 1;
+    int cnt = 0;
+#pragma unroll 1
+    for (int jj = 0; jj < 3 && cnt < kMaxNeighbors; ++jj) {
+        uint64_t const zy = jj == 0 ? sy0 : (jj == 1 ? sy1 : sy2);
+#pragma unroll 1
+        for (int kk = 0; kk < 3 && cnt < kMaxNeighbors; ++kk) {
+            uint64_t const zx = kk == 0 ? sx0 : (kk == 1 ? sx1 : sx2);
+            uint32_t slot;
+            if (!table_find(o.keys, o.log2cap, zx | zy, slot)) continue;
+            uint32_t const b = o.start[slot];
+            uint32_t const e = b + o.count[slot];
+#pragma unroll 1
+            for (uint32_t m = b; cnt < kMaxNeighbors && m != e; ++m) {
+                uint32_t const other = o.members[m];
+                if (same_set && other == self) continue;
+                float2 const vec = sub2(o.x[other], pos);
+                if (vec.x * vec.x + vec.y * vec.y >= reject_l2) continue;
+                float const dist = length2f(vec);
+                if (dist >= max_distance) continue;
+                uint64_t const key = (static_cast<uint64_t>(__float_as_uint(dist)) << 32) |
+                                     static_cast<uint64_t>(original_index(o, other));
+                if (cnt < kRegList) {
+                    int p = cnt;
+                    while (p > 0) {
+                        uint64_t const prev = list[(p - 1) * kTile];
+                        if (prev < key) break;
+                        list[p * kTile] = prev;
+                        --p;
+                    }
+                    list[p * kTile] = key;
+                }
+                ++cnt;
+            }
+        }
+    }
+    return cnt;
+}
+
 // Writes list entry k of particle i: index, W and GradW(-vector_to)
 // (compute_neighbor_kernels / compute_neighbor_kernel_gradients,
 // emerald/sph_common/neighborhood.cpp:178-210), the vector recomputed from
@@ -323,6 +377,49 @@ __global__ void __launch_bounds__(kTile) k_neighbors(Arena a, int write_kernels)
     }
     bool const kernels = write_kernels != 0;
     float2 const pos = a.x[i];
+    if (SOLID_OTHER && P.near_w) {
+        int32_t gx, gy;
+        grid_coord(pos, cell, gx, gy);
+        int64_t const ix = int64_t(gx) - P.near_x0;
+        int64_t const iy = int64_t(gy) - P.near_y0;
+        bool near = false;
+        if (ix >= 0 && iy >= 0 && ix < int64_t(P.near_w) && iy < int64_t(P.near_h)) {
+            uint64_t const bit = uint64_t(iy) * P.near_w + uint64_t(ix);
+            near = (a.near_bits[P.near_begin + (bit >> 5)] >> (bit & 31u)) & 1u;
+        }
+        if (!near) {
+            cnt_out[i] = 0;
+            return;
+        }
+    }
+    if (!(COMP && P.precision && kernels)) {
+        __shared__ uint64_t s_list[kRegList * kTile];
+        uint64_t* const list = s_list + threadIdx.x;
+        int const cnt = find_neighbors_smem(pos, i, !SOLID_OTHER, cell, cell, P.reject_l2, o, list);
+        cnt_out[i] = static_cast<uint8_t>(cnt);
+        if (cnt <= kRegList) {
+#pragma unroll 1
+            for (int k = 0; k < cnt; ++k) {
+                uint64_t const key = list[k * kTile];
+                write_entry(idx_out, w_out, gw_out, static_cast<size_t>(k) * stride + i,
+                            stored_slot(o, static_cast<uint32_t>(key & 0xffffffffu)),
+                            __uint_as_float(static_cast<uint32_t>(key >> 32)), pos, o.x, h,
+                            kernels);
+            }
+            return;
+        }
+        uint64_t full[kMaxNeighbors];
+        int const n64 = find_neighbors(pos, i, !SOLID_OTHER, cell, cell, o, full);
+#pragma unroll 1
+        for (int k = 0; k < n64; ++k) {
+            write_entry(idx_out, w_out, gw_out, static_cast<size_t>(k) * stride + i,
+                        stored_slot(o, static_cast<uint32_t>(full[k] & 0xffffffffu)),
+                        __uint_as_float(static_cast<uint32_t>(full[k] >> 32)), pos, o.x, h,
+                        kernels);
+        }
+        return;
+    }
+    // compensated scenes: the register list, with entries from double positions
     uint64_t r[kRegList];
     int const cnt = find_neighbors_reg(pos, i, !SOLID_OTHER, cell, cell, P.reject_l2, o, r);
     cnt_out[i] = static_cast<uint8_t>(cnt);

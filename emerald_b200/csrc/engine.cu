@@ -3,11 +3,13 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <climits>
 #include <atomic>
 #include <cstring>
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 namespace emerald {
 
@@ -109,6 +111,7 @@ size_t Engine::footprint(uint32_t fluid_capacity, uint32_t solid_capacity, int m
                    r(4 * (S / kTile));
     bytes += 12 * r(8 * N) + 18 * r(4 * N) + 2 * r(N);   // per-particle state and scratch
     bytes += 2 * r(16 * N);                                 // double positions and their staging
+    bytes += r(4 * (N / 4 + 64 * M));                       // boundary-proximity maps
     bytes += r(sort_scratch_bytes(uint32_t(N)));            // storage-order sort
     bytes += 2 * (2 * r(4 * E) + r(8 * E));                 // fluid and solid neighbour lists
     bytes += r(8 * ftab) + 2 * r(4 * ftab);                 // fluid cell table
@@ -133,6 +136,7 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
     if (ftab > 0xffffffffull || stab > 0xffffffffull) throw std::runtime_error("arena too large");
     ftab_ = RangeAllocator(uint32_t(ftab));
     stab_ = RangeAllocator(uint32_t(stab));
+    near_words_ = RangeAllocator(uint32_t(fluid_cap_ / 4 + 64ull * max_scenes_));
 
     auto dev = [&](size_t bytes) -> void* {
         void* p = nullptr;
@@ -183,6 +187,8 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
     a_.tkdiv = static_cast<float*>(dev(4 * N));
     a_.tkdens = static_cast<float*>(dev(4 * N));
     a_.toid = static_cast<uint32_t*>(dev(4 * N));
+    d_near_ = static_cast<uint32_t*>(dev(4ull * near_words_.capacity()));
+    a_.near_bits = d_near_;
     a_.x64 = static_cast<double2*>(dev(16 * N));
     a_.tx64 = static_cast<double2*>(dev(16 * N));
     order_buf_ = dev(sort_scratch_bytes(uint32_t(N)));
@@ -222,7 +228,10 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
     a_.loop_iterations = d_loop_iters_;
     cudaMemset(d_loop_iters_, 0, sizeof(unsigned long long) * 4);
     if (cudaStreamCreateWithFlags(&cap_st_, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&body_st_, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamCreateWithFlags(&body_st_, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&side_st_, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming) != cudaSuccess) {
         throw std::runtime_error("stream creation failed");
     }
     if (cudaMallocHost(reinterpret_cast<void**>(&h_running_), sizeof(int)) != cudaSuccess) {
@@ -252,6 +261,9 @@ Engine::~Engine() {
     destroy_graphs();
     if (cap_st_) cudaStreamDestroy(cap_st_);
     if (body_st_) cudaStreamDestroy(body_st_);
+    if (side_st_) cudaStreamDestroy(side_st_);
+    if (ev_fork_) cudaEventDestroy(ev_fork_);
+    if (ev_join_) cudaEventDestroy(ev_join_);
     for (auto& p : pending_) {
         cudaEventDestroy(p.start);
         cudaEventDestroy(p.stop);
@@ -433,6 +445,7 @@ int Engine::add_scene(SceneSpec const& spec) {
     P.sort_base = 0;
     P.reject_l2 = reject_threshold(P.cell_size);
     P.precision = ep.precision;
+    build_near_map(sc, spec.solid_xy, spec.n_solid);
     scenes_[id] = sc;
 
     for (uint32_t t = 0; t < sc.ftile_count; ++t) tile_scene_[ft + t] = id;
@@ -477,6 +490,55 @@ int Engine::add_scene(SceneSpec const& spec) {
     }
     check("add_scene");
     return id;
+}
+
+// Marks the 3x3 cell block around every boundary particle's cell (the cells
+// whose particles can have that boundary particle within the search radius,
+// emerald/sph_common/neighborhood.h:199-282), with the same float cell
+// arithmetic as the kernels. No map when the boundary is empty, its cell box
+// is above 2^26 cells, or the map arena is full.
+void Engine::build_near_map(Scene& sc, float const* solid_xy, uint32_t n_solid) {
+    SceneParams& P = sc.p;
+    P.near_w = P.near_h = 0;
+    P.near_begin = 0;
+    P.near_x0 = P.near_y0 = 0;
+    sc.near_words = 0;
+    if (!n_solid || !solid_xy) return;
+    std::vector<int32_t> cx(n_solid), cy(n_solid);
+    int64_t x0 = INT64_MAX, y0 = INT64_MAX, x1 = INT64_MIN, y1 = INT64_MIN;
+    for (uint32_t k = 0; k < n_solid; ++k) {
+        grid_coord(mk2(solid_xy[2 * k], solid_xy[2 * k + 1]), P.cell_size, cx[k], cy[k]);
+        x0 = std::min<int64_t>(x0, cx[k]);
+        y0 = std::min<int64_t>(y0, cy[k]);
+        x1 = std::max<int64_t>(x1, cx[k]);
+        y1 = std::max<int64_t>(y1, cy[k]);
+    }
+    int64_t const w = x1 - x0 + 3, h = y1 - y0 + 3;
+    if (w * h > (int64_t(1) << 26)) return;
+    uint64_t const words = (uint64_t(w) * uint64_t(h) + 31) / 32;
+    uint32_t begin = 0;
+    if (!near_words_.alloc(uint32_t(words), begin)) return;
+    std::vector<uint32_t> bits(words, 0u);
+    for (uint32_t k = 0; k < n_solid; ++k) {
+        for (int dy = 0; dy < 3; ++dy) {
+            for (int dx = 0; dx < 3; ++dx) {
+                uint64_t const b =
+                  uint64_t(cy[k] - y0 + dy) * uint64_t(w) + uint64_t(cx[k] - x0 + dx);
+                bits[b >> 5] |= 1u << (b & 31u);
+            }
+        }
+    }
+    if (cudaMemcpy(d_near_ + begin, bits.data(), 4 * words, cudaMemcpyHostToDevice) != cudaSuccess) {
+        near_words_.release(begin, uint32_t(words));
+        check("near map upload");
+        return;
+    }
+    P.near_begin = begin;
+    P.near_w = uint32_t(w);
+    P.near_h = uint32_t(h);
+    P.near_x0 = int32_t(x0 - 1);
+    P.near_y0 = int32_t(y0 - 1);
+    sc.near_words = uint32_t(words);
 }
 
 void Engine::rebuild_solids() {
@@ -534,6 +596,7 @@ void Engine::remove_scene(int id) {
     solid_tiles_.release(sc.stile_begin, sc.stile_count);
     ftab_.release(sc.p.ftab_begin, sc.ftab_size);
     stab_.release(sc.p.stab_begin, sc.stab_size);
+    if (sc.near_words) near_words_.release(sc.p.near_begin, sc.near_words);
     sc = Scene{};
     update_sort_bases();
     update_extent();
@@ -701,10 +764,27 @@ void Engine::emit_substep(int32_t method, bool reorder) {
     launch("begin_substep", [&] { launch_begin_substep(a_, max_scenes_, st); });
     // binning, three scan passes, scatter, per-cell ordering
     Arena const ext = extent_arena();
-    launch("build_cells", [&] { launch_build_cells(ext, false, tiles, d_scan_, st); }, 6);
     bool const kernels = method != kPcisph;
+    // The boundary lists read only positions and the static boundary tables,
+    // so they are built on a side stream (a parallel branch of the graph)
+    // while the fluid cells and fluid lists are built; the per-kernel timing
+    // mode keeps everything on one stream.
+    bool const fork = !timing_;
+    if (fork) {
+        cudaEventRecord(ev_fork_, st);
+        cudaStreamWaitEvent(side_st_, ev_fork_, 0);
+        launch("neighbors_solid",
+               [&] { launch_neighbors(a_, tiles, true, kernels, side_st_, compensated_); });
+        cudaEventRecord(ev_join_, side_st_);
+    }
+    launch("build_cells", [&] { launch_build_cells(ext, false, tiles, d_scan_, st); }, 6);
     launch("neighbors_fluid", [&] { launch_neighbors(a_, tiles, false, kernels, st, compensated_); });
-    launch("neighbors_solid", [&] { launch_neighbors(a_, tiles, true, kernels, st, compensated_); });
+    if (fork) {
+        cudaStreamWaitEvent(st, ev_join_, 0);
+    } else {
+        launch("neighbors_solid",
+               [&] { launch_neighbors(a_, tiles, true, kernels, st, compensated_); });
+    }
     switch (method) {
     case kDfsph:
         launch("dfsph_density_alpha", [&] { launch_dfsph_density_alpha(a_, tiles, compensated_, st); });

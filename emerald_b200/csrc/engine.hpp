@@ -167,6 +167,7 @@ private:
         SceneParams p{};
         uint32_t ftile_begin = 0, ftile_count = 0, stile_begin = 0, stile_count = 0;
         uint32_t ftab_size = 0, stab_size = 0;
+        uint32_t near_words = 0;
         bool active = false;
     };
 
@@ -183,6 +184,8 @@ private:
     void destroy_graphs();
     int max_iterations(int kind) const;
     void rebuild_solids();
+    // Boundary-proximity map of a scene from its boundary positions.
+    void build_near_map(Scene& sc, float const* solid_xy, uint32_t n_solid);
     // Extent of the arena the per-sub-step launches cover: the highest tile
     // and cell-table slot any resident scene uses, rounded up to 1/32 of the
     // capacity so that graphs are re-captured only when it moves by that much.
@@ -207,7 +210,8 @@ private:
     int* h_running_ = nullptr;
     std::vector<Scene> scenes_;
     std::vector<int32_t> tile_scene_, stile_scene_;
-    RangeAllocator fluid_tiles_, solid_tiles_, ftab_, stab_;
+    RangeAllocator fluid_tiles_, solid_tiles_, ftab_, stab_, near_words_;
+    uint32_t* d_near_ = nullptr;
     bool tiles_dirty_ = true;
     bool unrolled_ = false;
     bool use_graphs_ = true;
@@ -215,6 +219,8 @@ private:
     cudaStream_t cur_ = nullptr;  // stream the emitted work goes to
     cudaStream_t cap_st_ = nullptr;
     cudaStream_t body_st_ = nullptr;
+    cudaStream_t side_st_ = nullptr;  // parallel branch of a sub-step
+    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     std::map<int32_t, cudaGraphExec_t> graphs_;        // key: method * 2 + reorder
     std::map<int32_t, int64_t> graph_fixed_kernels_;
     int reorder_every_ = 16;

@@ -55,6 +55,12 @@ struct SceneParams {
     uint32_t sort_base;  // real particles of scenes stored before this one
     float reject_l2;     // smallest float whose sqrtf is >= cell_size
     int32_t precision;   // 0: the reference's FP32 arithmetic; 1: compensated (DFSPH_P)
+    // Cells within one cell of a boundary particle's cell: bit
+    // (y - near_y0) * near_w + (x - near_x0) of the words from near_begin.
+    // A fluid particle whose cell is clear has no boundary neighbours.
+    // near_w == 0: no map (every particle searches).
+    uint32_t near_begin, near_w, near_h;
+    int32_t near_x0, near_y0;
 };
 
 // Mutable per-scene state, device resident.
@@ -122,6 +128,7 @@ struct Arena {
     float* tkdiv;
     float* tkdens;
     uint32_t* toid;
+    uint32_t const* near_bits;  // boundary-proximity maps of the scenes
     double2* x64;   // positions accumulated in double (compensated mode)
     double2* tx64;
 
