@@ -573,6 +573,35 @@ __global__ void k_scan_apply(uint32_t const* in, uint32_t n, uint32_t const* sum
     }
 }
 
+// Cell ranges in one pass: every block scans its slots' counts and takes its
+// range of the members array with one atomic on the cursor count[n], which
+// the caller cleared with the counts. Cells land in block order, not slot
+// order; each cell's members stay contiguous, which is all the searches and
+// the sort products read (start[cell], count[cell]).
+__global__ void k_cell_ranges(uint32_t const* count, uint32_t n, uint32_t* start) {
+    size_t const base = static_cast<size_t>(blockIdx.x) * kScanBlock + threadIdx.x * kScanItems;
+    uint32_t vals[kScanItems];
+    uint32_t t = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        size_t const e = base + k;
+        vals[k] = e < n ? count[e] : 0u;
+        t += vals[k];
+    }
+    uint32_t excl;
+    uint32_t const total = block_exclusive_scan(t, excl);
+    __shared__ uint32_t block_base;
+    if (threadIdx.x == 0) {
+        block_base = total ? atomicAdd(const_cast<uint32_t*>(count) + n, total) : 0u;
+    }
+    __syncthreads();
+    uint32_t run = block_base + excl;
+    for (int k = 0; k < kScanItems; ++k) {
+        size_t const e = base + k;
+        if (e < n) start[e] = run;
+        run += vals[k];
+    }
+}
+
 }  // namespace
 
 uint32_t scan_scratch_words(uint32_t n) { return (n + kScanBlock - 1) / kScanBlock + 1; }
@@ -586,21 +615,26 @@ void launch_exclusive_scan(uint32_t const* in, uint32_t n, uint32_t* out, uint32
     k_scan_apply<<<nb, kScanThreads, 0, st>>>(in, n, scratch, out);
 }
 
+// The count arrays hold one word more than the table: the cursor of
+// k_cell_ranges, cleared with the counts.
 void launch_build_cells(Arena const& a, bool solid, uint32_t tiles, uint32_t* scan_scratch,
                         cudaStream_t st) {
+    (void)scan_scratch;
     if (solid) {
         cudaMemsetAsync(a.skeys, 0xff, sizeof(uint64_t) * a.stab_total, st);
-        cudaMemsetAsync(a.scount, 0, sizeof(uint32_t) * a.stab_total, st);
+        cudaMemsetAsync(a.scount, 0, sizeof(uint32_t) * (a.stab_total + 1), st);
         k_bin<true><<<tiles, kTile, 0, st>>>(a);
-        launch_exclusive_scan(a.scount, a.stab_total, a.sstart, scan_scratch, st);
+        k_cell_ranges<<<(a.stab_total + kScanBlock - 1) / kScanBlock, kScanThreads, 0, st>>>(
+          a.scount, a.stab_total, a.sstart);
         k_scatter<true><<<tiles, kTile, 0, st>>>(a);
         k_sort_cells<<<(a.stab_total + 255) / 256, 256, 0, st>>>(a.scount, a.sstart, a.smembers,
                                                                  nullptr, a.stab_total);
     } else {
         cudaMemsetAsync(a.fkeys, 0xff, sizeof(uint64_t) * a.ftab_total, st);
-        cudaMemsetAsync(a.fcount, 0, sizeof(uint32_t) * a.ftab_total, st);
+        cudaMemsetAsync(a.fcount, 0, sizeof(uint32_t) * (a.ftab_total + 1), st);
         k_bin<false><<<tiles, kTile, 0, st>>>(a);
-        launch_exclusive_scan(a.fcount, a.ftab_total, a.fstart, scan_scratch, st);
+        k_cell_ranges<<<(a.ftab_total + kScanBlock - 1) / kScanBlock, kScanThreads, 0, st>>>(
+          a.fcount, a.ftab_total, a.fstart);
         k_scatter<false><<<tiles, kTile, 0, st>>>(a);
         k_sort_cells<<<(a.ftab_total + 255) / 256, 256, 0, st>>>(a.fcount, a.fstart, a.members,
                                                                  a.oid, a.ftab_total);

@@ -114,9 +114,9 @@ size_t Engine::footprint(uint32_t fluid_capacity, uint32_t solid_capacity, int m
     bytes += r(4 * (N / 4 + 64 * M));                       // boundary-proximity maps
     bytes += r(sort_scratch_bytes(uint32_t(N)));            // storage-order sort
     bytes += 2 * (2 * r(4 * E) + r(8 * E));                 // fluid and solid neighbour lists
-    bytes += r(8 * ftab) + 2 * r(4 * ftab);                 // fluid cell table
+    bytes += r(8 * ftab) + r(4 * (ftab + 1)) + r(4 * ftab); // fluid cell table
     bytes += 3 * r(8 * S) + 4 * r(4 * S);                   // solid particles
-    bytes += r(8 * stab) + 2 * r(4 * stab);                 // solid cell table
+    bytes += r(8 * stab) + r(4 * (stab + 1)) + r(4 * stab); // solid cell table
     size_t const scan_words = std::max(scan_scratch_words(uint32_t(ftab)),
                                        scan_scratch_words(uint32_t(stab))) + 64;
     bytes += r(4 * scan_words) + r(sizeof(int)) + r(sizeof(unsigned long long) * 4);
@@ -207,7 +207,7 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
     a_.zkey = static_cast<uint64_t*>(dev(8 * N));
     a_.ftab_total = ftab_.capacity();
     a_.fkeys = static_cast<uint64_t*>(dev(8ull * a_.ftab_total));
-    a_.fcount = static_cast<uint32_t*>(dev(4ull * a_.ftab_total));
+    a_.fcount = static_cast<uint32_t*>(dev(4ull * (a_.ftab_total + 1)));  // + range cursor
     a_.fstart = static_cast<uint32_t*>(dev(4ull * a_.ftab_total));
     a_.xs = static_cast<float2*>(dev(8 * S));
     a_.vs = static_cast<float2*>(dev(8 * S));
@@ -218,7 +218,7 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
     a_.szkey = static_cast<uint64_t*>(dev(8 * S));
     a_.stab_total = stab_.capacity();
     a_.skeys = static_cast<uint64_t*>(dev(8ull * a_.stab_total));
-    a_.scount = static_cast<uint32_t*>(dev(4ull * a_.stab_total));
+    a_.scount = static_cast<uint32_t*>(dev(4ull * (a_.stab_total + 1)));
     a_.sstart = static_cast<uint32_t*>(dev(4ull * a_.stab_total));
     uint32_t const scan_words =
       std::max(scan_scratch_words(a_.ftab_total), scan_scratch_words(a_.stab_total)) + 64;
@@ -543,7 +543,7 @@ void Engine::build_near_map(Scene& sc, float const* solid_xy, uint32_t n_solid) 
 
 void Engine::rebuild_solids() {
     Arena const e = extent_arena();
-    launch("build_cells_solid", [&] { launch_build_cells(e, true, ext_stiles_, d_scan_, st_); }, 6);
+    launch("build_cells_solid", [&] { launch_build_cells(e, true, ext_stiles_, d_scan_, st_); }, 4);
 }
 
 namespace {
@@ -762,7 +762,7 @@ void Engine::emit_substep(int32_t method, bool reorder) {
     }
     launch("max_v2", [&] { launch_max_v2(a_, tiles, st); });
     launch("begin_substep", [&] { launch_begin_substep(a_, max_scenes_, st); });
-    // binning, three scan passes, scatter, per-cell ordering
+    // binning, cell ranges, scatter, per-cell ordering
     Arena const ext = extent_arena();
     bool const kernels = method != kPcisph;
     // The boundary lists read only positions and the static boundary tables,
@@ -777,7 +777,7 @@ void Engine::emit_substep(int32_t method, bool reorder) {
                [&] { launch_neighbors(a_, tiles, true, kernels, side_st_, compensated_); });
         cudaEventRecord(ev_join_, side_st_);
     }
-    launch("build_cells", [&] { launch_build_cells(ext, false, tiles, d_scan_, st); }, 6);
+    launch("build_cells", [&] { launch_build_cells(ext, false, tiles, d_scan_, st); }, 4);
     launch("neighbors_fluid", [&] { launch_neighbors(a_, tiles, false, kernels, st, compensated_); });
     if (fork) {
         cudaStreamWaitEvent(st, ev_join_, 0);

@@ -45,6 +45,9 @@ constexpr size_t kOffZkey = align256(kOffMembers + size_t(kMaxPoints) * 4);
 constexpr size_t kOffScan = align256(kOffZkey + size_t(kMaxPoints) * 8);
 constexpr size_t kScratchBytes = align256(kOffScan + size_t(kScanWords) * 4);
 
+// The cell build keeps a cursor one word past the counts.
+static_assert(kOffStart >= kOffCount + (size_t(kTableSize) + 1) * 4, "count cursor overlaps starts");
+
 static __device__ __align__(256) unsigned char g_static_scratch[kScratchBytes];
 
 // Writes the one-scene description the build kernels read.
