@@ -395,7 +395,7 @@ def run_serving(args, torch, E):
     reqs = W.serving_requests(args.serving_requests)
     scenes = [W.scene_for(r["nx"], r["ny"], r["seed"]) for r in reqs]
     srv = E.Server(120 * 10**9, "dfsph_p", max_scenes=max(64, len(reqs)),
-                   max_substeps_per_launch=8)
+                   max_substeps_per_launch=8, lanes=args.serving_lanes)
     ids = [None] * len(reqs)
     t_start = time.perf_counter()
 
@@ -426,6 +426,7 @@ def run_serving(args, torch, E):
            "request_ms_p99": round(float(np.percentile(total_ms, 99)), 1),
            "queue_ms_p99": round(st["queue_ms_p99"], 1),
            "resident_peak": st["resident_peak"], "arena_bytes": st["device_bytes"],
+           "lanes": args.serving_lanes,
            "max_avg_density_error": max(d[2]["error_average"] for d in done),
            "requests_above_0.1%": int(sum(d[2]["error_average"] > 0.001 for d in done))}
     # the same requests one at a time, bounded in time
@@ -549,6 +550,8 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=96,
                     help="requests of the served workload (0: skip it)")
     ap.add_argument("--serving-plain-seconds", type=float, default=30.0)
+    ap.add_argument("--serving-lanes", type=int, default=16,
+                    help="batch arenas the request loop steps concurrently")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -101,7 +101,15 @@ __global__ void k_max_v2(Arena a) {
     }
     uint32_t mb = (c.live && d == d && d > 0.0f) ? __float_as_uint(d) : 0u;
     for (int o = 16; o; o >>= 1) mb = max(mb, __shfl_xor_sync(0xffffffffu, mb, o));
-    if ((threadIdx.x & 31) == 0 && mb) atomicMax(&a.ss[c.s].max_v2, mb);
+    // one atomic per tile (a block is one scene's tile)
+    __shared__ uint32_t wmax[kTile / 32];
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = mb;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < kTile / 32; ++w) t = max(t, wmax[w]);
+        if (t) atomicMax(&a.ss[c.s].max_v2, t);
+    }
 }
 
 __device__ int64_t to_flicks_x86(double s) {
