@@ -3,8 +3,8 @@
 #include "engine.hpp"
 
 #include <algorithm>
-#include <climits>
 #include <atomic>
+#include <climits>
 #include <cstring>
 #include <mutex>
 #include <stdexcept>
@@ -734,7 +734,11 @@ void Engine::run_loop(int kind, int max_iter, int32_t method) {
             throw std::runtime_error("graph capture: body");
         }
         cur_ = body_st_;
-        emit_loop_body(kind, method, cond, true);
+        // Several iterations per body launch: every body kernel returns at
+        // once for scenes that have converged and the last exit test sets
+        // the loop condition, so the results are those of one iteration per
+        // body, with fewer body launches.
+        for (int u = 0; u < loop_unroll_; ++u) emit_loop_body(kind, method, cond, true);
         cur_ = outer;
         if (cudaStreamEndCapture(body_st_, &body) != cudaSuccess) {
             throw std::runtime_error("graph capture: body end");

@@ -223,7 +223,14 @@ private:
     cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     std::map<int32_t, cudaGraphExec_t> graphs_;        // key: method * 2 + reorder
     std::map<int32_t, int64_t> graph_fixed_kernels_;
-    int reorder_every_ = 16;
+#ifndef EMERALD_REORDER_EVERY
+#define EMERALD_REORDER_EVERY 16
+#endif
+    int reorder_every_ = EMERALD_REORDER_EVERY;
+#ifndef EMERALD_LOOP_UNROLL
+#define EMERALD_LOOP_UNROLL 3
+#endif
+    int loop_unroll_ = EMERALD_LOOP_UNROLL;  // solver iterations per conditional-loop body
     int64_t substeps_launched_ = 0;
     void* order_buf_ = nullptr;
     SortScratch order_sort_{};

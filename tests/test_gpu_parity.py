@@ -208,8 +208,9 @@ def test_large_scene_matches_oracle(E, oracle):
 
 @pytest.mark.parametrize("method", METHODS)
 def test_graph_and_eager_modes_agree(E, method):
-    """A sub-step as one CUDA graph (solver loops as conditional nodes) and
-    as host-driven kernel launches give the same bits and iteration counts."""
+    """A sub-step as one CUDA graph (solver loops as conditional nodes, three
+    iterations per body launch) and as host-driven kernel launches (one exit
+    test on the host per iteration) give the same bits and iteration counts."""
     scene = E.BlockScene(32, dx=F(1 / 64), seed=8, time_per_step_flicks=1411200, sub_steps=4,
                          iisph_max_pressure_iterations=50,
                          iisph_error_average_threshold=F(0.001))
@@ -223,7 +224,9 @@ def test_graph_and_eager_modes_agree(E, method):
         assert sa["pressure_iterations"] == sb["pressure_iterations"]
         assert_bitwise(a.state()[0], b.state()[0], "x")
         assert_bitwise(a.state()[1], b.state()[1], "v")
-    assert a.kernel_launches() == b.kernel_launches()
+    # a graph's loop body runs several iterations; kernels of iterations past
+    # convergence launch and return at once, so graphs launch at least as many
+    assert a.kernel_launches() >= b.kernel_launches()
 
 
 def test_dense_cells_take_the_fallback_path(E, oracle):
