@@ -62,9 +62,12 @@ Server::Server(emerald_server_config const& cfg) : cfg_(cfg) {
         uint32_t fluid = 0, solid = 0;
         capacities(per_lane_budget, per_lane_scenes, fluid, solid);
         lane->engine.reset(new Engine(fluid, solid, per_lane_scenes));
-        if (cudaStreamCreateWithFlags(&lane->stream, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreate(&lane->ev0) != cudaSuccess || cudaEventCreate(&lane->ev1) != cudaSuccess) {
-            throw std::runtime_error("stream or event creation failed");
+        if (cudaStreamCreateWithFlags(&lane->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            throw std::runtime_error("stream creation failed");
+        }
+        lane->marks.resize(size_t(cfg_.max_substeps_per_launch) + 1);
+        for (auto& e : lane->marks) {
+            if (cudaEventCreate(&e) != cudaSuccess) throw std::runtime_error("event creation failed");
         }
         lane->engine->set_stream(lane->stream);
         lane->room = lane->engine->room();
@@ -88,8 +91,9 @@ Server::~Server() {
     for (auto& lane : lanes_) {
         lane->engine.reset();
         if (lane->stream) cudaStreamDestroy(lane->stream);
-        if (lane->ev0) cudaEventDestroy(lane->ev0);
-        if (lane->ev1) cudaEventDestroy(lane->ev1);
+        for (auto e : lane->marks) {
+            if (e) cudaEventDestroy(e);
+        }
     }
 }
 
@@ -224,12 +228,16 @@ void Server::loop(Lane& lane) {
         std::vector<float> step_ms(size_t(std::max(k, 0)));
         int status = EMERALD_OK;
         try {
+            // the round's sub-steps back to back, one host wait at the end
+            cudaEventRecord(lane.marks[0], lane.stream);
             for (int32_t s = 0; s < k; ++s) {
-                cudaEventRecord(lane.ev0, lane.stream);
                 engine.substep(cfg_.method);
-                cudaEventRecord(lane.ev1, lane.stream);
-                cudaEventSynchronize(lane.ev1);
-                cudaEventElapsedTime(&step_ms[size_t(s)], lane.ev0, lane.ev1);
+                cudaEventRecord(lane.marks[size_t(s) + 1], lane.stream);
+            }
+            cudaEventSynchronize(lane.marks[size_t(k)]);
+            for (int32_t s = 0; s < k; ++s) {
+                cudaEventElapsedTime(&step_ms[size_t(s)], lane.marks[size_t(s)],
+                                     lane.marks[size_t(s) + 1]);
             }
             engine.check("server sub-step");
         } catch (std::exception const&) {

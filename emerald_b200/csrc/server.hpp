@@ -64,7 +64,8 @@ private:
         int index = 0;
         std::unique_ptr<Engine> engine;
         cudaStream_t stream = nullptr;
-        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        // marks[s] and marks[s + 1] bracket sub-step s of a launch round
+        std::vector<cudaEvent_t> marks;
         std::thread worker;
         std::vector<std::unique_ptr<ServerRequest>> running;
         // guarded by mu_
