@@ -104,6 +104,13 @@ class Tuning(ctypes.Structure):
                                for k in range(self.candidates)]}
 
 
+class Neighborhood(ctypes.Structure):
+    """emerald_neighborhood: device pointers of the reference's
+    Neighborhood_pointers layout (64 entries per particle, row-major)."""
+    _fields_ = [("counts", c_vp), ("indices", c_vp), ("distances", c_vp), ("vectors_to", c_vp),
+                ("kernels", c_vp), ("kernel_gradients", c_vp)]
+
+
 EXPORTS = {
     "emerald_default_params": (c_i32, [ctypes.POINTER(Params)]),
     "emerald_config": (c_i32, [ctypes.POINTER(Params), c_vp]),
@@ -159,6 +166,30 @@ EXPORTS = {
     "emerald_server_get_stats": (c_i32, [c_vp, ctypes.POINTER(ServerStats)]),
     "emerald_sim_autotune": (c_i32, [c_vp, c_i32, ctypes.POINTER(Tuning)]),
     "emerald_batch_autotune": (c_i32, [c_vp, c_i32, ctypes.POINTER(Tuning)]),
+    "emerald_compute_grid_coords": (c_i32, [c_sz, c_f, c_f, c_f, c_vp, c_vp, c_vp]),
+    "emerald_compute_z_indices": (c_i32, [c_sz, c_vp, c_vp, c_vp]),
+    "emerald_compute_neighbor_distances_and_vectors_to": (c_i32, [c_sz, c_vp, c_vp, c_vp, c_vp,
+                                                                  c_vp, c_vp, c_vp]),
+    "emerald_compute_neighbor_kernels": (c_i32, [c_sz, c_f, c_vp, c_vp, c_vp, c_vp]),
+    "emerald_compute_neighbor_kernel_gradients": (c_i32, [c_sz, c_f, c_vp, c_vp, c_vp, c_vp]),
+    "emerald_compute_densities": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp, Neighborhood, c_vp,
+                                          Neighborhood, c_vp]),
+    "emerald_compute_divergences": (c_i32, [c_sz, c_f, c_vp, c_vp, c_vp, Neighborhood, c_vp, c_vp,
+                                            Neighborhood, c_vp]),
+    "emerald_predict_density_stars": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp, c_vp,
+                                              Neighborhood, c_vp, c_vp, Neighborhood, c_vp]),
+    "emerald_apply_pressures_in_place": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp, c_vp,
+                                                 Neighborhood, c_vp, Neighborhood, c_vp]),
+    "emerald_compute_pressure_accelerations": (c_i32, [c_sz, c_f, c_vp, c_vp, c_vp, c_vp,
+                                                       Neighborhood, c_vp, Neighborhood, c_vp]),
+    "emerald_integrate_velocities_with_forces": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp, c_vp]),
+    "emerald_integrate_velocities": (c_i32, [c_sz, c_f, c_vp, c_vp, c_vp]),
+    "emerald_integrate_positions": (c_i32, [c_sz, c_f, c_vp, c_vp, c_vp]),
+    "emerald_compute_constant_volumes": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp]),
+    "emerald_max_vector_squared_magnitude": (c_i32, [c_sz, c_vp, c_vp, c_vp]),
+    "emerald_max_density_error": (c_i32, [c_sz, c_f, c_vp, c_vp, c_vp]),
+    "emerald_cfl_maximum_time_step": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp]),
+    "emerald_scalar_average_and_max": (c_i32, [c_sz, c_f, c_vp, c_vp, c_vp]),
     "emerald_neighbors_static": (c_i32, [c_vp, c_u32, c_f, c_vp, c_vp, c_vp, c_vp, c_u32, c_vp]),
     "emerald_kernel_launches": (c_i64, []),
     "emerald_last_error": (ctypes.c_char_p, []),

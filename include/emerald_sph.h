@@ -334,6 +334,105 @@ int emerald_server_wait(emerald_server* server, int64_t request, int32_t timeout
                         float* v, emerald_step_stats* stats, emerald_request_timing* timing);
 int emerald_server_get_stats(emerald_server* server, emerald_server_stats* out);
 
+/* ------------------------------------------- sph_common functions on device */
+
+/* The emerald/sph_common free functions on device memory, one call each, in
+ * the reference's argument order (count first, outputs before inputs) and
+ * arithmetic order: for the same inputs the outputs are bit-identical to the
+ * reference's. Every pointer is device memory; V2f arrays are interleaved
+ * (x, y) floats. Calls are asynchronous on `stream` (NULL: the legacy
+ * default stream) and allocate nothing. Reductions write their result to
+ * device memory. */
+
+/* Neighborhood_pointers (emerald/sph_common/neighborhood.h:126-133): counts
+ * per particle and, per particle, NEIGHBORHOOD_MAX_COUNT = 64 entries of
+ * each array, row-major (particle i's entry k at i * 64 + k). Members a call
+ * does not read may be NULL; a NULL `counts` in a solid neighbourhood skips
+ * the boundary pass. */
+typedef struct emerald_neighborhood {
+    uint8_t const* counts;
+    uint64_t const* indices;
+    float const* distances;
+    float const* vectors_to;       /* 2 floats per entry */
+    float const* kernels;
+    float const* kernel_gradients; /* 2 floats per entry */
+} emerald_neighborhood;
+
+/* compute_grid_coords (emerald/sph_common/common.cpp:57-67): int32 pairs. */
+int emerald_compute_grid_coords(size_t n, float cell_size, float bounds_min_x, float bounds_min_y,
+                                int32_t* grid_coords, float const* positions, void* stream);
+/* compute_z_indices (emerald/sph_common/common.cpp:69-76). */
+int emerald_compute_z_indices(size_t n, uint64_t* z_indices, int32_t const* grid_coords,
+                              void* stream);
+/* compute_neighbor_distances_and_vectors_to (emerald/sph_common/neighborhood.cpp:154-176). */
+int emerald_compute_neighbor_distances_and_vectors_to(size_t n, float* distances,
+                                                      float* vectors_to,
+                                                      float const* self_positions,
+                                                      float const* other_positions,
+                                                      uint8_t const* counts,
+                                                      uint64_t const* indices, void* stream);
+/* compute_neighbor_kernels / compute_neighbor_kernel_gradients
+ * (emerald/sph_common/neighborhood.cpp:178-210). */
+int emerald_compute_neighbor_kernels(size_t n, float support, float* kernels,
+                                     uint8_t const* counts, float const* distances, void* stream);
+int emerald_compute_neighbor_kernel_gradients(size_t n, float support, float* kernel_gradients,
+                                              uint8_t const* counts, float const* vectors_to,
+                                              void* stream);
+/* compute_densities (emerald/sph_common/density.cpp:47-72). */
+int emerald_compute_densities(size_t n, float support, float target_density, float* densities,
+                              float const* fluid_volumes, emerald_neighborhood fluid,
+                              float const* solid_volumes, emerald_neighborhood solid,
+                              void* stream);
+/* compute_divergences (emerald/sph_common/divergence.cpp:47-74). */
+int emerald_compute_divergences(size_t n, float target_density, float* divergences,
+                                float const* fluid_volumes, float const* fluid_velocities,
+                                emerald_neighborhood fluid, float const* solid_volumes,
+                                float const* solid_velocities, emerald_neighborhood solid,
+                                void* stream);
+/* predict_density_stars (emerald/sph_common/density.cpp:85-109). */
+int emerald_predict_density_stars(size_t n, float dt, float target_density, float* density_stars,
+                                  float const* densities, float const* fluid_volumes,
+                                  float const* fluid_velocities, emerald_neighborhood fluid,
+                                  float const* solid_volumes, float const* solid_velocities,
+                                  emerald_neighborhood solid, void* stream);
+/* apply_pressures_in_place (emerald/sph_common/pressure.cpp:52-80). */
+int emerald_apply_pressures_in_place(size_t n, float dt, float target_density, float* velocities,
+                                     float const* densities, float const* pressures,
+                                     float const* fluid_volumes, emerald_neighborhood fluid,
+                                     float const* solid_volumes, emerald_neighborhood solid,
+                                     void* stream);
+/* compute_pressure_accelerations (emerald/sph_common/pressure.cpp:154-178). */
+int emerald_compute_pressure_accelerations(size_t n, float target_density,
+                                           float* pressure_accelerations, float const* pressures,
+                                           float const* densities, float const* fluid_volumes,
+                                           emerald_neighborhood fluid, float const* solid_volumes,
+                                           emerald_neighborhood solid, void* stream);
+/* integrate_velocities_in_place with forces / with accelerations, and
+ * integrate_positions_in_place (emerald/sph_common/dynamics.cpp:24-51). */
+int emerald_integrate_velocities_with_forces(size_t n, float dt, float target_density,
+                                             float* velocities, float const* volumes,
+                                             float const* forces, void* stream);
+int emerald_integrate_velocities(size_t n, float dt, float* velocities,
+                                 float const* accelerations, void* stream);
+int emerald_integrate_positions(size_t n, float dt, float* positions, float const* velocities,
+                                void* stream);
+/* compute_constant_volumes (emerald/sph_common/volume.cpp:7-14). */
+int emerald_compute_constant_volumes(size_t n, float target_density, float mass_per_particle,
+                                     float* volumes, void* stream);
+/* max_vector_squared_magnitude and max_density_error
+ * (emerald/sph_common/common.cpp:78-92): *result (device) receives the value. */
+int emerald_max_vector_squared_magnitude(size_t n, float* result, float const* vectors,
+                                         void* stream);
+int emerald_max_density_error(size_t n, float target_density, float* result,
+                              float const* densities, void* stream);
+/* cfl_maximum_time_step (emerald/sph_common/cfl.cpp:12-21): *flicks (device). */
+int emerald_cfl_maximum_time_step(size_t n, float support, float factor, int64_t* flicks,
+                                  float const* velocities, void* stream);
+/* compute_scalar_average_and_max (emerald/sph_common/common.h:209-240):
+ * average_and_max (device) receives {average, max}. */
+int emerald_scalar_average_and_max(size_t n, float discretization, float* average_and_max,
+                                   float const* values, void* stream);
+
 /* ---------------------------------------------------- allocation-free build */
 
 /* No counterpart in the reference (which always allocates its std::vector

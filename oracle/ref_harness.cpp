@@ -22,6 +22,11 @@
 #include <emerald/sph2d_box/solids.h>
 #include <emerald/sph_common/common.h>
 #include <emerald/sph_common/neighborhood.h>
+#include <emerald/sph_common/cfl.h>
+#include <emerald/sph_common/density.h>
+#include <emerald/sph_common/divergence.h>
+#include <emerald/sph_common/dynamics.h>
+#include <emerald/sph_common/pressure.h>
 #include <emerald/sph_common/volume.h>
 #include <emerald/z_index/z_index.h>
 
@@ -557,6 +562,178 @@ float ref_max_vector_squared_magnitude(size_t n, float const* xy) {
 int64_t ref_cfl_maximum_time_step(size_t n, float support, float factor, float const* v_xy) {
     auto const v = to_v2f(v_xy, n);
     return cfl_maximum_time_step(n, support, factor, v.data()).count();
+}
+
+}  // extern "C"
+
+// ------------------------------------------------ sph_common free functions
+//
+// The reference's sph_common functions on flat host arrays, for comparing
+// the library's device versions with them: neighbour lists arrive row-major
+// (64 entries per particle, 64-bit indices) and are copied into the
+// reference's Neighborhood_vectors.
+
+namespace {
+
+Neighborhood_vectors nbhd_from(size_t n, uint8_t const* counts, uint64_t const* idx,
+                               float const* dist, float const* vec, float const* w,
+                               float const* gw) {
+    Neighborhood_vectors nb;
+    nb.resize(n);
+    for (size_t i = 0; i < n; ++i) {
+        nb.counts[i] = counts ? counts[i] : 0;
+        for (size_t k = 0; k < NEIGHBORHOOD_MAX_COUNT; ++k) {
+            size_t const e = i * NEIGHBORHOOD_MAX_COUNT + k;
+            nb.indices[i][k] = idx ? size_t(idx[e]) : 0;
+            nb.distances[i][k] = dist ? dist[e] : 0.0f;
+            nb.vectors_to[i][k] = vec ? V2f{vec[2 * e], vec[2 * e + 1]} : V2f{0.0f, 0.0f};
+            nb.kernels[i][k] = w ? w[e] : 0.0f;
+            nb.kernel_gradients[i][k] = gw ? V2f{gw[2 * e], gw[2 * e + 1]} : V2f{0.0f, 0.0f};
+        }
+    }
+    return nb;
+}
+
+}  // namespace
+
+extern "C" {
+
+void ref_common_grid_coords(size_t n, float cell, float bx, float by, int32_t* gc,
+                            float const* xy) {
+    auto const p = to_v2f(xy, n);
+    std::vector<V2i> out(n);
+    compute_grid_coords(n, cell, V2f{bx, by}, out.data(), p.data());
+    for (size_t i = 0; i < n; ++i) {
+        gc[2 * i] = out[i][0];
+        gc[2 * i + 1] = out[i][1];
+    }
+}
+
+void ref_common_z_indices(size_t n, uint64_t* z, int32_t const* gc) {
+    std::vector<V2i> g(n);
+    for (size_t i = 0; i < n; ++i) g[i] = V2i{gc[2 * i], gc[2 * i + 1]};
+    compute_z_indices(n, z, g.data());
+}
+
+void ref_common_distances_vectors(size_t n, size_t n_other, float* dist, float* vec,
+                                  float const* self_xy, float const* other_xy,
+                                  uint8_t const* counts, uint64_t const* idx) {
+    auto const p = to_v2f(self_xy, n);
+    auto const o = to_v2f(other_xy, n_other);
+    auto nb = nbhd_from(n, counts, idx, nullptr, nullptr, nullptr, nullptr);
+    compute_neighbor_distances_and_vectors_to(n, nb.distances.data(), nb.vectors_to.data(),
+                                              p.data(), o.data(), nb.counts.data(),
+                                              nb.indices.data());
+    for (size_t i = 0; i < n; ++i) {
+        for (size_t k = 0; k < NEIGHBORHOOD_MAX_COUNT; ++k) {
+            size_t const e = i * NEIGHBORHOOD_MAX_COUNT + k;
+            dist[e] = nb.distances[i][k];
+            vec[2 * e] = nb.vectors_to[i][k][0];
+            vec[2 * e + 1] = nb.vectors_to[i][k][1];
+        }
+    }
+}
+
+void ref_common_kernels(size_t n, float support, float* w, float* gw, uint8_t const* counts,
+                        float const* dist, float const* vec) {
+    auto nb = nbhd_from(n, counts, nullptr, dist, vec, nullptr, nullptr);
+    compute_neighbor_kernels(n, support, nb.kernels.data(), nb.counts.data(), nb.distances.data());
+    compute_neighbor_kernel_gradients(n, support, nb.kernel_gradients.data(), nb.counts.data(),
+                                      nb.vectors_to.data());
+    for (size_t i = 0; i < n; ++i) {
+        for (size_t k = 0; k < NEIGHBORHOOD_MAX_COUNT; ++k) {
+            size_t const e = i * NEIGHBORHOOD_MAX_COUNT + k;
+            w[e] = nb.kernels[i][k];
+            gw[2 * e] = nb.kernel_gradients[i][k][0];
+            gw[2 * e + 1] = nb.kernel_gradients[i][k][1];
+        }
+    }
+}
+
+void ref_common_densities(size_t n, float support, float rho0, float* out, float const* fvol,
+                          uint8_t const* fc, uint64_t const* fi, float const* fw,
+                          float const* svol, uint8_t const* sc, uint64_t const* si,
+                          float const* sw) {
+    auto const f = nbhd_from(n, fc, fi, nullptr, nullptr, fw, nullptr);
+    auto const s = nbhd_from(n, sc, si, nullptr, nullptr, sw, nullptr);
+    compute_densities(n, support, rho0, out, fvol, f.pointers(), svol, s.pointers());
+}
+
+void ref_common_divergences(size_t n, float rho0, float* out, float const* fvol,
+                            float const* fvel, uint8_t const* fc, uint64_t const* fi,
+                            float const* fgw, float const* svol, float const* svel, size_t n_solid,
+                            uint8_t const* sc, uint64_t const* si, float const* sgw) {
+    auto const f = nbhd_from(n, fc, fi, nullptr, nullptr, nullptr, fgw);
+    auto const s = nbhd_from(n, sc, si, nullptr, nullptr, nullptr, sgw);
+    auto const fv = to_v2f(fvel, n);
+    auto const sv = to_v2f(svel, n_solid);
+    compute_divergences(n, rho0, out, fvol, fv.data(), f.pointers(), svol, sv.data(),
+                        s.pointers());
+}
+
+void ref_common_density_stars(size_t n, float dt, float rho0, float* out, float const* rho,
+                              float const* fvol, float const* fvel, uint8_t const* fc,
+                              uint64_t const* fi, float const* fgw, float const* svol,
+                              float const* svel, size_t n_solid, uint8_t const* sc,
+                              uint64_t const* si, float const* sgw) {
+    auto const f = nbhd_from(n, fc, fi, nullptr, nullptr, nullptr, fgw);
+    auto const s = nbhd_from(n, sc, si, nullptr, nullptr, nullptr, sgw);
+    auto const fv = to_v2f(fvel, n);
+    auto const sv = to_v2f(svel, n_solid);
+    predict_density_stars(n, dt, rho0, out, rho, fvol, fv.data(), f.pointers(), svol, sv.data(),
+                          s.pointers());
+}
+
+void ref_common_apply_pressures(size_t n, float dt, float rho0, float* vel, float const* rho,
+                                float const* p, float const* fvol, uint8_t const* fc,
+                                uint64_t const* fi, float const* fgw, float const* svol,
+                                uint8_t const* sc, uint64_t const* si, float const* sgw) {
+    auto const f = nbhd_from(n, fc, fi, nullptr, nullptr, nullptr, fgw);
+    auto const s = nbhd_from(n, sc, si, nullptr, nullptr, nullptr, sgw);
+    auto v = to_v2f(vel, n);
+    apply_pressures_in_place(n, dt, rho0, v.data(), rho, p, fvol, f.pointers(), svol,
+                             s.pointers());
+    copy_out(v, vel);
+}
+
+void ref_common_pressure_accelerations(size_t n, float rho0, float* acc, float const* p,
+                                       float const* rho, float const* fvol, uint8_t const* fc,
+                                       uint64_t const* fi, float const* fgw, float const* svol,
+                                       uint8_t const* sc, uint64_t const* si, float const* sgw) {
+    auto const f = nbhd_from(n, fc, fi, nullptr, nullptr, nullptr, fgw);
+    auto const s = nbhd_from(n, sc, si, nullptr, nullptr, nullptr, sgw);
+    std::vector<V2f> a(n);
+    compute_pressure_accelerations(n, rho0, a.data(), p, rho, fvol, f.pointers(), svol,
+                                   s.pointers());
+    copy_out(a, acc);
+}
+
+void ref_common_integrate(size_t n, float dt, float rho0, float* vel_forces, float* vel_acc,
+                          float* pos, float const* vol, float const* forces, float const* acc,
+                          float const* vel_for_pos) {
+    auto vf = to_v2f(vel_forces, n);
+    auto const f = to_v2f(forces, n);
+    integrate_velocities_in_place(n, dt, rho0, vf.data(), vol, f.data());
+    copy_out(vf, vel_forces);
+    auto va = to_v2f(vel_acc, n);
+    auto const a = to_v2f(acc, n);
+    integrate_velocities_in_place(n, dt, va.data(), a.data());
+    copy_out(va, vel_acc);
+    auto x = to_v2f(pos, n);
+    auto const v = to_v2f(vel_for_pos, n);
+    integrate_positions_in_place(n, dt, x.data(), v.data());
+    copy_out(x, pos);
+}
+
+void ref_common_constant_volumes(size_t n, float rho0, float mass, float* vol) {
+    compute_constant_volumes(n, rho0, mass, vol);
+}
+
+void ref_common_average_and_max(size_t n, float discretization, float const* values,
+                                float* out) {
+    auto const r = compute_scalar_average_and_max(n, discretization, values);
+    out[0] = r.first;
+    out[1] = r.second;
 }
 
 }  // extern "C"

@@ -285,6 +285,19 @@ class Reference:
         L.ref_max_vector_squared_magnitude.argtypes = [c_sz, c_vp]
         L.ref_cfl_maximum_time_step.restype = c_i64
         L.ref_cfl_maximum_time_step.argtypes = [c_sz, c_f, c_f, c_vp]
+        # the sph_common functions on flat arrays (row-major 64-entry lists)
+        L.ref_common_grid_coords.argtypes = [c_sz, c_f, c_f, c_f, c_vp, c_vp]
+        L.ref_common_z_indices.argtypes = [c_sz, c_vp, c_vp]
+        L.ref_common_distances_vectors.argtypes = [c_sz, c_sz, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]
+        L.ref_common_kernels.argtypes = [c_sz, c_f, c_vp, c_vp, c_vp, c_vp, c_vp]
+        L.ref_common_densities.argtypes = [c_sz, c_f, c_f] + [c_vp] * 9
+        L.ref_common_divergences.argtypes = [c_sz, c_f] + [c_vp] * 8 + [c_sz] + [c_vp] * 3
+        L.ref_common_density_stars.argtypes = [c_sz, c_f, c_f] + [c_vp] * 9 + [c_sz] + [c_vp] * 3
+        L.ref_common_apply_pressures.argtypes = [c_sz, c_f, c_f] + [c_vp] * 11
+        L.ref_common_pressure_accelerations.argtypes = [c_sz, c_f] + [c_vp] * 11
+        L.ref_common_integrate.argtypes = [c_sz, c_f, c_f] + [c_vp] * 7
+        L.ref_common_constant_volumes.argtypes = [c_sz, c_f, c_f, c_vp]
+        L.ref_common_average_and_max.argtypes = [c_sz, c_f, c_vp, c_vp]
         self.L = L
 
     def default_params(self):

@@ -1,0 +1,295 @@
+"""The sph_common free functions on device memory against the reference's
+own functions (compiled from its sources), on the same inputs: every output
+bit for bit.
+
+Inputs: a jittered 24x24 block with its tank walls, neighbour lists from the
+oracle's search (equal to the reference's), and seeded velocities, pressures,
+densities and per-particle volumes."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import assert_bitwise
+from cpu_checkers import ptr
+from scenes import F
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def E():
+    import emerald_b200
+    return emerald_b200
+
+
+@pytest.fixture(scope="module")
+def case(E, oracle):
+    scene = E.BlockScene(24, dx=F(1 / 48), seed=21)
+    fluid = scene.fluid.astype(np.float32)
+    solid = scene.solid.astype(np.float32)
+    cell = F(2 * scene.support)
+    fc, fi, fd, fv = oracle.neighborhoods(fluid, fluid, True, cell)
+    sc, si, sd, sv = oracle.neighborhoods(fluid, solid, False, cell)
+    rng = np.random.Generator(np.random.PCG64(5))
+    n, ns = len(fluid), len(solid)
+    c = dict(
+        n=n, ns=ns, support=np.float32(scene.support), cell=cell, rho0=F(1000.0),
+        fluid=fluid, solid=solid,
+        fc=fc, fi=fi.astype(np.uint64), fd=fd, fv=np.ascontiguousarray(fv),
+        sc=sc, si=si.astype(np.uint64), sd=sd, sv=np.ascontiguousarray(sv),
+        fvol=(F(1 / 48) ** 2 * (1 + rng.uniform(-0.05, 0.05, n))).astype(np.float32),
+        svol=(F(1 / 48) ** 2 * (1 + rng.uniform(-0.05, 0.05, ns))).astype(np.float32),
+        vel=rng.normal(0, 0.3, (n, 2)).astype(np.float32),
+        svel=rng.normal(0, 0.05, (ns, 2)).astype(np.float32),
+        rho=(1000 + rng.normal(0, 20, n)).astype(np.float32),
+        p=np.abs(rng.normal(0, 500, n)).astype(np.float32),
+        acc=rng.normal(0, 2, (n, 2)).astype(np.float32),
+        forces=rng.normal(0, 1e-3, (n, 2)).astype(np.float32),
+    )
+    c["p"][::7] = 0.0
+    return c
+
+
+def dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+class Keep:
+    """Device copies that stay alive until the test ends (a temporary
+    tensor's memory may be reused before an asynchronous kernel reads it)."""
+
+    def __init__(self):
+        self.held = []
+
+    def __call__(self, a):
+        t = dev(a)
+        self.held.append(t)
+        return t.data_ptr()
+
+
+def host(t):
+    import torch
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def nbhd(E, counts, idx=None, dist=None, vec=None, w=None, gw=None):
+    keep = [x for x in (counts, idx, dist, vec, w, gw) if x is not None]
+    nb = E.Neighborhood(*[None if x is None else x.data_ptr() for x in
+                          (counts, idx, dist, vec, w, gw)])
+    nb._keep = keep
+    return nb
+
+
+def check(rc):
+    assert rc == 0, rc
+
+
+def test_grid_coords_and_z_indices(E, reference, case):
+    K = Keep()
+    n = case["n"]
+    x = dev(case["fluid"])
+    gc = dev(np.zeros((n, 2), np.int32))
+    check(E.lib.emerald_compute_grid_coords(n, case["cell"], F(-0.1), F(-0.05), gc.data_ptr(),
+                                            x.data_ptr(), None))
+    ref = np.zeros((n, 2), np.int32)
+    reference.L.ref_common_grid_coords(n, case["cell"], F(-0.1), F(-0.05), ptr(ref),
+                                       ptr(case["fluid"]))
+    assert_bitwise(host(gc), ref, "grid coords")
+    z = dev(np.zeros(n, np.uint64))
+    check(E.lib.emerald_compute_z_indices(n, z.data_ptr(), gc.data_ptr(), None))
+    rz = np.zeros(n, np.uint64)
+    reference.L.ref_common_z_indices(n, ptr(rz), ptr(ref))
+    assert_bitwise(host(z), rz, "z indices")
+
+
+def test_neighbor_geometry_and_kernels(E, reference, case):
+    K = Keep()
+    n, ns = case["n"], case["ns"]
+    for counts, idx, other in ((case["fc"], case["fi"], case["fluid"]),
+                               (case["sc"], case["si"], case["solid"])):
+        dist = dev(np.zeros((n, 64), np.float32))
+        vec = dev(np.zeros((n, 64, 2), np.float32))
+        check(E.lib.emerald_compute_neighbor_distances_and_vectors_to(
+            n, dist.data_ptr(), vec.data_ptr(), K(case["fluid"]),
+            K(other), K(counts), K(idx), None))
+        rd = np.zeros((n, 64), np.float32)
+        rv = np.zeros((n, 64, 2), np.float32)
+        reference.L.ref_common_distances_vectors(n, len(other), ptr(rd), ptr(rv),
+                                                 ptr(case["fluid"]), ptr(other), ptr(counts),
+                                                 ptr(idx))
+        mask = np.arange(64)[None, :] < counts[:, None]
+        assert_bitwise(np.where(mask, host(dist), 0), np.where(mask, rd, 0), "distances")
+        assert_bitwise(np.where(mask[..., None], host(vec), 0), np.where(mask[..., None], rv, 0),
+                       "vectors_to")
+        w = dev(np.zeros((n, 64), np.float32))
+        gw = dev(np.zeros((n, 64, 2), np.float32))
+        c_d = dev(counts)
+        check(E.lib.emerald_compute_neighbor_kernels(n, case["support"], w.data_ptr(),
+                                                     c_d.data_ptr(), dist.data_ptr(), None))
+        check(E.lib.emerald_compute_neighbor_kernel_gradients(n, case["support"], gw.data_ptr(),
+                                                              c_d.data_ptr(), vec.data_ptr(),
+                                                              None))
+        rw = np.zeros((n, 64), np.float32)
+        rgw = np.zeros((n, 64, 2), np.float32)
+        reference.L.ref_common_kernels(n, case["support"], ptr(rw), ptr(rgw), ptr(counts),
+                                       ptr(rd), ptr(rv))
+        assert_bitwise(np.where(mask, host(w), 0), np.where(mask, rw, 0), "kernels")
+        assert_bitwise(np.where(mask[..., None], host(gw), 0), np.where(mask[..., None], rgw, 0),
+                       "kernel gradients")
+    case["fw"], case["fgw"] = reference_kernels(reference, case, case["fc"], case["fd"], case["fv"])
+    case["sw"], case["sgw"] = reference_kernels(reference, case, case["sc"], case["sd"], case["sv"])
+
+
+def reference_kernels(reference, case, counts, dist, vec):
+    n = case["n"]
+    rw = np.zeros((n, 64), np.float32)
+    rgw = np.zeros((n, 64, 2), np.float32)
+    reference.L.ref_common_kernels(n, case["support"], ptr(rw), ptr(rgw), ptr(counts),
+                                   ptr(np.ascontiguousarray(dist)), ptr(vec))
+    return rw, rgw
+
+
+def lists(E, reference, case):
+    if "fw" not in case:
+        case["fw"], case["fgw"] = reference_kernels(reference, case, case["fc"], case["fd"],
+                                                    case["fv"])
+        case["sw"], case["sgw"] = reference_kernels(reference, case, case["sc"], case["sd"],
+                                                    case["sv"])
+    d = {k: dev(case[k]) for k in ("fc", "fi", "fw", "fgw", "sc", "si", "sw", "sgw")}
+    f = nbhd(E, d["fc"], d["fi"], None, None, d["fw"], d["fgw"])
+    s = nbhd(E, d["sc"], d["si"], None, None, d["sw"], d["sgw"])
+    return f, s
+
+
+def test_densities_divergences_and_stars(E, reference, case):
+    K = Keep()
+    n, ns = case["n"], case["ns"]
+    f, s = lists(E, reference, case)
+    fvol, svol = dev(case["fvol"]), dev(case["svol"])
+    rho = dev(np.zeros(n, np.float32))
+    check(E.lib.emerald_compute_densities(n, case["support"], case["rho0"], rho.data_ptr(),
+                                          fvol.data_ptr(), f, svol.data_ptr(), s, None))
+    rr = np.zeros(n, np.float32)
+    reference.L.ref_common_densities(n, case["support"], case["rho0"], ptr(rr), ptr(case["fvol"]),
+                                     ptr(case["fc"]), ptr(case["fi"]), ptr(case["fw"]),
+                                     ptr(case["svol"]), ptr(case["sc"]), ptr(case["si"]),
+                                     ptr(case["sw"]))
+    assert_bitwise(host(rho), rr, "densities")
+    vel, svel = dev(case["vel"]), dev(case["svel"])
+    div = dev(np.zeros(n, np.float32))
+    check(E.lib.emerald_compute_divergences(n, case["rho0"], div.data_ptr(), fvol.data_ptr(),
+                                            vel.data_ptr(), f, svol.data_ptr(), svel.data_ptr(),
+                                            s, None))
+    rd = np.zeros(n, np.float32)
+    reference.L.ref_common_divergences(n, case["rho0"], ptr(rd), ptr(case["fvol"]),
+                                       ptr(case["vel"]), ptr(case["fc"]), ptr(case["fi"]),
+                                       ptr(case["fgw"]), ptr(case["svol"]), ptr(case["svel"]), ns,
+                                       ptr(case["sc"]), ptr(case["si"]), ptr(case["sgw"]))
+    assert_bitwise(host(div), rd, "divergences")
+    stars = dev(np.zeros(n, np.float32))
+    dt = F(3e-4)
+    check(E.lib.emerald_predict_density_stars(n, dt, case["rho0"], stars.data_ptr(),
+                                              K(case["rho"]), fvol.data_ptr(),
+                                              vel.data_ptr(), f, svol.data_ptr(),
+                                              svel.data_ptr(), s, None))
+    rs = np.zeros(n, np.float32)
+    reference.L.ref_common_density_stars(n, dt, case["rho0"], ptr(rs), ptr(case["rho"]),
+                                         ptr(case["fvol"]), ptr(case["vel"]), ptr(case["fc"]),
+                                         ptr(case["fi"]), ptr(case["fgw"]), ptr(case["svol"]),
+                                         ptr(case["svel"]), ns, ptr(case["sc"]), ptr(case["si"]),
+                                         ptr(case["sgw"]))
+    assert_bitwise(host(stars), rs, "density stars")
+
+
+def test_pressure_terms(E, reference, case):
+    K = Keep()
+    n = case["n"]
+    f, s = lists(E, reference, case)
+    fvol, svol = dev(case["fvol"]), dev(case["svol"])
+    rho, p = dev(case["rho"]), dev(case["p"])
+    vel = dev(case["vel"])
+    dt = F(2.5e-4)
+    check(E.lib.emerald_apply_pressures_in_place(n, dt, case["rho0"], vel.data_ptr(),
+                                                 rho.data_ptr(), p.data_ptr(), fvol.data_ptr(), f,
+                                                 svol.data_ptr(), s, None))
+    rv = case["vel"].copy()
+    reference.L.ref_common_apply_pressures(n, dt, case["rho0"], ptr(rv), ptr(case["rho"]),
+                                           ptr(case["p"]), ptr(case["fvol"]), ptr(case["fc"]),
+                                           ptr(case["fi"]), ptr(case["fgw"]), ptr(case["svol"]),
+                                           ptr(case["sc"]), ptr(case["si"]), ptr(case["sgw"]))
+    assert_bitwise(host(vel), rv, "velocities after apply_pressures_in_place")
+    acc = dev(np.zeros((n, 2), np.float32))
+    check(E.lib.emerald_compute_pressure_accelerations(n, case["rho0"], acc.data_ptr(),
+                                                       p.data_ptr(), rho.data_ptr(),
+                                                       fvol.data_ptr(), f, svol.data_ptr(), s,
+                                                       None))
+    ra = np.zeros((n, 2), np.float32)
+    reference.L.ref_common_pressure_accelerations(n, case["rho0"], ptr(ra), ptr(case["p"]),
+                                                  ptr(case["rho"]), ptr(case["fvol"]),
+                                                  ptr(case["fc"]), ptr(case["fi"]),
+                                                  ptr(case["fgw"]), ptr(case["svol"]),
+                                                  ptr(case["sc"]), ptr(case["si"]),
+                                                  ptr(case["sgw"]))
+    assert_bitwise(host(acc), ra, "pressure accelerations")
+
+
+def test_integration_volumes_and_reductions(E, reference, case):
+    K = Keep()
+    n = case["n"]
+    dt = F(4e-4)
+    vf, va, x = dev(case["vel"]), dev(case["vel"]), dev(case["fluid"])
+    check(E.lib.emerald_integrate_velocities_with_forces(n, dt, case["rho0"], vf.data_ptr(),
+                                                         K(case["fvol"]),
+                                                         K(case["forces"]), None))
+    check(E.lib.emerald_integrate_velocities(n, dt, va.data_ptr(), K(case["acc"]),
+                                             None))
+    check(E.lib.emerald_integrate_positions(n, dt, x.data_ptr(), K(case["vel"]),
+                                            None))
+    rvf, rva, rx = case["vel"].copy(), case["vel"].copy(), case["fluid"].copy()
+    reference.L.ref_common_integrate(n, dt, case["rho0"], ptr(rvf), ptr(rva), ptr(rx),
+                                     ptr(case["fvol"]), ptr(case["forces"]), ptr(case["acc"]),
+                                     ptr(case["vel"]))
+    assert_bitwise(host(vf), rvf, "velocities from forces")
+    assert_bitwise(host(va), rva, "velocities from accelerations")
+    assert_bitwise(host(x), rx, "positions")
+    vol = dev(np.zeros(n, np.float32))
+    check(E.lib.emerald_compute_constant_volumes(n, case["rho0"], F(0.37), vol.data_ptr(), None))
+    rvol = np.zeros(n, np.float32)
+    reference.L.ref_common_constant_volumes(n, case["rho0"], F(0.37), ptr(rvol))
+    assert_bitwise(host(vol), rvol, "constant volumes")
+    out = dev(np.zeros(1, np.float32))
+    check(E.lib.emerald_max_vector_squared_magnitude(n, out.data_ptr(),
+                                                     K(case["vel"]), None))
+    assert host(out)[0] == reference.L.ref_max_vector_squared_magnitude(n, ptr(case["vel"]))
+    check(E.lib.emerald_max_density_error(n, case["rho0"], out.data_ptr(),
+                                          K(case["rho"]), None))
+    assert host(out)[0] == reference.L.ref_max_density_error(n, case["rho0"], ptr(case["rho"]))
+    fl = dev(np.zeros(1, np.int64))
+    for factor in (F(0.4), F(0.2)):
+        check(E.lib.emerald_cfl_maximum_time_step(n, case["support"], factor, fl.data_ptr(),
+                                                  K(case["vel"]), None))
+        assert host(fl)[0] == reference.L.ref_cfl_maximum_time_step(n, case["support"], factor,
+                                                                    ptr(case["vel"]))
+    zeros = dev(np.zeros((n, 2), np.float32))
+    check(E.lib.emerald_cfl_maximum_time_step(n, case["support"], F(0.4), fl.data_ptr(),
+                                              zeros.data_ptr(), None))
+    assert host(fl)[0] == reference.L.ref_cfl_maximum_time_step(
+        n, case["support"], F(0.4), ptr(np.zeros((n, 2), np.float32)))
+    vals = np.random.Generator(np.random.PCG64(9)).normal(0, 0.01, n).astype(np.float32)
+    am = dev(np.zeros(2, np.float32))
+    for disc in (F(1000.0), F(37.0)):
+        check(E.lib.emerald_scalar_average_and_max(n, disc, am.data_ptr(), K(vals),
+                                                   None))
+        ram = np.zeros(2, np.float32)
+        reference.L.ref_common_average_and_max(n, disc, ptr(vals), ptr(ram))
+        assert_bitwise(host(am), ram, "average and max")
+
+
+def test_empty_and_invalid(E):
+    K = Keep()
+    assert E.lib.emerald_compute_densities(0, F(0.01), F(1000), None, None, E.Neighborhood(),
+                                           None, E.Neighborhood(), None) == 0
+    assert E.lib.emerald_compute_neighbor_kernels(10, F(0.0), None, None, None, None) == 22
