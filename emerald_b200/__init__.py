@@ -190,6 +190,46 @@ EXPORTS = {
     "emerald_max_density_error": (c_i32, [c_sz, c_f, c_vp, c_vp, c_vp]),
     "emerald_cfl_maximum_time_step": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp]),
     "emerald_scalar_average_and_max": (c_i32, [c_sz, c_f, c_vp, c_vp, c_vp]),
+    "emerald_iisph_compute_diis": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp, Neighborhood, c_vp,
+                                           Neighborhood, c_vp]),
+    "emerald_iisph_compute_aiis_and_density_stars": (
+        c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, Neighborhood, c_vp, c_vp,
+                Neighborhood, c_vp]),
+    "emerald_iisph_compute_sum_dij_pjs": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp, c_vp,
+                                                  Neighborhood, c_vp]),
+    "emerald_iisph_compute_betas": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                            Neighborhood, c_vp, Neighborhood, c_vp]),
+    "emerald_iisph_compute_new_pressures": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                                    c_vp]),
+    "emerald_dfsph_p_compute_shared_coeffs": (c_i32, [c_sz, c_f, c_vp, c_vp, c_vp, Neighborhood,
+                                                      c_vp, Neighborhood, c_vp]),
+    "emerald_dfsph_p_compute_density_pseudo_pressures": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp,
+                                                                 c_vp, c_vp]),
+    "emerald_dfsph_p_compute_divergence_pseudo_pressures": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp,
+                                                                    c_vp, c_vp]),
+    "emerald_pcisph_compute_densities": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp, c_vp]),
+    "emerald_pcisph_accumulate_density_from_solids": (c_i32, [c_sz, c_f, c_vp, c_vp, c_vp, c_vp,
+                                                              c_vp, c_vp]),
+    "emerald_pcisph_update_pressures": (c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp]),
+    "emerald_pcisph_accumulate_pressure_forces": (c_i32, [c_sz, c_f, c_f, c_f] + [c_vp] * 10),
+    "emerald_pcisph_accumulate_pressure_forces_from_solids": (c_i32, [c_sz, c_f, c_f] +
+                                                              [c_vp] * 8),
+    "emerald_iisph_ap_density_stars_and_diagonals": (
+        c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp, c_vp, c_vp, Neighborhood, c_vp, c_vp,
+                Neighborhood, c_vp]),
+    "emerald_iisph_ap_iterate_pressures_in_place": (
+        c_i32, [c_sz, c_f, c_f, c_f, c_vp, c_vp, c_vp, c_vp, c_vp, Neighborhood, c_vp,
+                Neighborhood, c_vp, c_vp]),
+    "emerald_iisph_pseudo_ap_density_stars_and_pseudo_diagonals": (
+        c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp, c_vp, c_vp, Neighborhood, c_vp, c_vp,
+                Neighborhood, c_vp]),
+    "emerald_iisph_pseudo_ap_compute_pseudo_pressure_displacements": (
+        c_i32, [c_sz, c_f, c_vp, c_vp, c_vp, c_vp, Neighborhood, c_vp, Neighborhood, c_vp]),
+    "emerald_iisph_pseudo_ap_iterate_pseudo_pressures_in_place": (
+        c_i32, [c_sz, c_f, c_f, c_vp, c_vp, c_vp, c_vp, c_vp, Neighborhood, c_vp, Neighborhood,
+                c_vp, c_vp]),
+    "emerald_iisph_pseudo_ap_integrate_velocities_and_positions_in_place": (
+        c_i32, [c_sz, c_f, c_vp, c_vp, c_vp, c_vp]),
     "emerald_neighbors_static": (c_i32, [c_vp, c_u32, c_f, c_vp, c_vp, c_vp, c_vp, c_u32, c_vp]),
     "emerald_kernel_launches": (c_i64, []),
     "emerald_last_error": (ctypes.c_char_p, []),

@@ -433,6 +433,122 @@ int emerald_cfl_maximum_time_step(size_t n, float support, float factor, int64_t
 int emerald_scalar_average_and_max(size_t n, float discretization, float* average_and_max,
                                    float const* values, void* stream);
 
+/* ------------------------------------------ sph2d_box solver ops on device */
+
+/* The solvers' operator functions (emerald/sph2d_box/{iisph,dfsph_p,pcisph,
+ * iisph_ap,iisph_pseudo_ap}_ops.h) on device memory, with the conventions of
+ * the sph_common section above: the reference's argument order and
+ * arithmetic order, bit-identical outputs, asynchronous on `stream`, no
+ * allocation, a NULL solid `counts` skipping the boundary terms. Where the
+ * reference returns the iteration's (average, max) error pair, `result` is
+ * device memory of EMERALD_ITERATION_RESULT_FLOATS floats, 8-byte aligned:
+ * result[0] receives the average, result[1] the maximum, and the rest is
+ * working storage. */
+#define EMERALD_ITERATION_RESULT_FLOATS 4
+
+/* iisph_compute_diis (emerald/sph2d_box/iisph_ops.h:13-24). */
+int emerald_iisph_compute_diis(size_t n, float dt, float target_density, float* diis,
+                               float const* self_densities, float const* fluid_volumes,
+                               emerald_neighborhood fluid, float const* solid_volumes,
+                               emerald_neighborhood solid, void* stream);
+/* iisph_compute_aiis_and_density_stars (emerald/sph2d_box/iisph_ops.h:26-42). */
+int emerald_iisph_compute_aiis_and_density_stars(
+  size_t n, float dt, float target_density, float* aiis, float* density_stars, float const* diis,
+  float const* densities, float const* fluid_volumes, float const* fluid_velocities,
+  emerald_neighborhood fluid, float const* solid_volumes, float const* solid_velocities,
+  emerald_neighborhood solid, void* stream);
+/* iisph_compute_sum_dij_pjs (emerald/sph2d_box/iisph_ops.h:44-51). */
+int emerald_iisph_compute_sum_dij_pjs(size_t n, float dt, float target_density,
+                                      float* sum_dij_pjs, float const* volumes,
+                                      float const* densities, float const* pressures,
+                                      emerald_neighborhood neighborhood, void* stream);
+/* iisph_compute_betas (emerald/sph2d_box/iisph_ops.h:53-64). */
+int emerald_iisph_compute_betas(size_t n, float dt, float target_density, float* betas,
+                                float const* densities, float const* pressures,
+                                float const* diis, float const* sum_dij_pjs,
+                                float const* fluid_volumes, emerald_neighborhood fluid,
+                                float const* solid_volumes, emerald_neighborhood solid,
+                                void* stream);
+/* iisph_compute_new_pressures (emerald/sph2d_box/iisph_ops.h:66-73). */
+int emerald_iisph_compute_new_pressures(size_t n, float omega, float target_density,
+                                        float* betas_in_new_pressures_out,
+                                        float const* old_pressures, float const* alphas,
+                                        float const* density_stars, float* result, void* stream);
+
+/* dfsph_p_compute_shared_coeffs, _density_pseudo_pressures and
+ * _divergence_pseudo_pressures (emerald/sph2d_box/dfsph_p_ops.h:13-37). */
+int emerald_dfsph_p_compute_shared_coeffs(size_t n, float target_density, float* shared_coeffs,
+                                          float const* densities, float const* fluid_volumes,
+                                          emerald_neighborhood fluid, float const* solid_volumes,
+                                          emerald_neighborhood solid, void* stream);
+int emerald_dfsph_p_compute_density_pseudo_pressures(size_t n, float dt, float target_density,
+                                                     float* density_pseudo_pressures,
+                                                     float const* density_stars,
+                                                     float const* shared_coeffs, void* stream);
+int emerald_dfsph_p_compute_divergence_pseudo_pressures(size_t n, float dt, float target_density,
+                                                        float* divergence_pseudo_pressures,
+                                                        float const* divergences,
+                                                        float const* shared_coeffs, void* stream);
+
+/* The PCISPH operators (emerald/sph2d_box/pcisph_ops.h:12-61), with the
+ * reference's separate neighbour arrays (64 entries per particle). */
+int emerald_pcisph_compute_densities(size_t n, float mass_per_particle, float support,
+                                     float* densities, uint8_t const* neighbor_counts,
+                                     float const* neighbor_kernels, void* stream);
+int emerald_pcisph_accumulate_density_from_solids(size_t n, float target_density,
+                                                  float* densities, float const* solid_volumes,
+                                                  uint8_t const* solid_neighbor_counts,
+                                                  uint64_t const* solid_neighbor_indices,
+                                                  float const* solid_neighbor_kernels,
+                                                  void* stream);
+int emerald_pcisph_update_pressures(size_t n, float target_density,
+                                    float pressure_correction_denom, float* pressures,
+                                    float const* densities, void* stream);
+int emerald_pcisph_accumulate_pressure_forces(
+  size_t n, float mass_per_particle, float support, float viscosity, float* pressure_forces,
+  uint8_t const* neighbor_counts, uint64_t const* neighbor_indices,
+  float const* neighbor_distances, float const* neighbor_vectors_to,
+  float const* neighbor_kernel_gradients, float const* velocities, float const* pressures,
+  float const* densities, void* stream);
+int emerald_pcisph_accumulate_pressure_forces_from_solids(
+  size_t n, float mass_per_particle, float target_density, float* pressure_forces,
+  float const* solid_volumes, uint8_t const* solid_neighbor_counts,
+  uint64_t const* solid_neighbor_indices, float const* solid_neighbor_kernel_gradients,
+  float const* pressures, float const* densities, void* stream);
+
+/* iisph_ap_density_stars_and_diagonals and iisph_ap_iterate_pressures_in_place
+ * (emerald/sph2d_box/iisph_ap_ops.h:13-42). */
+int emerald_iisph_ap_density_stars_and_diagonals(
+  size_t n, float dt, float target_density, float* density_stars, float* diagonals,
+  float const* densities, float const* fluid_volumes, float const* fluid_velocities,
+  emerald_neighborhood fluid, float const* solid_volumes, float const* solid_velocities,
+  emerald_neighborhood solid, void* stream);
+int emerald_iisph_ap_iterate_pressures_in_place(
+  size_t n, float dt, float target_density, float omega, float* pressures,
+  float const* density_stars, float const* pressure_accelerations, float const* diagonals,
+  float const* fluid_volumes, emerald_neighborhood fluid, float const* solid_volumes,
+  emerald_neighborhood solid, float* result, void* stream);
+
+/* The IISPH_PSEUDO_AP operators (emerald/sph2d_box/iisph_pseudo_ap_ops.h:13-65). */
+int emerald_iisph_pseudo_ap_density_stars_and_pseudo_diagonals(
+  size_t n, float dt, float target_density, float* density_stars, float* pseudo_diagonals,
+  float const* densities, float const* fluid_volumes, float const* fluid_velocities,
+  emerald_neighborhood fluid, float const* solid_volumes, float const* solid_velocities,
+  emerald_neighborhood solid, void* stream);
+int emerald_iisph_pseudo_ap_compute_pseudo_pressure_displacements(
+  size_t n, float target_density, float* pseudo_pressure_displacements,
+  float const* pseudo_pressures, float const* densities, float const* fluid_volumes,
+  emerald_neighborhood fluid, float const* solid_volumes, emerald_neighborhood solid,
+  void* stream);
+int emerald_iisph_pseudo_ap_iterate_pseudo_pressures_in_place(
+  size_t n, float target_density, float omega, float* pseudo_pressures,
+  float const* density_stars, float const* pseudo_pressure_displacements,
+  float const* pseudo_diagonals, float const* fluid_volumes, emerald_neighborhood fluid,
+  float const* solid_volumes, emerald_neighborhood solid, float* result, void* stream);
+int emerald_iisph_pseudo_ap_integrate_velocities_and_positions_in_place(
+  size_t n, float dt, float* velocities, float* positions,
+  float const* pseudo_pressure_displacements, void* stream);
+
 /* ---------------------------------------------------- allocation-free build */
 
 /* No counterpart in the reference (which always allocates its std::vector

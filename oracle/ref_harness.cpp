@@ -737,3 +737,191 @@ void ref_common_average_and_max(size_t n, float discretization, float const* val
 }
 
 }  // extern "C"
+
+//------------------------------------------------------------------------------
+// The reference's solver operator functions (emerald/sph2d_box/*_ops.cpp) on
+// flat host arrays. A neighbour set arrives as six pointers in the layout of
+// Neighborhood_pointers, row-major with 64-bit indices; V2f arrays are
+// interleaved floats. The iteration functions' (average, max) pairs are
+// written to out[0], out[1].
+
+namespace {
+
+struct ref_nb {
+    uint8_t const* counts;
+    uint64_t const* indices;
+    float const* distances;
+    float const* vectors_to;
+    float const* kernels;
+    float const* kernel_gradients;
+};
+
+Neighborhood_vectors nb_of(size_t n, ref_nb const* p) {
+    return nbhd_from(n, p->counts, p->indices, p->distances, p->vectors_to, p->kernels,
+                     p->kernel_gradients);
+}
+
+}  // namespace
+
+extern "C" {
+
+void ref_ops_iisph_diis(size_t n, float dt, float rho0, float* diis, float const* rho,
+                        float const* fvol, ref_nb const* f, float const* svol, ref_nb const* s) {
+    auto const F = nb_of(n, f);
+    auto const S = nb_of(n, s);
+    std::vector<V2f> d(n);
+    iisph_compute_diis(n, dt, rho0, d.data(), rho, fvol, F.pointers(), svol, S.pointers());
+    copy_out(d, diis);
+}
+
+void ref_ops_iisph_aiis_stars(size_t n, float dt, float rho0, float* aiis, float* stars,
+                              float const* diis, float const* rho, float const* fvol,
+                              float const* fvel, ref_nb const* f, float const* svol,
+                              float const* svel, size_t n_solid, ref_nb const* s) {
+    auto const F = nb_of(n, f);
+    auto const S = nb_of(n, s);
+    auto const d = to_v2f(diis, n);
+    auto const fv = to_v2f(fvel, n);
+    auto const sv = to_v2f(svel, n_solid);
+    iisph_compute_aiis_and_density_stars(n, dt, rho0, aiis, stars, d.data(), rho, fvol, fv.data(),
+                                         F.pointers(), svol, sv.data(), S.pointers());
+}
+
+void ref_ops_iisph_sum_dij_pjs(size_t n, float dt, float rho0, float* out, float const* vol,
+                               float const* rho, float const* p, ref_nb const* nb) {
+    auto const N = nb_of(n, nb);
+    std::vector<V2f> o(n);
+    iisph_compute_sum_dij_pjs(n, dt, rho0, o.data(), vol, rho, p, N.pointers());
+    copy_out(o, out);
+}
+
+void ref_ops_iisph_betas(size_t n, float dt, float rho0, float* betas, float const* rho,
+                         float const* p, float const* diis, float const* sdp, float const* fvol,
+                         ref_nb const* f, float const* svol, ref_nb const* s) {
+    auto const F = nb_of(n, f);
+    auto const S = nb_of(n, s);
+    auto const d = to_v2f(diis, n);
+    auto const sd = to_v2f(sdp, n);
+    iisph_compute_betas(n, dt, rho0, betas, rho, p, d.data(), sd.data(), fvol, F.pointers(), svol,
+                        S.pointers());
+}
+
+void ref_ops_iisph_new_pressures(size_t n, float omega, float rho0, float* io,
+                                 float const* old_p, float const* alphas, float const* stars,
+                                 float* out) {
+    auto const r = iisph_compute_new_pressures(n, omega, rho0, io, old_p, alphas, stars);
+    out[0] = r.first;
+    out[1] = r.second;
+}
+
+void ref_ops_dfsph_shared_coeffs(size_t n, float rho0, float* out, float const* rho,
+                                 float const* fvol, ref_nb const* f, float const* svol,
+                                 ref_nb const* s) {
+    auto const F = nb_of(n, f);
+    auto const S = nb_of(n, s);
+    dfsph_p_compute_shared_coeffs(n, rho0, out, rho, fvol, F.pointers(), svol, S.pointers());
+}
+
+void ref_ops_dfsph_pseudo_pressures(size_t n, float dt, float rho0, float* density_pp,
+                                    float* divergence_pp, float const* stars, float const* div,
+                                    float const* coeffs) {
+    dfsph_p_compute_density_pseudo_pressures(n, dt, rho0, density_pp, stars, coeffs);
+    dfsph_p_compute_divergence_pseudo_pressures(n, dt, rho0, divergence_pp, div, coeffs);
+}
+
+void ref_ops_pcisph_densities(size_t n, float mass, float support, float rho0, float* rho,
+                              ref_nb const* f, float const* svol, ref_nb const* s) {
+    auto const F = nb_of(n, f);
+    auto const S = nb_of(n, s);
+    pcisph_compute_densities(n, mass, support, rho, F.counts.data(), F.kernels.data());
+    pcisph_accumulate_density_from_solids(n, rho0, rho, svol, S.counts.data(), S.indices.data(),
+                                          S.kernels.data());
+}
+
+void ref_ops_pcisph_update_pressures(size_t n, float rho0, float denom, float* p,
+                                     float const* rho) {
+    pcisph_update_pressures(n, rho0, denom, p, rho);
+}
+
+void ref_ops_pcisph_forces(size_t n, float mass, float support, float viscosity, float rho0,
+                           float* forces, ref_nb const* f, float const* vel, float const* p,
+                           float const* rho, float const* svol, ref_nb const* s) {
+    auto const F = nb_of(n, f);
+    auto const S = nb_of(n, s);
+    auto fo = to_v2f(forces, n);
+    auto const v = to_v2f(vel, n);
+    pcisph_accumulate_pressure_forces(n, mass, support, viscosity, fo.data(), F.counts.data(),
+                                      F.indices.data(), F.distances.data(), F.vectors_to.data(),
+                                      F.kernel_gradients.data(), v.data(), p, rho);
+    pcisph_accumulate_pressure_forces_from_solids(n, mass, rho0, fo.data(), svol, S.counts.data(),
+                                                  S.indices.data(), S.kernel_gradients.data(), p,
+                                                  rho);
+    copy_out(fo, forces);
+}
+
+void ref_ops_ap_stars_diagonals(int pseudo, size_t n, float dt, float rho0, float* stars,
+                                float* diag, float const* rho, float const* fvol,
+                                float const* fvel, ref_nb const* f, float const* svol,
+                                float const* svel, size_t n_solid, ref_nb const* s) {
+    auto const F = nb_of(n, f);
+    auto const S = nb_of(n, s);
+    auto const fv = to_v2f(fvel, n);
+    auto const sv = to_v2f(svel, n_solid);
+    if (pseudo) {
+        iisph_pseudo_ap_density_stars_and_pseudo_diagonals(n, dt, rho0, stars, diag, rho, fvol,
+                                                           fv.data(), F.pointers(), svol,
+                                                           sv.data(), S.pointers());
+    } else {
+        iisph_ap_density_stars_and_diagonals(n, dt, rho0, stars, diag, rho, fvol, fv.data(),
+                                             F.pointers(), svol, sv.data(), S.pointers());
+    }
+}
+
+void ref_ops_ap_iterate(size_t n, float dt, float rho0, float omega, float* p,
+                        float const* stars, float const* acc, float const* diag,
+                        float const* fvol, ref_nb const* f, float const* svol, ref_nb const* s,
+                        float* out) {
+    auto const F = nb_of(n, f);
+    auto const S = nb_of(n, s);
+    auto const a = to_v2f(acc, n);
+    auto const r = iisph_ap_iterate_pressures_in_place(n, dt, rho0, omega, p, stars, a.data(),
+                                                       diag, fvol, F.pointers(), svol,
+                                                       S.pointers());
+    out[0] = r.first;
+    out[1] = r.second;
+}
+
+void ref_ops_pseudo_displacements(size_t n, float rho0, float* out, float const* pp,
+                                  float const* rho, float const* fvol, ref_nb const* f,
+                                  float const* svol, ref_nb const* s) {
+    auto const F = nb_of(n, f);
+    auto const S = nb_of(n, s);
+    std::vector<V2f> d(n);
+    iisph_pseudo_ap_compute_pseudo_pressure_displacements(n, rho0, d.data(), pp, rho, fvol,
+                                                          F.pointers(), svol, S.pointers());
+    copy_out(d, out);
+}
+
+void ref_ops_pseudo_iterate(size_t n, float rho0, float omega, float* pp, float const* stars,
+                            float const* disp, float const* diag, float const* fvol,
+                            ref_nb const* f, float const* svol, ref_nb const* s, float* out) {
+    auto const F = nb_of(n, f);
+    auto const S = nb_of(n, s);
+    auto const d = to_v2f(disp, n);
+    auto const r = iisph_pseudo_ap_iterate_pseudo_pressures_in_place(
+      n, rho0, omega, pp, stars, d.data(), diag, fvol, F.pointers(), svol, S.pointers());
+    out[0] = r.first;
+    out[1] = r.second;
+}
+
+void ref_ops_pseudo_integrate(size_t n, float dt, float* vel, float* pos, float const* disp) {
+    auto v = to_v2f(vel, n);
+    auto x = to_v2f(pos, n);
+    auto const d = to_v2f(disp, n);
+    iisph_pseudo_ap_integrate_velocities_and_positions_in_place(n, dt, v.data(), x.data(),
+                                                                d.data());
+    copy_out(v, vel);
+    copy_out(x, pos);
+}
+
+}  // extern "C"

@@ -298,6 +298,24 @@ class Reference:
         L.ref_common_integrate.argtypes = [c_sz, c_f, c_f] + [c_vp] * 7
         L.ref_common_constant_volumes.argtypes = [c_sz, c_f, c_f, c_vp]
         L.ref_common_average_and_max.argtypes = [c_sz, c_f, c_vp, c_vp]
+        # the solver operator functions; neighbour sets by pointer to six
+        # pointers (RefNb)
+        L.ref_ops_iisph_diis.argtypes = [c_sz, c_f, c_f] + [c_vp] * 6
+        L.ref_ops_iisph_aiis_stars.argtypes = [c_sz, c_f, c_f] + [c_vp] * 9 + [c_sz, c_vp]
+        L.ref_ops_iisph_sum_dij_pjs.argtypes = [c_sz, c_f, c_f] + [c_vp] * 5
+        L.ref_ops_iisph_betas.argtypes = [c_sz, c_f, c_f] + [c_vp] * 9
+        L.ref_ops_iisph_new_pressures.argtypes = [c_sz, c_f, c_f] + [c_vp] * 5
+        L.ref_ops_dfsph_shared_coeffs.argtypes = [c_sz, c_f] + [c_vp] * 6
+        L.ref_ops_dfsph_pseudo_pressures.argtypes = [c_sz, c_f, c_f] + [c_vp] * 5
+        L.ref_ops_pcisph_densities.argtypes = [c_sz, c_f, c_f, c_f] + [c_vp] * 4
+        L.ref_ops_pcisph_update_pressures.argtypes = [c_sz, c_f, c_f, c_vp, c_vp]
+        L.ref_ops_pcisph_forces.argtypes = [c_sz, c_f, c_f, c_f, c_f] + [c_vp] * 7
+        L.ref_ops_ap_stars_diagonals.argtypes = [ctypes.c_int, c_sz, c_f, c_f] + [c_vp] * 8 + \
+            [c_sz, c_vp]
+        L.ref_ops_ap_iterate.argtypes = [c_sz, c_f, c_f, c_f] + [c_vp] * 9
+        L.ref_ops_pseudo_displacements.argtypes = [c_sz, c_f] + [c_vp] * 7
+        L.ref_ops_pseudo_iterate.argtypes = [c_sz, c_f, c_f] + [c_vp] * 9
+        L.ref_ops_pseudo_integrate.argtypes = [c_sz, c_f, c_vp, c_vp, c_vp]
         self.L = L
 
     def default_params(self):

@@ -33,6 +33,24 @@ def test_python_bindings_cover_header():
     assert set(header_symbols()) == set(E.EXPORTS)
 
 
+def header_arities():
+    text = open(os.path.join(ROOT, "include", "emerald_sph.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for name, params in re.findall(r"\b(emerald_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        params = params.strip()
+        out[name] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_python_bindings_match_header_arity():
+    """Each binding's argument list has as many entries as the prototype."""
+    arity = header_arities()
+    wrong = {n: (arity[n], len(E.EXPORTS[n][1])) for n in arity
+             if len(E.EXPORTS[n][1]) != arity[n]}
+    assert not wrong, wrong
+
+
 @pytest.mark.parametrize("x,y,z", [(0b111, 0b111, 0b111111), (0xFFFF, 0xFFFF, 0xFFFFFFFF),
                                    (0, 0xFFFF, 0xAAAAAAAA),
                                    (0xFFFFFFFF, 0xFFFFFFFF, 0xFFFFFFFFFFFFFFFF)])
