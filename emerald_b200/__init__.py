@@ -132,6 +132,7 @@ EXPORTS = {
     "emerald_sim_get_state": (c_i32, [c_vp, c_vp, c_vp]),
     "emerald_sim_set_state": (c_i32, [c_vp, c_vp, c_vp]),
     "emerald_sim_get_solid": (c_i32, [c_vp, c_vp, c_vp]),
+    "emerald_sim_set_solid": (c_i32, [c_vp, c_vp, c_vp, c_vp]),
     "emerald_sim_get_array": (c_i32, [c_vp, ctypes.c_char_p, c_vp, ctypes.POINTER(c_i32)]),
     "emerald_sim_get_neighbors": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp]),
     "emerald_sim_get_sort": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
@@ -153,6 +154,7 @@ EXPORTS = {
     "emerald_batch_scene_stats": (c_i32, [c_vp, c_i32, ctypes.POINTER(StepStats)]),
     "emerald_batch_get_state": (c_i32, [c_vp, c_i32, c_vp, c_vp]),
     "emerald_batch_set_state": (c_i32, [c_vp, c_i32, c_vp, c_vp]),
+    "emerald_batch_set_solid": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp]),
     "emerald_batch_free": (c_i32, [c_vp, ctypes.POINTER(c_sz), ctypes.POINTER(c_i32)]),
     "emerald_batch_set_stream": (c_i32, [c_vp, c_vp]),
     "emerald_batch_synchronize": (c_i32, [c_vp]),
@@ -446,6 +448,15 @@ class Simulation:
         v = None if v is None else _f32(v)
         _check(lib.emerald_sim_set_state(self._h, _ptr(x), _ptr(v)), "set_state")
 
+    def set_solid(self, xy=None, v=None, volumes=None):
+        """Moves the boundary between sub-steps: new positions (rebuilding its
+        cell tables and, unless `volumes` is given, its volumes), velocities
+        or volumes; None keeps each."""
+        xy = None if xy is None else _f32(xy)
+        v = None if v is None else _f32(v)
+        volumes = None if volumes is None else np.ascontiguousarray(volumes, np.float32)
+        _check(lib.emerald_sim_set_solid(self._h, _ptr(xy), _ptr(v), _ptr(volumes)), "set_solid")
+
     def solid(self):
         xy = np.zeros((self.ns, 2), np.float32)
         vol = np.zeros(self.ns, np.float32)
@@ -592,6 +603,13 @@ class Batch:
         x = None if x is None else _f32(x)
         v = None if v is None else _f32(v)
         _check(lib.emerald_batch_set_state(self._h, sid, _ptr(x), _ptr(v)), "set_state")
+
+    def set_solid(self, sid, xy=None, v=None, volumes=None):
+        xy = None if xy is None else _f32(xy)
+        v = None if v is None else _f32(v)
+        volumes = None if volumes is None else np.ascontiguousarray(volumes, np.float32)
+        _check(lib.emerald_batch_set_solid(self._h, sid, _ptr(xy), _ptr(v), _ptr(volumes)),
+               "set_solid")
 
     def free(self):
         n = c_sz()

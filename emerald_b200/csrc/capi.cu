@@ -283,6 +283,15 @@ int emerald_sim_get_solid(emerald_sim* sim, float* xy, float* volumes) {
     });
 }
 
+int emerald_sim_set_solid(emerald_sim* sim, float const* solid_xy, float const* solid_v,
+                          float const* solid_volumes) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    return guarded([&] {
+        sim->engine.set_solid(sim->scene, solid_xy, solid_v, solid_volumes);
+        return EMERALD_OK;
+    });
+}
+
 int emerald_sim_get_array(emerald_sim* sim, char const* name, float* out, int32_t* width) {
     if (!sim || !name) return fail(EMERALD_EINVAL, "bad arguments");
     return guarded([&] {
@@ -418,6 +427,15 @@ int emerald_batch_set_state(emerald_batch* batch, int32_t scene, float const* x,
     if (!batch || !batch->engine.scene_used(scene)) return fail(EMERALD_EINVAL, "bad scene");
     return guarded([&] {
         batch->engine.set_state(scene, x, v);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_batch_set_solid(emerald_batch* batch, int32_t scene, float const* solid_xy,
+                            float const* solid_v, float const* solid_volumes) {
+    if (!batch || !batch->engine.scene_used(scene)) return fail(EMERALD_EINVAL, "bad scene");
+    return guarded([&] {
+        batch->engine.set_solid(scene, solid_xy, solid_v, solid_volumes);
         return EMERALD_OK;
     });
 }

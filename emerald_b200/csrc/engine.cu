@@ -1098,6 +1098,29 @@ void Engine::get_solid(int id, float* xy, float* volumes) {
     check("get_solid");
 }
 
+void Engine::set_solid(int id, float const* xy, float const* v, float const* volumes) {
+    Scene& sc = scenes_[id];
+    SceneParams& P = sc.p;
+    uint32_t const b = P.solid_begin, n = P.solid_count;
+    if (!n) return;
+    if (xy) {
+        cudaMemcpyAsync(a_.xs + b, xy, 8ull * n, cudaMemcpyHostToDevice, st_);
+        cudaStreamSynchronize(st_);
+        if (sc.near_words) near_words_.release(P.near_begin, sc.near_words);
+        build_near_map(sc, xy, n);
+        upload_params(id);
+        rebuild_solids();
+    }
+    if (v) cudaMemcpyAsync(a_.vs + b, v, 8ull * n, cudaMemcpyHostToDevice, st_);
+    if (volumes) {
+        cudaMemcpyAsync(a_.vols + b, volumes, 4ull * n, cudaMemcpyHostToDevice, st_);
+    } else if (xy) {
+        launch("solid_volumes", [&] { launch_solid_volumes(a_, ext_stiles_, 1.7f, id, st_); });
+    }
+    cudaStreamSynchronize(st_);
+    check("set_solid");
+}
+
 bool Engine::get_array(int id, std::string const& name, float* out, int& width) {
     SceneParams const& P = scenes_[id].p;
     void const* src = nullptr;

@@ -104,6 +104,11 @@ public:
     void get_state(int id, float* x, float* v);
     void set_state(int id, float const* x, float const* v);
     void get_solid(int id, float* xy, float* volumes);
+    // Replaces a scene's boundary particles between sub-steps (count kept):
+    // positions (NULL keeps them; new ones rebuild the boundary cell tables
+    // and proximity map), velocities (NULL keeps them) and volumes (NULL:
+    // recomputed from new positions, kept otherwise).
+    void set_solid(int id, float const* xy, float const* v, float const* volumes);
     bool get_array(int id, std::string const& name, float* out, int& width);
     void get_neighbors(int id, bool solid, uint8_t* counts, uint32_t* idx, float* w, float* gw);
     size_t get_sort(int id, bool solid, int32_t* gc, uint64_t* z, uint64_t* pair_z,

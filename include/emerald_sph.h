@@ -176,6 +176,20 @@ int emerald_sim_time(emerald_sim const* sim, int64_t* flicks);
 int emerald_sim_get_state(emerald_sim* sim, float* x, float* v);
 int emerald_sim_set_state(emerald_sim* sim, float const* x, float const* v);
 int emerald_sim_get_solid(emerald_sim* sim, float* xy, float* volumes);
+/* Replaces the boundary between sub-steps, for moving (kinematic) walls and
+ * prescribed rigid motion. The reference's step functions take the
+ * Solid_state by const reference on every call (e.g.
+ * emerald/sph2d_box/dfsph_p.cpp:376-396), and its velocities enter the
+ * divergence and density-star sums (emerald/sph_common/divergence.cpp:47-74,
+ * emerald/sph2d_box/iisph_ops.cpp:87-221). solid_xy: the n_solid positions,
+ * original order (NULL keeps them; new ones rebuild the boundary cell tables
+ * as compute_neighbor_data_and_volumes does, emerald/sph2d_box/solids.cpp:76-137);
+ * solid_v: velocities (NULL keeps them; they start at zero); solid_volumes:
+ * NULL recomputes the volumes from new positions with compute_volumes
+ * (solids.cpp:52-74) and keeps them otherwise. The count is fixed at
+ * creation. */
+int emerald_sim_set_solid(emerald_sim* sim, float const* solid_xy, float const* solid_v,
+                          float const* solid_volumes);
 
 /* Per-particle solver temporaries by their Temp_data name
  * (emerald/sph2d_box/state.h:34-69): "densities", "pressures",
@@ -250,6 +264,9 @@ int emerald_batch_step(emerald_batch* batch, int32_t method, int32_t n_substeps)
 int emerald_batch_scene_stats(emerald_batch* batch, int32_t scene, emerald_step_stats* stats);
 int emerald_batch_get_state(emerald_batch* batch, int32_t scene, float* x, float* v);
 int emerald_batch_set_state(emerald_batch* batch, int32_t scene, float const* x, float const* v);
+/* emerald_sim_set_solid for one scene of a batch. */
+int emerald_batch_set_solid(emerald_batch* batch, int32_t scene, float const* solid_xy,
+                            float const* solid_v, float const* solid_volumes);
 /* Largest fluid range and scene slots still free. */
 int emerald_batch_free(emerald_batch* batch, size_t* fluid, int32_t* scenes);
 int emerald_batch_set_stream(emerald_batch* batch, void* cuda_stream);

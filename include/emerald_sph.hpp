@@ -23,14 +23,18 @@
 //     object goes away);
 //   * flicks: anything with `.count()` (std::chrono::duration) or an integer.
 //
-// Each call uploads the state, runs one frame on the GPU, downloads the new
-// state and, if user_colors is callable, calls it on the host with the
+// Each call uploads the state, passes on a boundary whose positions or
+// velocities differ from the previous call's (a moving wall: the reference
+// takes the Solid_state anew on every call), runs one frame on the GPU,
+// downloads the new state and, if user_colors is callable, calls it on the
+// host with the
 // frame's densities, as compute_colors does (emerald/sph2d_box/colors.cpp:22-38).
 // user_forces is not called: the device applies gravity, which is what the
 // reference's default_gravity_forces (emerald/sph2d_box/forces.cpp:63-83)
 // computes; callers with other forces stay on the reference path.
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <map>
 #include <memory>
@@ -68,6 +72,12 @@ template <class T>
 struct has_volumes<T, std::void_t<decltype(std::declval<T const&>().volumes)>>
   : std::is_same<typename std::decay<decltype(std::declval<T const&>().volumes)>::type,
                  std::vector<float>> {};
+
+template <class T, class = void>
+struct has_velocities : std::false_type {};
+template <class T>
+struct has_velocities<T, std::void_t<decltype(std::declval<T const&>().velocities)>>
+  : std::true_type {};
 
 template <class V>
 float const* floats(std::vector<V> const& v) {
@@ -136,6 +146,7 @@ struct Context {
     size_t n_fluid = 0;
     int64_t time = 0;
     std::vector<float> densities;
+    std::vector<float> solid_xy, solid_v;  // the boundary the device holds
     ~Context() {
         if (sim) emerald_sim_destroy(sim);
     }
@@ -168,7 +179,40 @@ Context& context(void const* key, Config const& config, Solid_state const& solid
           "emerald_sim_create");
     slot->n_fluid = n_fluid;
     slot->time = time;
+    size_t const ns = solid.positions.size();
+    slot->solid_xy.assign(floats(solid.positions), floats(solid.positions) + 2 * ns);
+    slot->solid_v.assign(2 * ns, 0.0f);
     return *slot;
+}
+
+// Sends the caller's boundary to the device when its positions or
+// velocities changed since the last call (same count; a different count
+// needs a new simulation).
+template <class Solid_state>
+void sync_solid(Context& ctx, Solid_state const& solid) {
+    size_t const ns = solid.positions.size();
+    if (2 * ns != ctx.solid_xy.size()) {
+        throw std::invalid_argument("the boundary particle count changed");
+    }
+    float const* xy = floats(solid.positions);
+    bool const moved = ns && !std::equal(xy, xy + 2 * ns, ctx.solid_xy.begin());
+    float const* v = nullptr;
+    bool vchanged = false;
+    if constexpr (has_velocities<typename std::decay<Solid_state>::type>::value) {
+        if (solid.velocities.size() == ns && ns) {
+            v = floats(solid.velocities);
+            vchanged = !std::equal(v, v + 2 * ns, ctx.solid_v.begin());
+        }
+    }
+    if (!moved && !vchanged) return;
+    float const* vols = nullptr;
+    if constexpr (has_volumes<typename std::decay<Solid_state>::type>::value) {
+        if (moved && solid.volumes.size() == ns) vols = solid.volumes.data();
+    }
+    check(emerald_sim_set_solid(ctx.sim, moved ? xy : nullptr, vchanged ? v : nullptr, vols),
+          "emerald_sim_set_solid");
+    if (moved) std::copy(xy, xy + 2 * ns, ctx.solid_xy.begin());
+    if (vchanged) std::copy(v, v + 2 * ns, ctx.solid_v.begin());
 }
 
 template <class State, class Config, class Solid_state, class Colors>
@@ -183,6 +227,7 @@ State step(int32_t method, int64_t global_time, Config const& config, State&& st
     if (ctx.time != global_time) {
         throw std::invalid_argument("global_time does not continue the device simulation's clock");
     }
+    sync_solid(ctx, solid);
     check(emerald_sim_set_state(ctx.sim, floats(state.positions), floats(state.velocities)),
           "emerald_sim_set_state");
     emerald_step_stats stats{};

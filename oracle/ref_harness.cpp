@@ -309,6 +309,27 @@ void ref_sim_set_solid_volumes(void* h, float const* volumes) {
     std::memcpy(sim->solid_state.volumes.data(), volumes, sim->solid_state.volumes.size() * sizeof(float));
 }
 
+// Replaces the boundary between frames the way a caller of the step
+// functions would: a new Solid_state from positions and velocities through
+// compute_neighbor_data_and_volumes (emerald/sph2d_box/solids.cpp:76-137),
+// whose volumes `volumes` overrides (NULL xy keeps the positions; NULL
+// volumes with NULL xy keeps the volumes).
+void ref_sim_set_solid(void* h, float const* xy, float const* v, float const* volumes) {
+    auto* sim = static_cast<Ref_sim*>(h);
+    size_t const n = sim->solid_state.positions.size();
+    Solid_state solid;
+    solid.positions = xy ? to_v2f(xy, n) : sim->solid_state.positions;
+    solid.velocities = v ? to_v2f(v, n) : sim->solid_state.velocities;
+    solid.colors = sim->solid_state.colors;
+    std::vector<float> const old_volumes = sim->solid_state.volumes;
+    sim->solid_state = compute_neighbor_data_and_volumes(sim->config.params, std::move(solid));
+    if (volumes) {
+        std::memcpy(sim->solid_state.volumes.data(), volumes, n * sizeof(float));
+    } else if (!xy) {
+        sim->solid_state.volumes = old_volumes;
+    }
+}
+
 int64_t ref_sim_time(void* h) { return static_cast<Ref_sim*>(h)->time.count(); }
 
 // Method numbering follows EZ_EXAMPLE_SIM::Method

@@ -5,10 +5,14 @@
 // step calls are spelled exactly as in EZ_EXAMPLE_SIM::step
 // (emerald/sph2d_box/simulation.cpp:41-93).
 //
-//   step_dropin <method 0-4> <frames> <out.bin>
+//   step_dropin <method 0-4> <frames> <out.bin> [wall speed]
 //
 // Runs the reference's default dam break (world_walls + dam_break scenes)
-// and writes positions, velocities and colours after the last frame.
+// and writes positions, velocities and colours after the last frame. With a
+// wall speed (m/s), the caller moves the boundary particles left of x = 0
+// along x before every frame (frame f, from 1, at f * speed * 2 ms) and
+// gives them that velocity, as a caller of the reference moves a wall: by
+// passing a changed Solid_state to the next step call.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -65,9 +69,11 @@ using User_colors_function = std::function<void(size_t, float, float, float, C4f
 using namespace emerald_b200::sph2d_box;
 
 int main(int argc, char** argv) {
-    if (argc != 4) return 2;
+    if (argc != 4 && argc != 5) return 2;
     int const method = std::atoi(argv[1]);
     int const frames = std::atoi(argv[2]);
+    bool const moving = argc == 5;
+    float const speed = moving ? float(std::atof(argv[4])) : 0.0f;
     emerald_params p{};
     emerald_b200::check(emerald_default_params(&p), "defaults");
     float cfg[4];
@@ -119,9 +125,19 @@ int main(int argc, char** argv) {
             colors[i] = {c, c, 1.0f, 1.0f};
         }
     };
+    std::vector<ref::V2f> const walls0 = solid_state.positions;
+    float const step = float(double(speed) * 0.002);
     ref::flicks time{0};
     try {
         for (int f = 0; f < frames; ++f) {
+            if (moving) {
+                for (size_t k = 0; k < walls0.size(); ++k) {
+                    if (walls0[k].x < 0.0f) {
+                        solid_state.positions[k].x = walls0[k].x + float(f + 1) * step;
+                        solid_state.velocities[k] = {speed, 0.0f};
+                    }
+                }
+            }
             switch (method) {
             case 0:
                 state = pcisph_simulation_step(time, config, std::move(state), solid_state,

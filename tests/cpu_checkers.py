@@ -270,6 +270,7 @@ class Reference:
         L.ref_sim_sub_step.argtypes = [c_vp, ctypes.c_int, c_f, c_f]
         L.ref_sim_frame.argtypes = [c_vp, ctypes.c_int]
         L.ref_sim_get_state.argtypes = [c_vp, c_vp, c_vp]
+        L.ref_sim_set_solid.argtypes = [c_vp, c_vp, c_vp, c_vp]
         L.ref_sim_set_state.argtypes = [c_vp, c_vp, c_vp]
         L.ref_sim_get_array.argtypes = [c_vp, ctypes.c_char_p, c_vp]
         L.ref_sim_get_neighbors.argtypes = [c_vp, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp,
@@ -420,6 +421,12 @@ class RefSim:
         x = None if x is None else np.ascontiguousarray(x, np.float32)
         v = None if v is None else np.ascontiguousarray(v, np.float32)
         self.lib.L.ref_sim_set_state(self.h, ptr(x), ptr(v))
+
+    def set_solid(self, xy=None, v=None, volumes=None):
+        xy = None if xy is None else np.ascontiguousarray(xy, np.float32)
+        v = None if v is None else np.ascontiguousarray(v, np.float32)
+        volumes = None if volumes is None else np.ascontiguousarray(volumes, np.float32)
+        self.lib.L.ref_sim_set_solid(self.h, ptr(xy), ptr(v), ptr(volumes))
 
     def array(self, name):
         w = self.lib.L.ref_sim_get_array(self.h, name.encode(), None)

@@ -52,3 +52,39 @@ def test_dropin_header_frames(driver, tmp_path, method):
                 np.float32(0.0), np.float32(1.0)).astype(np.float32)
     assert_bitwise(colors[:, 0], c, "%s colours" % name)
     assert np.all(colors[:, 2] == 1.0) and np.all(colors[:, 3] == 1.0)
+
+
+@pytest.mark.parametrize("method", [("dfsph_p", 4), ("iisph", 1)])
+def test_dropin_moving_wall(driver, tmp_path, method):
+    """A caller that moves the left wall between step calls: the header
+    passes the changed boundary on (emerald_sim_set_solid), and the frames
+    equal the C ABI run with the same boundary per frame."""
+    import emerald_b200 as E
+    name, mid = method
+    path = str(tmp_path / "out.bin")
+    subprocess.run([driver, str(mid), "2", path, "-2.0"], check=True)
+    raw = open(path, "rb").read()
+    n = int(np.frombuffer(raw[:8], np.uint64)[0])
+    body = np.frombuffer(raw[8:], np.float32)
+    x = body[:2 * n].reshape(n, 2)
+
+    p = E.default_params()
+    walls0 = E.world_walls(p)
+    fluid = E.dam_break(p, walls0)
+    left = walls0[:, 0] < 0
+    step = np.float32(-2.0 * 0.002)
+    v = np.zeros_like(walls0)
+    v[left, 0] = np.float32(-2.0)
+    sim = None
+    for f in range(1, 3):
+        xy = walls0.copy()
+        xy[left, 0] = walls0[left, 0] + np.float32(f) * step
+        if sim is None:
+            sim = E.Simulation(p, xy, fluid)
+            sim.set_solid(None, v, None)
+        else:
+            sim.set_solid(xy, v, None)
+        sim.frame(name)
+    assert left.any()
+    assert_bitwise(x, sim.state()[0], "%s positions with a moving wall" % name)
+    sim.close()
