@@ -262,6 +262,7 @@ def run_gpu(args):
                        "parallelism": "replicas" if world > 1 else "single scene",
                        "l2": "flushed between timed steps (256 MiB write)",
                        "autotuned_chunks": tuning["chunks"],
+                       "autotuned_prefetch": tuning["prefetch"],
                        "p50_step_ms": round(float(np.percentile(step_ms, 50)), 4),
                        "p99_step_ms": round(float(np.percentile(step_ms, 99)), 4),
                        "last_step": {k: last[k] for k in ("dt", "pressure_iterations",

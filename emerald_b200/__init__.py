@@ -94,14 +94,29 @@ class RequestTiming(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("apply_chunk", c_i32), ("divergence_chunk", c_i32), ("iisph_sum_chunk", c_i32),
                 ("iisph_beta_chunk", c_i32), ("candidates", c_i32),
-                ("candidate_chunks", (c_i32 * 4) * 8), ("candidate_ms", c_f * 8)]
+                ("candidate_chunks", (c_i32 * 4) * 8), ("candidate_ms", c_f * 8),
+                ("prefetch", c_i32 * 4), ("candidate_prefetch", (c_i32 * 4) * 8)]
 
     def as_dict(self):
         fams = ("apply", "divergence", "iisph_sum", "iisph_beta")
         return {"chunks": {f: getattr(self, f + "_chunk") for f in fams},
+                "prefetch": dict(zip(fams, list(self.prefetch))),
                 "candidates": [{"chunks": dict(zip(fams, list(self.candidate_chunks[k]))),
+                                "prefetch": dict(zip(fams, list(self.candidate_prefetch[k]))),
                                 "ms_per_substep": round(self.candidate_ms[k], 4)}
                                for k in range(self.candidates)]}
+
+
+def _tuning_struct(chunks, prefetch=None):
+    """A Tuning from {family: chunk} and {family: 0/1} (None unpins)."""
+    if chunks is None:
+        return None
+    fams = ("apply", "divergence", "iisph_sum", "iisph_beta")
+    t = Tuning()
+    for k, f in enumerate(fams):
+        setattr(t, f + "_chunk", int(chunks[f]))
+        t.prefetch[k] = int((prefetch or {}).get(f, 0))
+    return t
 
 
 class Neighborhood(ctypes.Structure):
@@ -167,6 +182,8 @@ EXPORTS = {
                                     ctypes.POINTER(RequestTiming)]),
     "emerald_server_get_stats": (c_i32, [c_vp, ctypes.POINTER(ServerStats)]),
     "emerald_sim_autotune": (c_i32, [c_vp, c_i32, ctypes.POINTER(Tuning)]),
+    "emerald_sim_set_tuning": (c_i32, [c_vp, ctypes.POINTER(Tuning)]),
+    "emerald_batch_set_tuning": (c_i32, [c_vp, ctypes.POINTER(Tuning)]),
     "emerald_batch_autotune": (c_i32, [c_vp, c_i32, ctypes.POINTER(Tuning)]),
     "emerald_compute_grid_coords": (c_i32, [c_sz, c_f, c_f, c_f, c_vp, c_vp, c_vp]),
     "emerald_compute_z_indices": (c_i32, [c_sz, c_vp, c_vp, c_vp]),
@@ -518,6 +535,13 @@ class Simulation:
         _check(lib.emerald_sim_autotune(self._h, method_id(method), ctypes.byref(t)), "autotune")
         return t.as_dict()
 
+    def set_tuning(self, chunks=None, prefetch=None):
+        """Pins the gather kernels' chunks and prefetch flags (as autotune
+        reports them); no arguments unpins."""
+        t = _tuning_struct(chunks, prefetch)
+        _check(lib.emerald_sim_set_tuning(self._h, None if t is None else ctypes.byref(t)),
+               "set_tuning")
+
     def enable_timing(self, on=True):
         _check(lib.emerald_sim_enable_timing(self._h, int(on)), "enable_timing")
 
@@ -632,6 +656,11 @@ class Batch:
         t = Tuning()
         _check(lib.emerald_batch_autotune(self._h, method_id(method), ctypes.byref(t)), "autotune")
         return t.as_dict()
+
+    def set_tuning(self, chunks=None, prefetch=None):
+        t = _tuning_struct(chunks, prefetch)
+        _check(lib.emerald_batch_set_tuning(self._h, None if t is None else ctypes.byref(t)),
+               "set_tuning")
 
 
 class Server:

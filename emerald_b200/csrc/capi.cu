@@ -8,6 +8,7 @@
 
 #include "../../include/emerald_sph.h"
 #include "engine.hpp"
+#include "kernels.cuh"
 #include "server.hpp"
 
 namespace emerald {
@@ -478,17 +479,21 @@ int autotune_into(Engine& engine, int32_t method, emerald_tuning* out) {
             Engine::TuneReport const r = engine.autotune(method);
             if (out) {
                 *out = emerald_tuning{};
-                out->apply_chunk = r.chosen.apply;
-                out->divergence_chunk = r.chosen.divergence;
-                out->iisph_sum_chunk = r.chosen.iisph_sum;
-                out->iisph_beta_chunk = r.chosen.iisph_beta;
+                auto split = [](int v, int32_t& chunk, int32_t& prefetch) {
+                    chunk = v & ~kPrefetchLists;
+                    prefetch = (v & kPrefetchLists) ? 1 : 0;
+                };
+                split(r.chosen.apply, out->apply_chunk, out->prefetch[0]);
+                split(r.chosen.divergence, out->divergence_chunk, out->prefetch[1]);
+                split(r.chosen.iisph_sum, out->iisph_sum_chunk, out->prefetch[2]);
+                split(r.chosen.iisph_beta, out->iisph_beta_chunk, out->prefetch[3]);
                 out->candidates = r.count;
                 for (int k = 0; k < r.count && k < 8; ++k) {
                     Engine::Tuning const& t = r.candidates[k];
-                    out->candidate_chunks[k][0] = t.apply;
-                    out->candidate_chunks[k][1] = t.divergence;
-                    out->candidate_chunks[k][2] = t.iisph_sum;
-                    out->candidate_chunks[k][3] = t.iisph_beta;
+                    split(t.apply, out->candidate_chunks[k][0], out->candidate_prefetch[k][0]);
+                    split(t.divergence, out->candidate_chunks[k][1], out->candidate_prefetch[k][1]);
+                    split(t.iisph_sum, out->candidate_chunks[k][2], out->candidate_prefetch[k][2]);
+                    split(t.iisph_beta, out->candidate_chunks[k][3], out->candidate_prefetch[k][3]);
                     out->candidate_ms[k] = r.ms[k];
                 }
             }
@@ -499,6 +504,46 @@ int autotune_into(Engine& engine, int32_t method, emerald_tuning* out) {
     });
 }
 }  // namespace
+
+namespace {
+int set_tuning_of(Engine& engine, emerald_tuning const* t) {
+    if (!t) {
+        engine.set_tuning(nullptr);
+        return EMERALD_OK;
+    }
+    int32_t const chunks[4] = {t->apply_chunk, t->divergence_chunk, t->iisph_sum_chunk,
+                               t->iisph_beta_chunk};
+    int v[4];
+    for (int k = 0; k < 4; ++k) {
+        if (chunks[k] != 1 && chunks[k] != 4 && chunks[k] != 8) {
+            return fail(EMERALD_EINVAL, "chunks must be 1, 4 or 8");
+        }
+        if (t->prefetch[k] != 0 && t->prefetch[k] != 1) {
+            return fail(EMERALD_EINVAL, "prefetch flags must be 0 or 1");
+        }
+        v[k] = chunks[k] | (t->prefetch[k] ? kPrefetchLists : 0);
+    }
+    Engine::Tuning tu;
+    tu.apply = v[0];
+    tu.divergence = v[1];
+    tu.iisph_sum = v[2];
+    tu.iisph_beta = v[3];
+    return guarded([&] {
+        engine.set_tuning(&tu);
+        return EMERALD_OK;
+    });
+}
+}  // namespace
+
+int emerald_sim_set_tuning(emerald_sim* sim, emerald_tuning const* tuning) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    return set_tuning_of(sim->engine, tuning);
+}
+
+int emerald_batch_set_tuning(emerald_batch* batch, emerald_tuning const* tuning) {
+    if (!batch) return fail(EMERALD_EINVAL, "batch is NULL");
+    return set_tuning_of(batch->engine, tuning);
+}
 
 int emerald_sim_autotune(emerald_sim* sim, int32_t method, emerald_tuning* out) {
     if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");

@@ -878,7 +878,7 @@ uint64_t Engine::tuning_key(int32_t method) const {
 
 void Engine::substep(int32_t method) {
     if (active_scenes() == 0) return;
-    if (!tuning_locked_) {
+    if (!tuning_locked_ && !tuning_pinned_) {
         std::lock_guard<std::mutex> lock(g_tuning_mutex);
         auto const it = g_tuning_cache.find(tuning_key(method));
         if (it != g_tuning_cache.end() && !(it->second == tuning_)) {
@@ -966,7 +966,11 @@ Engine::TuneReport Engine::autotune(int32_t method, int substeps) {
     int64_t const global0 = g_launches.load();
     std::vector<Tuning> cand;
     if (method == kDfsph) {
-        int const opts[][2] = {{4, 8}, {1, 4}, {4, 4}, {1, 8}, {8, 8}};
+        // chunks, with kPrefetchLists (P) where the warps first ask L2 for
+        // their list rows: it pays when the lists do not stay in L2
+        int const P = kPrefetchLists;
+        int const opts[][2] = {{4, 8}, {1, 4}, {4, 4}, {1, 8}, {8, 8},
+                               {1 | P, 4 | P}, {4 | P, 8 | P}, {1 | P, 4}};
         for (auto const& o : opts) {
             Tuning t = tuning_;
             t.apply = o[0];
@@ -974,7 +978,9 @@ Engine::TuneReport Engine::autotune(int32_t method, int substeps) {
             cand.push_back(t);
         }
     } else {
-        int const opts[][2] = {{4, 4}, {1, 1}, {1, 4}, {4, 1}, {8, 4}};
+        int const P = kPrefetchLists;
+        int const opts[][2] = {{4, 4}, {1, 1}, {1, 4}, {4, 1}, {8, 4},
+                               {4 | P, 4 | P}, {1 | P, 1 | P}, {4 | P, 1 | P}};
         for (auto const& o : opts) {
             Tuning t = tuning_;
             t.iisph_sum = o[0];
@@ -1034,6 +1040,14 @@ Engine::TuneReport Engine::autotune(int32_t method, int substeps) {
     }
     rep.chosen = tuning_;
     return rep;
+}
+
+void Engine::set_tuning(Tuning const* t) {
+    tuning_pinned_ = t != nullptr;
+    if (t && !(*t == tuning_)) {
+        tuning_ = *t;
+        destroy_graphs();
+    }
 }
 
 // ------------------------------------------------------------ accessors

@@ -161,11 +161,15 @@ public:
     // the same method and size class.
     TuneReport autotune(int32_t method, int substeps = 4);
     Tuning const& tuning() const { return tuning_; }
+    // Pins the gather kernels' settings (no cache lookups until unpinned);
+    // nullptr unpins.
+    void set_tuning(Tuning const* t);
 
 private:
     uint64_t tuning_key(int32_t method) const;
     Tuning tuning_{};
     bool tuning_locked_ = false;
+    bool tuning_pinned_ = false;
     int32_t last_method_ = -1;
     struct Scene {
         bool used = false;

@@ -65,7 +65,9 @@ void launch_iter_check(Arena const& a, int nscenes, int kind, int* running,
 // comp: some resident scene is in compensated mode (selects the kernel variant)
 void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st);
 // chunk: neighbour entries loaded together in the gather sums (1, 4 or 8;
-// every choice gives the same bits)
+// every choice gives the same bits), plus kPrefetchLists to have each warp
+// ask L2 for its list rows before the sums
+constexpr int kPrefetchLists = 16;
 void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int external,
                             int skip_done, bool comp, cudaStream_t st, int chunk = 4);
 void launch_dfsph_divergence(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st,

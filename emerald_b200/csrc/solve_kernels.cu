@@ -293,6 +293,22 @@ __global__ void k_iter_check(Arena a, int nscenes, int kind, int* running,
 constexpr int kDivergenceChunk = 8;
 constexpr int kPressureChunk = 4;
 
+// Each warp of a gather kernel may first ask L2 for its fluid list rows
+// (lane k: slot k's 128 index bytes and 256 gradient bytes), so that the
+// sums' list loads find them there. Every lane of the warp calls it; lanes
+// without a live particle pass count 0.
+__device__ __forceinline__ void prefetch_fluid_lists(Arena const& a, int count) {
+    int const lane = threadIdx.x & 31;
+    int const slots = static_cast<int>(__reduce_max_sync(0xffffffffu, uint32_t(count)));
+    if (lane < slots) {
+        size_t const e = static_cast<size_t>(lane) * a.stride +
+                         static_cast<size_t>(blockIdx.x) * kTile + (threadIdx.x & ~31u);
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(a.nf_idx + e));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(a.nf_gw + e));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(a.nf_gw + e + 16));
+    }
+}
+
 // Neighbour values the IISPH beta sum gathers.
 struct IisphNeighbor {
     float rho, p;
@@ -583,10 +599,12 @@ __global__ void k_dfsph_density_alpha(Arena a) {
 // apply_pressures_in_place over the cached q; with `external`, the velocity
 // first takes the external-force step (the DFSPH density warm start follows
 // integrate_velocities_in_place, dfsph_p.cpp:349-365).
-template <int MODE, int CH>
+template <int MODE, int CH, int PF>
 __global__ void k_apply_pressures(Arena a, int which_q, int external, int skip_done) {
     Ctx c;
-    if (!enter(a, skip_done != 0, c) || !c.live) return;
+    if (!enter(a, skip_done != 0, c)) return;
+    if (PF) prefetch_fluid_lists(a, c.live ? int(a.nf_cnt[c.i]) : 0);
+    if (!c.live) return;
     SceneParams const& P = a.sp[c.s];
     float const dt = a.ss[c.s].dt;
     float2 v = a.v[c.i];
@@ -598,7 +616,7 @@ __global__ void k_apply_pressures(Arena a, int which_q, int external, int skip_d
 
 // compute_divergences + dfsph_p_compute_divergence_pseudo_pressures
 // (dfsph_p_ops.cpp:100-126) + the divergence error of dfsph_p.cpp:187-200.
-template <int MODE, int CH>
+template <int MODE, int CH, int PF>
 __global__ void k_dfsph_divergence(Arena a) {
     Ctx c;
     if (!enter(a, true, c)) return;
@@ -606,6 +624,7 @@ __global__ void k_dfsph_divergence(Arena a) {
     SceneState* S = &a.ss[c.s];
     float const dt = S->dt;
     float err = 0.0f;
+    if (PF) prefetch_fluid_lists(a, c.live ? int(a.nf_cnt[c.i]) : 0);
     if (c.live) {
         uint32_t const i = c.i;
         float const d = (MODE && P.precision) ? divergence_of<true, CH>(a, P, i)
@@ -627,7 +646,7 @@ __global__ void k_dfsph_divergence(Arena a) {
 // predict_density_stars (density.cpp:75-109) +
 // dfsph_p_compute_density_pseudo_pressures (dfsph_p_ops.cpp:74-98) + the
 // density error of dfsph_p.cpp:134-148.
-template <int MODE, int CH>
+template <int MODE, int CH, int PF>
 __global__ void k_dfsph_density(Arena a) {
     Ctx c;
     if (!enter(a, true, c)) return;
@@ -636,6 +655,7 @@ __global__ void k_dfsph_density(Arena a) {
     float const dt = S->dt;
     float const rho0 = P.rho0;
     float err = 0.0f;
+    if (PF) prefetch_fluid_lists(a, c.live ? int(a.nf_cnt[c.i]) : 0);
     if (c.live) {
         uint32_t const i = c.i;
         float const rho = a.rho[i];
@@ -777,10 +797,12 @@ __global__ void k_iisph_aii(Arena a) {
 }
 
 // iisph_compute_sum_dij_pjs (iisph_ops.cpp:202-235).
-template <int CH>
+template <int CH, int PF>
 __global__ void k_iisph_sum_dij(Arena a) {
     Ctx c;
-    if (!enter(a, true, c) || !c.live) return;
+    if (!enter(a, true, c)) return;
+    if (PF) prefetch_fluid_lists(a, c.live ? int(a.nf_cnt[c.i]) : 0);
+    if (!c.live) return;
     SceneParams const& P = a.sp[c.s];
     SceneState const& S = a.ss[c.s];
     uint32_t const i = c.i;
@@ -804,7 +826,7 @@ __global__ void k_iisph_sum_dij(Arena a) {
 
 // iisph_compute_betas (iisph_ops.cpp:237-330) followed by
 // iisph_compute_new_pressures for the same particle (iisph_ops.cpp:332-425).
-template <int CH>
+template <int CH, int PF>
 __global__ void k_iisph_beta_pressure(Arena a) {
     Ctx c;
     if (!enter(a, true, c)) return;
@@ -812,6 +834,7 @@ __global__ void k_iisph_beta_pressure(Arena a) {
     SceneState* S = &a.ss[c.s];
     float err = 0.0f;
     bool counted = false;
+    if (PF) prefetch_fluid_lists(a, c.live ? int(a.nf_cnt[c.i]) : 0);
     if (c.live) {
         uint32_t const i = c.i;
         size_t const stride = a.stride;
@@ -1179,6 +1202,25 @@ __global__ void k_pc_final(Arena a) {
 
 // ------------------------------------------------------------ launchers
 
+// Launches K(mode, chunk, prefetch) for the runtime choice: mode 1 when
+// `comp`, chunk 1, 4 or 8 (anything else: 8), prefetch 0 or 1.
+#define EMLD_DISPATCH(K, comp, ch, pf)                                        \
+    do {                                                                      \
+        if (comp) {                                                           \
+            if (pf) {                                                         \
+                if ((ch) == 1) K(1, 1, 1); else if ((ch) == 4) K(1, 4, 1); else K(1, 8, 1); \
+            } else {                                                          \
+                if ((ch) == 1) K(1, 1, 0); else if ((ch) == 4) K(1, 4, 0); else K(1, 8, 0); \
+            }                                                                 \
+        } else {                                                              \
+            if (pf) {                                                         \
+                if ((ch) == 1) K(0, 1, 1); else if ((ch) == 4) K(0, 4, 1); else K(0, 8, 1); \
+            } else {                                                          \
+                if ((ch) == 1) K(0, 1, 0); else if ((ch) == 4) K(0, 4, 0); else K(0, 8, 0); \
+            }                                                                 \
+        }                                                                     \
+    } while (0)
+
 void launch_max_v2(Arena const& a, uint32_t tiles, cudaStream_t st) {
     k_max_v2<<<tiles, kTile, 0, st>>>(a);
 }
@@ -1204,49 +1246,25 @@ void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, bool comp, cudaS
 }
 void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int external,
                             int skip_done, bool comp, cudaStream_t st, int chunk) {
-    if (comp) {
-    switch (chunk) {
-        case 1: k_apply_pressures<1, 1><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done); break;
-        case 4: k_apply_pressures<1, 4><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done); break;
-        default: k_apply_pressures<1, 8><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done); break;
-        }
-    } else {
-    switch (chunk) {
-        case 1: k_apply_pressures<0, 1><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done); break;
-        case 4: k_apply_pressures<0, 4><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done); break;
-        default: k_apply_pressures<0, 8><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done); break;
-        }
-    }
+    bool const pf = (chunk & kPrefetchLists) != 0;
+    int const ch = chunk & ~kPrefetchLists;
+#define EMLD_APPLY(M, C, F) k_apply_pressures<M, C, F><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done)
+    EMLD_DISPATCH(EMLD_APPLY, comp, ch, pf);
+#undef EMLD_APPLY
 }
 void launch_dfsph_divergence(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st, int chunk) {
-    if (comp) {
-    switch (chunk) {
-        case 1: k_dfsph_divergence<1, 1><<<tiles, kTile, 0, st>>>(a); break;
-        case 4: k_dfsph_divergence<1, 4><<<tiles, kTile, 0, st>>>(a); break;
-        default: k_dfsph_divergence<1, 8><<<tiles, kTile, 0, st>>>(a); break;
-        }
-    } else {
-    switch (chunk) {
-        case 1: k_dfsph_divergence<0, 1><<<tiles, kTile, 0, st>>>(a); break;
-        case 4: k_dfsph_divergence<0, 4><<<tiles, kTile, 0, st>>>(a); break;
-        default: k_dfsph_divergence<0, 8><<<tiles, kTile, 0, st>>>(a); break;
-        }
-    }
+    bool const pf = (chunk & kPrefetchLists) != 0;
+    int const ch = chunk & ~kPrefetchLists;
+#define EMLD_DIV(M, C, F) k_dfsph_divergence<M, C, F><<<tiles, kTile, 0, st>>>(a)
+    EMLD_DISPATCH(EMLD_DIV, comp, ch, pf);
+#undef EMLD_DIV
 }
 void launch_dfsph_density(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st, int chunk) {
-    if (comp) {
-    switch (chunk) {
-        case 1: k_dfsph_density<1, 1><<<tiles, kTile, 0, st>>>(a); break;
-        case 4: k_dfsph_density<1, 4><<<tiles, kTile, 0, st>>>(a); break;
-        default: k_dfsph_density<1, 8><<<tiles, kTile, 0, st>>>(a); break;
-        }
-    } else {
-    switch (chunk) {
-        case 1: k_dfsph_density<0, 1><<<tiles, kTile, 0, st>>>(a); break;
-        case 4: k_dfsph_density<0, 4><<<tiles, kTile, 0, st>>>(a); break;
-        default: k_dfsph_density<0, 8><<<tiles, kTile, 0, st>>>(a); break;
-        }
-    }
+    bool const pf = (chunk & kPrefetchLists) != 0;
+    int const ch = chunk & ~kPrefetchLists;
+#define EMLD_DENS(M, C, F) k_dfsph_density<M, C, F><<<tiles, kTile, 0, st>>>(a)
+    EMLD_DISPATCH(EMLD_DENS, comp, ch, pf);
+#undef EMLD_DENS
 }
 void launch_integrate_positions(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st) {
     if (comp) {
@@ -1262,18 +1280,18 @@ void launch_iisph_aii(Arena const& a, uint32_t tiles, cudaStream_t st) {
     k_iisph_aii<<<tiles, kTile, 0, st>>>(a);
 }
 void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk) {
-    switch (chunk) {
-    case 1: k_iisph_sum_dij<1><<<tiles, kTile, 0, st>>>(a); break;
-    case 4: k_iisph_sum_dij<4><<<tiles, kTile, 0, st>>>(a); break;
-    default: k_iisph_sum_dij<8><<<tiles, kTile, 0, st>>>(a); break;
-    }
+    bool const pf = (chunk & kPrefetchLists) != 0;
+    int const ch = chunk & ~kPrefetchLists;
+#define EMLD_SUM(M, C, F) k_iisph_sum_dij<C, F><<<tiles, kTile, 0, st>>>(a)
+    EMLD_DISPATCH(EMLD_SUM, false, ch, pf);
+#undef EMLD_SUM
 }
 void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk) {
-    switch (chunk) {
-    case 1: k_iisph_beta_pressure<1><<<tiles, kTile, 0, st>>>(a); break;
-    case 4: k_iisph_beta_pressure<4><<<tiles, kTile, 0, st>>>(a); break;
-    default: k_iisph_beta_pressure<8><<<tiles, kTile, 0, st>>>(a); break;
-    }
+    bool const pf = (chunk & kPrefetchLists) != 0;
+    int const ch = chunk & ~kPrefetchLists;
+#define EMLD_BETA(M, C, F) k_iisph_beta_pressure<C, F><<<tiles, kTile, 0, st>>>(a)
+    EMLD_DISPATCH(EMLD_BETA, false, ch, pf);
+#undef EMLD_BETA
 }
 void launch_make_q(Arena const& a, uint32_t tiles, cudaStream_t st) {
     k_make_q<<<tiles, kTile, 0, st>>>(a);

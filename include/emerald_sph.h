@@ -275,24 +275,33 @@ int emerald_batch_kernel_launches(emerald_batch* batch, int64_t* count);
 
 /* -------------------------------------------------------------- autotuning */
 
-/* Neighbour entries each gather-sum kernel loads together (1, 4 or 8). Every
+/* Neighbour entries each gather-sum kernel loads together (1, 4 or 8), and
+ * whether its warps first ask L2 for their list rows (prefetch 1). Every
  * choice gives the same bits. Autotuning (DFSPH_P and IISPH) times a few
  * whole sub-steps of `method` with each candidate setting, every candidate
  * from the same state (restored afterwards, so the simulation is left as it
  * was), after at least one sub-step of that method, and keeps the fastest,
  * also for later simulations and batches of the same method and size class
  * (log2 of the active particle count). candidate_ms[k]: mean sub-step time
- * of candidate k, whose chunks are candidate_chunks[k] (apply, divergence,
- * iisph_sum, iisph_beta). No counterpart in the reference. */
+ * of candidate k, whose chunks and prefetch flags are candidate_chunks[k]
+ * and candidate_prefetch[k] (apply, divergence, iisph_sum, iisph_beta;
+ * prefetch[] in the same order). No counterpart in the reference. */
 typedef struct emerald_tuning {
     int32_t apply_chunk, divergence_chunk, iisph_sum_chunk, iisph_beta_chunk;
     int32_t candidates;
     int32_t candidate_chunks[8][4];
     float candidate_ms[8];
+    int32_t prefetch[4];
+    int32_t candidate_prefetch[8][4];
 } emerald_tuning;
 
 int emerald_sim_autotune(emerald_sim* sim, int32_t method, emerald_tuning* out);
 int emerald_batch_autotune(emerald_batch* batch, int32_t method, emerald_tuning* out);
+/* Pins the settings of *tuning (its chunks and prefetch flags; the candidate
+ * fields are ignored) until the next call; NULL returns to the tuned or
+ * default settings. */
+int emerald_sim_set_tuning(emerald_sim* sim, emerald_tuning const* tuning);
+int emerald_batch_set_tuning(emerald_batch* batch, emerald_tuning const* tuning);
 
 /* ----------------------------------------------------------------- serving */
 

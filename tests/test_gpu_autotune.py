@@ -1,6 +1,7 @@
-"""Autotuning of the gather kernels' load chunks: it picks among variants
-that give the same bits, so a run that tunes midway equals one that does
-not; it leaves the simulation's state as it found it."""
+"""Autotuning of the gather kernels' load chunks and list prefetch: it picks
+among variants that give the same bits, so a run that tunes midway equals
+one that does not; it leaves the simulation's state as it found it; and
+every candidate, pinned, gives the same bits."""
 import pytest
 
 from conftest import assert_bitwise
@@ -51,7 +52,7 @@ def test_batch_tuning(E):
     ids = [b.add_block_scene(s) for s in scs]
     b.step("iisph", 2)
     t = b.autotune("iisph")
-    assert len(t["candidates"]) == 5 and all(c["ms_per_substep"] > 0 for c in t["candidates"])
+    assert len(t["candidates"]) == 8 and all(c["ms_per_substep"] > 0 for c in t["candidates"])
     b.step("iisph", 4)
     for sid, s in zip(ids, scs):
         sim = E.Simulation.from_block_scene(s)
@@ -67,3 +68,32 @@ def test_tuning_needs_a_substep_of_the_method(E):
     with pytest.raises(E.EmeraldError):
         sim.autotune("dfsph_p")
     sim.autotune("iisph")
+
+
+@pytest.mark.parametrize("method", ["dfsph_p", "iisph"])
+def test_every_candidate_gives_the_same_bits(E, method):
+    sc = scene(E, 40, 5)
+    ref = E.Simulation.from_block_scene(sc)
+    ref.advance(method, 8)
+    probe = E.Simulation.from_block_scene(sc)
+    probe.advance(method, 1)
+    cands = probe.autotune(method)["candidates"]
+    assert any(any(c["prefetch"].values()) for c in cands)
+    for c in cands:
+        sim = E.Simulation.from_block_scene(sc)
+        sim.set_tuning(c["chunks"], c["prefetch"])
+        sim.advance(method, 8)
+        assert_bitwise(sim.state()[0], ref.state()[0], "x with %r" % c)
+        assert_bitwise(sim.state()[1], ref.state()[1], "v with %r" % c)
+        sim.close()
+
+
+def test_set_tuning_rejects_bad_values(E):
+    sim = E.Simulation.from_block_scene(scene(E, 12, 1))
+    with pytest.raises(E.EmeraldError):
+        sim.set_tuning({"apply": 3, "divergence": 4, "iisph_sum": 4, "iisph_beta": 4})
+    with pytest.raises(E.EmeraldError):
+        sim.set_tuning({"apply": 4, "divergence": 4, "iisph_sum": 4, "iisph_beta": 4},
+                       {"apply": 2})
+    sim.set_tuning()
+    sim.close()
