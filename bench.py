@@ -189,8 +189,9 @@ def run_gpu(args):
 
     # end to end through the C ABI over the same sub-steps as the timed
     # region: a second simulation of the same scene takes the same warm-up
-    # (the trajectory is bit-identical), then every sub-step copies the state
-    # in from pinned host memory, advances and copies it back out
+    # (the trajectory is bit-identical), then every sub-step is one
+    # emerald_sim_advance_host call: the state copied in from pinned host
+    # memory, advanced, and copied back out
     sim_e = E.Simulation.from_block_scene(scene)
     for _ in range(args.warmup):
         sim_e.advance("dfsph_p", 1, stats=False)
@@ -204,9 +205,7 @@ def run_gpu(args):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(e2e_steps):
-        sim_e.set_state(xn, vn)
-        sim_e.advance("dfsph_p", 1, stats=False)
-        sim_e.state(xn, vn)
+        sim_e.advance_host("dfsph_p", 1, xn, vn)
     e1.record()
     torch.cuda.synchronize()
     sim_e.close()

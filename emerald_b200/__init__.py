@@ -142,6 +142,8 @@ EXPORTS = {
     "emerald_sim_sub_step": (c_i32, [c_vp, c_i32, c_f, c_f, ctypes.POINTER(StepStats)]),
     "emerald_sim_frame": (c_i32, [c_vp, c_i32, ctypes.POINTER(StepStats)]),
     "emerald_sim_advance": (c_i32, [c_vp, c_i32, c_i32, ctypes.POINTER(StepStats)]),
+    "emerald_sim_advance_host": (c_i32, [c_vp, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp,
+                                         ctypes.POINTER(StepStats)]),
     "emerald_sim_counts": (c_i32, [c_vp, ctypes.POINTER(c_sz), ctypes.POINTER(c_sz)]),
     "emerald_sim_time": (c_i32, [c_vp, ctypes.POINTER(c_i64)]),
     "emerald_sim_get_state": (c_i32, [c_vp, c_vp, c_vp]),
@@ -445,6 +447,16 @@ class Simulation:
         _check(lib.emerald_sim_advance(self._h, method_id(method), n_substeps,
                                        ctypes.byref(st) if stats else None), "advance")
         return st.as_dict()
+
+    def advance_host(self, method, n_substeps, x, v, stats=False):
+        """Copies x, v (C-contiguous float32 (n, 2) host arrays, e.g. pinned)
+        in, advances n sub-steps and copies the new state back into them,
+        with one wait for the device."""
+        st = StepStats()
+        _check(lib.emerald_sim_advance_host(self._h, method_id(method), n_substeps, _ptr(x),
+                                            _ptr(v), _ptr(x), _ptr(v),
+                                            ctypes.byref(st) if stats else None), "advance_host")
+        return st.as_dict() if stats else None
 
     def time(self):
         t = c_i64()

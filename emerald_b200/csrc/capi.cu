@@ -244,6 +244,20 @@ int emerald_sim_advance(emerald_sim* sim, int32_t method, int32_t n_substeps,
     });
 }
 
+int emerald_sim_advance_host(emerald_sim* sim, int32_t method, int32_t n_substeps,
+                             float const* x_in, float const* v_in, float* x_out, float* v_out,
+                             emerald_step_stats* stats) {
+    if (!sim || !valid_method(method) || n_substeps < 0) return fail(EMERALD_EINVAL, "bad arguments");
+    return guarded([&] {
+        sim->engine.set_state(sim->scene, x_in, v_in, false);
+        sim->engine.set_mode(sim->scene, kFrame, 0.0f);
+        for (int k = 0; k < n_substeps; ++k) sim->engine.substep(method);
+        sim->engine.get_state(sim->scene, x_out, v_out, true);
+        if (stats) fill_stats(sim->engine.scene_state(sim->scene), stats, n_substeps);
+        return EMERALD_OK;
+    });
+}
+
 int emerald_sim_counts(emerald_sim const* sim, size_t* n_fluid, size_t* n_solid) {
     if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
     if (n_fluid) *n_fluid = sim->engine.fluid_count(sim->scene);

@@ -1070,7 +1070,7 @@ std::vector<SceneState> Engine::all_states() {
 
 // Positions and velocities in original particle order: gathered through
 // slot_of into the reorder staging buffers, then copied out.
-void Engine::get_state(int id, float* x, float* v) {
+void Engine::get_state(int id, float* x, float* v, bool sync) {
     SceneParams const& P = scenes_[id].p;
     uint32_t const b = P.fluid_begin, n = P.fluid_count;
     if (x) {
@@ -1081,11 +1081,11 @@ void Engine::get_state(int id, float* x, float* v) {
         launch_gather_f2(a_, b, n, a_.v, a_.tv + b, st_);
         cudaMemcpyAsync(v, a_.tv + b, 8ull * n, cudaMemcpyDeviceToHost, st_);
     }
-    cudaStreamSynchronize(st_);
+    if (sync) cudaStreamSynchronize(st_);
     check("get_state");
 }
 
-void Engine::set_state(int id, float const* x, float const* v) {
+void Engine::set_state(int id, float const* x, float const* v, bool sync) {
     SceneParams const& P = scenes_[id].p;
     uint32_t const b = P.fluid_begin, n = P.fluid_count;
     if (x) {
@@ -1097,7 +1097,7 @@ void Engine::set_state(int id, float const* x, float const* v) {
         cudaMemcpyAsync(a_.tv + b, v, 8ull * n, cudaMemcpyHostToDevice, st_);
         launch_scatter_f2(a_, b, n, a_.tv + b, a_.v, st_);
     }
-    cudaStreamSynchronize(st_);
+    if (sync) cudaStreamSynchronize(st_);
     check("set_state");
 }
 

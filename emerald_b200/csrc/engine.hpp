@@ -101,8 +101,10 @@ public:
     void substep(int32_t method);
 
     // Synchronous accessors of one scene (original particle order).
-    void get_state(int id, float* x, float* v);
-    void set_state(int id, float const* x, float const* v);
+    // sync = false leaves the copies queued on the engine's stream (the
+    // caller synchronizes before it touches the host buffers).
+    void get_state(int id, float* x, float* v, bool sync = true);
+    void set_state(int id, float const* x, float const* v, bool sync = true);
     void get_solid(int id, float* xy, float* volumes);
     // Replaces a scene's boundary particles between sub-steps (count kept):
     // positions (NULL keeps them; new ones rebuild the boundary cell tables

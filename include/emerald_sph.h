@@ -170,6 +170,14 @@ int emerald_sim_frame(emerald_sim* sim, int32_t method, emerald_step_stats* stat
  * successive emerald_sim_frame calls would. */
 int emerald_sim_advance(emerald_sim* sim, int32_t method, int32_t n_substeps,
                         emerald_step_stats* stats);
+/* emerald_sim_set_state(x_in, v_in), emerald_sim_advance and
+ * emerald_sim_get_state(x_out, v_out) in one call, with one wait for the
+ * device at the end: the copies and the sub-steps are queued back to back
+ * on the simulation's stream. Any of the four buffers may be NULL; x_in may
+ * be x_out (and v_in v_out). Pinned host memory copies at DMA speed. */
+int emerald_sim_advance_host(emerald_sim* sim, int32_t method, int32_t n_substeps,
+                             float const* x_in, float const* v_in, float* x_out, float* v_out,
+                             emerald_step_stats* stats);
 
 int emerald_sim_counts(emerald_sim const* sim, size_t* n_fluid, size_t* n_solid);
 int emerald_sim_time(emerald_sim const* sim, int64_t* flicks);

@@ -131,6 +131,25 @@ def test_advance_equals_frames(E):
     assert a.time() == b.time()
 
 
+def test_advance_host_equals_separate_calls(E):
+    """One emerald_sim_advance_host call per sub-step (state in, advance,
+    state out) equals set_state, advance and get_state."""
+    scene = E.BlockScene(24, dx=F(1 / 48), seed=6, time_per_step_flicks=1411200, sub_steps=4)
+    a = E.Simulation.from_block_scene(scene)
+    b = E.Simulation.from_block_scene(scene)
+    x, v = a.state()
+    for _ in range(4):
+        a.set_state(x, v)
+        a.advance("dfsph_p", 1)
+        x, v = a.state()
+    xb, vb = b.state()
+    for _ in range(4):
+        b.advance_host("dfsph_p", 1, xb, vb)
+    assert_bitwise(xb, x, "x")
+    assert_bitwise(vb, v, "v")
+    assert a.time() == b.time()
+
+
 def test_default_scene_frames(E):
     """The reference's own dam break (hex lattice, world walls with 16 blocks,
     boundary volumes 1.7/sum W computed on the GPU)."""
