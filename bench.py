@@ -34,6 +34,17 @@ WORKLOAD = ("DFSPH_P dam break, 512x512=262144 fluid particles, dx=1/1024, suppo
             "100 correction iterations at most")
 
 
+def configure_scene(side):
+    """The single-scene workload at side x side fluid particles, dx = 1/(2 side)
+    (512: the default 262,144-particle dam break; 1024: 1,048,576)."""
+    global N_SIDE, DX, WORKLOAD
+    N_SIDE = side
+    DX = np.float32(1.0 / (2 * side))
+    WORKLOAD = ("DFSPH_P dam break, %dx%d=%d fluid particles, dx=1/%d, support=dx, "
+                "3 boundary rows, CFL dt<=5e-4 s, div tol 0.1%%/s, density tol 0.05%%, "
+                "100 correction iterations at most" % (side, side, side * side, 2 * side))
+
+
 def scene_kwargs():
     # 100 correction iterations: with the reference's default cap of 15 the
     # density solve stops above 0.1% average error on most sub-steps of this
@@ -563,7 +574,10 @@ def main():
     ap.add_argument("--serving-plain-seconds", type=float, default=30.0)
     ap.add_argument("--serving-lanes", type=int, default=16,
                     help="batch arenas the request loop steps concurrently")
+    ap.add_argument("--side", type=int, default=512,
+                    help="fluid block side of the single-scene workload (side^2 particles)")
     args = ap.parse_args()
+    configure_scene(args.side)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
