@@ -406,7 +406,8 @@ def run_serving(args, torch, E):
     reqs = W.serving_requests(args.serving_requests)
     scenes = [W.scene_for(r["nx"], r["ny"], r["seed"]) for r in reqs]
     srv = E.Server(120 * 10**9, "dfsph_p", max_scenes=max(64, len(reqs)),
-                   max_substeps_per_launch=8, lanes=args.serving_lanes)
+                   max_substeps_per_launch=args.serving_substeps, lanes=args.serving_lanes,
+                   order=args.serving_order)
     ids = [None] * len(reqs)
     t_start = time.perf_counter()
 
@@ -437,7 +438,8 @@ def run_serving(args, torch, E):
            "request_ms_p99": round(float(np.percentile(total_ms, 99)), 1),
            "queue_ms_p99": round(st["queue_ms_p99"], 1),
            "resident_peak": st["resident_peak"], "arena_bytes": st["device_bytes"],
-           "lanes": args.serving_lanes,
+           "lanes": args.serving_lanes, "order": args.serving_order,
+           "substeps_per_launch": args.serving_substeps,
            "max_avg_density_error": max(d[2]["error_average"] for d in done),
            "requests_above_0.1%": int(sum(d[2]["error_average"] > 0.001 for d in done))}
     # the same requests one at a time, bounded in time
@@ -574,6 +576,11 @@ def main():
     ap.add_argument("--serving-plain-seconds", type=float, default=30.0)
     ap.add_argument("--serving-lanes", type=int, default=16,
                     help="batch arenas the request loop steps concurrently")
+    ap.add_argument("--serving-substeps", type=int, default=8,
+                    help="sub-steps a lane runs between admission points")
+    ap.add_argument("--serving-order", default="largest_first",
+                    choices=["arrival", "largest_first"],
+                    help="request loop queue order")
     ap.add_argument("--side", type=int, default=512,
                     help="fluid block side of the single-scene workload (side^2 particles)")
     args = ap.parse_args()

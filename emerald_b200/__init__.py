@@ -68,7 +68,7 @@ class StepStats(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", c_sz), ("method", c_i32), ("max_scenes", c_i32),
-                ("max_substeps_per_launch", c_i32), ("lanes", c_i32)]
+                ("max_substeps_per_launch", c_i32), ("lanes", c_i32), ("order", c_i32)]
 
 
 class ServerStats(ctypes.Structure):
@@ -684,9 +684,10 @@ class Server:
     ETIMEOUT = 110
 
     def __init__(self, hbm_budget_bytes, method="dfsph_p", max_scenes=256,
-                 max_substeps_per_launch=8, lanes=4):
+                 max_substeps_per_launch=8, lanes=4, order="arrival"):
         cfg = ServerConfig(int(hbm_budget_bytes), method_id(method), int(max_scenes),
-                           int(max_substeps_per_launch), int(lanes))
+                           int(max_substeps_per_launch), int(lanes),
+                           {"arrival": 0, "largest_first": 1}[order])
         h = c_vp()
         _check(lib.emerald_server_create(ctypes.byref(cfg), ctypes.byref(h)),
                "emerald_server_create")

@@ -50,6 +50,7 @@ Server::Server(emerald_server_config const& cfg) : cfg_(cfg) {
     if (cfg_.max_scenes < 1) cfg_.max_scenes = 1;
     if (cfg_.max_substeps_per_launch < 1) cfg_.max_substeps_per_launch = 8;
     if (cfg_.lanes < 1) cfg_.lanes = 4;
+    if (cfg_.order != 1) cfg_.order = 0;
     if (cudaGetDevice(&device_) != cudaSuccess) {
         cudaGetLastError();
         throw std::runtime_error("no current CUDA device");
@@ -114,7 +115,18 @@ int Server::submit(std::unique_ptr<ServerRequest> r, int64_t& id) {
     r->remaining = r->substeps;
     r->submitted = std::chrono::steady_clock::now();
     id = r->id;
-    queue_.push_back(std::move(r));
+    if (cfg_.order == 1) {
+        // largest work first; equal work keeps arrival order
+        double const w = double(r->n_fluid) * double(r->substeps);
+        auto pos = queue_.begin();
+        while (pos != queue_.end() &&
+               double((*pos)->n_fluid) * double((*pos)->substeps) >= w) {
+            ++pos;
+        }
+        queue_.insert(pos, std::move(r));
+    } else {
+        queue_.push_back(std::move(r));
+    }
     ++submitted_;
     ++version_;
     work_cv_.notify_all();
@@ -125,7 +137,7 @@ int Server::preferred_lane(ServerRequest const& r) const {
     int best = -1;
     for (auto const& lane : lanes_) {
         if (!lane->room.fits(r.n_fluid, r.n_solid)) continue;
-        if (best < 0 || lane->resident_particles < lanes_[size_t(best)]->resident_particles) {
+        if (best < 0 || lane->resident_work < lanes_[size_t(best)]->resident_work) {
             best = lane->index;
         }
     }
@@ -140,9 +152,10 @@ void Server::resident_changed_locked(int delta) {
     resident_peak_ = std::max<int32_t>(resident_peak_, resident_);
 }
 
-// First fit in arrival order: every queued request for which this lane is
-// the least-loaded lane with room joins this lane's batch; a large request
-// that fits nowhere yet keeps its place while smaller ones behind it start.
+// First fit in queue order: every queued request for which this lane is
+// the lane with room and the least resident work joins this lane's batch; a
+// large request that fits nowhere yet keeps its place while smaller ones
+// behind it start.
 void Server::admit_locked(Lane& lane) {
     for (auto it = queue_.begin(); it != queue_.end();) {
         ServerRequest& r = **it;
@@ -177,6 +190,7 @@ void Server::admit_locked(Lane& lane) {
         std::vector<float>().swap(r.fluid_xy);
         std::vector<float>().swap(r.fluid_v);
         lane.resident_particles += double(r.n_fluid);
+        lane.resident_work += double(r.n_fluid) * double(r.remaining);
         lane.running.push_back(std::move(*it));
         it = queue_.erase(it);
         resident_changed_locked(+1);
@@ -209,6 +223,7 @@ void Server::loop(Lane& lane) {
             }
             lane.running.clear();
             lane.resident_particles = 0.0;
+            lane.resident_work = 0.0;
             done_cv_.notify_all();
             break;
         }
@@ -266,6 +281,7 @@ void Server::loop(Lane& lane) {
         batch_substeps_ += k;
         scene_substeps_ += int64_t(k) * int64_t(resident);
         particle_substeps_ += double(k) * particles;
+        lane.resident_work = std::max(0.0, lane.resident_work - double(k) * particles);
         lane.room = engine.room();
         auto const now = std::chrono::steady_clock::now();
         for (auto it = lane.running.begin(); it != lane.running.end();) {

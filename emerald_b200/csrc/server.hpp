@@ -71,10 +71,12 @@ private:
         // guarded by mu_
         Engine::Room room{};
         double resident_particles = 0.0;
+        double resident_work = 0.0;  // sum of fluid particles x sub-steps left
     };
 
     void loop(Lane& lane);
-    // Lane that request r should join now: the least-loaded one with room.
+    // Lane that request r should join now: the one with room and the least
+    // resident work.
     int preferred_lane(ServerRequest const& r) const;
     void admit_locked(Lane& lane);
     void resident_changed_locked(int delta);

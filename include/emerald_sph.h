@@ -314,14 +314,16 @@ int emerald_batch_set_tuning(emerald_batch* batch, emerald_tuning const* tuning)
 /* ----------------------------------------------------------------- serving */
 
 /* A request loop over batches: requests (a scene and a sub-step count) are
- * queued by any host thread, admitted in arrival order as soon as an arena
- * has room for them (first fit: a large request waiting for room does not
- * hold back smaller ones behind it; each goes to the least-loaded lane with
- * room), stepped together with every other scene of its arena, and retired
- * as soon as their sub-steps are done, which frees their room for the
- * queue. The device memory budget is split evenly over `lanes` arenas, each
- * with its own stream and host thread, sized once at creation. No
- * counterpart in the reference (one scene per process). */
+ * queued by any host thread, admitted as soon as an arena has room for them
+ * (first fit: a large request waiting for room does not hold back smaller
+ * ones behind it; each goes to the lane with the least resident work,
+ * fluid particles times sub-steps left, among those with room), stepped
+ * together with every other scene of its arena, and retired as soon as
+ * their sub-steps are done, which frees their room for the queue. The queue
+ * is in arrival order, or (order = 1) largest work first, which shortens
+ * the tail of a burst. The device memory budget is split evenly over
+ * `lanes` arenas, each with its own stream and host thread, sized once at
+ * creation. No counterpart in the reference (one scene per process). */
 typedef struct emerald_server emerald_server;
 
 typedef struct emerald_server_config {
@@ -330,6 +332,7 @@ typedef struct emerald_server_config {
     int32_t max_scenes;              /* scenes resident at once */
     int32_t max_substeps_per_launch; /* sub-steps between admission points (0: 8) */
     int32_t lanes;                   /* arenas stepped concurrently (0: 4) */
+    int32_t order;                   /* queue: 0 arrival order, 1 largest work first */
 } emerald_server_config;
 
 typedef struct emerald_server_stats {

@@ -38,8 +38,10 @@ def alone(E, sc, n):
     return x, v, st
 
 
-def test_requests_equal_alone_under_continuous_batching(E):
-    srv = E.Server(3 << 20, "dfsph_p", max_scenes=8, max_substeps_per_launch=3, lanes=2)
+@pytest.mark.parametrize("order", ["arrival", "largest_first"])
+def test_requests_equal_alone_under_continuous_batching(E, order):
+    srv = E.Server(3 << 20, "dfsph_p", max_scenes=8, max_substeps_per_launch=3, lanes=2,
+                   order=order)
     cap = srv.stats()["fluid_capacity"]  # of one lane
     assert cap >= 512, cap
     jobs = [(12, None, 3, 7), (16, None, 4, 11), (20, 10, 5, 4), (14, None, 6, 9),
