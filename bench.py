@@ -125,6 +125,16 @@ def traffic_from_profile(kernel):
     return None
 
 
+# What bounds a kernel whose HBM fraction is low by design (from its ncu
+# summary under profiles/).
+LIMITERS = {
+    "neighbors_fluid": "instruction issue: 58% of issue slots busy, 3-4% of peak DRAM "
+                       "throughput (profiles/k_neighbors.dfsph_262k.md)",
+}
+GATHER_KERNELS = ("apply_pressures", "apply_pressures_ext", "dfsph_density", "dfsph_divergence",
+                  "dfsph_density_alpha")
+
+
 # Algorithmic bytes per launch (each element a kernel must touch, once, plus
 # the neighbour lists it streams: 4 B index + 8 B kernel gradient per entry,
 # 4 B kernel value where used).
@@ -256,6 +266,22 @@ def run_gpu(args):
                     "peak_source": peak_kind, "traffic": traffic_from_profile(top_name),
                     "algorithmic_bytes_per_launch": alg,
                     "avg_launch_us": round(per_launch_s * 1e6, 2)}
+        if top_name in LIMITERS:
+            roofline["limiter"] = LIMITERS[top_name]
+    # the same figures for the gather-sum kernel with the largest share (the
+    # solver's memory-bound work)
+    gather = [kv for kv in ranked if kv[0] in GATHER_KERNELS]
+    gather_roofline = None
+    if gather:
+        g_name, (g_ms, g_launches) = gather[0]
+        g_s = g_ms / g_launches / 1000.0
+        g_alg = algorithmic_bytes(g_name, n, nnz_f, nnz_s, n_s)
+        g_ach = g_alg / g_s / 1e9
+        gather_roofline = {"bound": "hbm", "kernel": g_name, "achieved": round(g_ach, 1),
+                           "peak": peak, "unit": "GB/s", "frac": round(g_ach / peak, 4),
+                           "peak_source": peak_kind, "traffic": traffic_from_profile(g_name),
+                           "algorithmic_bytes_per_launch": g_alg,
+                           "avg_launch_us": round(g_s * 1e6, 2)}
     kernel_table = {k: {"ms_total": round(v[0], 3), "launches": v[1],
                         "share": round(v[0] / sum(x[0] for x in times.values()), 4)}
                     for k, v in ranked[:12]}
@@ -286,6 +312,7 @@ def run_gpu(args):
                                    "sum(int64(err*1000))/(1000 n); the exact FP64 mean "
                                    "of the per-particle errors is beside it"}},
             "roofline": roofline,
+            "gather_roofline": gather_roofline,
             "kernels": kernel_table,
             "e2e": {"value": round(e2e_value, 1), "unit": "particle-steps/s",
                     "h2d_bytes_per_step": int(2 * n * 8), "d2h_bytes_per_step": int(2 * n * 8),
