@@ -224,3 +224,24 @@ def test_oracle_thread_count_invariance(oracle):
         outs.append(sim.state()[0])
     oracle.set_threads(1)
     assert_bitwise(outs[0], outs[1], "x")
+
+
+def test_literal_h2dx_scene_is_unstable_in_the_reference(reference):
+    """The configs' literal kernel radius (support h = 2 dx) with the
+    reference's own mass per particle and boundary volumes (compute_volumes,
+    1.7 / sum W) blows up within the first DFSPH frame in the compiled
+    reference itself, which is why the benchmark scenes use support = dx."""
+    import emerald_b200 as E
+    from cpu_checkers import RefParams
+    dx = F(1 / 128)
+    sc = E.BlockScene(64, dx=dx, seed=1, support_ratio=2.0, time_per_step_flicks=1411200,
+                      sub_steps=4, dfsph_max_correction_iterations=100,
+                      dfsph_divergence_error_average_threshold=F(0.001),
+                      dfsph_density_error_average_threshold=F(0.0005))
+    d = sc.params.as_dict()
+    rp = {k: d[k] for k, _ in RefParams._fields_ if k in d}
+    rp.update(mass_per_particle_override=0.0, pressure_correction_denom_override=0.0)
+    ref = reference.sim(rp, sc.solid, sc.fluid, None, None)
+    ref.frame("dfsph_p")
+    v = ref.state()[1].astype(np.float64)
+    assert np.sqrt((v * v).sum(1)).max() > 100.0
