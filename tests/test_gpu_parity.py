@@ -278,3 +278,27 @@ def test_dense_cells_take_the_fallback_path(E, oracle):
         mask = np.arange(64)[None, :] < oc[:, None]
         assert_bitwise(np.where(mask, idx, 0), np.where(mask, oi, 0),
                        "%s indices" % ("solid" if is_solid else "fluid"))
+
+
+def test_pcisph_literal_support_matches_reference(E, reference):
+    """PCISPH at the configs' literal support h = 2 dx (about 45 neighbours
+    per particle, so every list takes the 64-entry path) against the
+    compiled reference, frame by frame."""
+    from cpu_checkers import RefParams
+    sc = E.BlockScene(48, dx=F(1 / 96), seed=3, support_ratio=2.0, time_per_step_flicks=1411200,
+                      sub_steps=4)
+    d = sc.params.as_dict()
+    rp = {k: d[k] for k, _ in RefParams._fields_ if k in d}
+    rp.update(mass_per_particle_override=d["mass_per_particle"],
+              pressure_correction_denom_override=d["pressure_correction_denom"])
+    ref = reference.sim(rp, sc.solid, sc.fluid, None, sc.solid_volumes)
+    sim = E.Simulation.from_block_scene(sc)
+    for f in range(3):
+        ref.frame("pcisph")
+        sim.frame("pcisph")
+        assert_bitwise(sim.state()[0], ref.state()[0], "x after frame %d" % f)
+        assert_bitwise(sim.state()[1], ref.state()[1], "v after frame %d" % f)
+    counts = sim.neighbors(False)[0]
+    assert counts.mean() > 30, counts.mean()
+    assert_bitwise(counts, ref.neighbors()[0], "neighbour counts")
+    sim.close()
