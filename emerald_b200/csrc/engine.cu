@@ -546,9 +546,14 @@ void Engine::rebuild_solids() {
     launch("build_cells_solid", [&] { launch_build_cells(e, true, ext_stiles_, d_scan_, st_); }, 4);
 }
 
+// Launch extents grow and shrink in steps of 1/EMERALD_EXTENT_DIV of the
+// arena (at least min_quantum): a change re-captures the sub-step graphs.
+#ifndef EMERALD_EXTENT_DIV
+#define EMERALD_EXTENT_DIV 32
+#endif
 namespace {
 uint32_t round_extent(uint64_t used, uint32_t capacity, uint32_t min_quantum) {
-    uint64_t const q = std::max<uint64_t>(min_quantum, capacity / 32);
+    uint64_t const q = std::max<uint64_t>(min_quantum, capacity / EMERALD_EXTENT_DIV);
     uint64_t const r = (used + q - 1) / q * q;
     return uint32_t(std::min<uint64_t>(std::max<uint64_t>(r, 1), capacity));
 }
