@@ -1,4 +1,5 @@
-// FP64 GPU oracle of the DFSPH_P sub-step: test infrastructure only.
+// FP64 GPU oracle of the DFSPH_P and IISPH sub-steps: test infrastructure
+// only.
 //
 // The same formulas and neighbour-list order as the reference's sph_common
 // and dfsph_p code (cubic spline W/GradW, emerald/sph_common/kernels.h:12-64;
@@ -6,7 +7,9 @@
 // emerald/sph_common/divergence.cpp:5-74; apply_pressures_in_place,
 // emerald/sph_common/pressure.cpp:9-80; DFSPH_P coefficients and pseudo
 // pressures, emerald/sph2d_box/dfsph_p_ops.cpp:19-126; the sub-step order of
-// emerald/sph2d_box/dfsph_p.cpp:325-373), evaluated in double. It states the
+// emerald/sph2d_box/dfsph_p.cpp:325-373; the IISPH coefficients, pressure
+// iteration and sub-step order of emerald/sph2d_box/iisph_ops.cpp:20-425
+// and emerald/sph2d_box/iisph.cpp:23-151), evaluated in double. It states the
 // error of the FP32 results: the caller passes each sub-step's dt and the
 // iteration counts the FP32 run took, so the two runs differ only in
 // arithmetic precision.
@@ -40,6 +43,9 @@ struct Sim {
     double* vols = nullptr;
     double *rho = nullptr, *alpha = nullptr, *kdiv = nullptr, *kdens = nullptr, *qdiv = nullptr,
            *qdens = nullptr, *rho_star = nullptr, *div = nullptr;
+    // IISPH: diagonal terms, pressures (current and next), sum_j dij pj
+    double2 *dii = nullptr, *sdp = nullptr;
+    double *aii = nullptr, *pres = nullptr, *pres_next = nullptr;
     // neighbour lists, slot-major: entry k of particle i at k * n + i
     int *fcnt = nullptr, *scnt = nullptr, *fidx = nullptr, *sidx = nullptr;
     double *fw = nullptr, *sw = nullptr;
@@ -277,6 +283,146 @@ __global__ void k_kappa(Sim s, double dt, int kind) {
     }
 }
 
+// ---------------------------------------------------------------- IISPH
+
+// External gravity and dii = -dt^2 sum_j m_j gradW_ij / rho_i^2 over fluid
+// then boundary neighbours (iisph_ops.cpp:20-90); zero initial pressures.
+__global__ void k_iisph_dii(Sim s, double dt) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const rho0 = s.p.rho0;
+    double const fmass = rho0 * s.p.fluid_volume;
+    s.v[i].y += dt * (-(s.p.mass * s.p.gravity)) / fmass;
+    double const denom = s.rho[i] * s.rho[i];
+    double2 dii = make_double2(0.0, 0.0);
+    int const cf = s.fcnt[i];
+    if (cf && denom != 0.0) {
+        double2 g = make_double2(0.0, 0.0);
+        for (int k = 0; k < cf; ++k) {
+            size_t const e = size_t(k) * s.n + i;
+            g.x += fmass * s.fgw[e].x;
+            g.y += fmass * s.fgw[e].y;
+        }
+        dii = make_double2(-dt * dt * g.x / denom, -dt * dt * g.y / denom);
+    }
+    int const cs = s.scnt[i];
+    if (cs && denom != 0.0) {
+        double2 g = make_double2(0.0, 0.0);
+        for (int k = 0; k < cs; ++k) {
+            size_t const e = size_t(k) * s.n + i;
+            double const m = rho0 * s.vols[s.sidx[e]];
+            g.x += m * s.sgw[e].x;
+            g.y += m * s.sgw[e].y;
+        }
+        dii.x += -dt * dt * g.x / denom;
+        dii.y += -dt * dt * g.y / denom;
+    }
+    s.dii[i] = dii;
+    s.pres[i] = 0.0;
+}
+
+// aii and the predicted density rho* (iisph_ops.cpp:92-200); the boundary
+// is at rest.
+__global__ void k_iisph_aii(Sim s, double dt) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const rho0 = s.p.rho0;
+    double const fmass = rho0 * s.p.fluid_volume;
+    double2 const dii = s.dii[i];
+    double2 const vi = s.v[i];
+    double aii = 0.0, dd = 0.0;
+    int const cf = s.fcnt[i];
+    for (int k = 0; k < cf; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        int const j = s.fidx[e];
+        double2 const g = s.fgw[e];
+        double const dj = s.rho[j] * s.rho[j];
+        if (dj != 0.0) {
+            // dji = -dij = dt^2 m gradW_ij / rho_j^2
+            double2 const dji = make_double2(dt * dt * fmass * g.x / dj, dt * dt * fmass * g.y / dj);
+            aii += fmass * ((dii.x - dji.x) * g.x + (dii.y - dji.y) * g.y);
+        }
+        dd += dt * fmass * ((vi.x - s.v[j].x) * g.x + (vi.y - s.v[j].y) * g.y);
+    }
+    int const cs = s.scnt[i];
+    for (int k = 0; k < cs; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        double const m = s.vols[s.sidx[e]] * rho0;
+        double2 const g = s.sgw[e];
+        aii += m * (dii.x * g.x + dii.y * g.y);
+        dd += dt * m * (vi.x * g.x + vi.y * g.y);
+    }
+    s.aii[i] = aii;
+    s.rho_star[i] = s.rho[i] + dd;
+}
+
+// sum_j dij pj over fluid neighbours (iisph_ops.cpp:202-235).
+__global__ void k_iisph_sdp(Sim s, double dt) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const fmass = s.p.rho0 * s.p.fluid_volume;
+    double2 sum = make_double2(0.0, 0.0);
+    int const cf = s.fcnt[i];
+    for (int k = 0; k < cf; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        int const j = s.fidx[e];
+        double const dj = s.rho[j] * s.rho[j];
+        if (dj == 0.0) continue;
+        double const c = -dt * dt * fmass * s.pres[j] / dj;
+        sum.x += c * s.fgw[e].x;
+        sum.y += c * s.fgw[e].y;
+    }
+    s.sdp[i] = sum;
+}
+
+// beta_i (iisph_ops.cpp:237-330) and the relaxed Jacobi pressure update
+// p_i <- max(0, mix(p_i, (rho0 - rho*_i - beta_i) / aii, omega))
+// (iisph_ops.cpp:332-425).
+__global__ void k_iisph_pressures(Sim s, double dt, double omega) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const rho0 = s.p.rho0;
+    double const fmass = rho0 * s.p.fluid_volume;
+    double const pi = s.pres[i];
+    double2 const si = s.sdp[i];
+    double beta = 0.0;
+    int const cf = s.fcnt[i];
+    for (int k = 0; k < cf; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        int const j = s.fidx[e];
+        double2 const g = s.fgw[e];
+        double const dj = s.rho[j] * s.rho[j];
+        double2 dji = make_double2(0.0, 0.0);
+        if (dj != 0.0) dji = make_double2(dt * dt * fmass * g.x / dj, dt * dt * fmass * g.y / dj);
+        double const pj = s.pres[j];
+        double2 const djj = s.dii[j];
+        double2 const sj = s.sdp[j];
+        double const tx = si.x - djj.x * pj - (sj.x - dji.x * pi);
+        double const ty = si.y - djj.y * pj - (sj.y - dji.y * pi);
+        beta += fmass * (tx * g.x + ty * g.y);
+    }
+    int const cs = s.scnt[i];
+    for (int k = 0; k < cs; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        beta += rho0 * s.vols[s.sidx[e]] * (si.x * s.sgw[e].x + si.y * s.sgw[e].y);
+    }
+    double const alpha = s.aii[i];
+    double out = pi;
+    if (alpha != 0.0) {
+        double const p_new = (rho0 - s.rho_star[i] - beta) / alpha;
+        out = pi * (1.0 - omega) + p_new * omega;
+        if (out < 0.0) out = 0.0;
+    }
+    s.pres_next[i] = out;
+}
+
+// q_i = p_i / rho_i^2 of the final pressures, for apply_pressures_in_place.
+__global__ void k_iisph_q(Sim s) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    s.qdens[i] = q_of(s.pres[i], s.rho[i]);
+}
+
 __global__ void k_positions(Sim s, double dt) {
     size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
     if (i >= s.n) return;
@@ -309,6 +455,8 @@ typedef struct fp64_params {
     double support, rho0, mass, fluid_volume, gravity;
 } fp64_params;
 
+int fp64_destroy(void* h);
+
 int fp64_create(fp64_params const* p, double const* solid_xy, double const* solid_vols, size_t ns,
                 double const* fluid_xy, double const* fluid_v, size_t n, void** out) {
     Sim* s = new Sim;
@@ -328,6 +476,11 @@ int fp64_create(fp64_params const* p, double const* solid_xy, double const* soli
     s->qdens = dalloc<double>(n);
     s->rho_star = dalloc<double>(n);
     s->div = dalloc<double>(n);
+    s->dii = dalloc<double2>(n);
+    s->sdp = dalloc<double2>(n);
+    s->aii = dalloc<double>(n);
+    s->pres = dalloc<double>(n);
+    s->pres_next = dalloc<double>(n);
     s->fcnt = dalloc<int>(n);
     s->scnt = dalloc<int>(n);
     s->fidx = dalloc<int>(E);
@@ -340,7 +493,11 @@ int fp64_create(fp64_params const* p, double const* solid_xy, double const* soli
     s->skeys = dalloc<unsigned long long>(ns);
     s->fvals = dalloc<int>(n);
     s->svals = dalloc<int>(ns);
-    if (!s->sgw || !s->svals || !s->fvals) return 12;
+    if (!s->sgw || !s->svals || !s->fvals || !s->dii || !s->sdp || !s->aii || !s->pres ||
+        !s->pres_next) {
+        fp64_destroy(s);
+        return 12;
+    }
     cudaMemcpy(s->x, fluid_xy, 16 * n, cudaMemcpyHostToDevice);
     if (fluid_v) {
         cudaMemcpy(s->v, fluid_v, 16 * n, cudaMemcpyHostToDevice);
@@ -361,7 +518,8 @@ int fp64_destroy(void* h) {
     void* ptrs[] = {s->x,    s->v,    s->xs,    s->vols,  s->rho,   s->alpha, s->kdiv,
                     s->kdens, s->qdiv, s->qdens, s->rho_star, s->div, s->fcnt,  s->scnt,
                     s->fidx, s->sidx, s->fw,    s->sw,    s->fgw,   s->sgw,   s->fkeys,
-                    s->skeys, s->fvals, s->svals};
+                    s->skeys, s->fvals, s->svals, s->dii, s->sdp, s->aii, s->pres,
+                    s->pres_next};
     for (void* p : ptrs) cudaFree(p);
     delete s;
     return 0;
@@ -392,7 +550,35 @@ int fp64_sub_step(void* h, double dt, int new_frame, int div_iters, int dens_ite
     return e == cudaSuccess ? 0 : 1000;
 }
 
-// "x", "v" (2 doubles per particle), "densities", "alphas", "counts".
+// One IISPH sub-step of length dt running `iters` pressure iterations with
+// relaxation omega (the sub-step of emerald/sph2d_box/iisph.cpp:23-151).
+int fp64_sub_step_iisph(void* h, double dt, int iters, double omega) {
+    Sim& s = *static_cast<Sim*>(h);
+    size_t const n = s.n;
+    double const cell = 2.0 * s.p.support;
+    sort_cells(s.x, n, cell, s.fkeys, s.fvals);
+    k_neighbors<<<grid(n), 128>>>(s, s.x, n, s.fkeys, s.fvals, true, s.fcnt, s.fidx, s.fw, s.fgw);
+    k_neighbors<<<grid(n), 128>>>(s, s.xs, s.ns, s.skeys, s.svals, false, s.scnt, s.sidx, s.sw,
+                                  s.sgw);
+    k_density_alpha<<<grid(n), 128>>>(s, 0);
+    k_iisph_dii<<<grid(n), 128>>>(s, dt);
+    k_iisph_aii<<<grid(n), 128>>>(s, dt);
+    for (int it = 0; it < iters; ++it) {
+        k_iisph_sdp<<<grid(n), 128>>>(s, dt);
+        k_iisph_pressures<<<grid(n), 128>>>(s, dt, omega);
+        double* t = s.pres;
+        s.pres = s.pres_next;
+        s.pres_next = t;
+    }
+    k_iisph_q<<<grid(n), 128>>>(s);
+    k_apply<<<grid(n), 128>>>(s, s.qdens, dt, 0);
+    k_positions<<<grid(n), 128>>>(s, dt);
+    cudaError_t const e = cudaDeviceSynchronize();
+    return e == cudaSuccess ? 0 : 1000;
+}
+
+// "x", "v" (2 doubles per particle), "densities", "alphas", "pressures"
+// (IISPH), "counts".
 int fp64_get(void* h, char const* name, double* out) {
     Sim& s = *static_cast<Sim*>(h);
     size_t const n = s.n;
@@ -400,6 +586,9 @@ int fp64_get(void* h, char const* name, double* out) {
     if (!std::strcmp(name, "v")) return cudaMemcpy(out, s.v, 16 * n, cudaMemcpyDeviceToHost) ? 1000 : 0;
     if (!std::strcmp(name, "densities")) {
         return cudaMemcpy(out, s.rho, 8 * n, cudaMemcpyDeviceToHost) ? 1000 : 0;
+    }
+    if (!std::strcmp(name, "pressures")) {
+        return cudaMemcpy(out, s.pres, 8 * n, cudaMemcpyDeviceToHost) ? 1000 : 0;
     }
     if (!std::strcmp(name, "alphas")) {
         return cudaMemcpy(out, s.alpha, 8 * n, cudaMemcpyDeviceToHost) ? 1000 : 0;

@@ -465,9 +465,9 @@ class RefSim:
 
 
 class FP64Oracle:
-    """The FP64 GPU oracle of the DFSPH_P sub-step (oracle/fp64/dfsph_fp64.cu):
-    the same formulas and list order in double, driven with each FP32
-    sub-step's dt and iteration counts."""
+    """The FP64 GPU oracle of the DFSPH_P and IISPH sub-steps
+    (oracle/fp64/dfsph_fp64.cu): the same formulas and list order in double,
+    driven with each FP32 sub-step's dt and iteration counts."""
 
     path = os.path.join(ORACLE_DIR, "libfp64_oracle.so")
 
@@ -484,6 +484,7 @@ class FP64Oracle:
         lib.fp64_destroy.argtypes = [vp]
         lib.fp64_sub_step.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int]
+        lib.fp64_sub_step_iisph.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double]
         lib.fp64_get.argtypes = [vp, ctypes.c_char_p, vp]
         self.lib = lib
 
@@ -511,6 +512,10 @@ class FP64Sim:
     def sub_step(self, dt, new_frame, div_iters, dens_iters):
         rc = self.o.lib.fp64_sub_step(self.h, float(dt), int(new_frame), int(div_iters),
                                       int(dens_iters))
+        assert rc == 0, rc
+
+    def sub_step_iisph(self, dt, iters, omega):
+        rc = self.o.lib.fp64_sub_step_iisph(self.h, float(dt), int(iters), float(omega))
         assert rc == 0, rc
 
     def get(self, name):

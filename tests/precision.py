@@ -1,9 +1,9 @@
-"""Error of the FP32 DFSPH_P results against the FP64 GPU oracle.
+"""Error of the FP32 DFSPH_P and IISPH results against the FP64 GPU oracle.
 
 The FP32 run (the CUDA path, in either precision mode) advances CFL-adaptive
 sub-steps; the FP64 oracle repeats each sub-step with the same dt, frame
-boundaries and iteration counts, so the two differ only in arithmetic
-precision. Reported per checkpoint: per-particle density error (relative,
+boundaries and iteration counts (and, for IISPH, the same relaxation omega),
+so the two differ only in arithmetic precision. Reported per checkpoint: per-particle density error (relative,
 L_inf and RMS), position error (in units of the particle spacing, max and
 RMS) and the kinetic-energy difference."""
 import numpy as np
@@ -20,11 +20,20 @@ def dfsph_scene(E, n_side, precision, seed=1):
                         precision=precision)
 
 
-def compare(E, n_side, steps, checkpoints, precision, seed=1, offset=0.0):
-    """Rows of error statistics at the given sub-steps. `offset` moves the
-    whole scene (fluid and walls) by (offset, offset) metres, rounded to
-    float, before either run starts."""
-    scene = dfsph_scene(E, n_side, precision, seed)
+def iisph_scene(E, n_side, precision, seed=1):
+    return E.BlockScene(n_side, dx=np.float32(1.0 / (2 * n_side)), seed=seed,
+                        time_per_step_flicks=1411200, sub_steps=4,
+                        iisph_max_pressure_iterations=50,
+                        iisph_error_average_threshold=np.float32(0.001),
+                        precision=precision)
+
+
+def compare(E, n_side, steps, checkpoints, precision, seed=1, offset=0.0, method="dfsph_p"):
+    """Rows of error statistics at the given sub-steps of `method` ("dfsph_p"
+    or "iisph"). `offset` moves the whole scene (fluid and walls) by
+    (offset, offset) metres, rounded to float, before either run starts."""
+    make = dfsph_scene if method == "dfsph_p" else iisph_scene
+    scene = make(E, n_side, precision, seed)
     p = scene.params
     off = np.float32(offset)
     fluid = (scene.fluid + off).astype(np.float32)
@@ -38,9 +47,13 @@ def compare(E, n_side, steps, checkpoints, precision, seed=1, offset=0.0):
     rows = []
     for step in range(1, steps + 1):
         new_frame = sim.time() % tps == 0
-        st = sim.advance("dfsph_p", 1)
-        ref.sub_step(float(np.float32(st["dt"])), new_frame, st["divergence_iterations"],
-                     st["pressure_iterations"])
+        st = sim.advance(method, 1)
+        if method == "dfsph_p":
+            ref.sub_step(float(np.float32(st["dt"])), new_frame, st["divergence_iterations"],
+                         st["pressure_iterations"])
+        else:
+            ref.sub_step_iisph(float(np.float32(st["dt"])), st["pressure_iterations"],
+                               float(p.iisph_omega))
         if step in checkpoints:
             x, v = sim.state()
             rho = sim.array("densities").astype(np.float64)
@@ -51,13 +64,20 @@ def compare(E, n_side, steps, checkpoints, precision, seed=1, offset=0.0):
             dpos = np.hypot(*(x.astype(np.float64) - x64).T) / dx
             ke = 0.5 * mass * float(np.sum(v.astype(np.float64) ** 2))
             ke64 = 0.5 * mass * float(np.sum(v64 ** 2))
+            extra = {}
+            if method == "iisph":
+                pr = sim.array("pressures").astype(np.float64)
+                pr64 = ref.get("pressures")
+                scale = float(np.abs(pr64).max()) or 1.0
+                extra = dict(pressure_linf=float(np.abs(pr - pr64).max()) / scale,
+                             pressure_rms=float(np.sqrt(np.mean((pr - pr64) ** 2))) / scale)
             rows.append(dict(step=step, density_linf=float(drel.max()),
                              density_rms=float(np.sqrt(np.mean(drel ** 2))),
                              position_max_dx=float(dpos.max()),
                              position_rms_dx=float(np.sqrt(np.mean(dpos ** 2))),
                              kinetic_energy=ke, kinetic_energy_fp64=ke64,
                              energy_rel_diff=abs(ke - ke64) / ke64 if ke64 else 0.0,
-                             iterations=st["pressure_iterations"]))
+                             iterations=st["pressure_iterations"], **extra))
     ref.close()
     sim.close()
     return rows

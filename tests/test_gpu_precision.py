@@ -61,3 +61,29 @@ def test_compensated_mode_meets_tolerance(E):
     for _ in range(30):
         st = sim.advance("dfsph_p", 1)
         assert st["error_average"] <= 0.0005 or st["pressure_iterations"] == 100, st
+
+
+def test_iisph_fp64_oracle_first_step_agrees(E):
+    """IISPH after one sub-step: densities within 1e-5 relative of double
+    precision, positions within 1e-4 dx, and the pressures the FP32 solve
+    ends with within 1e-3 of the largest FP64 pressure."""
+    from precision import compare
+    for mode in (E.PRECISION_REFERENCE, E.PRECISION_COMPENSATED):
+        r = compare(E, 48, 1, {1}, mode, method="iisph")[0]
+        print("iisph mode", mode, r)
+        assert r["iterations"] >= 2, r
+        assert r["density_linf"] < 1e-5, r
+        assert r["position_max_dx"] < 1e-4, r
+        assert r["pressure_linf"] < 1e-3, r
+
+
+def test_iisph_fp64_oracle_ten_steps(E):
+    """Ten IISPH sub-steps of a 96x96 block: the FP32 run stays close to the
+    FP64 oracle (RMS position error below 1e-3 dx, kinetic energy within
+    1%), in both precision modes."""
+    from precision import compare
+    for mode in (E.PRECISION_REFERENCE, E.PRECISION_COMPENSATED):
+        r = compare(E, 96, 10, {10}, mode, method="iisph")[0]
+        print("iisph 10 sub-steps, mode", mode, r)
+        assert r["position_rms_dx"] < 1e-3, r
+        assert r["energy_rel_diff"] < 1e-2, r
