@@ -54,7 +54,7 @@ struct SceneParams {
     float fixed_dt;
     uint32_t sort_base;  // real particles of scenes stored before this one
     float reject_l2;     // smallest float whose sqrtf is >= cell_size
-    int32_t precision;   // 0: the reference's FP32 arithmetic; 1: compensated (DFSPH_P)
+    int32_t precision;   // 0: the reference's FP32 arithmetic; 1: FP64 positions (+ Kahan sums under DFSPH_P)
     // Cells within one cell of a boundary particle's cell: bit
     // (y - near_y0) * near_w + (x - near_x0) of the words from near_begin.
     // A fluid particle whose cell is clear has no boundary neighbours.

@@ -680,18 +680,37 @@ __global__ void k_dfsph_density(Arena a) {
 
 // integrate_positions_in_place (dynamics.cpp:46-51). Compensated mode
 // accumulates the positions in double and stores their float rounding.
+// x_i += dt * v (+ shift): the reference's FP32 update, or for a
+// compensated scene the FP64 accumulator (the positions the neighbour search
+// takes its vectors from) rounded once into x_i. Every method's position
+// update goes through here, so a compensated scene's FP64 positions stay
+// current whichever method advances it.
+__device__ __forceinline__ void advance_position(Arena const& a, SceneParams const& P,
+                                                 uint32_t i, float dt, float2 v,
+                                                 float2 shift = {0.0f, 0.0f}, bool shifted = false) {
+    if (P.precision) {
+        double2 x = a.x64[i];
+        x.x += static_cast<double>(dt) * static_cast<double>(v.x);
+        x.y += static_cast<double>(dt) * static_cast<double>(v.y);
+        if (shifted) {
+            x.x += static_cast<double>(shift.x);
+            x.y += static_cast<double>(shift.y);
+        }
+        a.x64[i] = x;
+        a.x[i] = mk2(static_cast<float>(x.x), static_cast<float>(x.y));
+        return;
+    }
+    float2 const x = add2(a.x[i], scl2(dt, v));
+    a.x[i] = shifted ? add2(x, shift) : x;
+}
+
 template <int MODE>
 __global__ void k_integrate_positions(Arena a) {
     Ctx c;
     if (!enter(a, false, c) || !c.live) return;
     float const dt = a.ss[c.s].dt;
     if (MODE && a.sp[c.s].precision) {
-        float2 const v = a.v[c.i];
-        double2 x = a.x64[c.i];
-        x.x += static_cast<double>(dt) * static_cast<double>(v.x);
-        x.y += static_cast<double>(dt) * static_cast<double>(v.y);
-        a.x64[c.i] = x;
-        a.x[c.i] = mk2(static_cast<float>(x.x), static_cast<float>(x.y));
+        advance_position(a, a.sp[c.s], c.i, dt, a.v[c.i]);
         return;
     }
     a.x[c.i] = add2(a.x[c.i], scl2(dt, a.v[c.i]));
@@ -908,7 +927,7 @@ __global__ void k_apply_integrate(Arena a) {
     float const dt = a.ss[c.s].dt;
     float2 const v = apply_pressure_of(a, P, c.i, a.v[c.i], a.qdens, dt);
     a.v[c.i] = v;
-    a.x[c.i] = add2(a.x[c.i], scl2(dt, v));
+    advance_position(a, P, c.i, dt, v);
 }
 
 // ------------------------------------------------- IISPH_AP / PSEUDO_AP
@@ -1052,10 +1071,10 @@ __global__ void k_ap_finish(Arena a, int pseudo) {
     if (!pseudo) {
         float2 const v = add2(a.v[i], scl2(dt, acc));
         a.v[i] = v;
-        a.x[i] = add2(a.x[i], scl2(dt, v));
+        advance_position(a, P, i, dt, v);
     } else {
         float2 const vstar = a.v[i];
-        a.x[i] = add2(add2(a.x[i], scl2(dt, vstar)), acc);
+        advance_position(a, P, i, dt, vstar, acc, true);
         if (safe_v(vstar, dt)) a.v[i] = add2(vstar, div2(acc, dt));
     }
 }
@@ -1195,7 +1214,7 @@ __global__ void k_pc_final(Arena a) {
     float const dt = a.ss[c.s].dt;
     float2 const v = add2(a.vext[c.i], scl2(dt / P.mass, a.fp[c.i]));
     a.v[c.i] = v;
-    a.x[c.i] = add2(a.x[c.i], scl2(dt, v));
+    advance_position(a, P, c.i, dt, v);
 }
 
 }  // namespace

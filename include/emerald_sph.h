@@ -67,12 +67,13 @@ typedef struct emerald_params {
 } emerald_params;
 
 /* Arithmetic of a scene. REFERENCE (default): the reference's FP32
- * operations in its order, bit-identical results. COMPENSATED (DFSPH_P
- * only; other methods keep REFERENCE): neighbour sums in FP32 with Kahan
- * compensation, positions accumulated in FP64 and the neighbour vectors
- * x_i - x_j taken from them. The solver's exit test is the reference's in
- * both modes (an exact int64 sum and an FP64 division); the exact FP64 mean
- * of the errors is reported in emerald_step_stats. */
+ * operations in its order, bit-identical results. COMPENSATED: positions
+ * accumulated in FP64 and the neighbour vectors x_i - x_j taken from them
+ * (every method); under DFSPH_P also the neighbour sums in FP32 with Kahan
+ * compensation (the other methods keep the reference's sums). The solver's
+ * exit test is the reference's in both modes (an exact int64 sum and an
+ * FP64 division); the exact FP64 mean of the errors is reported in
+ * emerald_step_stats. */
 #define EMERALD_PRECISION_REFERENCE 0
 #define EMERALD_PRECISION_COMPENSATED 1
 

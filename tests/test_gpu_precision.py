@@ -87,3 +87,29 @@ def test_iisph_fp64_oracle_ten_steps(E):
         print("iisph 10 sub-steps, mode", mode, r)
         assert r["position_rms_dx"] < 1e-3, r
         assert r["energy_rel_diff"] < 1e-2, r
+        assert r["density_linf"] < 1e-3, r
+
+
+@pytest.mark.parametrize("method", ["pcisph", "iisph", "iisph_ap", "iisph_pseudo_ap", "dfsph_p"])
+def test_compensated_positions_follow_every_method(E, method):
+    """A compensated scene keeps its FP64 positions (which the neighbour
+    search reads) current under every method: ten sub-steps in compensated
+    mode stay within rounding of the same ten in reference mode (RMS
+    position difference below 1e-3 dx; a stale FP64 copy would leave the
+    neighbour vectors at the initial positions and differ by far more)."""
+    from precision import dfsph_scene, iisph_scene
+    make = dfsph_scene if method == "dfsph_p" else iisph_scene
+    out = []
+    for mode in (E.PRECISION_REFERENCE, E.PRECISION_COMPENSATED):
+        sc = make(E, 48, mode)
+        sim = E.Simulation.from_block_scene(sc)
+        for _ in range(10):
+            sim.advance(method, 1)
+        out.append(sim.state()[0].astype(np.float64))
+        sim.close()
+    dx = float(sc.dx)
+    d = np.hypot(*(out[1] - out[0]).T) / dx
+    print(method, "compensated vs reference after 10 sub-steps: RMS %.3e dx, max %.3e dx" % (
+        float(np.sqrt(np.mean(d ** 2))), float(d.max())))
+    assert np.all(np.isfinite(out[1]))
+    assert float(np.sqrt(np.mean(d ** 2))) < 1e-3
