@@ -302,3 +302,61 @@ def test_pcisph_literal_support_matches_reference(E, reference):
     assert counts.mean() > 30, counts.mean()
     assert_bitwise(counts, ref.neighbors()[0], "neighbour counts")
     sim.close()
+
+
+def spray_fluid(sc):
+    """The block plus particles in the air, all farther than 2h from one
+    another and from the block: ten lone droplets (no neighbours), two pairs
+    h/2 apart, and two particles at the same position (distance 0, so W(0)
+    and a zero gradient) on a cell corner (x = 7 cells, y = 12 cells of
+    2h = 1/16 m, exact in float)."""
+    h = float(sc.params.support)
+    drops = [(x, y) for y in (0.8, 0.9) for x in (0.1, 0.3, 0.5, 0.7, 0.9)]
+    pairs = [(0.2, 0.7), (0.2 + 0.5 * h, 0.7), (0.6, 0.7), (0.6 + 0.5 * h, 0.7)]
+    same = [(0.4375, 0.75), (0.4375, 0.75)]
+    extra = np.array(drops + pairs + same, np.float32)
+    return np.concatenate([sc.fluid, extra]).astype(np.float32), len(extra)
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_spray_scene_matches_reference(E, reference, method):
+    """Zero-neighbour particles, two-particle clusters and coincident
+    particles take the empty-list and zero-gradient branches of every
+    solver (dii, aii and alpha of 0, pressures left as they were); two
+    frames equal the compiled reference bit for bit."""
+    from cpu_checkers import RefParams
+    sc = E.BlockScene(16, dx=F(1 / 32), seed=12, time_per_step_flicks=1411200, sub_steps=4,
+                      iisph_max_pressure_iterations=50,
+                      iisph_error_average_threshold=F(0.001))
+    fluid, n_extra = spray_fluid(sc)
+    d = sc.params.as_dict()
+    rp = {k: d[k] for k, _ in RefParams._fields_ if k in d}
+    rp.update(mass_per_particle_override=d["mass_per_particle"],
+              pressure_correction_denom_override=d["pressure_correction_denom"])
+    ref = reference.sim(rp, sc.solid, fluid, None, sc.solid_volumes)
+    sim = E.Simulation(sc.params, sc.solid, fluid, None, sc.solid_volumes)
+    for f in range(2):
+        ref.frame(method)
+        sim.frame(method)
+        assert_bitwise(sim.state()[0], ref.state()[0], "%s x after frame %d" % (method, f))
+        assert_bitwise(sim.state()[1], ref.state()[1], "%s v after frame %d" % (method, f))
+    counts = sim.neighbors(False)[0]
+    assert np.all(counts[-n_extra:-6] == 0)
+    assert np.all(counts[-6:] == 1)
+    x = sim.state()[0]
+    assert np.array_equal(x[-1], x[-2])
+    sim.close()
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_empty_fluid_scene_steps(E, method):
+    """A scene with walls and no fluid particles frames without error and
+    returns empty state arrays."""
+    sc = E.BlockScene(16, dx=F(1 / 32), seed=12, time_per_step_flicks=1411200, sub_steps=4)
+    sim = E.Simulation(sc.params, sc.solid, np.zeros((0, 2), np.float32), None,
+                       sc.solid_volumes)
+    st = sim.frame(method)
+    assert st["sub_steps"] >= 1
+    x, v = sim.state()
+    assert x.shape == (0, 2) and v.shape == (0, 2)
+    sim.close()
