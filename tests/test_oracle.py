@@ -245,3 +245,28 @@ def test_literal_h2dx_scene_is_unstable_in_the_reference(reference):
     ref.frame("dfsph_p")
     v = ref.state()[1].astype(np.float64)
     assert np.sqrt((v * v).sum(1)).max() > 100.0
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_oracle_traces_match_reference(oracle, method):
+    """All 1000 fixed-dt sub-steps of the reference's trace fixtures
+    (tests/golden/trace_<method>.npz; the 128 x 128 dam-break block of
+    tests/traces.py): density-error and kinetic-energy traces equal at every
+    sub-step, positions and velocities bit-identical after sub-steps 1, 10,
+    100 and 1000. About 12 s per solver on 8 host threads."""
+    import traces as T
+    g = dict(np.load(os.path.join(GOLDEN, "trace_scene.npz")))
+    ref = np.load(os.path.join(GOLDEN, "trace_%s.npz" % method))
+    p = dict(_golden_sim(oracle, method)[1])
+    p.update(support=g["dx"], mass_per_particle=g["mass"], pressure_correction_denom=g["denom"],
+             seconds_per_sub_step=T.PCISPH_DT)
+    oracle.set_threads(os.cpu_count() or 1)
+    try:
+        sim = oracle.sim(p, g["solid"], g["solid_volumes"], g["fluid"])
+        tr = T.run_trace(sim, method, g["mass"])
+    finally:
+        oracle.set_threads(1)
+    for key in ("kinetic_energy", "avg_error", "max_error", "exact_error"):
+        assert np.array_equal(tr[key], ref[key]), (method, key)
+    for s, h in zip(ref["digest_steps"], ref["digests"]):
+        assert tr["digests"][int(s)] == str(h), (method, int(s))
