@@ -29,6 +29,14 @@ N_SIDE = 512
 DX = np.float32(1.0 / 1024)
 TPS_FLICKS = 1411200  # 2e-3 s: DFSPH sub-steps between tps/60 and tps/4 = 5e-4 s
 DFSPH_CAP = 100
+# IISPH pressure iterations at most in the batched workload: with the plain
+# configuration's 50, the widest and tallest blocks of the 512 end their
+# sub-steps above 0.1% average density error; the C oracle run on those
+# scenes reaches 0.1% within 200.
+BATCH_IISPH_CAP = 200
+# 0.1% as the solvers hold it: their exit test is average <= 0.001f in FP32,
+# so an average of exactly 0.001f meets the tolerance.
+TOL_0_1 = np.float32(0.001)
 WORKLOAD = ("DFSPH_P dam break, 512x512=262144 fluid particles, dx=1/1024, support=dx, "
             "3 boundary rows, CFL dt<=5e-4 s, div tol 0.1%/s, density tol 0.05%, "
             "100 correction iterations at most")
@@ -306,7 +314,7 @@ def run_gpu(args):
                                                           "error_average", "error_max")},
                        "density_error_after_timing": {
                            "steps": len(errs), "max_avg_error": max(errs),
-                           "steps_above_0.1%": int(sum(e > 0.001 for e in errs)),
+                           "steps_above_0.1%": int(sum(e > TOL_0_1 for e in errs)),
                            "max_exact_mean_error": max(exact),
                            "note": "avg error is the reference's metric "
                                    "sum(int64(err*1000))/(1000 n); the exact FP64 mean "
@@ -395,7 +403,8 @@ def run_batched(args, torch, E, rank, world, barrier):
     sizes = [s["nx"] * s["ny"] for s in specs]
     mine = W.assign_scenes(sizes, world)[rank]
     scenes = [W.scene_for(specs[k]["nx"], specs[k]["ny"], specs[k]["seed"],
-                          specs[k]["viscosity"]) for k in mine]
+                          specs[k]["viscosity"], iisph_max_pressure_iterations=BATCH_IISPH_CAP)
+              for k in mine]
     nf = sum(len(s.fluid) for s in scenes)
     ns = sum(len(s.solid) for s in scenes)
     b = E.Batch(nf + 128 * len(scenes), ns + 128 * len(scenes), len(scenes))
@@ -426,7 +435,8 @@ def run_batched(args, torch, E, rank, world, barrier):
     b.close()
     out = {"workload": "%d IISPH dam breaks per GPU, fluid count log-uniform in [1024, 65536], "
                        "aspect U[0.25,4], viscosity U[0.001,0.05] (unused by IISPH), "
-                       "support=dx, CFL dt<=5e-4 s, 50-iteration cap, 0.1%% tolerance" % count,
+                       "support=dx, CFL dt<=5e-4 s, %d-iteration cap, 0.1%% tolerance" % (
+                           count, BATCH_IISPH_CAP),
            "scenes": len(scenes) * world, "fluid_particles": nf, "boundary_particles": ns,
            "steps": steps, "warmup": warm,
            "scene_steps_per_s": round(len(scenes) * world * steps / total_s, 1),
@@ -435,7 +445,7 @@ def run_batched(args, torch, E, rank, world, barrier):
            "p50_step_ms": round(float(np.percentile(step_ms, 50)), 3),
            "p99_step_ms": round(float(np.percentile(step_ms, 99)), 3),
            "max_avg_density_error": err,
-           "scenes_above_0.1%": int(sum(st["error_average"] > 0.001 for st in stats)),
+           "scenes_above_0.1%": int(sum(st["error_average"] > TOL_0_1 for st in stats)),
            "iterations_last_step": [min(iters), max(iters)],
            "autotuned": tuning,
            "gpu_launches": int(launches)}
@@ -513,7 +523,7 @@ def run_serving(args, torch, E):
            "lanes": args.serving_lanes, "order": args.serving_order,
            "substeps_per_launch": args.serving_substeps,
            "max_avg_density_error": max(d[2]["error_average"] for d in done),
-           "requests_above_0.1%": int(sum(d[2]["error_average"] > 0.001 for d in done))}
+           "requests_above_0.1%": int(sum(d[2]["error_average"] > TOL_0_1 for d in done))}
     # the same requests one at a time, bounded in time
     t0 = time.perf_counter()
     served = 0
