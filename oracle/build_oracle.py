@@ -8,8 +8,8 @@
    Built only where ``/root/reference`` exists; the built file is git-ignored
    but travels with the working tree.
 
-3. ``oracle/libfp64_oracle.so`` — the FP64 GPU oracle of the DFSPH_P
-   sub-step (``oracle/fp64/dfsph_fp64.cu``), which states the error of the
+3. ``oracle/libfp64_oracle.so`` — the FP64 GPU oracle of the five solvers'
+   sub-steps (``oracle/fp64/dfsph_fp64.cu``), which states the error of the
    FP32 results; used by tests only.
 
 The first two are compiled ``-O2 -ffp-contract=off`` (IEEE single-precision

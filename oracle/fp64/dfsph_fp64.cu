@@ -1,5 +1,5 @@
-// FP64 GPU oracle of the DFSPH_P and IISPH sub-steps: test infrastructure
-// only.
+// FP64 GPU oracle of the DFSPH_P, IISPH, IISPH_AP, IISPH_PSEUDO_AP and
+// PCISPH sub-steps: test infrastructure only.
 //
 // The same formulas and neighbour-list order as the reference's sph_common
 // and dfsph_p code (cubic spline W/GradW, emerald/sph_common/kernels.h:12-64;
@@ -9,7 +9,13 @@
 // pressures, emerald/sph2d_box/dfsph_p_ops.cpp:19-126; the sub-step order of
 // emerald/sph2d_box/dfsph_p.cpp:325-373; the IISPH coefficients, pressure
 // iteration and sub-step order of emerald/sph2d_box/iisph_ops.cpp:20-425
-// and emerald/sph2d_box/iisph.cpp:23-151), evaluated in double. It states the
+// and emerald/sph2d_box/iisph.cpp:23-151; the AP diagonal and Jacobi step of
+// emerald/sph2d_box/iisph_ap_ops.cpp:19-194 and iisph_pseudo_ap_ops.cpp:19-343
+// with the sub-step orders of iisph_ap.cpp:44-189 and
+// iisph_pseudo_ap.cpp:64-194; the PCISPH predictor-corrector passes of
+// emerald/sph2d_box/pcisph_ops.cpp:18-178 and pcisph.cpp:36-164, with the
+// lists' distances and kernels recomputed at the predicted positions,
+// neighborhoods_from_state.cpp:103-128), evaluated in double. It states the
 // error of the FP32 results: the caller passes each sub-step's dt and the
 // iteration counts the FP32 run took, so the two runs differ only in
 // arithmetic precision.
@@ -46,6 +52,9 @@ struct Sim {
     // IISPH: diagonal terms, pressures (current and next), sum_j dij pj
     double2 *dii = nullptr, *sdp = nullptr;
     double *aii = nullptr, *pres = nullptr, *pres_next = nullptr;
+    // PCISPH: velocity after external forces, predicted velocity and
+    // position, pressure force; AP: pressure accelerations (displacements)
+    double2 *vext = nullptr, *vstar = nullptr, *xstar = nullptr, *fpres = nullptr, *acc = nullptr;
     // neighbour lists, slot-major: entry k of particle i at k * n + i
     int *fcnt = nullptr, *scnt = nullptr, *fidx = nullptr, *sidx = nullptr;
     double *fw = nullptr, *sw = nullptr;
@@ -430,6 +439,297 @@ __global__ void k_positions(Sim s, double dt) {
     s.x[i].y += dt * s.v[i].y;
 }
 
+// ------------------------------------------------------- IISPH_AP / PSEUDO_AP
+
+// integrate_velocities_in_place with the gravity force (dynamics.cpp:24-37).
+__global__ void k_external(Sim s, double dt) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const denom = s.p.rho0 * s.p.fluid_volume;
+    s.v[i].y += dt * (-(s.p.mass * s.p.gravity)) / denom;
+}
+
+// iisph_ap_density_stars_and_diagonals (iisph_ap_ops.cpp:19-90) and its
+// pseudo form (iisph_pseudo_ap_ops.cpp:19-117, without the dt^2): diagonal
+// -dt^2 (|sum m gradW|^2 + m_i sum_f m |gradW|^2) / rho^2 and
+// rho* = rho + dt * divergence; the boundary is at rest.
+__global__ void k_ap_diag(Sim s, double dt, int pseudo) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const rho0 = s.p.rho0;
+    double const fmass = rho0 * s.p.fluid_volume;
+    int const cf = s.fcnt[i];
+    int const cs = s.scnt[i];
+    double const rho = s.rho[i];
+    if (!(cf + cs)) {
+        s.rho_star[i] = rho;
+        s.aii[i] = 0.0;
+        return;
+    }
+    double2 const vi = s.v[i];
+    double2 sum = make_double2(0.0, 0.0);
+    double sdot = 0.0, div = 0.0;
+    for (int k = 0; k < cf; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        double2 const g = s.fgw[e];
+        double2 const vj = s.v[s.fidx[e]];
+        sum.x += fmass * g.x;
+        sum.y += fmass * g.y;
+        sdot += fmass * (g.x * g.x + g.y * g.y);
+        div += fmass * ((vi.x - vj.x) * g.x + (vi.y - vj.y) * g.y);
+    }
+    for (int k = 0; k < cs; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        double2 const g = s.sgw[e];
+        double const m = s.vols[s.sidx[e]] * rho0;
+        sum.x += m * g.x;
+        sum.y += m * g.y;
+        div += m * (vi.x * g.x + vi.y * g.y);
+    }
+    double const denom = rho * rho;
+    double numer = -(sum.x * sum.x + sum.y * sum.y + fmass * sdot);
+    if (!pseudo) numer *= dt * dt;
+    s.aii[i] = denom != 0.0 ? numer / denom : 0.0;
+    s.rho_star[i] = rho + dt * div;
+}
+
+// compute_pressure_accelerations (pressure.cpp:83-178) of the current
+// pressures; under PSEUDO_AP the same sum gives the displacements
+// (iisph_pseudo_ap_ops.cpp:119-224).
+__global__ void k_ap_accel(Sim s) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const rho0 = s.p.rho0;
+    double const fmass = rho0 * s.p.fluid_volume;
+    double const qi = q_of(s.pres[i], s.rho[i]);
+    double2 a = make_double2(0.0, 0.0);
+    int const cf = s.fcnt[i];
+    for (int k = 0; k < cf; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        int const j = s.fidx[e];
+        double const f = -fmass * (qi + q_of(s.pres[j], s.rho[j]));
+        a.x += f * s.fgw[e].x;
+        a.y += f * s.fgw[e].y;
+    }
+    int const cs = s.scnt[i];
+    for (int k = 0; k < cs; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        double const f = -(rho0 * s.vols[s.sidx[e]]) * qi;
+        a.x += f * s.sgw[e].x;
+        a.y += f * s.sgw[e].y;
+    }
+    s.acc[i] = a;
+}
+
+// One relaxed Jacobi step p <- max(0, p + omega (s - A p) / diag)
+// (iisph_ap_ops.cpp:92-194, iisph_pseudo_ap_ops.cpp:226-323).
+__global__ void k_ap_iterate(Sim s, double dt, double omega, int pseudo) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const rho0 = s.p.rho0;
+    double const fmass = rho0 * s.p.fluid_volume;
+    int const cf = s.fcnt[i];
+    int const cs = s.scnt[i];
+    double const diag = s.aii[i];
+    if ((!cf && !cs) || (pseudo && diag == 0.0)) {
+        s.pres[i] = 0.0;
+        return;
+    }
+    double2 const ai = s.acc[i];
+    double api = 0.0;
+    for (int k = 0; k < cf; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        double2 const aj = s.acc[s.fidx[e]];
+        api += fmass * ((ai.x - aj.x) * s.fgw[e].x + (ai.y - aj.y) * s.fgw[e].y);
+    }
+    for (int k = 0; k < cs; ++k) {
+        size_t const e = size_t(k) * s.n + i;
+        api += (rho0 * s.vols[s.sidx[e]]) * (ai.x * s.sgw[e].x + ai.y * s.sgw[e].y);
+    }
+    if (!pseudo) api *= dt * dt;
+    double const source = rho0 - s.rho_star[i];
+    double p = s.pres[i] + (diag != 0.0 ? omega * (source - api) / diag : 0.0);
+    s.pres[i] = p < 0.0 ? 0.0 : p;
+}
+
+// integrate_velocities_and_positions_in_place (dynamics.cpp:53-63), or the
+// PSEUDO_AP update x += dt v* + dx, v = v* + dx / dt
+// (iisph_pseudo_ap_ops.cpp:325-343).
+__global__ void k_ap_finish(Sim s, double dt, int pseudo) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double2 const a = s.acc[i];
+    double2 v = s.v[i];
+    double2 x = s.x[i];
+    if (!pseudo) {
+        v.x += dt * a.x;
+        v.y += dt * a.y;
+        x.x += dt * v.x;
+        x.y += dt * v.y;
+    } else {
+        x.x += dt * v.x + a.x;
+        x.y += dt * v.y + a.y;
+        if (dt != 0.0) {
+            v.x += a.x / dt;
+            v.y += a.y / dt;
+        }
+    }
+    s.v[i] = v;
+    s.x[i] = x;
+}
+
+// ---------------------------------------------------------------- PCISPH
+
+// Velocity after the external force, v_ext = v + (dt / m) F_gravity
+// (pcisph.cpp:36-80), and zero pressures.
+__global__ void k_pc_init(Sim s, double dt) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const m = s.p.mass;
+    double2 v = s.v[i];
+    v.y += (dt / m) * (-(m * s.p.gravity));
+    s.vext[i] = v;
+    s.pres[i] = 0.0;
+    s.fpres[i] = make_double2(0.0, 0.0);
+}
+
+// Predicted velocity and position of one pass (pcisph.cpp:82-110).
+__global__ void k_pc_predict(Sim s, double dt, int pass) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const mult = dt / s.p.mass;
+    double2 v = s.vext[i];
+    if (pass > 0) {
+        v.x += mult * s.fpres[i].x;
+        v.y += mult * s.fpres[i].y;
+    }
+    s.vstar[i] = v;
+    s.xstar[i] = make_double2(s.x[i].x + dt * v.x, s.x[i].y + dt * v.y);
+}
+
+// The fixed lists' kernels at the predicted positions
+// (compute_neighbor_distances_and_vectors_to, neighborhood.cpp:154-176, then
+// the kernels of neighborhood.cpp:178-210).
+__global__ void k_pc_kernels(Sim s) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const h = s.p.support;
+    double2 const xi = s.xstar[i];
+    for (int set = 0; set < 2; ++set) {
+        int const c = set ? s.scnt[i] : s.fcnt[i];
+        int const* idx = set ? s.sidx : s.fidx;
+        double2 const* other = set ? s.xs : s.xstar;
+        double* w = set ? s.sw : s.fw;
+        double2* gw = set ? s.sgw : s.fgw;
+        for (int k = 0; k < c; ++k) {
+            size_t const e = size_t(k) * s.n + i;
+            double2 const xj = other[idx[e]];
+            double const vx = xj.x - xi.x, vy = xj.y - xi.y;
+            double const d = sqrt(vx * vx + vy * vy);
+            w[e] = kernel_w(d, h);
+            double2 g = make_double2(0.0, 0.0);
+            if (d > 0.0) {
+                double const dw = kernel_dw(d, h);
+                g = make_double2(-vx / d * dw, -vy / d * dw);
+            }
+            gw[e] = g;
+        }
+    }
+}
+
+// pcisph_compute_densities, pcisph_accumulate_density_from_solids and
+// pcisph_update_pressures (pcisph_ops.cpp:18-76).
+__global__ void k_pc_density(Sim s, double denom) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const m = s.p.mass;
+    double const rho0 = s.p.rho0;
+    double ws = kernel_w(0.0, s.p.support);
+    int const cf = s.fcnt[i];
+    for (int k = 0; k < cf; ++k) ws += s.fw[size_t(k) * s.n + i];
+    double rho = m * ws;
+    int const cs = s.scnt[i];
+    if (cs) {
+        double vf = 0.0;
+        for (int k = 0; k < cs; ++k) {
+            size_t const e = size_t(k) * s.n + i;
+            vf += s.vols[s.sidx[e]] * s.sw[e];
+        }
+        rho += rho0 * vf;
+    }
+    s.rho[i] = rho;
+    double const err = rho - rho0;
+    s.pres[i] += (err > 0.0 ? err : 0.0) / denom;
+}
+
+// pcisph_accumulate_pressure_forces with the artificial viscosity
+// (alpha = viscosity, beta = 2, N2 = 0.01 h^2) and
+// pcisph_accumulate_pressure_forces_from_solids (pcisph_ops.cpp:78-178).
+__global__ void k_pc_forces(Sim s, double viscosity) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const m = s.p.mass;
+    double const rho0 = s.p.rho0;
+    double const H = s.p.support;
+    double const N2 = 0.01 * H * H;
+    double const rho = s.rho[i];
+    double const pors = s.pres[i] / (rho * rho);
+    double2 f = make_double2(0.0, 0.0);
+    int const cf = s.fcnt[i];
+    if (cf) {
+        double2 const xi = s.xstar[i];
+        double2 const vi = s.vstar[i];
+        double2 pf = make_double2(0.0, 0.0);
+        for (int k = 0; k < cf; ++k) {
+            size_t const e = size_t(k) * s.n + i;
+            int const j = s.fidx[e];
+            double2 const g = s.fgw[e];
+            double const rj = s.rho[j];
+            double const c = pors + s.pres[j] / (rj * rj);
+            pf.x += c * g.x;
+            pf.y += c * g.y;
+            double const tx = s.xstar[j].x - xi.x, ty = s.xstar[j].y - xi.y;
+            double const dvr = tx * (s.vstar[j].x - vi.x) + ty * (s.vstar[j].y - vi.y);
+            if (dvr < 0.0) {
+                double const dist = sqrt(tx * tx + ty * ty);
+                double const mu = H * dvr / (dist + N2);
+                double const den = (rho + rj) / 2.0;
+                double const visc = ((-1.0 * viscosity * mu) + (2.0 * mu * mu)) / den;
+                pf.x += visc * g.x;
+                pf.y += visc * g.y;
+            }
+        }
+        f.x += -(m * m) * pf.x;
+        f.y += -(m * m) * pf.y;
+    }
+    int const cs = s.scnt[i];
+    if (cs) {
+        double2 vg = make_double2(0.0, 0.0);
+        for (int k = 0; k < cs; ++k) {
+            size_t const e = size_t(k) * s.n + i;
+            double const vol = s.vols[s.sidx[e]];
+            vg.x += vol * s.sgw[e].x;
+            vg.y += vol * s.sgw[e].y;
+        }
+        f.x += -m * rho0 * pors * vg.x;
+        f.y += -m * rho0 * pors * vg.y;
+    }
+    s.fpres[i] = f;
+}
+
+// v = v_ext + (dt / m) F_pressure, x += dt v (pcisph.cpp:150-164).
+__global__ void k_pc_final(Sim s, double dt) {
+    size_t const i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= s.n) return;
+    double const mult = dt / s.p.mass;
+    double2 v = s.vext[i];
+    v.x += mult * s.fpres[i].x;
+    v.y += mult * s.fpres[i].y;
+    s.v[i] = v;
+    s.x[i].x += dt * v.x;
+    s.x[i].y += dt * v.y;
+}
+
 template <class T>
 T* dalloc(size_t count) {
     void* p = nullptr;
@@ -481,6 +781,11 @@ int fp64_create(fp64_params const* p, double const* solid_xy, double const* soli
     s->aii = dalloc<double>(n);
     s->pres = dalloc<double>(n);
     s->pres_next = dalloc<double>(n);
+    s->vext = dalloc<double2>(n);
+    s->vstar = dalloc<double2>(n);
+    s->xstar = dalloc<double2>(n);
+    s->fpres = dalloc<double2>(n);
+    s->acc = dalloc<double2>(n);
     s->fcnt = dalloc<int>(n);
     s->scnt = dalloc<int>(n);
     s->fidx = dalloc<int>(E);
@@ -494,7 +799,7 @@ int fp64_create(fp64_params const* p, double const* solid_xy, double const* soli
     s->fvals = dalloc<int>(n);
     s->svals = dalloc<int>(ns);
     if (!s->sgw || !s->svals || !s->fvals || !s->dii || !s->sdp || !s->aii || !s->pres ||
-        !s->pres_next) {
+        !s->pres_next || !s->vext || !s->vstar || !s->xstar || !s->fpres || !s->acc) {
         fp64_destroy(s);
         return 12;
     }
@@ -519,7 +824,7 @@ int fp64_destroy(void* h) {
                     s->kdens, s->qdiv, s->qdens, s->rho_star, s->div, s->fcnt,  s->scnt,
                     s->fidx, s->sidx, s->fw,    s->sw,    s->fgw,   s->sgw,   s->fkeys,
                     s->skeys, s->fvals, s->svals, s->dii, s->sdp, s->aii, s->pres,
-                    s->pres_next};
+                    s->pres_next, s->vext, s->vstar, s->xstar, s->fpres, s->acc};
     for (void* p : ptrs) cudaFree(p);
     delete s;
     return 0;
@@ -573,6 +878,53 @@ int fp64_sub_step_iisph(void* h, double dt, int iters, double omega) {
     k_iisph_q<<<grid(n), 128>>>(s);
     k_apply<<<grid(n), 128>>>(s, s.qdens, dt, 0);
     k_positions<<<grid(n), 128>>>(s, dt);
+    cudaError_t const e = cudaDeviceSynchronize();
+    return e == cudaSuccess ? 0 : 1000;
+}
+
+// One IISPH_AP (pseudo 0) or IISPH_PSEUDO_AP (pseudo 1) sub-step of length dt
+// running `iters` Jacobi iterations with relaxation omega.
+int fp64_sub_step_ap(void* h, double dt, int iters, double omega, int pseudo) {
+    Sim& s = *static_cast<Sim*>(h);
+    size_t const n = s.n;
+    double const cell = 2.0 * s.p.support;
+    sort_cells(s.x, n, cell, s.fkeys, s.fvals);
+    k_neighbors<<<grid(n), 128>>>(s, s.x, n, s.fkeys, s.fvals, true, s.fcnt, s.fidx, s.fw, s.fgw);
+    k_neighbors<<<grid(n), 128>>>(s, s.xs, s.ns, s.skeys, s.svals, false, s.scnt, s.sidx, s.sw,
+                                  s.sgw);
+    k_density_alpha<<<grid(n), 128>>>(s, 0);
+    k_external<<<grid(n), 128>>>(s, dt);
+    k_ap_diag<<<grid(n), 128>>>(s, dt, pseudo);
+    cudaMemset(s.pres, 0, 8 * n);
+    for (int it = 0; it < iters; ++it) {
+        k_ap_accel<<<grid(n), 128>>>(s);
+        k_ap_iterate<<<grid(n), 128>>>(s, dt, omega, pseudo);
+    }
+    k_ap_accel<<<grid(n), 128>>>(s);
+    k_ap_finish<<<grid(n), 128>>>(s, dt, pseudo);
+    cudaError_t const e = cudaDeviceSynchronize();
+    return e == cudaSuccess ? 0 : 1000;
+}
+
+// One PCISPH sub-step of length dt running `passes` predictor-corrector
+// passes, with the PCISPH viscosity and the pressure-correction denominator
+// of Simulation_config.
+int fp64_sub_step_pcisph(void* h, double dt, int passes, double viscosity, double denom) {
+    Sim& s = *static_cast<Sim*>(h);
+    size_t const n = s.n;
+    double const cell = 2.0 * s.p.support;
+    sort_cells(s.x, n, cell, s.fkeys, s.fvals);
+    k_neighbors<<<grid(n), 128>>>(s, s.x, n, s.fkeys, s.fvals, true, s.fcnt, s.fidx, s.fw, s.fgw);
+    k_neighbors<<<grid(n), 128>>>(s, s.xs, s.ns, s.skeys, s.svals, false, s.scnt, s.sidx, s.sw,
+                                  s.sgw);
+    k_pc_init<<<grid(n), 128>>>(s, dt);
+    for (int pass = 0; pass < passes; ++pass) {
+        k_pc_predict<<<grid(n), 128>>>(s, dt, pass);
+        k_pc_kernels<<<grid(n), 128>>>(s);
+        k_pc_density<<<grid(n), 128>>>(s, denom);
+        k_pc_forces<<<grid(n), 128>>>(s, viscosity);
+    }
+    k_pc_final<<<grid(n), 128>>>(s, dt);
     cudaError_t const e = cudaDeviceSynchronize();
     return e == cudaSuccess ? 0 : 1000;
 }

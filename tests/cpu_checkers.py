@@ -485,6 +485,10 @@ class FP64Oracle:
         lib.fp64_sub_step.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int]
         lib.fp64_sub_step_iisph.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double]
+        lib.fp64_sub_step_ap.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_int]
+        lib.fp64_sub_step_pcisph.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                             ctypes.c_double]
         lib.fp64_get.argtypes = [vp, ctypes.c_char_p, vp]
         self.lib = lib
 
@@ -516,6 +520,15 @@ class FP64Sim:
 
     def sub_step_iisph(self, dt, iters, omega):
         rc = self.o.lib.fp64_sub_step_iisph(self.h, float(dt), int(iters), float(omega))
+        assert rc == 0, rc
+
+    def sub_step_ap(self, dt, iters, omega, pseudo):
+        rc = self.o.lib.fp64_sub_step_ap(self.h, float(dt), int(iters), float(omega), int(pseudo))
+        assert rc == 0, rc
+
+    def sub_step_pcisph(self, dt, passes, viscosity, denom):
+        rc = self.o.lib.fp64_sub_step_pcisph(self.h, float(dt), int(passes), float(viscosity),
+                                             float(denom))
         assert rc == 0, rc
 
     def get(self, name):

@@ -1,9 +1,10 @@
-"""Error of the FP32 DFSPH_P and IISPH results against the FP64 GPU oracle.
+"""Error of the FP32 results of every solver against the FP64 GPU oracle.
 
-The FP32 run (the CUDA path, in either precision mode) advances CFL-adaptive
-sub-steps; the FP64 oracle repeats each sub-step with the same dt, frame
-boundaries and iteration counts (and, for IISPH, the same relaxation omega),
-so the two differ only in arithmetic precision. Reported per checkpoint: per-particle density error (relative,
+The FP32 run (the CUDA path, in either precision mode) advances its
+sub-steps (CFL-adaptive, or PCISPH's fixed ones); the FP64 oracle repeats
+each sub-step with the same dt, frame boundaries and iteration counts (and
+the same relaxation omega, viscosity and PCISPH denominator), so the two
+differ only in arithmetic precision. Reported per checkpoint: per-particle density error (relative,
 L_inf and RMS), position error (in units of the particle spacing, max and
 RMS) and the kinetic-energy difference."""
 import numpy as np
@@ -29,9 +30,10 @@ def iisph_scene(E, n_side, precision, seed=1):
 
 
 def compare(E, n_side, steps, checkpoints, precision, seed=1, offset=0.0, method="dfsph_p"):
-    """Rows of error statistics at the given sub-steps of `method` ("dfsph_p"
-    or "iisph"). `offset` moves the whole scene (fluid and walls) by
-    (offset, offset) metres, rounded to float, before either run starts."""
+    """Rows of error statistics at the given sub-steps of `method` ("dfsph_p",
+    "iisph", "iisph_ap", "iisph_pseudo_ap" or "pcisph"). `offset` moves the
+    whole scene (fluid and walls) by (offset, offset) metres, rounded to
+    float, before either run starts."""
     make = dfsph_scene if method == "dfsph_p" else iisph_scene
     scene = make(E, n_side, precision, seed)
     p = scene.params
@@ -48,12 +50,17 @@ def compare(E, n_side, steps, checkpoints, precision, seed=1, offset=0.0, method
     for step in range(1, steps + 1):
         new_frame = sim.time() % tps == 0
         st = sim.advance(method, 1)
+        dt = float(np.float32(st["dt"]))
         if method == "dfsph_p":
-            ref.sub_step(float(np.float32(st["dt"])), new_frame, st["divergence_iterations"],
-                         st["pressure_iterations"])
+            ref.sub_step(dt, new_frame, st["divergence_iterations"], st["pressure_iterations"])
+        elif method == "iisph":
+            ref.sub_step_iisph(dt, st["pressure_iterations"], float(p.iisph_omega))
+        elif method in ("iisph_ap", "iisph_pseudo_ap"):
+            ref.sub_step_ap(dt, st["pressure_iterations"], float(p.iisph_omega),
+                            method == "iisph_pseudo_ap")
         else:
-            ref.sub_step_iisph(float(np.float32(st["dt"])), st["pressure_iterations"],
-                               float(p.iisph_omega))
+            ref.sub_step_pcisph(dt, st["pressure_iterations"], float(p.viscosity),
+                                float(p.pressure_correction_denom))
         if step in checkpoints:
             x, v = sim.state()
             rho = sim.array("densities").astype(np.float64)
@@ -65,13 +72,16 @@ def compare(E, n_side, steps, checkpoints, precision, seed=1, offset=0.0, method
             ke = 0.5 * mass * float(np.sum(v.astype(np.float64) ** 2))
             ke64 = 0.5 * mass * float(np.sum(v64 ** 2))
             extra = {}
-            if method == "iisph":
+            if method in ("iisph", "iisph_ap", "iisph_pseudo_ap"):
                 pr = sim.array("pressures").astype(np.float64)
                 pr64 = ref.get("pressures")
                 scale = float(np.abs(pr64).max()) or 1.0
                 extra = dict(pressure_linf=float(np.abs(pr - pr64).max()) / scale,
                              pressure_rms=float(np.sqrt(np.mean((pr - pr64) ** 2))) / scale)
+            vscale = float(np.abs(v64).max()) or 1.0
             rows.append(dict(step=step, density_linf=float(drel.max()),
+                             velocity_linf_rel=float(np.abs(v.astype(np.float64) - v64).max())
+                             / vscale,
                              density_rms=float(np.sqrt(np.mean(drel ** 2))),
                              position_max_dx=float(dpos.max()),
                              position_rms_dx=float(np.sqrt(np.mean(dpos ** 2))),

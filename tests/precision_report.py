@@ -1,5 +1,5 @@
-"""Prints the FP32-vs-FP64 error table of the DFSPH_P or IISPH path (both
-precision modes) as markdown; test infrastructure (it drives the FP64 oracle).
+"""Prints the FP32-vs-FP64 error table of one solver (both precision modes)
+as markdown; test infrastructure (it drives the FP64 oracle).
 
     python tests/precision_report.py --n-side 1024 --steps 1000 --at 1,10,1000
     python tests/precision_report.py --method iisph --n-side 256 --steps 100 --at 1,10,100
@@ -19,7 +19,8 @@ def main():
     ap.add_argument("--n-side", type=int, default=1024)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--at", default="1,10,1000")
-    ap.add_argument("--method", default="dfsph_p", choices=("dfsph_p", "iisph"))
+    ap.add_argument("--method", default="dfsph_p",
+                    choices=("dfsph_p", "iisph", "iisph_ap", "iisph_pseudo_ap", "pcisph"))
     args = ap.parse_args()
     import emerald_b200 as E
     from precision import compare

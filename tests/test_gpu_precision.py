@@ -1,4 +1,4 @@
-"""Precision modes of the DFSPH_P path against the FP64 GPU oracle.
+"""Precision modes of every solver against the FP64 GPU oracle.
 
 REFERENCE mode is the reference's FP32 arithmetic (bit-exact with it, see
 test_gpu_parity.py); COMPENSATED mode uses Kahan-compensated neighbour sums,
@@ -113,3 +113,35 @@ def test_compensated_positions_follow_every_method(E, method):
         float(np.sqrt(np.mean(d ** 2))), float(d.max())))
     assert np.all(np.isfinite(out[1]))
     assert float(np.sqrt(np.mean(d ** 2))) < 1e-3
+
+
+@pytest.mark.parametrize("method", ["iisph_ap", "iisph_pseudo_ap", "pcisph"])
+def test_fp64_oracle_first_step_every_solver(E, method):
+    """IISPH_AP, IISPH_PSEUDO_AP and PCISPH after one sub-step of a 48x48
+    block: densities within 1e-5 relative of double precision and velocities
+    within 1e-4 of the largest FP64 speed (AP: about 2e-5 measured), 1e-3 for
+    PCISPH (1.1e-4 measured: its artificial viscosity acts only on pairs
+    with v_ij . x_ij < 0, and for pairs near zero FP32 and FP64 take
+    different branches). A term missing from either side shows as 1e-2 or
+    more. Both precision modes."""
+    from precision import compare
+    vtol = 1e-3 if method == "pcisph" else 1e-4
+    for mode in (E.PRECISION_REFERENCE, E.PRECISION_COMPENSATED):
+        r = compare(E, 48, 1, {1}, mode, method=method)[0]
+        print(method, "mode", mode, r)
+        assert r["iterations"] >= 2, r
+        assert r["density_linf"] < 1e-5, r
+        assert r["velocity_linf_rel"] < vtol, r
+        if method != "pcisph":
+            assert r["pressure_linf"] < 1e-3, r
+
+
+@pytest.mark.parametrize("method", ["iisph_ap", "iisph_pseudo_ap", "pcisph"])
+def test_fp64_oracle_ten_steps_every_solver(E, method):
+    """Ten sub-steps of a 96x96 block: kinetic energy within 1% of the FP64
+    oracle and densities within 1e-3 relative, in reference mode."""
+    from precision import compare
+    r = compare(E, 96, 10, {10}, E.PRECISION_REFERENCE, method=method)[0]
+    print(method, "10 sub-steps", r)
+    assert r["energy_rel_diff"] < 1e-2, r
+    assert r["density_linf"] < 1e-3, r
