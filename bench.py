@@ -121,11 +121,15 @@ def traffic_from_profile(kernel):
     """DRAM bytes per launch of `kernel` (dram__bytes_read.sum +
     dram__bytes_write.sum from one ncu capture of this workload), as recorded
     in the committed summaries under profiles/ ("traffic_bytes_per_launch
-    k_<kernel> = N" lines); None when no capture covers the kernel."""
+    k_<kernel> = N" lines in the files named for this workload, e.g.
+    *.dfsph_262k.md); None when no capture of this workload covers the
+    kernel."""
     import glob
     import re
+    n = N_SIDE * N_SIDE
+    tag = "dfsph_%dm" % (n // 2 ** 20) if n % 2 ** 20 == 0 else "dfsph_%dk" % (n // 1000)
     pat = re.compile(r"^traffic_bytes_per_launch\s+k_%s\s*=\s*(\d+)" % re.escape(kernel))
-    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.%s.md" % tag))):
         for line in open(path):
             m = pat.match(line.strip())
             if m:
