@@ -288,8 +288,9 @@ __global__ void k_iter_check(Arena a, int nscenes, int kind, int* running,
 // neighbour value, then folds them into the sum in order. The loads of a
 // chunk are independent, so they are in flight together; the sum is the
 // same sequence of operations as a plain loop. The chunk of each kernel is
-// a launch-time choice among 1, 4 and 8 (Tuning, set by the autotuner);
-// defaults measured on B200 at 262,144 particles.
+// a launch-time choice among 1, 4 and 8 (Tuning, set by the autotuner).
+// These two are the chunks of callers that pass none (the IISPH final
+// velocity update); the engine's DFSPH launches pass their Tuning's.
 constexpr int kDivergenceChunk = 8;
 constexpr int kPressureChunk = 4;
 
