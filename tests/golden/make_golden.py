@@ -1,8 +1,8 @@
 """Regenerates the golden fixtures in tests/golden/ from the reference.
 
 Runs the unmodified emerald sources compiled against the project's shims
-(oracle/_ref/libemerald_ref.so, built by oracle/build_oracle.py from
-/root/reference) and stores small inputs and outputs as .npz files:
+(oracle/_ref/libemerald_ref.so, built by oracle/build_oracle.py from the
+reference's sources) and stores small inputs and outputs as .npz files:
 
 * uniform_7927.npz: the 7927-point fixture of the reference's own tests
   (emerald/sph_common/tests/test_neighborhood.cpp:18-31: std::mt19937_64{17272},

@@ -1,8 +1,8 @@
 """Regenerates the 1000-sub-step trace fixtures in tests/golden/ from the reference.
 
 Runs the unmodified emerald sources compiled against the project's shims
-(oracle/_ref/libemerald_ref.so, built by oracle/build_oracle.py from
-/root/reference) on the scene described in tests/traces.py and stores, for
+(oracle/_ref/libemerald_ref.so, built by oracle/build_oracle.py from the
+reference's sources) on the scene described in tests/traces.py and stores, for
 each solver, trace_<method>.npz: the per-sub-step density error (the
 reference's average metric, max and exact mean) and kinetic energy, and the
 SHA-256 of positions and velocities after sub-steps 1, 10, 100 and 1000.
