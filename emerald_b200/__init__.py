@@ -361,6 +361,7 @@ def kernel_launches():
 
 
 STATIC_MAX_POINTS = 65536
+MAX_NEIGHBORS = 64  # EMERALD_MAX_NEIGHBORS
 
 
 def neighbors_static(d_xy, n, support, d_counts, d_idx, d_w, d_gw, stride, stream=None):

@@ -91,6 +91,10 @@ void fill_stats(SceneState const& s, emerald_step_stats* out, int substeps) {
 
 }  // namespace
 
+namespace emerald {
+int set_last_error(int code, char const* msg) { return fail(code, msg); }
+}  // namespace emerald
+
 extern "C" {
 
 char const* emerald_last_error(void) { return t_error.c_str(); }

@@ -9,9 +9,7 @@
 // lists and scan scratch live in g_static_scratch below, sized for
 // EMERALD_STATIC_MAX_POINTS points (about 3.4 MB held by every device that
 // loads the library, until the process exits).
-#include <array>
 #include <cstdint>
-#include <mutex>
 
 #include "../../include/emerald_sph.h"
 #include "engine_types.cuh"
@@ -25,6 +23,11 @@ namespace {
 constexpr uint32_t kMaxPoints = EMERALD_STATIC_MAX_POINTS;
 constexpr uint32_t kTableLog2 = 17;  // 2^17 slots >= 2 * kMaxPoints
 constexpr uint32_t kTableSize = (1u << kTableLog2) + 1;
+// Linear probing over the whole table finds a free slot while one is left;
+// kMaxPoints points make at most kMaxPoints cells, under half the slots, so
+// the build never flags a full table.
+static_assert((1u << kTableLog2) >= 2u * kMaxPoints, "cell table must hold twice the points");
+static_assert(kMaxNeighbors == EMERALD_MAX_NEIGHBORS, "list slots differ from the header's");
 constexpr uint32_t kMaxTiles = kMaxPoints / kTile;
 constexpr uint32_t kScanWords = (kTableSize + 2047) / 2048 + 64;
 
@@ -72,12 +75,9 @@ __global__ void k_static_setup(Arena a, uint32_t n, float support, float reject_
     }
 }
 
-// Device address of g_static_scratch per device, resolved on the first call
-// made with that device current.
-std::mutex g_mutex;
-std::array<unsigned char*, 64> g_addr{};
-
 }  // namespace
+
+int set_last_error(int code, char const* msg);
 
 }  // namespace emerald
 
@@ -86,28 +86,35 @@ using namespace emerald;
 extern "C" int emerald_neighbors_static(void const* d_xy, uint32_t n, float support,
                                         uint8_t* d_counts, uint32_t* d_idx, float* d_w,
                                         void* d_gw, uint32_t stride, void* stream) {
-    if (n > kMaxPoints) return EMERALD_EINVAL;
-    if (!(support > 0.0f) || stride < n) return EMERALD_EINVAL;
+    if (n > kMaxPoints) {
+        return set_last_error(EMERALD_EINVAL, "more points than EMERALD_STATIC_MAX_POINTS");
+    }
+    if (!(support > 0.0f)) return set_last_error(EMERALD_EINVAL, "support must be positive");
+    if (stride < n) return set_last_error(EMERALD_EINVAL, "stride is smaller than n");
     if (n == 0) return EMERALD_OK;
-    if (!d_xy || !d_counts || !d_idx || !d_w || !d_gw) return EMERALD_EINVAL;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= int(g_addr.size())) {
+    if (!d_xy || !d_counts || !d_idx || !d_w || !d_gw) {
+        return set_last_error(EMERALD_EINVAL, "a device pointer is NULL");
+    }
+    // Positions and gradients are read and written as float2, index and
+    // kernel-value lists as 32-bit words.
+    if ((reinterpret_cast<uintptr_t>(d_xy) | reinterpret_cast<uintptr_t>(d_gw)) % 8 != 0) {
+        return set_last_error(EMERALD_EINVAL, "d_xy and d_gw must be 8-byte aligned");
+    }
+    if ((reinterpret_cast<uintptr_t>(d_idx) | reinterpret_cast<uintptr_t>(d_w)) % 4 != 0) {
+        return set_last_error(EMERALD_EINVAL, "d_idx and d_w must be 4-byte aligned");
+    }
+    // The array's device address, looked up on every call with the caller's
+    // device current: each device (and each context a device gets after
+    // cudaDeviceReset) has its own copy of g_static_scratch, and the host
+    // symbol itself is not a device address.
+    void* ptr = nullptr;
+    cudaError_t const e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+    if (e != cudaSuccess || !ptr) {
         cudaGetLastError();
-        return EMERALD_ECUDA;
+        return set_last_error(EMERALD_ECUDA, e != cudaSuccess ? cudaGetErrorString(e)
+                                                              : "no device address for the scratch");
     }
-    unsigned char* base = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_mutex);
-        if (!g_addr[dev]) {
-            void* ptr = nullptr;
-            if (cudaGetSymbolAddress(&ptr, g_static_scratch) != cudaSuccess || !ptr) {
-                cudaGetLastError();
-                return EMERALD_ECUDA;
-            }
-            g_addr[dev] = static_cast<unsigned char*>(ptr);
-        }
-        base = g_addr[dev];
-    }
+    unsigned char* const base = static_cast<unsigned char*>(ptr);
     cudaStream_t const st = static_cast<cudaStream_t>(stream);
     Arena a{};
     a.sp = reinterpret_cast<SceneParams const*>(base + kOffParams);
@@ -134,5 +141,7 @@ extern "C" int emerald_neighbors_static(void const* d_xy, uint32_t n, float supp
     // The table is cleared by the build itself (keys to empty, counts to zero).
     launch_build_cells(a, false, tiles, reinterpret_cast<uint32_t*>(base + kOffScan), st);
     launch_neighbors(a, tiles, false, true, st);
-    return cudaGetLastError() == cudaSuccess ? EMERALD_OK : EMERALD_ECUDA;
+    cudaError_t const le = cudaGetLastError();
+    if (le != cudaSuccess) return set_last_error(EMERALD_ECUDA, cudaGetErrorString(le));
+    return EMERALD_OK;
 }

@@ -31,6 +31,11 @@ extern "C" {
 #define EMERALD_ECUDA 1000
 #define EMERALD_ESOLVER 1001
 
+/* Neighbour slots per particle, NEIGHBORHOOD_MAX_COUNT
+ * (emerald/sph_common/neighborhood.h:38). Every list buffer of this API has
+ * this many slots per particle. */
+#define EMERALD_MAX_NEIGHBORS 64
+
 /* Solver methods, numbered as EZ_EXAMPLE_SIM::Method
  * (emerald/sph2d_box/simulation.h:25). */
 #define EMERALD_PCISPH 0
@@ -383,7 +388,7 @@ int emerald_server_get_stats(emerald_server* server, emerald_server_stats* out);
  * device memory. */
 
 /* Neighborhood_pointers (emerald/sph_common/neighborhood.h:126-133): counts
- * per particle and, per particle, NEIGHBORHOOD_MAX_COUNT = 64 entries of
+ * per particle and, per particle, EMERALD_MAX_NEIGHBORS = 64 entries of
  * each array, row-major (particle i's entry k at i * 64 + k). Members a call
  * does not read may be NULL; a NULL `counts` in a solid neighbourhood skips
  * the boundary pass. */
@@ -596,14 +601,21 @@ int emerald_iisph_pseudo_ap_integrate_velocities_and_positions_in_place(
  * the device. Builds the neighbour lists of n points (device float2
  * positions) against themselves, cell size 2*support with the grid at the
  * origin, exactly as the simulation's fluid build: counts[n] and, slot-major,
- * idx/w/gw[k*stride + i] for the k-th neighbour of point i (gw holds float2).
+ * idx/w/gw[k*stride + i] for the k-th neighbour of point i, k below
+ * EMERALD_MAX_NEIGHBORS. Size the outputs for that many slots whatever
+ * neighbour count you expect: d_idx and d_w hold EMERALD_MAX_NEIGHBORS *
+ * stride 32-bit words, d_gw EMERALD_MAX_NEIGHBORS * stride float2, and a
+ * dense point fills all 64 slots. d_xy and d_gw must be 8-byte aligned,
+ * d_idx and d_w 4-byte aligned (EMERALD_EINVAL otherwise).
  * Allocates nothing: its scratch is a static device array sized for
  * EMERALD_STATIC_MAX_POINTS points, held by every device that loads the
- * library until exit. n above that limit returns EMERALD_EINVAL. The first
- * call on each device resolves the array's device address with that device
- * current; make that first call before any stream capture. All calls share
- * the array, so calls whose work overlaps on the GPU race; order them on one
- * stream. Work is enqueued on `stream` (NULL: the legacy default stream). */
+ * library until exit. n above that limit returns EMERALD_EINVAL. Each call
+ * looks up the array's device address with the caller's device current
+ * (each device, and each new context after cudaDeviceReset, has its own
+ * copy); make the first call on a device before any stream capture. All
+ * calls share the array, so calls whose work overlaps on the GPU race; order
+ * them on one stream. Work is enqueued on `stream` (NULL: the legacy default
+ * stream). */
 #define EMERALD_STATIC_MAX_POINTS 65536
 int emerald_neighbors_static(void const* d_xy, uint32_t n, float support, uint8_t* d_counts,
                              uint32_t* d_idx, float* d_w, void* d_gw, uint32_t stride,

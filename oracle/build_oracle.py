@@ -3,10 +3,13 @@
 1. ``oracle/liboracle_sph.so`` — the project's own C restatement of the
    reference SPH path (``oracle/sph_oracle.c``).
 2. ``oracle/_ref/libemerald_ref.so`` — the UNMODIFIED emerald reference
-   sources, compiled in place from ``/root/reference`` against the
+   sources, compiled in place from the reference checkout against the
    project-written shims in ``oracle/ref_shim`` plus ``oracle/ref_harness.cpp``.
-   Built only where ``/root/reference`` exists; the built file is git-ignored
-   but travels with the working tree.
+   The checkout is the directory named by ``--reference DIR`` or the
+   ``EMERALD_REFERENCE_ROOT`` environment variable, else the build
+   container's read-only copy at ``/root/reference``. Built only where that
+   directory exists; the built file is git-ignored but travels with the
+   working tree.
 
 3. ``oracle/libfp64_oracle.so`` — the FP64 GPU oracle of the five solvers'
    sub-steps (``oracle/fp64/dfsph_fp64.cu``), which states the error of the
@@ -22,7 +25,23 @@ import sys
 from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = "/root/reference"
+DEFAULT_REF_ROOT = "/root/reference"
+
+
+def reference_root(argv=()):
+    """The reference checkout: ``--reference DIR`` in ``argv`` (this script's
+    command line), else ``EMERALD_REFERENCE_ROOT``, else the build
+    container's copy."""
+    argv = list(argv)
+    for k, a in enumerate(argv):
+        if a == "--reference" and k + 1 < len(argv):
+            return argv[k + 1]
+        if a.startswith("--reference="):
+            return a.split("=", 1)[1]
+    return os.environ.get("EMERALD_REFERENCE_ROOT") or DEFAULT_REF_ROOT
+
+
+REF_ROOT = reference_root()
 REF_OUT = os.path.join(HERE, "_ref")
 ORACLE_SO = os.path.join(HERE, "liboracle_sph.so")
 REF_SO = os.path.join(REF_OUT, "libemerald_ref.so")
@@ -114,6 +133,8 @@ def build_reference(force=False):
 
 
 def main():
+    global REF_ROOT
+    REF_ROOT = reference_root(sys.argv[1:])
     force = "--force" in sys.argv
     if os.path.exists(os.path.join(HERE, "sph_oracle.c")):
         print(build_oracle(force))

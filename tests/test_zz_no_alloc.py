@@ -63,10 +63,42 @@ def test_static_build_matches_simulation_on_two_calls():
             assert_bitwise(a, b, name)
 
 
+def test_static_build_at_the_size_limit():
+    """Exactly EMERALD_STATIC_MAX_POINTS points (a 256 x 256 block): the last
+    tile of the static arena and the fullest cell table it can hold."""
+    import torch
+
+    import emerald_b200 as E
+    scene = E.BlockScene(256, dx=F(1 / 512), seed=23)
+    assert len(scene.fluid) == E.STATIC_MAX_POINTS
+    want = reference_lists(E, scene)
+    got = static_lists(E, torch, scene.fluid, scene.support)
+    for name, a, b in zip(("counts", "indices", "W", "grad W"), got, want):
+        assert_bitwise(a, b, name)
+
+
+def call_static(E, xy, n, cnt, idx, w, gw, stride):
+    rc = E.lib.emerald_neighbors_static(ctypes.c_void_p(xy), n, 0.01, ctypes.c_void_p(cnt),
+                                        ctypes.c_void_p(idx), ctypes.c_void_p(w),
+                                        ctypes.c_void_p(gw), stride, None)
+    return rc, E.lib.emerald_last_error().decode()
+
+
 def test_static_build_rejects_oversize():
     import emerald_b200 as E
-    rc = E.lib.emerald_neighbors_static(ctypes.c_void_p(1), E.STATIC_MAX_POINTS + 1, 0.01,
-                                        ctypes.c_void_p(1), ctypes.c_void_p(1),
-                                        ctypes.c_void_p(1), ctypes.c_void_p(1),
-                                        E.STATIC_MAX_POINTS + 1, None)
-    assert rc == 22
+    n = E.STATIC_MAX_POINTS + 1
+    rc, msg = call_static(E, 256, n, 256, 256, 256, 256, n)
+    assert rc == 22 and "EMERALD_STATIC_MAX_POINTS" in msg
+
+
+def test_static_build_rejects_misaligned_buffers():
+    """float2 positions and gradients need 8-byte alignment, the 32-bit lists
+    4-byte; the call returns EMERALD_EINVAL before it enqueues anything (the
+    pointers here are never dereferenced)."""
+    import emerald_b200 as E
+    rc, msg = call_static(E, 260, 16, 256, 256, 256, 256, 16)
+    assert rc == 22 and "8-byte" in msg
+    rc, msg = call_static(E, 256, 16, 256, 256, 256, 260, 16)
+    assert rc == 22 and "8-byte" in msg
+    rc, msg = call_static(E, 256, 16, 256, 258, 256, 256, 16)
+    assert rc == 22 and "4-byte" in msg
