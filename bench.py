@@ -306,6 +306,7 @@ def run_gpu(args):
             "ms_per_step": round(max_ms / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "fluid_particles": n, "boundary_particles": n_s,
+                       "window": {"first_sub_step": args.warmup, "sub_steps": args.steps},
                        "neighbours_per_particle": round(nnz_f / n, 2),
                        "parallelism": "replicas" if world > 1 else "single scene",
                        "l2": "flushed between timed steps (256 MiB write)",
@@ -546,100 +547,98 @@ def run_serving(args, torch, E):
     return out
 
 
-def reference_sim(threads):
+def reference_scene(R):
+    """The single-scene workload built by the reference harness alone
+    (oracle/_ref: no code of this library is loaded): the reference's default
+    Parameters with the workload's overrides, the mt19937_64 block, the
+    boundary rows, the square-lattice mass from the reference's own kernels
+    and boundary volumes m / rho0. tests/test_bench_scene.py checks that it
+    equals the GPU arm's scene bit for bit."""
+    rp = R.default_params()
+    kw = scene_kwargs()
+    rp.update(support=np.float32(kw["dx"]), length=np.float32(1.0), seed=kw["seed"],
+              time_per_step_flicks=kw["time_per_step_flicks"], sub_steps=kw["sub_steps"],
+              dfsph_max_correction_iterations=kw["dfsph_max_correction_iterations"],
+              dfsph_divergence_error_average_threshold=kw[
+                  "dfsph_divergence_error_average_threshold"],
+              dfsph_density_error_average_threshold=kw["dfsph_density_error_average_threshold"])
+    mass, denom = R.lattice_config(rp, DX, np.float32(5e-4))
+    rp["mass_per_particle_override"] = mass
+    rp["pressure_correction_denom_override"] = denom
+    fluid = R.block_scene(N_SIDE, N_SIDE, DX, 0.0, 0.0, 0.01, kw["seed"])
+    solid = R.wall_scene(DX, 1.0, 3)
+    volumes = np.full(len(solid), np.float32(mass) / np.float32(rp["target_density"]),
+                      np.float32)
+    return rp, fluid, solid, volumes
+
+
+def reference_window(threads, skip, count, max_seconds):
+    """Times DFSPH_P sub-steps [skip, skip + count) of the workload from rest
+    on the reference's CPU code (oracle/_ref: emerald's sources with TBB
+    replaced by a std::thread pool of `threads` threads), through the
+    reference's own CFL-adaptive frame loop: the same sub-steps the GPU arm
+    times after `skip` warm-up sub-steps. Returns None when oracle/_ref is not
+    built, else (fluid count, sub-steps timed, seconds)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import emerald_b200 as E
     from cpu_checkers import Reference
     if not Reference.available:
-        return None, None, None
+        return None
     R = Reference()
     R.set_threads(threads)
-    scene = E.BlockScene(N_SIDE, **scene_kwargs())
-    rp = R.default_params()
-    p = scene.params.as_dict()
-    for k in rp:
-        if k in p:
-            rp[k] = p[k]
-    rp["mass_per_particle_override"] = p["mass_per_particle"]
-    rp["pressure_correction_denom_override"] = p["pressure_correction_denom"]
-    sim = R.sim(rp, scene.solid, scene.fluid, None, scene.solid_volumes)
-    return R, sim, scene
+    rp, fluid, solid, volumes = reference_scene(R)
+    sim = R.sim(rp, solid, fluid, None, volumes)
+    timed, seconds = sim.run_window("dfsph_p", skip, count, max_seconds)
+    return sim.n, timed, seconds
 
 
 def cpu_baseline(args, sample_seconds=15.0):
-    """The reference's own CPU code (oracle/_ref: emerald sources with TBB
-    replaced by a std::thread pool) on this host's cores: DFSPH frames of the
-    same scene from its initial state."""
+    """The reference's own CPU code on this host's cores over the start of
+    the GPU arm's timed window (the sub-steps after the same warm-up),
+    bounded to about `sample_seconds` of timed work."""
     threads = os.cpu_count() or 1
-    R, sim, scene = reference_sim(threads)
-    if sim is None:
+    r = reference_window(threads, args.warmup, args.steps, sample_seconds)
+    if r is None:
         return {"value": None, "unit": "particle-steps/s", "cores": threads,
                 "kind": "reference", "sample": "unavailable: oracle/_ref not built"}
-    import emerald_b200 as E
-    t0 = time.perf_counter()
-    frames = 0
-    while time.perf_counter() - t0 < sample_seconds and frames < 200:
-        sim.frame("dfsph_p")
-        frames += 1
-    elapsed = time.perf_counter() - t0
-    # The GPU path is bit-identical, so its frame statistics give the
-    # reference's sub-step count for the same frames (counted untimed).
-    gsim = E.Simulation.from_block_scene(scene)
-    substeps = sum(gsim.frame("dfsph_p")["sub_steps"] for _ in range(frames))
-    n = sim.n
-    return {"value": round(n * substeps / elapsed, 1), "unit": "particle-steps/s",
+    n, timed, seconds = r
+    return {"value": round(n * timed / seconds, 1), "unit": "particle-steps/s",
             "cores": threads, "kind": "reference",
-            "sample": "%d DFSPH frames (%d sub-steps) of the same scene from its initial state, "
-                      "%.1f s; TBB replaced by a std::thread pool of %d threads" % (
-                          frames, substeps, elapsed, threads)}
+            "sample": "DFSPH_P sub-steps %d-%d of the same scene from rest (the first %d of the "
+                      "timed window, after the same %d warm-up sub-steps), %.2f s; reference "
+                      "sources with TBB replaced by a std::thread pool of %d threads" % (
+                          args.warmup, args.warmup + timed - 1, timed, args.warmup, seconds,
+                          threads)}
 
 
 def run_reference(args):
+    """The reference arm: the reference's CPU implementation (oracle/_ref)
+    over the GPU arm's window, sub-steps [warmup, warmup + steps) of the same
+    scene from rest, on all host threads. Only rank 0 runs; no code of this
+    library is loaded."""
     world, rank, local = dist_env()
     if rank != 0:
         return None
     threads = os.cpu_count() or 1
-    R, sim, scene = reference_sim(threads)
-    if sim is None:
+    budget = 150.0
+    r = reference_window(threads, args.warmup, args.steps, budget)
+    if r is None:
         return {"impl": "reference", "unavailable": "oracle/_ref (reference compiled with shims) "
                 "is not built on this machine"}
-    import emerald_b200 as E
-    from cpu_checkers import Oracle
-    # One step = one CFL-adaptive DFSPH frame of the reference, as the GPU arm
-    # runs them. The reference's frame call does not report its sub-step
-    # count, so the C oracle (bit-identical to it) replays each frame untimed
-    # to count them. Bounded so the whole run ends within minutes.
-    O = Oracle()
-    O.set_threads(threads)
-    d = scene.params.as_dict()
-    cfg = E.config(scene.params)
-    op = {k: d[k] for k in d if k not in ("seed", "length")}
-    op.update(mass_per_particle=cfg["mass_per_particle"],
-              pressure_correction_denom=cfg["pressure_correction_denom"],
-              seconds_per_sub_step=cfg["seconds_per_sub_step"])
-    osim = O.sim(op, scene.solid, scene.solid_volumes, scene.fluid)
-    budget = 60.0
-    frames = 0
-    substeps = 0
-    elapsed = 0.0
-    for k in range(args.steps):
-        t0 = time.perf_counter()
-        sim.frame("dfsph_p")
-        elapsed += time.perf_counter() - t0
-        substeps += osim.frame("dfsph_p")
-        frames += 1
-        if elapsed > budget:
-            break
-    done = substeps
-    value = sim.n * substeps / elapsed
-    sample = ("%d of %d requested DFSPH frames (%d CFL-adaptive sub-steps) of the scene from its "
-              "initial state, %.1f s timed, %d host threads; sub-steps counted by the C oracle "
-              "untimed" % (frames, args.steps, substeps, elapsed, threads))
+    n, timed, seconds = r
+    value = n * timed / seconds
+    sample = ("DFSPH_P sub-steps %d-%d of the scene from rest through the reference's own "
+              "CFL-adaptive frame loop, after %d untimed warm-up sub-steps, %.2f s timed, %d host "
+              "threads%s" % (args.warmup, args.warmup + timed - 1, args.warmup, seconds, threads,
+                             "" if timed == args.steps else
+                             "; ended after %d of %d sub-steps at the %.0f s budget" % (
+                                 timed, args.steps, budget)))
     return {"impl": "reference", "metric": METRIC, "value": round(value, 1),
-            "unit": "particle-steps/s", "n_gpus": world, "steps": frames, "warmup": 0,
-            "ms_per_step": round(elapsed * 1000.0 / max(done, 1), 3), "higher_is_better": True,
+            "unit": "particle-steps/s", "n_gpus": world, "steps": timed, "warmup": args.warmup,
+            "ms_per_step": round(seconds * 1000.0 / max(timed, 1), 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "fluid_particles": sim.n},
+            "config": {"workload": WORKLOAD, "fluid_particles": n,
+                       "window": {"first_sub_step": args.warmup, "sub_steps": timed},
+                       "same_steps": timed == args.steps},
             "cpu_baseline": {"value": round(value, 1), "unit": "particle-steps/s",
                              "cores": threads, "kind": "reference", "sample": sample},
             "e2e": {"value": round(value, 1), "unit": "particle-steps/s",

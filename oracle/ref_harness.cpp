@@ -32,6 +32,8 @@
 
 #include <tbb/tbb_shim.h>
 
+#include <chrono>
+#include <cmath>
 #include <cstring>
 #include <random>
 #include <string>
@@ -112,6 +114,7 @@ struct Ref_sim {
     User_forces_function forces;
     User_colors_function colors;
     flicks time{0};
+    int64_t sub_steps_run = 0;  // sub-steps of ref_sim_run_window since creation
 };
 
 std::vector<V2f> to_v2f(float const* xy, size_t n) {
@@ -239,6 +242,58 @@ void ref_block_scene(uint32_t nx,
             ++k;
         }
     }
+}
+
+// The mass per particle and PCISPH denominator of a square lattice at
+// spacing dx: the sums of the Simulation_config constructor
+// (emerald/sph2d_box/config.cpp:16-132) taken over the lattice points
+// (i dx, j dx), |i|, |j| <= ceil(2 support / dx) + 1, about the origin (rows
+// j outer, columns i inner), with the reference's own kernels::W and GradW.
+// out: mass_per_particle, pressure_correction_denom (dt in place of
+// seconds_per_sub_step).
+void ref_lattice_config(ref_params const* p, float dx, float dt, float* out) {
+    float const h = p->support;
+    int const reach = static_cast<int>(std::ceil(2.0 * double(h) / double(dx))) + 1;
+    float muchness = 0.0f;
+    V2f gradw_sum{0.0f, 0.0f};
+    float gradw_dot_gradw_sum = 0.0f;
+    for (int j = -reach; j <= reach; ++j) {
+        for (int i = -reach; i <= reach; ++i) {
+            V2f const point{static_cast<float>(i) * dx, static_cast<float>(j) * dx};
+            V2f const delta_position = V2f{0.0f, 0.0f} - point;
+            float const w = kernels::W(delta_position.length(), h);
+            if (w > 0.0f) muchness += w;
+            V2f const gradw = kernels::GradW(delta_position, h);
+            gradw_sum += gradw;
+            gradw_dot_gradw_sum += gradw.dot(gradw);
+        }
+    }
+    out[0] = p->target_density / muchness;
+    float const beta = 2.0f * sqr(dt / muchness);
+    out[1] = beta * (gradw_sum.dot(gradw_sum) + gradw_dot_gradw_sum);
+}
+
+// Boundary rows of the synthetic dam-break tank [0, length]^2: `layers` rows
+// at spacing dx below the floor (x from -layers to n + layers - 1 cells) and
+// outside each side wall, row by row (floor, left, right), n = round(length /
+// dx). Returns the point count; xy may be NULL to count only.
+size_t ref_wall_scene(float dx, float length, int layers, float* xy) {
+    int const n = static_cast<int>(std::lround(double(length) / double(dx)));
+    size_t k = 0;
+    auto put = [&](float x, float y) {
+        if (xy) {
+            xy[2 * k] = x;
+            xy[2 * k + 1] = y;
+        }
+        ++k;
+    };
+    for (int l = 0; l < layers; ++l) {
+        float const off = (static_cast<float>(l) + 0.5f) * dx;
+        for (int i = -layers; i < n + layers; ++i) put((static_cast<float>(i) + 0.5f) * dx, -off);
+        for (int j = 0; j < n; ++j) put(-off, (static_cast<float>(j) + 0.5f) * dx);
+        for (int j = 0; j < n; ++j) put(length + off, (static_cast<float>(j) + 0.5f) * dx);
+    }
+    return k;
 }
 
 // n points with both coordinates drawn from
@@ -414,6 +469,64 @@ int ref_sim_frame(void* h, int method) {
     }
     sim->time += sim->config.params.time_per_step;
     return 0;
+}
+
+// Runs CFL-adaptive frames through the reference's own frame loop
+// (std_adaptive_time_step, emerald/sph2d_box/adaptive_time_step.h:35-122,
+// with each method's sub-step function, resize function, denominators and
+// CFL factor as its X_simulation_step passes them) and times a window of its
+// sub-steps: sub-steps are numbered from 0 since the simulation's creation;
+// those numbered [skip, skip + count) are timed one by one with a steady
+// clock, those after the window are not run (the frame loop finishes with
+// the state unchanged, so the state is that after skip + count sub-steps).
+// Once the timed seconds pass max_seconds (> 0) the window ends early.
+// Returns the number of sub-steps timed, -1 for PCISPH (no adaptive frames)
+// or an unknown method; *seconds receives their total time.
+int64_t ref_sim_run_window(void* h, int method, int64_t skip, int64_t count, double max_seconds,
+                           double* seconds) {
+    auto* sim = static_cast<Ref_sim*>(h);
+    int64_t end = skip + count;
+    int64_t timed = 0;
+    double total = 0.0;
+    using Sub = void (*)(float, float, Simulation_config const&, State&, Solid_state const&,
+                         Temp_data&, User_forces_function const&);
+    using Resize = void (*)(size_t, Temp_data&);
+    Sub sub = nullptr;
+    Resize resize = nullptr;
+    int min_denom = 60, max_denom = 4;
+    float cfl = 0.4f;
+    switch (method) {
+    case 1: sub = iisph_sub_step; resize = iisph_resize_temp_arrays; max_denom = 6; cfl = 0.2f; break;
+    case 2: sub = iisph_ap_sub_step; resize = iisph_ap_resize_temp_arrays; break;
+    case 3: sub = iisph_pseudo_ap_sub_step; resize = iisph_pseudo_ap_resize_temp_arrays; break;
+    case 4: sub = dfsph_p_sub_step; resize = dfsph_p_resize_and_init_temp_arrays; break;
+    default: return -1;
+    }
+    auto timed_sub = [&](float t, float dt, Simulation_config const& c, State& st,
+                         Solid_state const& solid, Temp_data& temp,
+                         User_forces_function const& forces) {
+        int64_t const k = sim->sub_steps_run;
+        if (k >= end) return;
+        ++sim->sub_steps_run;
+        if (k < skip) {
+            sub(t, dt, c, st, solid, temp, forces);
+            return;
+        }
+        auto const t0 = std::chrono::steady_clock::now();
+        sub(t, dt, c, st, solid, temp, forces);
+        total += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        ++timed;
+        if (max_seconds > 0.0 && total > max_seconds) end = sim->sub_steps_run;
+    };
+    while (sim->sub_steps_run < end) {
+        sim->state = std_adaptive_time_step(std::nullopt, resize, timed_sub, min_denom, max_denom,
+                                            cfl, sim->time, sim->config, std::move(sim->state),
+                                            sim->solid_state, sim->temp, sim->forces,
+                                            sim->colors);
+        sim->time += sim->config.params.time_per_step;
+    }
+    if (seconds) *seconds = total;
+    return timed;
 }
 
 void ref_sim_get_state(void* h, float* x, float* v) {

@@ -255,6 +255,12 @@ class Reference:
         L.ref_block_scene.argtypes = [ctypes.c_uint32, ctypes.c_uint32, c_f, c_f, c_f, c_f,
                                       c_u64, c_vp]
         L.ref_uniform_points.argtypes = [c_sz, c_u64, c_f, c_f, c_vp]
+        L.ref_lattice_config.argtypes = [ctypes.POINTER(RefParams), c_f, c_f, c_vp]
+        L.ref_wall_scene.restype = c_sz
+        L.ref_wall_scene.argtypes = [c_f, c_f, ctypes.c_int, c_vp]
+        L.ref_sim_run_window.restype = c_i64
+        L.ref_sim_run_window.argtypes = [c_vp, ctypes.c_int, c_i64, c_i64, ctypes.c_double,
+                                         ctypes.POINTER(ctypes.c_double)]
         L.ref_sim_create.restype = c_vp
         L.ref_sim_create.argtypes = [ctypes.POINTER(RefParams), c_vp, c_sz, c_vp, c_vp, c_sz]
         L.ref_sim_destroy.argtypes = [c_vp]
@@ -346,6 +352,19 @@ class Reference:
         self.L.ref_block_scene(nx, ny, dx, x0, y0, jitter, seed, ptr(xy))
         return xy
 
+    def lattice_config(self, params, dx, dt):
+        """(mass_per_particle, pressure_correction_denom) of a square lattice
+        at spacing dx, from the reference's kernels."""
+        out = np.zeros(2, np.float32)
+        self.L.ref_lattice_config(ctypes.byref(self._params(params)), dx, dt, ptr(out))
+        return out[0], out[1]
+
+    def wall_scene(self, dx, length=1.0, layers=3):
+        n = self.L.ref_wall_scene(dx, length, layers, None)
+        xy = np.zeros((n, 2), np.float32)
+        self.L.ref_wall_scene(dx, length, layers, ptr(xy))
+        return xy
+
     def uniform_points(self, n, seed, lo, hi):
         xy = np.zeros((n, 2), np.float32)
         self.L.ref_uniform_points(n, seed, lo, hi, ptr(xy))
@@ -407,6 +426,16 @@ class RefSim:
 
     def frame(self, method):
         assert self.lib.L.ref_sim_frame(self.h, METHODS.get(method, method)) == 0
+
+    def run_window(self, method, skip, count, max_seconds=0.0):
+        """Adaptive frames through the reference's frame loop; sub-steps
+        [skip, skip + count) since creation timed one by one (ended early once
+        max_seconds > 0 is passed). Returns (sub-steps timed, seconds)."""
+        sec = ctypes.c_double(0.0)
+        k = self.lib.L.ref_sim_run_window(self.h, METHODS.get(method, method), skip, count,
+                                          max_seconds, ctypes.byref(sec))
+        assert k >= 0
+        return int(k), sec.value
 
     def time(self):
         return self.lib.L.ref_sim_time(self.h)
