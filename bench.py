@@ -117,7 +117,7 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def traffic_from_profile(kernel):
+def traffic_from_profile(kernel, n=None):
     """DRAM bytes per launch of `kernel` (dram__bytes_read.sum +
     dram__bytes_write.sum from one ncu capture of this workload), as recorded
     in the committed summaries under profiles/ ("traffic_bytes_per_launch
@@ -126,7 +126,7 @@ def traffic_from_profile(kernel):
     kernel."""
     import glob
     import re
-    n = N_SIDE * N_SIDE
+    n = N_SIDE * N_SIDE if n is None else n
     tag = "dfsph_%dm" % (n // 2 ** 20) if n % 2 ** 20 == 0 else "dfsph_%dk" % (n // 1000)
     pat = re.compile(r"^traffic_bytes_per_launch\s+k_%s\s*=\s*(\d+)" % re.escape(kernel))
     for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.%s.md" % tag))):
@@ -163,6 +163,81 @@ def algorithmic_bytes(kernel, n, nnz_f, nnz_s, n_s):
         "neighbors_solid": 16.0 * nnz_s + n * (8 + 1) + 12.0 * n_s,
     }
     return table.get(kernel)
+
+
+def kernel_rooflines(times, n, nnz_f, nnz_s, n_s):
+    """Achieved algorithmic GB/s of every gather-sum kernel and of the
+    neighbour build, from their mean CUDA-event launch times, against the
+    HBM peak; the ncu DRAM traffic per launch where a committed capture of
+    this workload covers the kernel."""
+    peak, peak_kind = measured_peak()
+    out = {}
+    for name in GATHER_KERNELS + ("neighbors_fluid", "neighbors_solid"):
+        if name not in times:
+            continue
+        ms, launches = times[name]
+        per_s = ms / launches / 1000.0
+        alg = algorithmic_bytes(name, n, nnz_f, nnz_s, n_s)
+        ach = alg / per_s / 1e9
+        out[name] = {"avg_launch_us": round(per_s * 1e6, 2), "launches": launches,
+                     "algorithmic_bytes_per_launch": alg, "achieved": round(ach, 1),
+                     "frac": round(ach / peak, 4), "traffic": traffic_from_profile(name, n)}
+    return {"peak": peak, "unit": "GB/s", "peak_source": peak_kind, "kernels": out}
+
+
+def run_side1m(args, torch, E, flush):
+    """The north-star configuration: the DFSPH_P dam break at 1024 x 1024 =
+    1,048,576 fluid particles (dx = 1/2048, support = dx), the same warm-up
+    and sub-step window as the headline, L2 flushed between sub-steps, then a
+    pass with CUDA events around every kernel for the per-kernel rooflines
+    of the gather kernels."""
+    side = 1024
+    dx = np.float32(1.0 / (2 * side))
+    kw = scene_kwargs()
+    kw["dx"] = dx
+    scene = E.BlockScene(side, **kw)
+    sim = E.Simulation.from_block_scene(scene)
+    n = sim.n
+    for _ in range(args.warmup):
+        sim.advance("dfsph_p", 1, stats=False)
+    tuning = sim.autotune("dfsph_p")
+    steps = max(args.steps, 1)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    torch.cuda.synchronize()
+    for k in range(steps):
+        flush.zero_()
+        ev[k][0].record()
+        sim.advance("dfsph_p", 1, stats=False)
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    sim.enable_timing(True)
+    errs = []
+    for _ in range(max(3, min(steps, 50))):
+        flush.zero_()
+        errs.append(sim.advance("dfsph_p", 1)["error_average"])
+    times = sim.kernel_times()
+    sim.enable_timing(False)
+    counts_f = sim.neighbors(False)[0]
+    counts_s = sim.neighbors(True)[0]
+    nnz_f, nnz_s = float(counts_f.sum()), float(counts_s.sum())
+    roof = kernel_rooflines(times, n, nnz_f, nnz_s, sim.ns)
+    total = sum(v[0] for v in times.values())
+    sim.close()
+    return {"workload": "DFSPH_P dam break, 1024x1024=1048576 fluid particles, dx=1/2048, "
+                        "support=dx, 3 boundary rows, CFL dt<=5e-4 s, div tol 0.1%/s, density "
+                        "tol 0.05%, 100 correction iterations at most",
+            "window": {"first_sub_step": args.warmup, "sub_steps": steps},
+            "value": round(n * steps / (ms / 1000.0), 1), "unit": "particle-steps/s",
+            "ms_per_step": round(ms / steps, 4),
+            "neighbours_per_particle": round(nnz_f / n, 2),
+            "autotuned_chunks": tuning["chunks"], "autotuned_prefetch": tuning["prefetch"],
+            "max_avg_density_error": max(errs),
+            "gather_rooflines": roof,
+            "kernels": {k: {"ms_total": round(v[0], 3), "launches": v[1],
+                            "share": round(v[0] / total, 4)}
+                        for k, v in sorted(times.items(), key=lambda kv: -kv[1][0])[:12]}}
 
 
 def run_gpu(args):
@@ -326,6 +401,7 @@ def run_gpu(args):
                                    "of the per-particle errors is beside it"}},
             "roofline": roofline,
             "gather_roofline": gather_roofline,
+            "gather_rooflines": kernel_rooflines(times, n, nnz_f, nnz_s, n_s),
             "kernels": kernel_table,
             "e2e": {"value": round(e2e_value, 1), "unit": "particle-steps/s",
                     "h2d_bytes_per_step": int(2 * n * 8), "d2h_bytes_per_step": int(2 * n * 8),
@@ -340,6 +416,10 @@ def run_gpu(args):
         batched = run_batched(args, torch, E, rank, world, barrier)
         if rank == 0:
             result["batched"] = batched
+    if args.side1m and world == 1 and N_SIDE != 1024:
+        flush1 = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+        result["side1m"] = run_side1m(args, torch, E, flush1)
+        del flush1
     if args.serving_requests > 0 and world == 1:
         result["serving"] = run_serving(args, torch, E)
     if args.literal_steps > 0 and world == 1:
@@ -668,6 +748,8 @@ def main():
                     help="request loop queue order")
     ap.add_argument("--literal-steps", type=int, default=20,
                     help="PCISPH sub-steps of the scene at the literal support h = 2 dx (0: skip)")
+    ap.add_argument("--no-side1m", dest="side1m", action="store_false",
+                    help="skip the 1,048,576-particle north-star scene")
     ap.add_argument("--side", type=int, default=512,
                     help="fluid block side of the single-scene workload (side^2 particles)")
     args = ap.parse_args()

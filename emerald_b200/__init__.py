@@ -29,7 +29,11 @@ c_vp = ctypes.c_void_p
 
 
 class EmeraldError(RuntimeError):
-    pass
+    """A failed C-ABI call; `code` is its EMERALD_* status."""
+
+    def __init__(self, msg, code=None):
+        super().__init__(msg)
+        self.code = code
 
 
 class Params(ctypes.Structure):
@@ -79,7 +83,7 @@ class ServerStats(ctypes.Structure):
         ("step_ms_p50", c_f), ("step_ms_p99", c_f), ("request_ms_p50", c_f),
         ("request_ms_p99", c_f), ("queue_ms_p50", c_f), ("queue_ms_p99", c_f),
         ("fluid_capacity", c_sz), ("solid_capacity", c_sz), ("device_bytes", c_sz),
-        ("resident_peak", c_i32), ("status", c_i32),
+        ("resident_peak", c_i32), ("status", c_i32), ("cancelled", c_i64),
     ]
 
     def as_dict(self):
@@ -126,6 +130,29 @@ class Neighborhood(ctypes.Structure):
                 ("kernels", c_vp), ("kernel_gradients", c_vp)]
 
 
+class ForceTerm(ctypes.Structure):
+    """emerald_force_term: kind (FORCE_GRAVITY, FORCE_POLE, FORCE_DRAG) and
+    its arguments a, b, c."""
+    _fields_ = [("kind", c_i32), ("a", c_f), ("b", c_f), ("c", c_f)]
+
+
+FORCE_GRAVITY, FORCE_POLE, FORCE_DRAG = 1, 2, 3
+MAX_FORCE_TERMS = 4
+# emerald_forces_fn(user, count, time, dt, mass, radius, forces, positions, velocities)
+FORCES_FN = ctypes.CFUNCTYPE(None, c_vp, ctypes.c_size_t, c_f, c_f, c_f, c_f,
+                             ctypes.POINTER(c_f), ctypes.POINTER(c_f), ctypes.POINTER(c_f))
+
+
+def force_terms(terms):
+    """A ctypes array of emerald_force_term from (kind, a, b, c) tuples
+    (missing arguments are zero)."""
+    arr = (ForceTerm * max(len(terms), 1))()
+    for k, t in enumerate(terms):
+        t = tuple(t) + (0.0,) * (4 - len(t))
+        arr[k] = ForceTerm(int(t[0]), float(t[1]), float(t[2]), float(t[3]))
+    return arr
+
+
 EXPORTS = {
     "emerald_default_params": (c_i32, [ctypes.POINTER(Params)]),
     "emerald_config": (c_i32, [ctypes.POINTER(Params), c_vp]),
@@ -150,6 +177,10 @@ EXPORTS = {
     "emerald_sim_set_state": (c_i32, [c_vp, c_vp, c_vp]),
     "emerald_sim_get_solid": (c_i32, [c_vp, c_vp, c_vp]),
     "emerald_sim_set_solid": (c_i32, [c_vp, c_vp, c_vp, c_vp]),
+    "emerald_sim_set_forces": (c_i32, [c_vp, c_vp, c_i32]),
+    "emerald_sim_set_force_callback": (c_i32, [c_vp, FORCES_FN, c_vp]),
+    "emerald_sim_snapshot": (c_i32, [c_vp, c_vp, c_sz, ctypes.POINTER(c_sz)]),
+    "emerald_sim_restore": (c_i32, [c_vp, c_vp, c_sz]),
     "emerald_sim_get_array": (c_i32, [c_vp, ctypes.c_char_p, c_vp, ctypes.POINTER(c_i32)]),
     "emerald_sim_get_neighbors": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp]),
     "emerald_sim_get_sort": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
@@ -172,6 +203,7 @@ EXPORTS = {
     "emerald_batch_get_state": (c_i32, [c_vp, c_i32, c_vp, c_vp]),
     "emerald_batch_set_state": (c_i32, [c_vp, c_i32, c_vp, c_vp]),
     "emerald_batch_set_solid": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp]),
+    "emerald_batch_set_forces": (c_i32, [c_vp, c_i32, c_vp, c_i32]),
     "emerald_batch_free": (c_i32, [c_vp, ctypes.POINTER(c_sz), ctypes.POINTER(c_i32)]),
     "emerald_batch_set_stream": (c_i32, [c_vp, c_vp]),
     "emerald_batch_synchronize": (c_i32, [c_vp]),
@@ -183,6 +215,7 @@ EXPORTS = {
     "emerald_server_wait": (c_i32, [c_vp, c_i64, c_i32, c_vp, c_vp, ctypes.POINTER(StepStats),
                                     ctypes.POINTER(RequestTiming)]),
     "emerald_server_get_stats": (c_i32, [c_vp, ctypes.POINTER(ServerStats)]),
+    "emerald_server_cancel": (c_i32, [c_vp, c_i64]),
     "emerald_sim_autotune": (c_i32, [c_vp, c_i32, ctypes.POINTER(Tuning)]),
     "emerald_sim_set_tuning": (c_i32, [c_vp, ctypes.POINTER(Tuning)]),
     "emerald_batch_set_tuning": (c_i32, [c_vp, ctypes.POINTER(Tuning)]),
@@ -280,7 +313,7 @@ def _ptr(a):
 def _check(rc, what):
     if rc != 0:
         msg = lib.emerald_last_error()
-        raise EmeraldError("%s failed (%d): %s" % (what, rc, msg.decode() if msg else ""))
+        raise EmeraldError("%s failed (%d): %s" % (what, rc, msg.decode() if msg else ""), rc)
 
 
 def _f32(a, shape_tail=None):
@@ -487,6 +520,46 @@ class Simulation:
         volumes = None if volumes is None else np.ascontiguousarray(volumes, np.float32)
         _check(lib.emerald_sim_set_solid(self._h, _ptr(xy), _ptr(v), _ptr(volumes)), "set_solid")
 
+    def snapshot(self):
+        """The simulation's checkpoint (emerald_sim_snapshot) as bytes."""
+        size = c_sz()
+        _check(lib.emerald_sim_snapshot(self._h, None, 0, ctypes.byref(size)), "snapshot")
+        buf = ctypes.create_string_buffer(size.value)
+        _check(lib.emerald_sim_snapshot(self._h, buf, size.value, ctypes.byref(size)), "snapshot")
+        return buf.raw
+
+    def restore(self, data):
+        """Loads a checkpoint taken by snapshot() (emerald_sim_restore)."""
+        buf = ctypes.create_string_buffer(bytes(data), len(data))
+        _check(lib.emerald_sim_restore(self._h, buf, len(data)), "restore")
+
+    def set_forces(self, terms):
+        """Device force terms, (kind, a, b, c) tuples evaluated in order
+        (emerald_sim_set_forces); [] applies no external force."""
+        arr = force_terms(terms)
+        _check(lib.emerald_sim_set_forces(self._h, ctypes.cast(arr, c_vp), len(terms)),
+               "set_forces")
+
+    def set_force_callback(self, fn):
+        """A host force function called once per sub-step at the solver's
+        force point: fn(time, dt, mass, radius, forces, positions, velocities)
+        with (n, 2) float32 views, forces zeroed, to be filled in place. None
+        removes it."""
+        if fn is None:
+            self._force_cb = None
+            _check(lib.emerald_sim_set_force_callback(self._h, FORCES_FN(), None),
+                   "set_force_callback")
+            return
+        n = self.n
+
+        def trampoline(user, count, time, dt, mass, radius, f, x, v):
+            view = lambda p: np.ctypeslib.as_array(p, shape=(count, 2))
+            fn(time, dt, mass, radius, view(f), view(x), view(v))
+
+        self._force_cb = FORCES_FN(trampoline)
+        _check(lib.emerald_sim_set_force_callback(self._h, self._force_cb, None),
+               "set_force_callback")
+
     def solid(self):
         xy = np.zeros((self.ns, 2), np.float32)
         vol = np.zeros(self.ns, np.float32)
@@ -648,6 +721,12 @@ class Batch:
         _check(lib.emerald_batch_set_solid(self._h, sid, _ptr(xy), _ptr(v), _ptr(volumes)),
                "set_solid")
 
+    def set_forces(self, sid, terms):
+        """Device force terms of one scene (emerald_batch_set_forces)."""
+        arr = force_terms(terms)
+        _check(lib.emerald_batch_set_forces(self._h, sid, ctypes.cast(arr, c_vp), len(terms)),
+               "set_forces")
+
     def free(self):
         n = c_sz()
         k = c_i32()
@@ -683,6 +762,7 @@ class Server:
 
     ENOSPC = 28
     ETIMEOUT = 110
+    ECANCELED = 125
 
     def __init__(self, hbm_budget_bytes, method="dfsph_p", max_scenes=256,
                  max_substeps_per_launch=8, lanes=4, order="arrival"):
@@ -745,3 +825,8 @@ class Server:
         out = ServerStats()
         _check(lib.emerald_server_get_stats(self._h, ctypes.byref(out)), "server_stats")
         return out.as_dict()
+
+    def cancel(self, rid):
+        """Cancels a queued, resident or finished request; wait() then
+        raises EmeraldError with code ECANCELED for it."""
+        _check(lib.emerald_server_cancel(self._h, int(rid)), "emerald_server_cancel")

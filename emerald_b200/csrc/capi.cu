@@ -1,4 +1,5 @@
 // extern "C" entry points of include/emerald_sph.h over the Engine.
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -61,6 +62,53 @@ int guarded(F&& f) {
 
 bool valid_method(int32_t m) { return m >= 0 && m <= 4; }
 
+// An infinity or a NaN among n host floats (the reference would carry it
+// into every neighbour sum; emerald/util/assert.h has no check for it).
+int check_finite(float const* p, size_t n, char const* what) {
+    if (!p) return EMERALD_OK;
+    for (size_t k = 0; k < n; ++k) {
+        if (!std::isfinite(p[k])) {
+            return fail(EMERALD_EINVAL, std::string(what) + " holds a non-finite value at float " +
+                                          std::to_string(k));
+        }
+    }
+    return EMERALD_OK;
+}
+
+int check_particles(float const* fluid_xy, float const* fluid_v, size_t n_fluid,
+                    float const* solid_xy, float const* solid_volumes, size_t n_solid) {
+    if (int rc = check_finite(fluid_xy, 2 * n_fluid, "fluid positions")) return rc;
+    if (int rc = check_finite(fluid_v, 2 * n_fluid, "fluid velocities")) return rc;
+    if (int rc = check_finite(solid_xy, 2 * n_solid, "boundary positions")) return rc;
+    return check_finite(solid_volumes, n_solid, "boundary volumes");
+}
+
+int check_forces(emerald_force_term const* terms, int32_t count) {
+    if (count < 0 || count > EMERALD_MAX_FORCE_TERMS) {
+        return fail(EMERALD_EINVAL, "between 0 and EMERALD_MAX_FORCE_TERMS force terms");
+    }
+    if (count && !terms) return fail(EMERALD_EINVAL, "terms is NULL");
+    for (int32_t k = 0; k < count; ++k) {
+        emerald_force_term const& t = terms[k];
+        if (t.kind != EMERALD_FORCE_GRAVITY && t.kind != EMERALD_FORCE_POLE &&
+            t.kind != EMERALD_FORCE_DRAG) {
+            return fail(EMERALD_EINVAL, "unknown force term kind");
+        }
+        if (!std::isfinite(t.a) || !std::isfinite(t.b) || !std::isfinite(t.c)) {
+            return fail(EMERALD_EINVAL, "force term arguments must be finite");
+        }
+    }
+    return EMERALD_OK;
+}
+
+std::vector<ForceTerm> to_terms(emerald_force_term const* terms, int32_t count) {
+    std::vector<ForceTerm> out(size_t(count) + 1);
+    for (int32_t k = 0; k < count; ++k) {
+        out[k] = ForceTerm{terms[k].kind, terms[k].a, terms[k].b, terms[k].c};
+    }
+    return out;
+}
+
 int check_params(emerald_params const* p) {
     if (!p) return fail(EMERALD_EINVAL, "params is NULL");
     if (!(p->support > 0.0f)) return fail(EMERALD_EINVAL, "support must be positive");
@@ -69,6 +117,16 @@ int check_params(emerald_params const* p) {
     if (p->sub_steps <= 0) return fail(EMERALD_EINVAL, "sub_steps must be positive");
     if (p->precision != EMERALD_PRECISION_REFERENCE && p->precision != EMERALD_PRECISION_COMPENSATED) {
         return fail(EMERALD_EINVAL, "unknown precision mode");
+    }
+    float const values[] = {p->length, p->gravity, p->viscosity, p->iisph_error_average_threshold,
+                            p->iisph_error_max_threshold, p->iisph_omega,
+                            p->dfsph_density_error_average_threshold,
+                            p->dfsph_density_error_max_threshold,
+                            p->dfsph_divergence_error_average_threshold,
+                            p->dfsph_divergence_error_max_threshold, p->mass_per_particle,
+                            p->pressure_correction_denom, p->support, p->target_density};
+    for (float const v : values) {
+        if (!std::isfinite(v)) return fail(EMERALD_EINVAL, "a parameter is not finite");
     }
     return EMERALD_OK;
 }
@@ -166,6 +224,9 @@ int emerald_sim_create(emerald_params const* params,
         return fail(EMERALD_EINVAL, "particle arrays are NULL");
     }
     if (n_fluid > (1u << 30) || n_solid > (1u << 30)) return fail(EMERALD_EINVAL, "too many particles");
+    if (int rc = check_particles(fluid_xy, fluid_v, n_fluid, solid_xy, solid_volumes, n_solid)) {
+        return rc;
+    }
     return guarded([&] {
         int dev = 0;
         if (cudaGetDevice(&dev) != cudaSuccess) {
@@ -211,10 +272,9 @@ int emerald_sim_begin_frame(emerald_sim* sim, int32_t method) {
 
 int emerald_sim_sub_step(emerald_sim* sim, int32_t method, float t, float dt,
                          emerald_step_stats* stats) {
-    (void)t;
     if (!sim || !valid_method(method)) return fail(EMERALD_EINVAL, "bad arguments");
     return guarded([&] {
-        sim->engine.set_mode(sim->scene, kFixedDt, dt);
+        sim->engine.set_mode(sim->scene, kFixedDt, dt, t);
         sim->engine.substep(method);
         if (stats) fill_stats(sim->engine.scene_state(sim->scene), stats, 1);
         return EMERALD_OK;
@@ -253,7 +313,9 @@ int emerald_sim_advance_host(emerald_sim* sim, int32_t method, int32_t n_substep
                              emerald_step_stats* stats) {
     if (!sim || !valid_method(method) || n_substeps < 0) return fail(EMERALD_EINVAL, "bad arguments");
     return guarded([&] {
-        sim->engine.set_state(sim->scene, x_in, v_in, false);
+        if (!sim->engine.set_state(sim->scene, x_in, v_in, false)) {
+            return fail(EMERALD_EINVAL, "non-finite positions or velocities (state unchanged)");
+        }
         sim->engine.set_mode(sim->scene, kFrame, 0.0f);
         for (int k = 0; k < n_substeps; ++k) sim->engine.substep(method);
         sim->engine.get_state(sim->scene, x_out, v_out, true);
@@ -289,7 +351,9 @@ int emerald_sim_get_state(emerald_sim* sim, float* x, float* v) {
 int emerald_sim_set_state(emerald_sim* sim, float const* x, float const* v) {
     if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
     return guarded([&] {
-        sim->engine.set_state(sim->scene, x, v);
+        if (!sim->engine.set_state(sim->scene, x, v)) {
+            return fail(EMERALD_EINVAL, "non-finite positions or velocities (state unchanged)");
+        }
         return EMERALD_OK;
     });
 }
@@ -305,8 +369,53 @@ int emerald_sim_get_solid(emerald_sim* sim, float* xy, float* volumes) {
 int emerald_sim_set_solid(emerald_sim* sim, float const* solid_xy, float const* solid_v,
                           float const* solid_volumes) {
     if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    size_t const ns = sim->engine.solid_count(sim->scene);
+    if (int rc = check_particles(nullptr, nullptr, 0, solid_xy, solid_volumes, ns)) return rc;
+    if (int rc = check_finite(solid_v, 2 * ns, "boundary velocities")) return rc;
     return guarded([&] {
         sim->engine.set_solid(sim->scene, solid_xy, solid_v, solid_volumes);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_snapshot(emerald_sim* sim, void* buffer, size_t capacity, size_t* size) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    return guarded([&] {
+        size_t const need = sim->engine.snapshot_size(sim->scene);
+        if (size) *size = need;
+        if (!buffer) return EMERALD_OK;
+        if (capacity < need) return fail(EMERALD_ENOSPC, "snapshot buffer too small");
+        sim->engine.snapshot(sim->scene, buffer);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_restore(emerald_sim* sim, void const* buffer, size_t size) {
+    if (!sim || !buffer) return fail(EMERALD_EINVAL, "bad arguments");
+    return guarded([&] {
+        try {
+            sim->engine.restore(sim->scene, buffer, size);
+        } catch (std::invalid_argument const& e) {
+            return fail(EMERALD_EINVAL, e.what());
+        }
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_set_forces(emerald_sim* sim, emerald_force_term const* terms, int32_t count) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    if (int rc = check_forces(terms, count)) return rc;
+    return guarded([&] {
+        std::vector<ForceTerm> const t = to_terms(terms, count);
+        sim->engine.set_forces(sim->scene, t.data(), count);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_sim_set_force_callback(emerald_sim* sim, emerald_forces_fn fn, void* user) {
+    if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
+    return guarded([&] {
+        sim->engine.set_force_callback(sim->scene, fn, user);
         return EMERALD_OK;
     });
 }
@@ -383,6 +492,9 @@ int emerald_batch_add_scene(emerald_batch* batch, emerald_params const* params,
     if ((n_fluid && !fluid_xy) || (n_solid && !solid_xy)) {
         return fail(EMERALD_EINVAL, "particle arrays are NULL");
     }
+    if (int rc = check_particles(fluid_xy, fluid_v, n_fluid, solid_xy, solid_volumes, n_solid)) {
+        return rc;
+    }
     return guarded([&] {
         SceneSpec spec;
         spec.params = *params;
@@ -445,7 +557,9 @@ int emerald_batch_get_state(emerald_batch* batch, int32_t scene, float* x, float
 int emerald_batch_set_state(emerald_batch* batch, int32_t scene, float const* x, float const* v) {
     if (!batch || !batch->engine.scene_used(scene)) return fail(EMERALD_EINVAL, "bad scene");
     return guarded([&] {
-        batch->engine.set_state(scene, x, v);
+        if (!batch->engine.set_state(scene, x, v)) {
+            return fail(EMERALD_EINVAL, "non-finite positions or velocities (state unchanged)");
+        }
         return EMERALD_OK;
     });
 }
@@ -453,8 +567,22 @@ int emerald_batch_set_state(emerald_batch* batch, int32_t scene, float const* x,
 int emerald_batch_set_solid(emerald_batch* batch, int32_t scene, float const* solid_xy,
                             float const* solid_v, float const* solid_volumes) {
     if (!batch || !batch->engine.scene_used(scene)) return fail(EMERALD_EINVAL, "bad scene");
+    size_t const ns = batch->engine.solid_count(scene);
+    if (int rc = check_particles(nullptr, nullptr, 0, solid_xy, solid_volumes, ns)) return rc;
+    if (int rc = check_finite(solid_v, 2 * ns, "boundary velocities")) return rc;
     return guarded([&] {
         batch->engine.set_solid(scene, solid_xy, solid_v, solid_volumes);
+        return EMERALD_OK;
+    });
+}
+
+int emerald_batch_set_forces(emerald_batch* batch, int32_t scene, emerald_force_term const* terms,
+                             int32_t count) {
+    if (!batch || !batch->engine.scene_used(scene)) return fail(EMERALD_EINVAL, "bad scene");
+    if (int rc = check_forces(terms, count)) return rc;
+    return guarded([&] {
+        std::vector<ForceTerm> const t = to_terms(terms, count);
+        batch->engine.set_forces(scene, t.data(), count);
         return EMERALD_OK;
     });
 }
@@ -598,6 +726,9 @@ int emerald_server_submit(emerald_server* server, emerald_params const* params,
         n_solid > (size_t(1) << 30)) {
         return fail(EMERALD_EINVAL, "bad particle arrays");
     }
+    if (int rc = check_particles(fluid_xy, fluid_v, n_fluid, solid_xy, solid_volumes, n_solid)) {
+        return rc;
+    }
     return guarded([&] {
         std::unique_ptr<ServerRequest> r(new ServerRequest);
         r->params = *params;
@@ -622,8 +753,18 @@ int emerald_server_wait(emerald_server* server, int64_t request, int32_t timeout
         int const rc = server->server.wait(request, timeout_ms, x, v, stats, timing);
         if (rc == EMERALD_ETIMEOUT) return fail(rc, "request not done yet");
         if (rc == EMERALD_ENOTFOUND) return fail(rc, "unknown request");
+        if (rc == EMERALD_ECANCELED) return fail(rc, "request was cancelled");
         if (rc != EMERALD_OK) return fail(rc, "request failed");
         return EMERALD_OK;
+    });
+}
+
+int emerald_server_cancel(emerald_server* server, int64_t request) {
+    if (!server) return fail(EMERALD_EINVAL, "server is NULL");
+    return guarded([&] {
+        int const rc = server->server.cancel(request);
+        if (rc == EMERALD_ENOTFOUND) return fail(rc, "unknown request");
+        return rc;
     });
 }
 

@@ -109,7 +109,7 @@ size_t Engine::footprint(uint32_t fluid_capacity, uint32_t solid_capacity, int m
     auto r = [](size_t b) { return std::max<size_t>(b, 16); };
     size_t bytes = r(sizeof(SceneParams) * M) + r(sizeof(SceneState) * M) + r(4 * (N / kTile)) +
                    r(4 * (S / kTile));
-    bytes += 12 * r(8 * N) + 18 * r(4 * N) + 2 * r(N);   // per-particle state and scratch
+    bytes += 13 * r(8 * N) + 18 * r(4 * N) + 2 * r(N);   // per-particle state and scratch
     bytes += 2 * r(16 * N);                                 // double positions and their staging
     bytes += r(4 * (N / 4 + 64 * M));                       // boundary-proximity maps
     bytes += r(sort_scratch_bytes(uint32_t(N)));            // storage-order sort
@@ -119,7 +119,8 @@ size_t Engine::footprint(uint32_t fluid_capacity, uint32_t solid_capacity, int m
     bytes += r(8 * stab) + r(4 * (stab + 1)) + r(4 * stab); // solid cell table
     size_t const scan_words = std::max(scan_scratch_words(uint32_t(ftab)),
                                        scan_scratch_words(uint32_t(stab))) + 64;
-    bytes += r(4 * scan_words) + r(sizeof(int)) + r(sizeof(unsigned long long) * 4);
+    bytes += r(4 * scan_words) + r(sizeof(int)) + r(sizeof(uint32_t)) +
+             r(sizeof(unsigned long long) * 4);
     return bytes;
 }
 
@@ -180,6 +181,7 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
     a_.xstar = static_cast<float2*>(dev(8 * N));
     a_.vstar = static_cast<float2*>(dev(8 * N));
     a_.fp = static_cast<float2*>(dev(8 * N));
+    a_.ext_f = static_cast<float2*>(dev(8 * N));
     a_.oid = static_cast<uint32_t*>(dev(4 * N));
     a_.slot_of = static_cast<uint32_t*>(dev(4 * N));
     a_.tx = static_cast<float2*>(dev(8 * N));
@@ -224,6 +226,7 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
       std::max(scan_scratch_words(a_.ftab_total), scan_scratch_words(a_.stab_total)) + 64;
     d_scan_ = static_cast<uint32_t*>(dev(4ull * scan_words));
     d_running_ = static_cast<int*>(dev(sizeof(int)));
+    d_flag_ = static_cast<uint32_t*>(dev(sizeof(uint32_t)));
     d_loop_iters_ = static_cast<unsigned long long*>(dev(sizeof(unsigned long long) * 4));
     a_.loop_iterations = d_loop_iters_;
     cudaMemset(d_loop_iters_, 0, sizeof(unsigned long long) * 4);
@@ -234,7 +237,8 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
         cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming) != cudaSuccess) {
         throw std::runtime_error("stream creation failed");
     }
-    if (cudaMallocHost(reinterpret_cast<void**>(&h_running_), sizeof(int)) != cudaSuccess) {
+    if (cudaMallocHost(reinterpret_cast<void**>(&h_running_), sizeof(int)) != cudaSuccess ||
+        cudaMallocHost(reinterpret_cast<void**>(&h_flag_), sizeof(uint32_t)) != cudaSuccess) {
         throw std::bad_alloc();
     }
     cudaMemset(d_ss_, 0, sizeof(SceneState) * max_scenes_);
@@ -272,6 +276,7 @@ Engine::~Engine() {
     if (sort_buf_) cudaFree(sort_buf_);
     for (void* p : allocations_) cudaFree(p);
     if (h_running_) cudaFreeHost(h_running_);
+    if (h_flag_) cudaFreeHost(h_flag_);
 }
 
 template <class F>
@@ -445,6 +450,12 @@ int Engine::add_scene(SceneSpec const& spec) {
     P.sort_base = 0;
     P.reject_l2 = reject_threshold(P.cell_size);
     P.precision = ep.precision;
+    // default_gravity_forces(params.gravity) (emerald/sph2d_box/forces.cpp:73-83)
+    P.force_count = 1;
+    P.force_array = 0;
+    P.force_terms[0] = ForceTerm{kForceGravity, ep.gravity, 0.0f, 0.0f};
+    P.fixed_t = 0.0f;
+    sc.draw_radius = cfg.draw_radius;
     build_near_map(sc, spec.solid_xy, spec.n_solid);
     scenes_[id] = sc;
 
@@ -617,13 +628,69 @@ void Engine::set_active(int id, bool active) {
     cudaStreamSynchronize(st_);
 }
 
-void Engine::set_mode(int id, int32_t mode, float fixed_dt) {
+void Engine::set_mode(int id, int32_t mode, float fixed_dt, float fixed_t) {
     if (!scene_used(id)) return;
     SceneParams& P = scenes_[id].p;
-    if (P.mode != mode || P.fixed_dt != fixed_dt) {
+    if (P.mode != mode || P.fixed_dt != fixed_dt ||
+        (mode == kFixedDt && !(P.fixed_t == fixed_t))) {
         P.mode = mode;
         P.fixed_dt = fixed_dt;
+        P.fixed_t = fixed_t;
         upload_params(id);
+    }
+}
+
+void Engine::set_forces(int id, ForceTerm const* terms, int count) {
+    if (!scene_used(id)) throw std::invalid_argument("no such scene");
+    if (count < 0 || count > kMaxForceTerms || (count && !terms)) {
+        throw std::invalid_argument("between 0 and 4 force terms");
+    }
+    SceneParams& P = scenes_[id].p;
+    P.force_count = count;
+    for (int k = 0; k < kMaxForceTerms; ++k) {
+        P.force_terms[k] = k < count ? terms[k] : ForceTerm{0, 0.0f, 0.0f, 0.0f};
+    }
+    upload_params(id);
+}
+
+void Engine::set_force_callback(int id, ForceCallback fn, void* user) {
+    if (!scene_used(id)) throw std::invalid_argument("no such scene");
+    Scene& sc = scenes_[id];
+    sc.force_fn = fn;
+    sc.force_user = user;
+    sc.p.force_array = fn ? 1 : 0;
+    upload_params(id);
+}
+
+bool Engine::has_force_callbacks() const {
+    for (auto const& sc : scenes_) {
+        if (sc.used && sc.active && sc.force_fn) return true;
+    }
+    return false;
+}
+
+// compute_all_external_forces with the scenes' host callbacks: the state at
+// this point of the sub-step goes to the host in original order, the
+// callback fills the zeroed forces, and they come back in storage order.
+// The time is the sub-step's, plus dt under DFSPH_P, whose force point
+// comes after the divergence solve (emerald/sph2d_box/dfsph_p.cpp:350).
+void Engine::host_forces(int32_t method) {
+    for (int id = 0; id < max_scenes_; ++id) {
+        Scene& sc = scenes_[id];
+        if (!sc.used || !sc.active || !sc.force_fn) continue;
+        uint32_t const b = sc.p.fluid_begin, n = sc.p.fluid_count;
+        SceneState const s = scene_state(id);
+        hx_.resize(2ull * n);
+        hv_.resize(2ull * n);
+        hf_.assign(2ull * n, 0.0f);
+        get_state(id, hx_.data(), hv_.data(), true);
+        float const time = method == kDfsph ? s.t + s.dt : s.t;
+        sc.force_fn(sc.force_user, n, time, s.dt, sc.p.mass, sc.draw_radius, hf_.data(),
+                    hx_.data(), hv_.data());
+        cudaMemcpyAsync(a_.tx + b, hf_.data(), 8ull * n, cudaMemcpyHostToDevice, st_);
+        launch_scatter_f2(a_, b, n, a_.tx + b, a_.ext_f, st_);
+        cudaStreamSynchronize(st_);
+        check("host forces");
     }
 }
 
@@ -799,11 +866,13 @@ void Engine::emit_substep(int32_t method, bool reorder) {
         launch("dfsph_density_alpha", [&] { launch_dfsph_density_alpha(a_, tiles, compensated_, st); });
         launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 0, compensated_, st, tuning_.apply); });
         run_loop(2, max_iterations(2), method);
+        if (!capturing_ && has_force_callbacks()) host_forces(method);
         launch("apply_pressures_ext", [&] { launch_apply_pressures(a_, tiles, 1, 1, 0, compensated_, st, tuning_.apply); });
         run_loop(1, max_iterations(1), method);
         launch("integrate_positions", [&] { launch_integrate_positions(a_, tiles, compensated_, st); });
         break;
     case kIisph:
+        if (!capturing_ && has_force_callbacks()) host_forces(method);
         launch("iisph_density_dii", [&] { launch_iisph_density_dii(a_, tiles, st); });
         launch("iisph_aii", [&] { launch_iisph_aii(a_, tiles, st); });
         run_loop(0, max_iterations(0), method);
@@ -813,6 +882,7 @@ void Engine::emit_substep(int32_t method, bool reorder) {
     case kIisphAp:
     case kIisphPseudoAp: {
         int const pseudo = method == kIisphPseudoAp ? 1 : 0;
+        if (!capturing_ && has_force_callbacks()) host_forces(method);
         launch("ap_density", [&] { launch_ap_density(a_, tiles, st); });
         launch("ap_diag", [&] { launch_ap_diag(a_, tiles, pseudo, st); });
         run_loop(0, max_iterations(0), method);
@@ -820,6 +890,7 @@ void Engine::emit_substep(int32_t method, bool reorder) {
         break;
     }
     case kPcisph:
+        if (!capturing_ && has_force_callbacks()) host_forces(method);
         launch("pc_init", [&] { launch_pc_init(a_, tiles, st); });
         run_loop(3, 6, method);
         launch("pc_final", [&] { launch_pc_final(a_, tiles, st); });
@@ -904,7 +975,7 @@ void Engine::substep(int32_t method) {
     }
     bool const reorder = reorder_every_ > 0 && (substeps_launched_ % reorder_every_) == 0;
     ++substeps_launched_;
-    if (use_graphs_ && !timing_) {
+    if (use_graphs_ && !timing_ && !has_force_callbacks()) {
         int const key = method * 2 + (reorder ? 1 : 0);
         auto it = graphs_.find(key);
         if (it == graphs_.end()) {
@@ -1090,20 +1161,144 @@ void Engine::get_state(int id, float* x, float* v, bool sync) {
     check("get_state");
 }
 
-void Engine::set_state(int id, float const* x, float const* v, bool sync) {
+bool Engine::set_state(int id, float const* x, float const* v, bool sync) {
     SceneParams const& P = scenes_[id].p;
     uint32_t const b = P.fluid_begin, n = P.fluid_count;
+    if (!x && !v) return true;
+    // the new values are staged and checked on the device before any of
+    // them replaces the scene's state
+    cudaMemsetAsync(d_flag_, 0, sizeof(uint32_t), st_);
     if (x) {
         cudaMemcpyAsync(a_.tx + b, x, 8ull * n, cudaMemcpyHostToDevice, st_);
-        launch_scatter_f2(a_, b, n, a_.tx + b, a_.x, st_);
-        launch_positions_to_double(a_, b, n, st_);
+        launch_flag_nonfinite(reinterpret_cast<float const*>(a_.tx + b), 2ull * n, d_flag_, st_);
     }
     if (v) {
         cudaMemcpyAsync(a_.tv + b, v, 8ull * n, cudaMemcpyHostToDevice, st_);
-        launch_scatter_f2(a_, b, n, a_.tv + b, a_.v, st_);
+        launch_flag_nonfinite(reinterpret_cast<float const*>(a_.tv + b), 2ull * n, d_flag_, st_);
     }
+    cudaMemcpyAsync(h_flag_, d_flag_, sizeof(uint32_t), cudaMemcpyDeviceToHost, st_);
+    cudaStreamSynchronize(st_);
+    check("set_state");
+    if (*h_flag_) return false;
+    if (x) {
+        launch_scatter_f2(a_, b, n, a_.tx + b, a_.x, st_);
+        launch_positions_to_double(a_, b, n, st_);
+    }
+    if (v) launch_scatter_f2(a_, b, n, a_.tv + b, a_.v, st_);
     if (sync) cudaStreamSynchronize(st_);
     check("set_state");
+    return true;
+}
+
+namespace {
+struct SnapshotHeader {
+    char magic[8];
+    uint32_t version;
+    uint32_t n_fluid, n_solid;
+    int32_t precision;
+    uint64_t bytes;
+};
+constexpr char kSnapshotMagic[8] = {'E', 'M', 'S', 'N', 'A', 'P', '0', '1'};
+
+size_t snapshot_bytes(uint32_t n, uint32_t ns, bool x64) {
+    return sizeof(SnapshotHeader) + sizeof(SceneState) + 16ull * n + 8ull * n +
+           (x64 ? 16ull * n : 0) + 20ull * ns;
+}
+}  // namespace
+
+size_t Engine::snapshot_size(int id) const {
+    SceneParams const& P = scenes_[id].p;
+    return snapshot_bytes(P.fluid_count, P.solid_count, P.precision != 0);
+}
+
+// Layout: header, SceneState, positions and velocities (float pairs), the
+// DFSPH divergence and density kappas, in compensated mode the FP64
+// positions (all in original particle order), then the boundary positions,
+// velocities and volumes.
+void Engine::snapshot(int id, void* out) {
+    SceneParams const& P = scenes_[id].p;
+    uint32_t const b = P.fluid_begin, n = P.fluid_count, ns = P.solid_count;
+    bool const x64 = P.precision != 0;
+    auto* p = static_cast<unsigned char*>(out);
+    SnapshotHeader h{};
+    std::memcpy(h.magic, kSnapshotMagic, 8);
+    h.version = 1;
+    h.n_fluid = n;
+    h.n_solid = ns;
+    h.precision = P.precision;
+    h.bytes = snapshot_bytes(n, ns, x64);
+    std::memcpy(p, &h, sizeof(h));
+    p += sizeof(h);
+    SceneState const s = scene_state(id);
+    std::memcpy(p, &s, sizeof(s));
+    p += sizeof(s);
+    get_state(id, reinterpret_cast<float*>(p), reinterpret_cast<float*>(p + 8ull * n), true);
+    p += 16ull * n;
+    launch_gather_f(a_, b, n, a_.kdiv, a_.tkdiv + b, st_);
+    cudaMemcpyAsync(p, a_.tkdiv + b, 4ull * n, cudaMemcpyDeviceToHost, st_);
+    launch_gather_f(a_, b, n, a_.kdens, a_.tkdens + b, st_);
+    cudaMemcpyAsync(p + 4ull * n, a_.tkdens + b, 4ull * n, cudaMemcpyDeviceToHost, st_);
+    p += 8ull * n;
+    if (x64) {
+        launch_gather_d2(a_, b, n, a_.x64, a_.tx64 + b, st_);
+        cudaMemcpyAsync(p, a_.tx64 + b, 16ull * n, cudaMemcpyDeviceToHost, st_);
+        p += 16ull * n;
+    }
+    cudaMemcpyAsync(p, a_.xs + P.solid_begin, 8ull * ns, cudaMemcpyDeviceToHost, st_);
+    cudaMemcpyAsync(p + 8ull * ns, a_.vs + P.solid_begin, 8ull * ns, cudaMemcpyDeviceToHost, st_);
+    cudaMemcpyAsync(p + 16ull * ns, a_.vols + P.solid_begin, 4ull * ns, cudaMemcpyDeviceToHost,
+                    st_);
+    cudaStreamSynchronize(st_);
+    check("snapshot");
+}
+
+void Engine::restore(int id, void const* data, size_t bytes) {
+    SceneParams const& P = scenes_[id].p;
+    uint32_t const b = P.fluid_begin, n = P.fluid_count, ns = P.solid_count;
+    bool const x64 = P.precision != 0;
+    auto const* p = static_cast<unsigned char const*>(data);
+    SnapshotHeader h{};
+    if (bytes < sizeof(h)) throw std::invalid_argument("snapshot too short");
+    std::memcpy(&h, p, sizeof(h));
+    if (std::memcmp(h.magic, kSnapshotMagic, 8) != 0 || h.version != 1) {
+        throw std::invalid_argument("not a snapshot of this library");
+    }
+    if (h.n_fluid != n || h.n_solid != ns || h.precision != P.precision) {
+        throw std::invalid_argument("snapshot of a scene with other particle counts or precision");
+    }
+    if (h.bytes != bytes || bytes != snapshot_bytes(n, ns, x64)) {
+        throw std::invalid_argument("snapshot size does not match");
+    }
+    p += sizeof(h);
+    SceneState s{};
+    std::memcpy(&s, p, sizeof(s));
+    p += sizeof(s);
+    float const* xv = reinterpret_cast<float const*>(p);
+    if (!set_state(id, xv, xv + 2ull * n, false)) {
+        throw std::invalid_argument("snapshot holds non-finite positions or velocities");
+    }
+    p += 16ull * n;
+    cudaMemcpyAsync(a_.tkdiv + b, p, 4ull * n, cudaMemcpyHostToDevice, st_);
+    launch_scatter_f(a_, b, n, a_.tkdiv + b, a_.kdiv, st_);
+    cudaMemcpyAsync(a_.tkdens + b, p + 4ull * n, 4ull * n, cudaMemcpyHostToDevice, st_);
+    launch_scatter_f(a_, b, n, a_.tkdens + b, a_.kdens, st_);
+    p += 8ull * n;
+    if (x64) {
+        cudaMemcpyAsync(a_.tx64 + b, p, 16ull * n, cudaMemcpyHostToDevice, st_);
+        launch_scatter_d2(a_, b, n, a_.tx64 + b, a_.x64, st_);
+        p += 16ull * n;
+    }
+    cudaStreamSynchronize(st_);
+    check("restore");
+    float const* sxy = reinterpret_cast<float const*>(p);
+    set_solid(id, sxy, sxy + 2ull * ns, sxy + 4ull * ns);
+    // the frame clock, counters and last statistics; the scene stays as
+    // active as it is now
+    int32_t const active = scenes_[id].active ? 1 : 0;
+    s.active = active;
+    cudaMemcpyAsync(d_ss_ + id, &s, sizeof(s), cudaMemcpyHostToDevice, st_);
+    cudaStreamSynchronize(st_);
+    check("restore");
 }
 
 void Engine::get_solid(int id, float* xy, float* volumes) {

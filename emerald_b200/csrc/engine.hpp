@@ -93,7 +93,26 @@ public:
     int add_scene(SceneSpec const& spec);
     void remove_scene(int id);
     void set_active(int id, bool active);
-    void set_mode(int id, int32_t mode, float fixed_dt);
+    // Frame mode, or fixed-dt mode with the caller's sub-step time t and dt.
+    void set_mode(int id, int32_t mode, float fixed_dt, float fixed_t = 0.0f);
+    // External forces of a scene (compute_all_external_forces,
+    // emerald/sph2d_box/forces.cpp:11-33): `count` terms (at most
+    // kMaxForceTerms; 0: none) evaluated on the device where the solver
+    // computes its forces. A new scene has one gravity term with the
+    // parameters' gravity, as default_gravity_forces gives.
+    void set_forces(int id, ForceTerm const* terms, int count);
+    // A host function standing for the reference's User_forces_function
+    // (emerald/sph2d_box/forces.h:13-21): once per sub-step, at the point of
+    // the sub-step where the solver computes its external forces, it gets
+    // the scene's positions and velocities at that point (original particle
+    // order), the sub-step's time and dt, the mass and draw radius, and
+    // fills the forces (zeroed first). Sub-steps of an engine with a
+    // callback run without graphs (the call needs the state on the host).
+    // NULL removes it; the force terms apply again.
+    using ForceCallback = void (*)(void* user, size_t count, float time, float dt, float mass,
+                                   float radius, float* forces, float const* positions,
+                                   float const* velocities);
+    void set_force_callback(int id, ForceCallback fn, void* user);
     bool scene_used(int id) const { return id >= 0 && id < (int)scenes_.size() && scenes_[id].used; }
 
     void set_stream(cudaStream_t st) { st_ = st; }
@@ -108,7 +127,19 @@ public:
     // sync = false leaves the copies queued on the engine's stream (the
     // caller synchronizes before it touches the host buffers).
     void get_state(int id, float* x, float* v, bool sync = true);
-    void set_state(int id, float const* x, float const* v, bool sync = true);
+    // Returns false, and leaves the scene as it was, when x or v holds an
+    // infinity or a NaN (checked on the device before anything is replaced;
+    // one stream synchronisation).
+    bool set_state(int id, float const* x, float const* v, bool sync = true);
+    // Checkpoint of one scene between sub-steps: its frame clock and
+    // counters (SceneState), positions, velocities and DFSPH kappas in
+    // original order, the FP64 positions of a compensated scene, and its
+    // boundary. restore() takes a snapshot of a scene with the same particle
+    // counts and precision mode; the sub-steps after it equal those after
+    // the snapshot was taken, bit for bit.
+    size_t snapshot_size(int id) const;
+    void snapshot(int id, void* out);
+    void restore(int id, void const* data, size_t bytes);
     void get_solid(int id, float* xy, float* volumes);
     // Replaces a scene's boundary particles between sub-steps (count kept):
     // positions (NULL keeps them; new ones rebuild the boundary cell tables
@@ -184,7 +215,14 @@ private:
         uint32_t ftab_size = 0, stab_size = 0;
         uint32_t near_words = 0;
         bool active = false;
+        float draw_radius = 0.0f;
+        ForceCallback force_fn = nullptr;
+        void* force_user = nullptr;
     };
+    bool has_force_callbacks() const;
+    // Calls the force callbacks of the active scenes and uploads their forces.
+    void host_forces(int32_t method);
+    std::vector<float> hx_, hv_, hf_;
 
     template <class F>
     void launch(char const* name, F&& f, int kernels = 1);
@@ -223,6 +261,8 @@ private:
     uint32_t* d_scan_ = nullptr;
     int* d_running_ = nullptr;
     int* h_running_ = nullptr;
+    uint32_t* d_flag_ = nullptr;
+    uint32_t* h_flag_ = nullptr;
     std::vector<Scene> scenes_;
     std::vector<int32_t> tile_scene_, stile_scene_;
     RangeAllocator fluid_tiles_, solid_tiles_, ftab_, stab_, near_words_;

@@ -31,6 +31,19 @@ enum StepMode : int { kFixedDt = 0, kFrame = 1 };
 // Error bits reported through SceneState::error.
 enum ErrorBits : int { kErrTableFull = 1, kErrNonFinite = 2 };
 
+// External force terms, the reference's force functions
+// (emerald/sph2d_box/forces.cpp): gravity (accumulate_gravity_forces,
+// :63-71, a = g), pole attraction with swirl
+// (accumulate_constant_pole_attraction_forces, :85-101, a = magnitude,
+// (b, c) = pole) and drag (accumulate_simple_drag_forces, :104-111,
+// a = magnitude, b = particle diameter). Numbered as EMERALD_FORCE_*.
+enum ForceKind : int32_t { kForceGravity = 1, kForcePole = 2, kForceDrag = 3 };
+constexpr int kMaxForceTerms = 4;
+struct ForceTerm {
+    int32_t kind;
+    float a, b, c;
+};
+
 // Constants of one scene (mirrors Parameters + Simulation_config,
 // emerald/sph2d_box/parameters.h:12-41, config.h:7-18).
 struct SceneParams {
@@ -61,6 +74,14 @@ struct SceneParams {
     // near_w == 0: no map (every particle searches).
     uint32_t near_begin, near_w, near_h;
     int32_t near_x0, near_y0;
+    // External forces where the solver computes them
+    // (compute_all_external_forces, emerald/sph2d_box/forces.cpp:11-33):
+    // zero, then each of the force_count terms in order; with force_array
+    // the host callback's forces in Arena::ext_f instead.
+    int32_t force_count;
+    int32_t force_array;
+    ForceTerm force_terms[kMaxForceTerms];
+    float fixed_t;  // the caller's sub-step time (fixed-dt mode)
 };
 
 // Mutable per-scene state, device resident.
@@ -117,6 +138,7 @@ struct Arena {
     float2* xstar;
     float2* vstar;
     float2* fp;     // PCISPH pressure forces
+    float2* ext_f;  // external forces from a host callback (storage order)
 
     // storage order: oid[slot] = original (scene-local) index of the particle
     // stored at `slot`; slot_of[fluid_begin + oid] = its slot. nullptr means

@@ -52,6 +52,14 @@ void launch_gather_f2(Arena const& a, uint32_t begin, uint32_t count, float2 con
                       cudaStream_t st);
 void launch_scatter_f2(Arena const& a, uint32_t begin, uint32_t count, float2 const* in, float2* dst,
                        cudaStream_t st);
+void launch_scatter_f(Arena const& a, uint32_t begin, uint32_t count, float const* in, float* dst,
+                      cudaStream_t st);
+void launch_gather_d2(Arena const& a, uint32_t begin, uint32_t count, double2 const* src,
+                      double2* out, cudaStream_t st);
+void launch_scatter_d2(Arena const& a, uint32_t begin, uint32_t count, double2 const* in,
+                       double2* dst, cudaStream_t st);
+// *flag |= 1 when p[0, n) holds an infinity or a NaN.
+void launch_flag_nonfinite(float const* p, size_t n, uint32_t* flag, cudaStream_t st);
 void launch_positions_to_double(Arena const& a, uint32_t begin, uint32_t count, cudaStream_t st);
 void launch_identity_order(Arena const& a, uint32_t begin, uint32_t count, cudaStream_t st);
 

@@ -92,6 +92,28 @@ __global__ void k_scatter_f2(Arena a, uint32_t begin, uint32_t count, float2 con
     uint32_t const k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < count) dst[a.slot_of[begin + k]] = in[k];
 }
+__global__ void k_scatter_f(Arena a, uint32_t begin, uint32_t count, float const* in, float* dst) {
+    uint32_t const k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) dst[a.slot_of[begin + k]] = in[k];
+}
+__global__ void k_gather_d2(Arena a, uint32_t begin, uint32_t count, double2 const* src,
+                            double2* out) {
+    uint32_t const k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) out[k] = src[a.slot_of[begin + k]];
+}
+__global__ void k_scatter_d2(Arena a, uint32_t begin, uint32_t count, double2 const* in,
+                             double2* dst) {
+    uint32_t const k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) dst[a.slot_of[begin + k]] = in[k];
+}
+
+// Sets *flag when any of the n floats is an infinity or a NaN (exponent bits
+// all ones).
+__global__ void k_flag_nonfinite(float const* p, size_t n, uint32_t* flag) {
+    size_t const k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    bool const bad = k < n && (__float_as_uint(p[k]) & 0x7f800000u) == 0x7f800000u;
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
+}
 
 // Double positions of a scene's particles from their float positions (at
 // creation and whenever the caller sets positions).
@@ -129,6 +151,21 @@ void launch_gather_f2(Arena const& a, uint32_t begin, uint32_t count, float2 con
 void launch_scatter_f2(Arena const& a, uint32_t begin, uint32_t count, float2 const* in, float2* dst,
                        cudaStream_t st) {
     if (count) k_scatter_f2<<<(count + 255) / 256, 256, 0, st>>>(a, begin, count, in, dst);
+}
+void launch_scatter_f(Arena const& a, uint32_t begin, uint32_t count, float const* in, float* dst,
+                      cudaStream_t st) {
+    if (count) k_scatter_f<<<(count + 255) / 256, 256, 0, st>>>(a, begin, count, in, dst);
+}
+void launch_gather_d2(Arena const& a, uint32_t begin, uint32_t count, double2 const* src,
+                      double2* out, cudaStream_t st) {
+    if (count) k_gather_d2<<<(count + 255) / 256, 256, 0, st>>>(a, begin, count, src, out);
+}
+void launch_scatter_d2(Arena const& a, uint32_t begin, uint32_t count, double2 const* in,
+                       double2* dst, cudaStream_t st) {
+    if (count) k_scatter_d2<<<(count + 255) / 256, 256, 0, st>>>(a, begin, count, in, dst);
+}
+void launch_flag_nonfinite(float const* p, size_t n, uint32_t* flag, cudaStream_t st) {
+    if (n) k_flag_nonfinite<<<unsigned((n + 255) / 256), 256, 0, st>>>(p, n, flag);
 }
 void launch_positions_to_double(Arena const& a, uint32_t begin, uint32_t count, cudaStream_t st) {
     if (count) k_positions_to_double<<<(count + 255) / 256, 256, 0, st>>>(a, begin, count);

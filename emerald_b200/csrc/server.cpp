@@ -198,6 +198,63 @@ void Server::admit_locked(Lane& lane) {
     }
 }
 
+void Server::retire_cancelled_locked(Lane& lane) {
+    auto const now = std::chrono::steady_clock::now();
+    for (auto it = lane.running.begin(); it != lane.running.end();) {
+        ServerRequest& r = **it;
+        if (!r.cancel) {
+            ++it;
+            continue;
+        }
+        lane.engine->remove_scene(r.scene);
+        lane.room = lane.engine->room();
+        lane.resident_particles -= double(r.n_fluid);
+        lane.resident_work = std::max(0.0, lane.resident_work -
+                                               double(r.n_fluid) * double(std::max(r.remaining, 0)));
+        r.status = EMERALD_ECANCELED;
+        r.finished = now;
+        resident_changed_locked(-1);
+        finished_[r.id] = std::move(*it);
+        it = lane.running.erase(it);
+        ++version_;
+        done_cv_.notify_all();
+    }
+}
+
+int Server::cancel(int64_t id) {
+    std::lock_guard<std::mutex> lock(mu_);
+    for (auto it = queue_.begin(); it != queue_.end(); ++it) {
+        if ((*it)->id != id) continue;
+        (*it)->status = EMERALD_ECANCELED;
+        (*it)->finished = std::chrono::steady_clock::now();
+        finished_[id] = std::move(*it);
+        queue_.erase(it);
+        ++cancelled_;
+        ++version_;
+        done_cv_.notify_all();
+        return EMERALD_OK;
+    }
+    for (auto const& lane : lanes_) {
+        for (auto const& r : lane->running) {
+            if (r->id != id) continue;
+            if (!r->cancel) ++cancelled_;
+            r->cancel = true;
+            ++version_;
+            work_cv_.notify_all();
+            return EMERALD_OK;
+        }
+    }
+    auto it = finished_.find(id);
+    if (it == finished_.end()) return EMERALD_ENOTFOUND;
+    if (it->second->status != EMERALD_ECANCELED) {
+        it->second->status = EMERALD_ECANCELED;
+        std::vector<float>().swap(it->second->x);
+        std::vector<float>().swap(it->second->v);
+        ++cancelled_;
+    }
+    return EMERALD_OK;
+}
+
 void Server::loop(Lane& lane) {
     cudaSetDevice(device_);
     Engine& engine = *lane.engine;
@@ -206,6 +263,7 @@ void Server::loop(Lane& lane) {
         uint64_t const seen = version_;
         if (!stop_ && loop_status_ == EMERALD_OK) {
             try {
+                retire_cancelled_locked(lane);
                 admit_locked(lane);
             } catch (std::exception const&) {
                 loop_status_ = EMERALD_ECUDA;
@@ -259,10 +317,12 @@ void Server::loop(Lane& lane) {
             status = EMERALD_ECUDA;
         }
         std::vector<ServerRequest*> fin;
+        lock.lock();
         for (auto& r : lane.running) {
             r->remaining -= k;
-            if (r->remaining <= 0) fin.push_back(r.get());
+            if (r->remaining <= 0 && !r->cancel) fin.push_back(r.get());
         }
+        lock.unlock();
         if (status == EMERALD_OK) {
             try {
                 for (ServerRequest* r : fin) {
@@ -271,6 +331,7 @@ void Server::loop(Lane& lane) {
                     engine.get_state(r->scene, r->x.data(), r->v.data());
                     r->final_state = engine.scene_state(r->scene);
                     engine.remove_scene(r->scene);
+                    r->scene = -1;
                 }
             } catch (std::exception const&) {
                 status = EMERALD_ECUDA;
@@ -290,11 +351,16 @@ void Server::loop(Lane& lane) {
                 ++it;
                 continue;
             }
-            r.status = status;
+            // a request cancelled during its last round keeps no result
+            r.status = (status == EMERALD_OK && r.cancel) ? EMERALD_ECANCELED : status;
             r.finished = now;
-            if (status == EMERALD_OK) {
+            if (r.status == EMERALD_OK) {
                 request_ms_.push_back(float(ms_between(r.submitted, r.finished)));
                 ++completed_;
+            } else if (r.cancel && r.scene >= 0) {
+                engine.remove_scene(r.scene);
+                r.scene = -1;
+                lane.room = engine.room();
             }
             lane.resident_particles -= double(r.n_fluid);
             resident_changed_locked(-1);
@@ -388,6 +454,7 @@ void Server::stats(emerald_server_stats& out) {
     }
     out.resident_peak = resident_peak_;
     out.status = loop_status_;
+    out.cancelled = cancelled_;
 }
 
 }  // namespace emerald

@@ -39,6 +39,7 @@ struct ServerRequest {
     int32_t remaining = 0;
     std::chrono::steady_clock::time_point submitted, admitted, finished;
     int status = EMERALD_OK;
+    bool cancel = false;  // retire at the lane's next admission point
     std::vector<float> x, v;
     SceneState final_state{};
 };
@@ -58,6 +59,8 @@ public:
     int wait(int64_t id, int32_t timeout_ms, float* x, float* v, emerald_step_stats* stats,
              emerald_request_timing* timing);
     void stats(emerald_server_stats& out);
+    // Cancels a queued, resident or finished request (emerald_server_cancel).
+    int cancel(int64_t id);
 
 private:
     struct Lane {
@@ -79,6 +82,8 @@ private:
     // resident work.
     int preferred_lane(ServerRequest const& r) const;
     void admit_locked(Lane& lane);
+    // Retires the lane's resident requests marked for cancellation.
+    void retire_cancelled_locked(Lane& lane);
     void resident_changed_locked(int delta);
 
     emerald_server_config cfg_;
@@ -94,7 +99,7 @@ private:
     int loop_status_ = EMERALD_OK;
 
     // statistics (guarded by mu_)
-    int64_t submitted_ = 0, completed_ = 0, rejected_ = 0;
+    int64_t submitted_ = 0, completed_ = 0, rejected_ = 0, cancelled_ = 0;
     int64_t batch_substeps_ = 0, scene_substeps_ = 0;
     double particle_substeps_ = 0.0;
     double busy_seconds_ = 0.0;

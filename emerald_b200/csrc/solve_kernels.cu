@@ -136,8 +136,7 @@ __global__ void k_begin_substep(Arena a, int nscenes) {
     S.error &= ~kErrNonFinite;
     if (P.mode == kFixedDt) {
         S.dt = P.fixed_dt;
-        S.t = static_cast<float>(static_cast<double>(S.substeps_total) *
-                                 static_cast<double>(P.fixed_dt));
+        S.t = P.fixed_t;
         S.new_frame = 0;
         S.max_v2 = 0;
         S.substeps_total += 1;
@@ -495,11 +494,46 @@ __device__ __forceinline__ float2 pressure_accel_of(Arena const& a, SceneParams 
     return out;
 }
 
-// integrate_velocities_in_place with the gravity force of
-// default_gravity_forces (dynamics.cpp:24-37, forces.cpp:63-83).
-__device__ __forceinline__ float2 integrate_external(SceneParams const& P, float2 v, float dt) {
+// compute_all_external_forces (emerald/sph2d_box/forces.cpp:11-33) for one
+// particle: the force starts at zero and takes the scene's terms in order,
+// each with the reference function's own arithmetic; a scene driven by a
+// host callback reads the callback's forces instead. v is the velocity at
+// the point of the sub-step where the solver computes the forces.
+__device__ __forceinline__ float2 external_force(Arena const& a, SceneParams const& P,
+                                                 uint32_t i, float2 v) {
+    if (P.force_array) return a.ext_f[i];
     float2 f = mk2(0.0f, 0.0f);
-    f.y -= P.mass * P.gravity;
+    for (int k = 0; k < P.force_count; ++k) {
+        ForceTerm const t = P.force_terms[k];
+        if (t.kind == kForceGravity) {
+            // accumulate_gravity_forces (forces.cpp:63-71)
+            f.y -= P.mass * t.a;
+        } else if (t.kind == kForcePole) {
+            // accumulate_constant_pole_attraction_forces (forces.cpp:85-101):
+            // pull along the unit vector to the pole (Imath normalized(),
+            // zero at the pole), plus the swirl (0, 0, magnitude / 8) x
+            // (rN, 0) written out component by component.
+            float2 const r = sub2(a.x[i], mk2(t.b, t.c));
+            float const l = length2f(r);
+            float2 const rn = (l == 0.0f) ? mk2(0.0f, 0.0f) : mk2(r.x / l, r.y / l);
+            f = sub2(f, mk2(t.a * rn.x, t.a * rn.y));
+            float const tz = 0.125f * t.a;
+            float const zero = 0.0f;
+            f = add2(f, mk2(zero * zero - tz * rn.y, tz * rn.x - zero * zero));
+        } else if (t.kind == kForceDrag) {
+            // accumulate_simple_drag_forces (forces.cpp:104-111)
+            float const m = -t.a * t.b;
+            f = add2(f, mk2(m * v.x, m * v.y));
+        }
+    }
+    return f;
+}
+
+// integrate_velocities_in_place (dynamics.cpp:24-37) with the scene's
+// external forces.
+__device__ __forceinline__ float2 integrate_external(Arena const& a, SceneParams const& P,
+                                                     uint32_t i, float2 v, float dt) {
+    float2 const f = external_force(a, P, i, v);
     float const denom = P.rho0 * P.fluid_volume;
     float2 const numer = scl2(dt, f);
     if (safe_v(numer, denom)) v = add2(v, div2(numer, denom));
@@ -609,7 +643,7 @@ __global__ void k_apply_pressures(Arena a, int which_q, int external, int skip_d
     SceneParams const& P = a.sp[c.s];
     float const dt = a.ss[c.s].dt;
     float2 v = a.v[c.i];
-    if (external) v = integrate_external(P, v, dt);
+    if (external) v = integrate_external(a, P, c.i, v, dt);
     float const* q = which_q ? a.qdens : a.qdiv;
     a.v[c.i] = (MODE && P.precision) ? apply_pressure_of<true, CH>(a, P, c.i, v, q, dt)
                                      : apply_pressure_of<false, CH>(a, P, c.i, v, q, dt);
@@ -731,7 +765,7 @@ __global__ void k_iisph_density_dii(Arena a) {
     float const rho0 = P.rho0;
     float const d = density_of(a, P, i);
     a.rho[i] = d;
-    a.v[i] = integrate_external(P, a.v[i], dt);
+    a.v[i] = integrate_external(a, P, i, a.v[i], dt);
     float const neg_dt2 = -sqrf(dt);
     float const denom = sqrf(d);
     float2 dii = mk2(0.0f, 0.0f);
@@ -940,7 +974,7 @@ __global__ void k_ap_density(Arena a) {
     SceneParams const& P = a.sp[c.s];
     float const dt = a.ss[c.s].dt;
     a.rho[c.i] = density_of(a, P, c.i);
-    a.v[c.i] = integrate_external(P, a.v[c.i], dt);
+    a.v[c.i] = integrate_external(a, P, c.i, a.v[c.i], dt);
     a.pbuf0[c.i] = 0.0f;
     a.qdens[c.i] = 0.0f;
 }
@@ -1089,9 +1123,9 @@ __global__ void k_pc_init(Arena a) {
     SceneParams const& P = a.sp[c.s];
     float const dt = a.ss[c.s].dt;
     float const mult = dt / P.mass;
-    float2 f = mk2(0.0f, 0.0f);
-    f.y -= P.mass * P.gravity;
-    a.vext[c.i] = add2(a.v[c.i], scl2(mult, f));
+    float2 const v = a.v[c.i];
+    float2 const f = external_force(a, P, c.i, v);
+    a.vext[c.i] = add2(v, scl2(mult, f));
     a.pbuf0[c.i] = 0.0f;
 }
 

@@ -30,6 +30,7 @@ extern "C" {
 #define EMERALD_ETIMEOUT 110
 #define EMERALD_ECUDA 1000
 #define EMERALD_ESOLVER 1001
+#define EMERALD_ECANCELED 125
 
 /* Neighbour slots per particle, NEIGHBORHOOD_MAX_COUNT
  * (emerald/sph_common/neighborhood.h:38). Every list buffer of this API has
@@ -205,6 +206,66 @@ int emerald_sim_get_solid(emerald_sim* sim, float* xy, float* volumes);
 int emerald_sim_set_solid(emerald_sim* sim, float const* solid_xy, float const* solid_v,
                           float const* solid_volumes);
 
+/* External forces. The reference computes them once per sub-step through
+ * compute_all_external_forces (emerald/sph2d_box/forces.cpp:11-33): the
+ * forces start at zero and the user's User_forces_function
+ * (emerald/sph2d_box/forces.h:13-21) adds to them, at the start of the
+ * sub-step under IISPH, IISPH_AP, IISPH_PSEUDO_AP and PCISPH and after the
+ * divergence solve under DFSPH_P. Two ways stand for that function here:
+ *
+ * force terms, evaluated on the device in the sub-step itself, in order,
+ * each with the arithmetic of the reference function it names:
+ *   EMERALD_FORCE_GRAVITY: accumulate_gravity_forces (forces.cpp:63-71),
+ *     F.y -= mass * a;
+ *   EMERALD_FORCE_POLE: accumulate_constant_pole_attraction_forces
+ *     (forces.cpp:85-101), magnitude a, pole (b, c);
+ *   EMERALD_FORCE_DRAG: accumulate_simple_drag_forces (forces.cpp:104-111),
+ *     magnitude a, particle diameter b.
+ * A new simulation has one gravity term with params->gravity, what
+ * default_gravity_forces(gravity) (forces.cpp:73-83) computes. count 0
+ * applies no external force; more than EMERALD_MAX_FORCE_TERMS terms, an
+ * unknown kind or a non-finite argument is EMERALD_EINVAL. */
+#define EMERALD_FORCE_GRAVITY 1
+#define EMERALD_FORCE_POLE 2
+#define EMERALD_FORCE_DRAG 3
+#define EMERALD_MAX_FORCE_TERMS 4
+typedef struct emerald_force_term {
+    int32_t kind;
+    float a, b, c;
+} emerald_force_term;
+int emerald_sim_set_forces(emerald_sim* sim, emerald_force_term const* terms, int32_t count);
+
+/* or a host function with the User_forces_function argument list plus a
+ * user pointer: once per sub-step, at the reference's force point, it gets
+ * the particle count, the time in seconds (the sub-step's start; plus dt
+ * under DFSPH_P, as dfsph_p.cpp:350 passes), dt, mass_per_particle,
+ * draw_radius, the forces to add to (count x 2 floats, zeroed first) and
+ * the positions and velocities at that point (original particle order).
+ * While a callback is set the sub-steps run without CUDA graphs, with one
+ * device-to-host and one host-to-device copy of the state per sub-step.
+ * NULL removes the callback and the force terms apply again. */
+typedef void (*emerald_forces_fn)(void* user, size_t count, float time, float dt, float mass,
+                                  float radius, float* forces, float const* positions,
+                                  float const* velocities);
+int emerald_sim_set_force_callback(emerald_sim* sim, emerald_forces_fn fn, void* user);
+
+/* Checkpoint and resume. The reference keeps a run's state in State and
+ * Temp_data (emerald/sph2d_box/state.h:13-69) and has no checkpoint; the
+ * DFSPH kappas there carry over between the sub-steps of a frame and are
+ * zeroed per frame (dfsph_p.cpp:214-229), so a resumable state holds them.
+ * emerald_sim_snapshot writes, between sub-steps, the frame clock in flicks
+ * with the position inside the frame, the sub-step counters and the last
+ * statistics, the positions, velocities and DFSPH kappas (original order),
+ * the FP64 positions of a compensated scene and the boundary (positions,
+ * velocities, volumes) into `buffer`; *size receives the bytes it needs
+ * (buffer NULL: only the size; capacity too small: EMERALD_ENOSPC).
+ * emerald_sim_restore loads one into a simulation of the same particle
+ * counts and precision mode (EMERALD_EINVAL otherwise, or for a damaged
+ * buffer); the sub-steps after it are bit-identical to those that followed
+ * the snapshot. Parameters and force settings are not part of it. */
+int emerald_sim_snapshot(emerald_sim* sim, void* buffer, size_t capacity, size_t* size);
+int emerald_sim_restore(emerald_sim* sim, void const* buffer, size_t size);
+
 /* Per-particle solver temporaries by their Temp_data name
  * (emerald/sph2d_box/state.h:34-69): "densities", "pressures",
  * "density_stars", "aiis", "alphas", "divergence_kappas", "density_kappas",
@@ -281,6 +342,9 @@ int emerald_batch_set_state(emerald_batch* batch, int32_t scene, float const* x,
 /* emerald_sim_set_solid for one scene of a batch. */
 int emerald_batch_set_solid(emerald_batch* batch, int32_t scene, float const* solid_xy,
                             float const* solid_v, float const* solid_volumes);
+/* emerald_sim_set_forces for one scene of a batch. */
+int emerald_batch_set_forces(emerald_batch* batch, int32_t scene, emerald_force_term const* terms,
+                             int32_t count);
 /* Largest fluid range and scene slots still free. */
 int emerald_batch_free(emerald_batch* batch, size_t* fluid, int32_t* scenes);
 int emerald_batch_set_stream(emerald_batch* batch, void* cuda_stream);
@@ -354,6 +418,7 @@ typedef struct emerald_server_stats {
     size_t device_bytes;                   /* all lanes */
     int32_t resident_peak;
     int32_t status; /* first error of the loop, EMERALD_OK while healthy */
+    int64_t cancelled; /* requests retired by emerald_server_cancel */
 } emerald_server_stats;
 
 typedef struct emerald_request_timing {
@@ -376,6 +441,14 @@ int emerald_server_submit(emerald_server* server, emerald_params const* params,
 int emerald_server_wait(emerald_server* server, int64_t request, int32_t timeout_ms, float* x,
                         float* v, emerald_step_stats* stats, emerald_request_timing* timing);
 int emerald_server_get_stats(emerald_server* server, emerald_server_stats* out);
+/* No counterpart in the reference (one scene per process, stopped by
+ * killing it). Cancels a request: a queued one leaves the queue at once; a
+ * resident one leaves its batch at the lane's next admission point, between
+ * sub-steps, and its room is freed (the other scenes of the batch go on
+ * unchanged, bit for bit); a finished one drops its result. emerald_server_wait
+ * then returns EMERALD_ECANCELED for it. EMERALD_ENOTFOUND for an unknown or
+ * already collected id. */
+int emerald_server_cancel(emerald_server* server, int64_t request);
 
 /* ------------------------------------------- sph_common functions on device */
 

@@ -26,21 +26,36 @@
 // Each call uploads the state, passes on a boundary whose positions or
 // velocities differ from the previous call's (a moving wall: the reference
 // takes the Solid_state anew on every call), runs one frame on the GPU,
-// downloads the new state and, if user_colors is callable, calls it on the
+// downloads the new state and, unless user_colors is empty, calls it on the
 // host with the
 // frame's densities, as compute_colors does (emerald/sph2d_box/colors.cpp:22-38).
-// user_forces is not called: the device applies gravity, which is what the
-// reference's default_gravity_forces (emerald/sph2d_box/forces.cpp:63-83)
-// computes; callers with other forces stay on the reference path.
+//
+// user_forces (emerald/sph2d_box/forces.h:13-21) is honoured as the
+// reference honours it, once per sub-step at the solver's force point:
+//   * default_gravity_forces(g) and Device_forces{...} from this header
+//     (the std::function holds them, found with target<>()) become force
+//     terms evaluated on the device inside the sub-step;
+//   * any other callable is called on the host with the state of that
+//     point of the sub-step (emerald_sim_set_force_callback; the sub-steps
+//     then run without graphs);
+//   * an empty function throws std::bad_function_call, as calling it in the
+//     reference does.
+// accumulate_gravity_forces, accumulate_constant_pole_attraction_forces and
+// accumulate_simple_drag_forces (emerald/sph2d_box/forces.cpp:63-111) are
+// provided for host force functions written against the reference.
 #pragma once
 
 #include <algorithm>
 #include <cstdint>
+#include <functional>
+#include <initializer_list>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <cmath>
+#include <limits>
 #include <type_traits>
 #include <utility>
 #include <vector>
@@ -63,6 +78,104 @@ private:
 inline void check(int rc, char const* what) {
     if (rc != EMERALD_OK) throw Error(rc, what);
 }
+
+namespace sph2d_box {
+
+// The reference's force functions (emerald/sph2d_box/forces.cpp:63-111) for
+// host force functions, on any two-float vector type with x and y members,
+// with the reference's arithmetic (Imath 2.x Vec2 operations).
+template <class V>
+void accumulate_gravity_forces(size_t const count, float const mass_per_particle,
+                               float const gravity, V* const forces) {
+    for (size_t i = 0; i < count; ++i) forces[i].y -= mass_per_particle * gravity;
+}
+
+template <class V>
+void accumulate_constant_pole_attraction_forces(size_t const count, float const magnitude,
+                                                V const pole, V* const forces,
+                                                V const* const positions) {
+    for (size_t i = 0; i < count; ++i) {
+        float const rx = positions[i].x - pole.x;
+        float const ry = positions[i].y - pole.y;
+        // Imath Vec2::length with its tiny-length rescale, then normalized()
+        float len;
+        float const l2 = rx * rx + ry * ry;
+        if (l2 < 2.0f * std::numeric_limits<float>::min()) {
+            float ax = rx >= 0.0f ? rx : -rx;
+            float ay = ry >= 0.0f ? ry : -ry;
+            float m = ax;
+            if (m < ay) m = ay;
+            if (m == 0.0f) {
+                len = 0.0f;
+            } else {
+                ax /= m;
+                ay /= m;
+                len = m * std::sqrt(ax * ax + ay * ay);
+            }
+        } else {
+            len = std::sqrt(l2);
+        }
+        float const nx = len == 0.0f ? 0.0f : rx / len;
+        float const ny = len == 0.0f ? 0.0f : ry / len;
+        forces[i].x -= magnitude * nx;
+        forces[i].y -= magnitude * ny;
+        // (0, 0, magnitude / 8) x (nx, ny, 0)
+        float const tz = 0.125f * magnitude;
+        float const zero = 0.0f;
+        forces[i].x += zero * zero - tz * ny;
+        forces[i].y += tz * nx - zero * zero;
+    }
+}
+
+template <class V>
+void accumulate_simple_drag_forces(size_t const count, float const magnitude,
+                                   float const particle_diameter, V* const forces,
+                                   V const* const velocities) {
+    float const m = -magnitude * particle_diameter;
+    for (size_t i = 0; i < count; ++i) {
+        forces[i].x += m * velocities[i].x;
+        forces[i].y += m * velocities[i].y;
+    }
+}
+
+// default_gravity_forces (emerald/sph2d_box/forces.cpp:73-83) as a functor
+// the step functions recognise and run on the device.
+struct Gravity_forces {
+    float gravity;
+    template <class V>
+    void operator()(size_t const count, float, float, float const mass_per_particle, float,
+                    V* const forces, V const* const, V const* const) const {
+        accumulate_gravity_forces(count, mass_per_particle, gravity, forces);
+    }
+};
+
+inline Gravity_forces default_gravity_forces(float const gravity) { return Gravity_forces{gravity}; }
+
+// Up to EMERALD_MAX_FORCE_TERMS device force terms (emerald_force_term) as a
+// User_forces_function: the step functions run them on the device; called
+// on the host it computes the same forces.
+struct Device_forces {
+    std::vector<emerald_force_term> terms;
+    Device_forces(std::initializer_list<emerald_force_term> t) : terms(t) {}
+    template <class V>
+    void operator()(size_t const count, float, float, float const mass_per_particle, float,
+                    V* const forces, V const* const positions, V const* const velocities) const {
+        for (auto const& t : terms) {
+            if (t.kind == EMERALD_FORCE_GRAVITY) {
+                accumulate_gravity_forces(count, mass_per_particle, t.a, forces);
+            } else if (t.kind == EMERALD_FORCE_POLE) {
+                V pole;
+                pole.x = t.b;
+                pole.y = t.c;
+                accumulate_constant_pole_attraction_forces(count, t.a, pole, forces, positions);
+            } else if (t.kind == EMERALD_FORCE_DRAG) {
+                accumulate_simple_drag_forces(count, t.a, t.b, forces, velocities);
+            }
+        }
+    }
+};
+
+}  // namespace sph2d_box
 
 namespace detail {
 
@@ -102,12 +215,14 @@ int64_t ticks(T const& t, long) {
     return int64_t(t);
 }
 
+// An empty std::function (or a null function pointer, or nullptr): the
+// only callables that can be empty. Lambdas and functors never are.
 template <class F>
-auto callable(F const& f, int) -> decltype(bool(f)) {
-    return bool(f);
+auto is_empty(F const& f, int) -> decltype(!bool(f)) {
+    return !bool(f);
 }
 template <class F>
-bool callable(F const&, long) {
+bool is_empty(F const&, long) {
     return false;
 }
 
@@ -215,9 +330,57 @@ void sync_solid(Context& ctx, Solid_state const& solid) {
     if (vchanged) std::copy(v, v + 2 * ns, ctx.solid_v.begin());
 }
 
-template <class State, class Config, class Solid_state, class Colors>
+template <class T, class F>
+auto held(F const& f, int) -> decltype(f.template target<T>()) {
+    return f.template target<T>();
+}
+template <class T, class F>
+T const* held(F const& f, long) {
+    if constexpr (std::is_same<typename std::decay<F>::type, T>::value) {
+        return &f;
+    } else {
+        return nullptr;
+    }
+}
+
+// Calls the caller's force function with its own vector type.
+template <class Forces, class V>
+void call_forces(void* user, size_t count, float time, float dt, float mass, float radius,
+                 float* forces, float const* positions, float const* velocities) {
+    (*static_cast<Forces const*>(user))(count, time, dt, mass, radius,
+                                        reinterpret_cast<V*>(forces),
+                                        reinterpret_cast<V const*>(positions),
+                                        reinterpret_cast<V const*>(velocities));
+}
+
+// Points the device simulation at the caller's forces for this call.
+template <class V, class Forces>
+void set_forces(Context& ctx, Forces const& user_forces) {
+    using sph2d_box::Device_forces;
+    using sph2d_box::Gravity_forces;
+    if (Gravity_forces const* g = held<Gravity_forces>(user_forces, 0)) {
+        emerald_force_term const t{EMERALD_FORCE_GRAVITY, g->gravity, 0.0f, 0.0f};
+        check(emerald_sim_set_force_callback(ctx.sim, nullptr, nullptr), "force callback");
+        check(emerald_sim_set_forces(ctx.sim, &t, 1), "emerald_sim_set_forces");
+        return;
+    }
+    if (Device_forces const* d = held<Device_forces>(user_forces, 0)) {
+        check(emerald_sim_set_force_callback(ctx.sim, nullptr, nullptr), "force callback");
+        check(emerald_sim_set_forces(ctx.sim, d->terms.data(), int32_t(d->terms.size())),
+              "emerald_sim_set_forces");
+        return;
+    }
+    if (is_empty(user_forces, 0)) throw std::bad_function_call();
+    check(emerald_sim_set_force_callback(
+            ctx.sim, &call_forces<typename std::decay<Forces>::type, V>,
+            const_cast<void*>(static_cast<void const*>(&user_forces))),
+          "emerald_sim_set_force_callback");
+}
+
+template <class State, class Config, class Solid_state, class Forces, class Colors>
 State step(int32_t method, int64_t global_time, Config const& config, State&& state,
-           Solid_state const& solid, void const* temp_key, Colors const& user_colors) {
+           Solid_state const& solid, void const* temp_key, Forces const& user_forces,
+           Colors const& user_colors) {
     size_t const n = state.positions.size();
     if (state.velocities.size() != n) {
         throw std::invalid_argument("positions and velocities differ in size");
@@ -230,12 +393,17 @@ State step(int32_t method, int64_t global_time, Config const& config, State&& st
     sync_solid(ctx, solid);
     check(emerald_sim_set_state(ctx.sim, floats(state.positions), floats(state.velocities)),
           "emerald_sim_set_state");
+    using V2 = typename std::decay<decltype(state.positions[0])>::type;
+    set_forces<V2>(ctx, user_forces);
     emerald_step_stats stats{};
-    check(emerald_sim_frame(ctx.sim, method, &stats), "emerald_sim_frame");
+    int const rc = emerald_sim_frame(ctx.sim, method, &stats);
+    // the callback points at user_forces, which lives only for this call
+    emerald_sim_set_force_callback(ctx.sim, nullptr, nullptr);
+    check(rc, "emerald_sim_frame");
     check(emerald_sim_get_state(ctx.sim, floats(state.positions), floats(state.velocities)),
           "emerald_sim_get_state");
     ctx.time += to_params(config).time_per_step_flicks;
-    if (callable(user_colors, 0)) {
+    if (!is_empty(user_colors, 0)) {
         ctx.densities.resize(n);
         int32_t width = 0;
         check(emerald_sim_get_array(ctx.sim, "densities", ctx.densities.data(), &width),
@@ -266,10 +434,9 @@ namespace sph2d_box {
                                           State&& state, Solid_state const& solid_state,       \
                                           Temp& temp, Forces const& user_forces,               \
                                           Colors const& user_colors) {                         \
-        (void)user_forces;                                                                     \
         return detail::step(method, detail::ticks(global_time, 0), config,                     \
                             std::forward<State>(state), solid_state,                           \
-                            static_cast<void const*>(&temp), user_colors);                     \
+                            static_cast<void const*>(&temp), user_forces, user_colors);        \
     }
 
 // emerald/sph2d_box/pcisph.cpp:166-204

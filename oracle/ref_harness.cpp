@@ -385,6 +385,60 @@ void ref_sim_set_solid(void* h, float const* xy, float const* v, float const* vo
     }
 }
 
+// Replaces the simulation's User_forces_function (default_gravity_forces,
+// emerald/sph2d_box/forces.cpp:73-83, until then) with one that applies
+// `count` terms in order through the reference's own force functions:
+// kind 1 accumulate_gravity_forces (a = gravity), 2
+// accumulate_constant_pole_attraction_forces (a = magnitude, pole (b, c)),
+// 3 accumulate_simple_drag_forces (a = magnitude, b = diameter).
+void ref_sim_set_forces(void* h, int32_t const* kinds, float const* args, int count) {
+    auto* sim = static_cast<Ref_sim*>(h);
+    std::vector<int32_t> const k(kinds, kinds + count);
+    std::vector<float> const a(args, args + 3 * count);
+    sim->forces = [k, a](size_t const n, float const, float const, float const mass,
+                         float const, V2f* const forces, V2f const* const positions,
+                         V2f const* const velocities) {
+        for (size_t t = 0; t < k.size(); ++t) {
+            float const x = a[3 * t], y = a[3 * t + 1], z = a[3 * t + 2];
+            if (k[t] == 1) accumulate_gravity_forces(n, mass, x, forces);
+            if (k[t] == 2) accumulate_constant_pole_attraction_forces(n, x, V2f{y, z}, forces, positions);
+            if (k[t] == 3) accumulate_simple_drag_forces(n, x, y, forces, velocities);
+        }
+    };
+}
+
+// The reference's force functions on host arrays: n forces (x, y pairs,
+// accumulated in place) from positions and velocities, with the terms of
+// ref_sim_set_forces applied in order.
+void ref_accumulate_forces(int32_t const* kinds, float const* args, int count, size_t n,
+                           float mass, float* forces, float const* positions,
+                           float const* velocities) {
+    auto* f = reinterpret_cast<V2f*>(forces);
+    auto const* x = reinterpret_cast<V2f const*>(positions);
+    auto const* v = reinterpret_cast<V2f const*>(velocities);
+    for (int t = 0; t < count; ++t) {
+        float const a = args[3 * t], b = args[3 * t + 1], c = args[3 * t + 2];
+        if (kinds[t] == 1) accumulate_gravity_forces(n, mass, a, f);
+        if (kinds[t] == 2) accumulate_constant_pole_attraction_forces(n, a, V2f{b, c}, f, x);
+        if (kinds[t] == 3) accumulate_simple_drag_forces(n, a, b, f, v);
+    }
+}
+
+// A C function as the User_forces_function (argument list of
+// emerald/sph2d_box/forces.h:13-21 plus a user pointer).
+typedef void (*ref_forces_fn)(void* user, size_t count, float time, float dt, float mass,
+                              float radius, float* forces, float const* positions,
+                              float const* velocities);
+void ref_sim_set_force_callback(void* h, ref_forces_fn fn, void* user) {
+    auto* sim = static_cast<Ref_sim*>(h);
+    sim->forces = [fn, user](size_t const n, float const t, float const dt, float const mass,
+                             float const radius, V2f* const forces, V2f const* const positions,
+                             V2f const* const velocities) {
+        fn(user, n, t, dt, mass, radius, reinterpret_cast<float*>(forces),
+           reinterpret_cast<float const*>(positions), reinterpret_cast<float const*>(velocities));
+    };
+}
+
 int64_t ref_sim_time(void* h) { return static_cast<Ref_sim*>(h)->time.count(); }
 
 // Method numbering follows EZ_EXAMPLE_SIM::Method

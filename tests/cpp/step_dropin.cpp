@@ -5,18 +5,23 @@
 // step calls are spelled exactly as in EZ_EXAMPLE_SIM::step
 // (emerald/sph2d_box/simulation.cpp:41-93).
 //
-//   step_dropin <method 0-4> <frames> <out.bin> [wall speed]
+//   step_dropin <method 0-4> <frames> <out.bin> [wall speed] [forces]
 //
 // Runs the reference's default dam break (world_walls + dam_break scenes)
 // and writes positions, velocities and colours after the last frame. With a
-// wall speed (m/s), the caller moves the boundary particles left of x = 0
-// along x before every frame (frame f, from 1, at f * speed * 2 ms) and
-// gives them that velocity, as a caller of the reference moves a wall: by
-// passing a changed Solid_state to the next step call.
+// non-zero wall speed (m/s), the caller moves the boundary particles left of
+// x = 0 along x before every frame (frame f, from 1, at f * speed * 2 ms)
+// and gives them that velocity, as a caller of the reference moves a wall:
+// by passing a changed Solid_state to the next step call. forces:
+// "gravity" (default_gravity_forces, the default), "host" (a capturing
+// lambda that adds gravity and a pole attraction with the reference's
+// accumulate functions, called on the host) or "device" (the same two terms
+// as Device_forces, run on the device).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <functional>
+#include <string>
 #include <vector>
 
 #include "emerald_sph.hpp"
@@ -69,11 +74,12 @@ using User_colors_function = std::function<void(size_t, float, float, float, C4f
 using namespace emerald_b200::sph2d_box;
 
 int main(int argc, char** argv) {
-    if (argc != 4 && argc != 5) return 2;
+    if (argc < 4 || argc > 6) return 2;
     int const method = std::atoi(argv[1]);
     int const frames = std::atoi(argv[2]);
-    bool const moving = argc == 5;
-    float const speed = moving ? float(std::atof(argv[4])) : 0.0f;
+    float const speed = argc >= 5 ? float(std::atof(argv[4])) : 0.0f;
+    bool const moving = speed != 0.0f;
+    std::string const force_mode = argc == 6 ? argv[5] : "gravity";
     emerald_params p{};
     emerald_b200::check(emerald_default_params(&p), "defaults");
     float cfg[4];
@@ -113,7 +119,26 @@ int main(int argc, char** argv) {
     state.velocities.assign(n, {0.0f, 0.0f});
 
     ref::Temp_data temp_data;
-    ref::User_forces_function user_forces;  // gravity is applied on the device
+    // The pole pull of the reference's commented-out example
+    // (emerald/sph2d_box/forces.cpp:24-28): a quarter of gravity towards the
+    // tank's centre.
+    float const g = config.params.gravity;
+    float const pole_magnitude = 0.25f * g * config.mass_per_particle;
+    ref::User_forces_function user_forces = default_gravity_forces(g);
+    if (force_mode == "host") {
+        user_forces = [g, pole_magnitude](size_t count, float, float, float mass, float,
+                                          ref::V2f* forces, ref::V2f const* positions,
+                                          ref::V2f const*) {
+            accumulate_gravity_forces(count, mass, g, forces);
+            accumulate_constant_pole_attraction_forces(count, pole_magnitude, ref::V2f{0.5f, 0.5f},
+                                                       forces, positions);
+        };
+    } else if (force_mode == "device") {
+        user_forces = Device_forces{{EMERALD_FORCE_GRAVITY, g, 0.0f, 0.0f},
+                                    {EMERALD_FORCE_POLE, pole_magnitude, 0.5f, 0.5f}};
+    } else if (force_mode != "gravity") {
+        return 2;
+    }
     float const rho0 = config.params.target_density;
     ref::User_colors_function user_colors = [rho0](size_t count, float, float, float,
                                                    ref::C4f* colors, ref::V2f const*,

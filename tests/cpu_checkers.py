@@ -258,6 +258,8 @@ class Reference:
         L.ref_lattice_config.argtypes = [ctypes.POINTER(RefParams), c_f, c_f, c_vp]
         L.ref_wall_scene.restype = c_sz
         L.ref_wall_scene.argtypes = [c_f, c_f, ctypes.c_int, c_vp]
+        L.ref_sim_set_forces.argtypes = [c_vp, c_vp, c_vp, ctypes.c_int]
+        L.ref_sim_set_force_callback.argtypes = [c_vp, c_vp, c_vp]
         L.ref_sim_run_window.restype = c_i64
         L.ref_sim_run_window.argtypes = [c_vp, ctypes.c_int, c_i64, c_i64, ctypes.c_double,
                                          ctypes.POINTER(ctypes.c_double)]
@@ -426,6 +428,20 @@ class RefSim:
 
     def frame(self, method):
         assert self.lib.L.ref_sim_frame(self.h, METHODS.get(method, method)) == 0
+
+    def set_forces(self, terms):
+        """The reference's force functions in order, (kind, a, b, c) tuples:
+        1 gravity, 2 constant pole attraction, 3 simple drag."""
+        kinds = np.array([t[0] for t in terms] or [0], np.int32)
+        args = np.array([(tuple(t[1:]) + (0.0,) * 3)[:3] for t in terms] or [(0, 0, 0)],
+                        np.float32)
+        self.lib.L.ref_sim_set_forces(self.h, ptr(kinds), ptr(args), len(terms))
+
+    def set_force_callback(self, cfunc):
+        """A ctypes emerald_forces_fn-compatible callback as the
+        User_forces_function; the caller keeps `cfunc` alive."""
+        self._cb = cfunc
+        self.lib.L.ref_sim_set_force_callback(self.h, ctypes.cast(cfunc, c_vp), None)
 
     def run_window(self, method, skip, count, max_seconds=0.0):
         """Adaptive frames through the reference's frame loop; sub-steps

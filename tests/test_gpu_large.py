@@ -1,0 +1,146 @@
+"""The largest workloads bit for bit: the 1,048,576-particle precision scene
+(1024 x 1024 fluid block, dx = 1/2048, support = dx) and PCISPH on the
+262,144-particle scene (512 x 512, dx = 1/1024), against the reference
+compiled from its own sources (oracle/_ref) and the C restatement, both on
+all host threads.
+
+With 24-bit storage keys, cell tables of 2^ceil(log2 2n) + 1 slots and
+32-bit list indices, these sizes are where a size-dependent fault would
+show: the sort products (grid coordinates, z keys, the (z, index) pair
+order, block indices and block ranges), every neighbour list entry (count,
+index, W, grad W) of both the fluid and the boundary lists, the state after
+two DFSPH sub-steps and the solver's iteration counts are all compared."""
+import gc
+import os
+
+import numpy as np
+import pytest
+
+from conftest import assert_bitwise
+from scenes import F
+
+pytestmark = pytest.mark.gpu
+
+THREADS = os.cpu_count() or 1
+
+
+def ref_params(E, sc):
+    from cpu_checkers import RefParams
+    d = sc.params.as_dict()
+    rp = {k: d[k] for k, _ in RefParams._fields_ if k in d}
+    rp.update(mass_per_particle_override=d["mass_per_particle"],
+              pressure_correction_denom_override=d["pressure_correction_denom"])
+    return rp
+
+
+def oracle_params(E, p):
+    d = p.as_dict()
+    cfg = E.config(p)
+    out = {k: d[k] for k in d if k not in ("seed", "length")}
+    out.update(mass_per_particle=cfg["mass_per_particle"],
+               pressure_correction_denom=cfg["pressure_correction_denom"],
+               seconds_per_sub_step=cfg["seconds_per_sub_step"])
+    return out
+
+
+def scene_1m(E):
+    return E.BlockScene(1024, dx=F(1 / 2048), seed=1, time_per_step_flicks=1411200, sub_steps=4,
+                        dfsph_max_correction_iterations=100,
+                        dfsph_divergence_error_average_threshold=F(0.001),
+                        dfsph_density_error_average_threshold=F(0.0005))
+
+
+def compare_lists(sim, other, solid, what):
+    a = sim.neighbors(solid)
+    b = other.neighbors(solid)
+    names = ("counts", "indices", "W", "grad W")
+    live = np.arange(64)[None, :] < a[0][:, None]
+    for name, u, w in zip(names, a, b):
+        if name != "counts":
+            # entries past a particle's count are unspecified on both sides
+            u = np.where(live[..., None] if u.ndim == 3 else live, u, 0)
+            w = np.where(live[..., None] if w.ndim == 3 else live, w, 0)
+        assert_bitwise(u, w, "%s %s %s" % (what, "boundary" if solid else "fluid", name))
+
+
+def test_north_star_scene_matches_reference():
+    """Two CFL-adaptive DFSPH_P sub-steps of the 1M scene from rest through
+    the reference's own frame loop (ref_sim_run_window) against
+    emerald_sim_advance: positions, velocities, the sort products and both
+    neighbour lists of the second sub-step."""
+    import emerald_b200 as E
+    from cpu_checkers import Reference
+    R = Reference()
+    R.set_threads(THREADS)
+    sc = scene_1m(E)
+    assert len(sc.fluid) == 1 << 20
+    sim = E.Simulation.from_block_scene(sc)
+    sim.advance("dfsph_p", 2)
+    ref = R.sim(ref_params(E, sc), sc.solid, sc.fluid, None, sc.solid_volumes)
+    timed, _ = ref.run_window("dfsph_p", 0, 2)
+    assert timed == 2
+    x, v = sim.state()
+    rx, rv = ref.state()
+    assert_bitwise(x, rx, "1M positions after 2 sub-steps")
+    assert_bitwise(v, rv, "1M velocities after 2 sub-steps")
+    for solid in (False, True):
+        s = sim.sort(solid)
+        r = ref.sort(solid)
+        for k in ("grid_coords", "z_indices", "pair_z", "pair_index", "block_indices", "blocks"):
+            assert_bitwise(s[k], np.asarray(r[k]).astype(s[k].dtype),
+                           "1M %s %s" % ("boundary" if solid else "fluid", k))
+        compare_lists(sim, ref, solid, "1M")
+    del ref
+    gc.collect()
+    sim.close()
+
+
+def test_north_star_scene_iterations_match_oracle(oracle):
+    """The same two sub-steps (dt = 5e-4 s, the CFL step from rest) against
+    the C restatement, which reports the solver's iteration counts: the
+    divergence and density iterations of each sub-step are equal."""
+    import emerald_b200 as E
+    sc = scene_1m(E)
+    sim = E.Simulation.from_block_scene(sc)
+    osim = oracle.sim(oracle_params(E, sc.params), sc.solid, sc.solid_volumes, sc.fluid)
+    oracle.set_threads(THREADS)
+    sim.begin_frame("dfsph_p")
+    osim.begin_frame("dfsph_p")
+    try:
+        for s in range(2):
+            ost = osim.sub_step("dfsph_p", F(s * 5e-4), F(5e-4))
+            st = sim.sub_step("dfsph_p", F(s * 5e-4), F(5e-4))
+            assert st["pressure_iterations"] == ost["pressure_iterations"], (s, st, ost)
+            assert st["divergence_iterations"] == ost["divergence_iterations"], (s, st, ost)
+            assert np.float32(st["error_average"]) == np.float32(ost["error_average"])
+    finally:
+        oracle.set_threads(1)
+    assert_bitwise(sim.state()[0], osim.state()[0], "1M positions (fixed dt)")
+    assert_bitwise(sim.state()[1], osim.state()[1], "1M velocities (fixed dt)")
+    del osim
+    gc.collect()
+    sim.close()
+
+
+def test_pcisph_262k_matches_reference():
+    """PCISPH on the 262,144-particle scene: two fixed sub-steps of
+    time_per_step / sub_steps = 5e-4 s against the compiled reference."""
+    import emerald_b200 as E
+    from cpu_checkers import Reference
+    R = Reference()
+    R.set_threads(THREADS)
+    sc = E.BlockScene(512, dx=F(1 / 1024), seed=1, time_per_step_flicks=1411200, sub_steps=4)
+    sim = E.Simulation.from_block_scene(sc)
+    ref = R.sim(ref_params(E, sc), sc.solid, sc.fluid, None, sc.solid_volumes)
+    sim.begin_frame("pcisph")
+    ref.begin_frame("pcisph")
+    for s in range(2):
+        sim.sub_step("pcisph", F(s * 5e-4), F(5e-4))
+        ref.sub_step("pcisph", F(s * 5e-4), F(5e-4))
+    x, v = sim.state()
+    rx, rv = ref.state()
+    assert_bitwise(x, rx, "PCISPH 262k positions")
+    assert_bitwise(v, rv, "PCISPH 262k velocities")
+    compare_lists(sim, ref, False, "PCISPH 262k")
+    compare_lists(sim, ref, True, "PCISPH 262k")
+    sim.close()

@@ -360,3 +360,27 @@ def test_empty_fluid_scene_steps(E, method):
     x, v = sim.state()
     assert x.shape == (0, 2) and v.shape == (0, 2)
     sim.close()
+
+
+def test_bench_arms_share_the_trajectory(E, reference):
+    """The bench's reference arm (sub-steps [W, W + K) of the reference's own
+    frame loop, scene built by the harness alone) and its GPU arm (W
+    sub-steps of warm-up, then K) end on the same state bit for bit, so both
+    time the same work."""
+    import bench
+    bench.configure_scene(48)
+    try:
+        rp, fluid, solid, volumes = bench.reference_scene(reference)
+        ref = reference.sim(rp, solid, fluid, None, volumes)
+        timed, _ = ref.run_window("dfsph_p", 5, 7)
+        assert timed == 7
+        sim = E.Simulation.from_block_scene(E.BlockScene(bench.N_SIDE, **bench.scene_kwargs()))
+        sim.advance("dfsph_p", 5, stats=False)
+        sim.advance("dfsph_p", 7, stats=False)
+        x, v = sim.state()
+        rx, rv = ref.state()
+        assert_bitwise(x, rx, "positions after the bench window")
+        assert_bitwise(v, rv, "velocities after the bench window")
+        sim.close()
+    finally:
+        bench.configure_scene(512)

@@ -140,3 +140,39 @@ def test_dropin_header_compiles():
                             os.path.join(root, "tests", "cpp", "step_dropin.cpp"), "-L", lib,
                             "-lemerald_b200", "-o", out], capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
+
+
+def test_non_finite_inputs_are_rejected_before_any_device_work():
+    """emerald_sim_create screens its host arrays (positions, velocities,
+    boundary positions and volumes) and the parameters for infinities and
+    NaNs and returns EMERALD_EINVAL naming the array, before it touches a
+    device (so this runs without a GPU)."""
+    p = E.default_params()
+    fluid = np.array([[0.1, 0.1], [0.2, 0.1], [0.3, 0.1]], np.float32)
+    solid = np.array([[0.0, -0.01], [0.1, -0.01]], np.float32)
+    h = ctypes.c_void_p()
+
+    def create(f, v, s, vol, params=p):
+        return E.lib.emerald_sim_create(ctypes.byref(params), E._ptr(s), E._ptr(vol), len(s),
+                                        E._ptr(f), E._ptr(v), len(f), ctypes.byref(h))
+
+    bad = fluid.copy()
+    bad[1, 0] = np.nan
+    assert create(bad, None, solid, None) == 22
+    assert b"fluid positions" in E.lib.emerald_last_error()
+    v = np.zeros_like(fluid)
+    v[2, 1] = np.inf
+    assert create(fluid, v, solid, None) == 22
+    assert b"fluid velocities" in E.lib.emerald_last_error()
+    s = solid.copy()
+    s[0, 1] = -np.inf
+    assert create(fluid, None, s, None) == 22
+    assert b"boundary positions" in E.lib.emerald_last_error()
+    vol = np.array([1.0, np.nan], np.float32)
+    assert create(fluid, None, solid, vol) == 22
+    assert b"boundary volumes" in E.lib.emerald_last_error()
+    q = E.default_params(gravity=float("nan"))
+    assert create(fluid, None, solid, None, q) == 22
+    assert b"not finite" in E.lib.emerald_last_error()
+    out = np.zeros(4, np.float32)
+    assert E.lib.emerald_config(ctypes.byref(q), E._ptr(out)) == 22
