@@ -98,8 +98,8 @@ class RequestTiming(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("apply_chunk", c_i32), ("divergence_chunk", c_i32), ("iisph_sum_chunk", c_i32),
                 ("iisph_beta_chunk", c_i32), ("candidates", c_i32),
-                ("candidate_chunks", (c_i32 * 4) * 8), ("candidate_ms", c_f * 8),
-                ("prefetch", c_i32 * 4), ("candidate_prefetch", (c_i32 * 4) * 8)]
+                ("candidate_chunks", (c_i32 * 4) * 16), ("candidate_ms", c_f * 16),
+                ("prefetch", c_i32 * 4), ("candidate_prefetch", (c_i32 * 4) * 16)]
 
     def as_dict(self):
         fams = ("apply", "divergence", "iisph_sum", "iisph_beta")
@@ -180,6 +180,7 @@ EXPORTS = {
     "emerald_sim_set_forces": (c_i32, [c_vp, c_vp, c_i32]),
     "emerald_sim_set_force_callback": (c_i32, [c_vp, FORCES_FN, c_vp]),
     "emerald_sim_snapshot": (c_i32, [c_vp, c_vp, c_sz, ctypes.POINTER(c_sz)]),
+    "emerald_sim_host_waits": (c_i32, [c_vp, ctypes.POINTER(c_i64)]),
     "emerald_sim_restore": (c_i32, [c_vp, c_vp, c_sz]),
     "emerald_sim_get_array": (c_i32, [c_vp, ctypes.c_char_p, c_vp, ctypes.POINTER(c_i32)]),
     "emerald_sim_get_neighbors": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp]),
@@ -519,6 +520,12 @@ class Simulation:
         v = None if v is None else _f32(v)
         volumes = None if volumes is None else np.ascontiguousarray(volumes, np.float32)
         _check(lib.emerald_sim_set_solid(self._h, _ptr(xy), _ptr(v), _ptr(volumes)), "set_solid")
+
+    def host_waits(self):
+        """Times the simulation waited on the host for the device."""
+        n = c_i64()
+        _check(lib.emerald_sim_host_waits(self._h, ctypes.byref(n)), "host_waits")
+        return n.value
 
     def snapshot(self):
         """The simulation's checkpoint (emerald_sim_snapshot) as bytes."""

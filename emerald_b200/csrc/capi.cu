@@ -285,13 +285,8 @@ int emerald_sim_frame(emerald_sim* sim, int32_t method, emerald_step_stats* stat
     if (!sim || !valid_method(method)) return fail(EMERALD_EINVAL, "bad arguments");
     return guarded([&] {
         sim->engine.set_mode(sim->scene, kFrame, 0.0f);
-        int n = 0;
         SceneState s{};
-        do {
-            sim->engine.substep(method);
-            ++n;
-            s = sim->engine.scene_state(sim->scene);
-        } while (s.remaining > 0 && n < 100000);
+        int const n = sim->engine.frame(sim->scene, method, s);
         fill_stats(s, stats, n);
         return EMERALD_OK;
     });
@@ -626,15 +621,16 @@ int autotune_into(Engine& engine, int32_t method, emerald_tuning* out) {
             if (out) {
                 *out = emerald_tuning{};
                 auto split = [](int v, int32_t& chunk, int32_t& prefetch) {
-                    chunk = v & ~kPrefetchLists;
-                    prefetch = (v & kPrefetchLists) ? 1 : 0;
+                    chunk = v & kChunkMask;
+                    prefetch = (v & kPersistentWarps) ? EMERALD_TUNE_PERSISTENT
+                                                      : ((v & kPrefetchLists) ? 1 : 0);
                 };
                 split(r.chosen.apply, out->apply_chunk, out->prefetch[0]);
                 split(r.chosen.divergence, out->divergence_chunk, out->prefetch[1]);
                 split(r.chosen.iisph_sum, out->iisph_sum_chunk, out->prefetch[2]);
                 split(r.chosen.iisph_beta, out->iisph_beta_chunk, out->prefetch[3]);
                 out->candidates = r.count;
-                for (int k = 0; k < r.count && k < 8; ++k) {
+                for (int k = 0; k < r.count && k < EMERALD_TUNE_CANDIDATES; ++k) {
                     Engine::Tuning const& t = r.candidates[k];
                     split(t.apply, out->candidate_chunks[k][0], out->candidate_prefetch[k][0]);
                     split(t.divergence, out->candidate_chunks[k][1], out->candidate_prefetch[k][1]);
@@ -664,10 +660,13 @@ int set_tuning_of(Engine& engine, emerald_tuning const* t) {
         if (chunks[k] != 1 && chunks[k] != 4 && chunks[k] != 8) {
             return fail(EMERALD_EINVAL, "chunks must be 1, 4 or 8");
         }
-        if (t->prefetch[k] != 0 && t->prefetch[k] != 1) {
-            return fail(EMERALD_EINVAL, "prefetch flags must be 0 or 1");
+        int32_t const mode = t->prefetch[k];
+        bool const persistent_ok = k < 2;  // the DFSPH_P families
+        if (mode != 0 && mode != 1 && !(mode == EMERALD_TUNE_PERSISTENT && persistent_ok)) {
+            return fail(EMERALD_EINVAL, "prefetch must be 0 or 1, or 2 for apply and divergence");
         }
-        v[k] = chunks[k] | (t->prefetch[k] ? kPrefetchLists : 0);
+        v[k] = chunks[k] | (mode == 1 ? kPrefetchLists : 0) |
+               (mode == EMERALD_TUNE_PERSISTENT ? kPersistentWarps : 0);
     }
     Engine::Tuning tu;
     tu.apply = v[0];
@@ -779,6 +778,12 @@ int emerald_server_get_stats(emerald_server* server, emerald_server_stats* out) 
 int emerald_sim_set_graphs(emerald_sim* sim, int32_t graphs) {
     if (!sim) return fail(EMERALD_EINVAL, "sim is NULL");
     sim->engine.set_graphs(graphs != 0);
+    return EMERALD_OK;
+}
+
+int emerald_sim_host_waits(emerald_sim* sim, int64_t* count) {
+    if (!sim || !count) return fail(EMERALD_EINVAL, "bad arguments");
+    *count = sim->engine.host_waits();
     return EMERALD_OK;
 }
 

@@ -120,7 +120,7 @@ size_t Engine::footprint(uint32_t fluid_capacity, uint32_t solid_capacity, int m
     size_t const scan_words = std::max(scan_scratch_words(uint32_t(ftab)),
                                        scan_scratch_words(uint32_t(stab))) + 64;
     bytes += r(4 * scan_words) + r(sizeof(int)) + r(sizeof(uint32_t)) +
-             r(sizeof(unsigned long long) * 4);
+             r(sizeof(unsigned long long) * kLoopSlots);
     return bytes;
 }
 
@@ -227,11 +227,12 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
     d_scan_ = static_cast<uint32_t*>(dev(4ull * scan_words));
     d_running_ = static_cast<int*>(dev(sizeof(int)));
     d_flag_ = static_cast<uint32_t*>(dev(sizeof(uint32_t)));
-    d_loop_iters_ = static_cast<unsigned long long*>(dev(sizeof(unsigned long long) * 4));
+    d_loop_iters_ = static_cast<unsigned long long*>(dev(sizeof(unsigned long long) * kLoopSlots));
     a_.loop_iterations = d_loop_iters_;
-    cudaMemset(d_loop_iters_, 0, sizeof(unsigned long long) * 4);
+    cudaMemset(d_loop_iters_, 0, sizeof(unsigned long long) * kLoopSlots);
     if (cudaStreamCreateWithFlags(&cap_st_, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&body_st_, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&frame_st_, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&side_st_, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming) != cudaSuccess) {
@@ -259,12 +260,16 @@ void Engine::destroy_graphs() {
     for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
     graphs_.clear();
     graph_fixed_kernels_.clear();
+    for (auto& kv : frame_graphs_) cudaGraphExecDestroy(kv.second);
+    frame_graphs_.clear();
+    frame_fixed_kernels_.clear();
 }
 
 Engine::~Engine() {
     destroy_graphs();
     if (cap_st_) cudaStreamDestroy(cap_st_);
     if (body_st_) cudaStreamDestroy(body_st_);
+    if (frame_st_) cudaStreamDestroy(frame_st_);
     if (side_st_) cudaStreamDestroy(side_st_);
     if (ev_fork_) cudaEventDestroy(ev_fork_);
     if (ev_join_) cudaEventDestroy(ev_join_);
@@ -319,7 +324,7 @@ void Engine::reset_timing() {
 
 KernelTimes const& Engine::kernel_times() {
     if (!pending_.empty()) {
-        cudaStreamSynchronize(st_);
+        host_wait(st_);
         for (auto& p : pending_) {
             float ms = 0.0f;
             cudaEventElapsedTime(&ms, p.start, p.stop);
@@ -625,7 +630,7 @@ void Engine::set_active(int id, bool active) {
     int32_t const v = active ? 1 : 0;
     cudaMemcpyAsync(reinterpret_cast<char*>(d_ss_ + id) + offsetof(SceneState, active), &v,
                     sizeof(int32_t), cudaMemcpyHostToDevice, st_);
-    cudaStreamSynchronize(st_);
+    host_wait(st_);
 }
 
 void Engine::set_mode(int id, int32_t mode, float fixed_dt, float fixed_t) {
@@ -689,7 +694,7 @@ void Engine::host_forces(int32_t method) {
                     hx_.data(), hv_.data());
         cudaMemcpyAsync(a_.tx + b, hf_.data(), 8ull * n, cudaMemcpyHostToDevice, st_);
         launch_scatter_f2(a_, b, n, a_.tx + b, a_.ext_f, st_);
-        cudaStreamSynchronize(st_);
+        host_wait(st_);
         check("host forces");
     }
 }
@@ -735,20 +740,20 @@ void Engine::emit_loop_body(int kind, int32_t method, cudaGraphConditionalHandle
         }
         break;
     case kIisph:
-        launch("iisph_sum_dij", [&] { launch_iisph_sum_dij(a_, tiles, st, tuning_.iisph_sum); });
-        launch("iisph_beta_pressure", [&] { launch_iisph_beta_pressure(a_, tiles, st, tuning_.iisph_beta); });
+        launch("iisph_sum_dij", [&] { launch_iisph_sum_dij(a_, tiles, st, tuning_.iisph_sum, compensated_); });
+        launch("iisph_beta_pressure", [&] { launch_iisph_beta_pressure(a_, tiles, st, tuning_.iisph_beta, compensated_); });
         break;
     case kIisphAp:
     case kIisphPseudoAp: {
         int const pseudo = method == kIisphPseudoAp ? 1 : 0;
-        launch("pressure_accel", [&] { launch_pressure_accel(a_, tiles, st); });
-        launch("ap_iterate", [&] { launch_ap_iterate(a_, tiles, pseudo, st); });
+        launch("pressure_accel", [&] { launch_pressure_accel(a_, tiles, st, compensated_); });
+        launch("ap_iterate", [&] { launch_ap_iterate(a_, tiles, pseudo, st, compensated_); });
         break;
     }
     case kPcisph:
         launch("pc_predict", [&] { launch_pc_predict(a_, tiles, st); });
-        launch("pc_density", [&] { launch_pc_density(a_, tiles, st); });
-        launch("pc_forces", [&] { launch_pc_forces(a_, tiles, st); });
+        launch("pc_density", [&] { launch_pc_density(a_, tiles, st, compensated_); });
+        launch("pc_forces", [&] { launch_pc_forces(a_, tiles, st, compensated_); });
         break;
     default: break;
     }
@@ -762,11 +767,12 @@ void Engine::emit_loop_body(int kind, int32_t method, cudaGraphConditionalHandle
 static int loop_body_kernels(int kind) { return kind == 3 ? 4 : 3; }
 
 int64_t Engine::kernel_launches() {
-    unsigned long long it[4] = {0, 0, 0, 0};
+    unsigned long long it[kLoopSlots] = {};
     cudaMemcpyAsync(it, d_loop_iters_, sizeof(it), cudaMemcpyDeviceToHost, st_);
-    cudaStreamSynchronize(st_);
+    host_wait(st_);
     int64_t n = host_launches_;
     for (int k = 0; k < 4; ++k) n += int64_t(it[k]) * loop_body_kernels(k);
+    for (int m = 0; m < 5; ++m) n += int64_t(it[4 + m]) * frame_body_kernels_[m];
     return n;
 }
 
@@ -821,7 +827,7 @@ void Engine::run_loop(int kind, int max_iter, int32_t method) {
         emit_loop_body(kind, method, 0, false);
         if (!unrolled_) {
             cudaMemcpyAsync(h_running_, d_running_, sizeof(int), cudaMemcpyDeviceToHost, cur_);
-            cudaStreamSynchronize(cur_);
+            host_wait(cur_);
             if (!*h_running_) break;
         }
     }
@@ -863,7 +869,10 @@ void Engine::emit_substep(int32_t method, bool reorder) {
     }
     switch (method) {
     case kDfsph:
-        launch("dfsph_density_alpha", [&] { launch_dfsph_density_alpha(a_, tiles, compensated_, st); });
+        launch("dfsph_density_alpha", [&] {
+            launch_dfsph_density_alpha(a_, tiles, compensated_, st,
+                                       (tuning_.divergence & kPersistentWarps) != 0);
+        });
         launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 0, compensated_, st, tuning_.apply); });
         run_loop(2, max_iterations(2), method);
         if (!capturing_ && has_force_callbacks()) host_forces(method);
@@ -873,20 +882,20 @@ void Engine::emit_substep(int32_t method, bool reorder) {
         break;
     case kIisph:
         if (!capturing_ && has_force_callbacks()) host_forces(method);
-        launch("iisph_density_dii", [&] { launch_iisph_density_dii(a_, tiles, st); });
-        launch("iisph_aii", [&] { launch_iisph_aii(a_, tiles, st); });
+        launch("iisph_density_dii", [&] { launch_iisph_density_dii(a_, tiles, st, compensated_); });
+        launch("iisph_aii", [&] { launch_iisph_aii(a_, tiles, st, compensated_); });
         run_loop(0, max_iterations(0), method);
         launch("make_q", [&] { launch_make_q(a_, tiles, st); });
-        launch("apply_integrate", [&] { launch_apply_integrate(a_, tiles, st); });
+        launch("apply_integrate", [&] { launch_apply_integrate(a_, tiles, st, compensated_); });
         break;
     case kIisphAp:
     case kIisphPseudoAp: {
         int const pseudo = method == kIisphPseudoAp ? 1 : 0;
         if (!capturing_ && has_force_callbacks()) host_forces(method);
-        launch("ap_density", [&] { launch_ap_density(a_, tiles, st); });
-        launch("ap_diag", [&] { launch_ap_diag(a_, tiles, pseudo, st); });
+        launch("ap_density", [&] { launch_ap_density(a_, tiles, st, compensated_); });
+        launch("ap_diag", [&] { launch_ap_diag(a_, tiles, pseudo, st, compensated_); });
         run_loop(0, max_iterations(0), method);
-        launch("ap_finish", [&] { launch_ap_finish(a_, tiles, pseudo, st); });
+        launch("ap_finish", [&] { launch_ap_finish(a_, tiles, pseudo, st, compensated_); });
         break;
     }
     case kPcisph:
@@ -904,7 +913,7 @@ void Engine::emit_substep(int32_t method, bool reorder) {
 // every kernel reads scene membership and parameters from device memory, so
 // the graph stays valid as scenes are added, removed or (de)activated.
 void Engine::capture_substep(int32_t method, bool reorder) {
-    cudaStreamSynchronize(st_);
+    host_wait(st_);
     if (cudaStreamBeginCapture(cap_st_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         throw std::runtime_error("graph capture: begin");
     }
@@ -937,6 +946,129 @@ void Engine::capture_substep(int32_t method, bool reorder) {
     graph_fixed_kernels_[method * 2 + (reorder ? 1 : 0)] = capture_kernels_;
 }
 
+// Records one frame of `method` into a graph: the storage-order re-sort
+// (when due), then a conditional while node whose body is one sub-step
+// followed by k_frame_check, which continues the loop while an active
+// scene's frame has sub-steps left. The solver loops inside the sub-step
+// are conditional nodes nested in that body.
+void Engine::capture_frame(int32_t method, bool reorder) {
+    host_wait(st_);
+    if (cudaStreamBeginCapture(cap_st_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        throw std::runtime_error("frame capture: begin");
+    }
+    capturing_ = true;
+    capture_kernels_ = 0;
+    cur_ = cap_st_;
+    cudaGraph_t g = nullptr;
+    auto abort = [&] {
+        cudaGraph_t dead = nullptr;
+        cudaStreamEndCapture(frame_st_, &dead);
+        cudaStreamEndCapture(cap_st_, &dead);
+        if (dead) cudaGraphDestroy(dead);
+        capturing_ = false;
+        cur_ = st_;
+    };
+    try {
+        launch("frame_begin", [&] { launch_frame_begin(a_, max_scenes_, cap_st_); });
+        if (reorder) {
+            int const bits = order_key_bits();
+            launch("reorder",
+                   [&] { launch_reorder(a_, order_sort_, ext_tiles_ * kTile, bits, cap_st_); },
+                   3 + 3 * (bits / 8));
+        }
+        cudaStreamCaptureStatus status;
+        cudaGraph_t outer = nullptr;
+        cudaGraphNode_t const* deps = nullptr;
+        size_t ndeps = 0;
+        if (cudaStreamGetCaptureInfo(cap_st_, &status, nullptr, &outer, &deps, &ndeps) !=
+              cudaSuccess ||
+            status != cudaStreamCaptureStatusActive) {
+            throw std::runtime_error("frame capture: no active capture");
+        }
+        cudaGraphConditionalHandle cond;
+        if (cudaGraphConditionalHandleCreate(&cond, outer, 1, cudaGraphCondAssignDefault) !=
+            cudaSuccess) {
+            throw std::runtime_error("frame capture: conditional handle");
+        }
+        cudaGraphNodeParams params{};
+        params.type = cudaGraphNodeTypeConditional;
+        params.conditional.handle = cond;
+        params.conditional.type = cudaGraphCondTypeWhile;
+        params.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (cudaGraphAddNode(&node, outer, deps, ndeps, &params) != cudaSuccess ||
+            cudaStreamUpdateCaptureDependencies(cap_st_, &node, 1,
+                                                cudaStreamSetCaptureDependencies) != cudaSuccess) {
+            throw std::runtime_error("frame capture: conditional node");
+        }
+        cudaGraph_t body = params.conditional.phGraph_out[0];
+        if (cudaStreamBeginCaptureToGraph(frame_st_, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            throw std::runtime_error("frame capture: body");
+        }
+        int64_t const outside = capture_kernels_;
+        cur_ = frame_st_;
+        emit_substep(method, false);
+        launch("frame_check",
+               [&] { launch_frame_check(a_, max_scenes_, method, cond, frame_st_); });
+        frame_body_kernels_[method] = capture_kernels_ - outside;
+        capture_kernels_ = outside;
+        if (cudaStreamEndCapture(frame_st_, &body) != cudaSuccess) {
+            throw std::runtime_error("frame capture: body end");
+        }
+        cur_ = cap_st_;
+    } catch (...) {
+        abort();
+        throw;
+    }
+    capturing_ = false;
+    cur_ = st_;
+    if (cudaStreamEndCapture(cap_st_, &g) != cudaSuccess) {
+        throw std::runtime_error("frame capture: end");
+    }
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t const e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        throw std::runtime_error(std::string("frame graph instantiate: ") + cudaGetErrorString(e));
+    }
+    frame_graphs_[method * 2 + (reorder ? 1 : 0)] = exec;
+    frame_fixed_kernels_[method * 2 + (reorder ? 1 : 0)] = capture_kernels_;
+}
+
+int Engine::frame(int id, int32_t method, SceneState& out) {
+    if (!use_graphs_ || timing_ || has_force_callbacks() || active_scenes() != 1 ||
+        !scenes_[id].active) {
+        // host loop: one sub-step at a time, the frame's end read after each
+        int n = 0;
+        do {
+            substep(method);
+            ++n;
+            out = scene_state(id);
+        } while (out.remaining > 0 && n < 100000);
+        return n;
+    }
+    prepare_substep(method);
+    bool const reorder = reorder_every_ > 0 && (frames_launched_ % 2) == 0;
+    ++frames_launched_;
+    int const key = method * 2 + (reorder ? 1 : 0);
+    auto it = frame_graphs_.find(key);
+    if (it == frame_graphs_.end()) {
+        capture_frame(method, reorder);
+        it = frame_graphs_.find(key);
+    }
+    if (cudaGraphLaunch(it->second, st_) != cudaSuccess) {
+        check("frame graph launch");
+        throw std::runtime_error("frame graph launch failed");
+    }
+    int64_t const fixed = frame_fixed_kernels_[key];
+    host_launches_ += fixed;
+    g_launches.fetch_add(fixed, std::memory_order_relaxed);
+    out = scene_state(id);
+    substeps_launched_ += out.call_substeps;
+    return out.call_substeps;
+}
+
 // Tunings chosen by autotune, per (method, log2 of the active particle
 // count); engines of the same size class start from them.
 namespace {
@@ -952,8 +1084,9 @@ uint64_t Engine::tuning_key(int32_t method) const {
     return uint64_t(method) * 64u + ceil_log2(std::max<uint64_t>(n, 1));
 }
 
-void Engine::substep(int32_t method) {
-    if (active_scenes() == 0) return;
+// Tuning cache lookup and per-scene method parameters before a sub-step or
+// frame of `method`.
+void Engine::prepare_substep(int32_t method) {
     if (!tuning_locked_ && !tuning_pinned_) {
         std::lock_guard<std::mutex> lock(g_tuning_mutex);
         auto const it = g_tuning_cache.find(tuning_key(method));
@@ -973,6 +1106,11 @@ void Engine::substep(int32_t method) {
             upload_params(id);
         }
     }
+}
+
+void Engine::substep(int32_t method) {
+    if (active_scenes() == 0) return;
+    prepare_substep(method);
     bool const reorder = reorder_every_ > 0 && (substeps_launched_ % reorder_every_) == 0;
     ++substeps_launched_;
     if (use_graphs_ && !timing_ && !has_force_callbacks()) {
@@ -1017,7 +1155,7 @@ Engine::TuneReport Engine::autotune(int32_t method, int substeps) {
     Region const regions[] = {{a_.x, 8 * N},      {a_.v, 8 * N},         {a_.kdiv, 4 * N},
                               {a_.kdens, 4 * N},  {a_.x64, 16 * N},      {a_.oid, 4 * N},
                               {a_.slot_of, 4 * N}, {d_ss_, sizeof(SceneState) * size_t(max_scenes_)},
-                              {d_loop_iters_, sizeof(unsigned long long) * 4}};
+                              {d_loop_iters_, sizeof(unsigned long long) * kLoopSlots}};
     size_t bytes = 0;
     for (auto const& r : regions) bytes += r.size;
     char* snap = nullptr;
@@ -1044,9 +1182,12 @@ Engine::TuneReport Engine::autotune(int32_t method, int substeps) {
     if (method == kDfsph) {
         // chunks, with kPrefetchLists (P) where the warps first ask L2 for
         // their list rows: it pays when the lists do not stay in L2
+        // and with kPersistentWarps (W), the persistent-warp kernels
         int const P = kPrefetchLists;
+        int const W = kPersistentWarps;
         int const opts[][2] = {{4, 8}, {1, 4}, {4, 4}, {1, 8}, {8, 8},
-                               {1 | P, 4 | P}, {4 | P, 8 | P}, {1 | P, 4}};
+                               {1 | P, 4 | P}, {4 | P, 8 | P}, {1 | P, 4},
+                               {1 | W, 4 | W}, {4 | W, 4 | W}, {1 | W, 1 | W}, {4 | W, 8 | W}};
         for (auto const& o : opts) {
             Tuning t = tuning_;
             t.apply = o[0];
@@ -1082,6 +1223,7 @@ Engine::TuneReport Engine::autotune(int32_t method, int substeps) {
             cudaEventRecord(e0, st_);
             for (int q = 0; q < substeps; ++q) substep(method);
             cudaEventRecord(e1, st_);
+            ++host_waits_;
             cudaEventSynchronize(e1);
             float ms = 0.0f;
             cudaEventElapsedTime(&ms, e0, e1);
@@ -1101,7 +1243,7 @@ Engine::TuneReport Engine::autotune(int32_t method, int substeps) {
     }
     rep.count = int(cand.size());
     tuning_locked_ = false;
-    cudaStreamSynchronize(st_);
+    host_wait(st_);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(snap);
@@ -1131,7 +1273,7 @@ void Engine::set_tuning(Tuning const* t) {
 SceneState Engine::scene_state(int id) {
     SceneState s{};
     cudaMemcpyAsync(&s, d_ss_ + id, sizeof(SceneState), cudaMemcpyDeviceToHost, st_);
-    cudaStreamSynchronize(st_);
+    host_wait(st_);
     check("scene_state");
     return s;
 }
@@ -1139,7 +1281,7 @@ SceneState Engine::scene_state(int id) {
 std::vector<SceneState> Engine::all_states() {
     std::vector<SceneState> s(max_scenes_);
     cudaMemcpyAsync(s.data(), d_ss_, sizeof(SceneState) * max_scenes_, cudaMemcpyDeviceToHost, st_);
-    cudaStreamSynchronize(st_);
+    host_wait(st_);
     check("all_states");
     return s;
 }
@@ -1157,7 +1299,7 @@ void Engine::get_state(int id, float* x, float* v, bool sync) {
         launch_gather_f2(a_, b, n, a_.v, a_.tv + b, st_);
         cudaMemcpyAsync(v, a_.tv + b, 8ull * n, cudaMemcpyDeviceToHost, st_);
     }
-    if (sync) cudaStreamSynchronize(st_);
+    if (sync) host_wait(st_);
     check("get_state");
 }
 
@@ -1177,7 +1319,7 @@ bool Engine::set_state(int id, float const* x, float const* v, bool sync) {
         launch_flag_nonfinite(reinterpret_cast<float const*>(a_.tv + b), 2ull * n, d_flag_, st_);
     }
     cudaMemcpyAsync(h_flag_, d_flag_, sizeof(uint32_t), cudaMemcpyDeviceToHost, st_);
-    cudaStreamSynchronize(st_);
+    host_wait(st_);
     check("set_state");
     if (*h_flag_) return false;
     if (x) {
@@ -1185,7 +1327,7 @@ bool Engine::set_state(int id, float const* x, float const* v, bool sync) {
         launch_positions_to_double(a_, b, n, st_);
     }
     if (v) launch_scatter_f2(a_, b, n, a_.tv + b, a_.v, st_);
-    if (sync) cudaStreamSynchronize(st_);
+    if (sync) host_wait(st_);
     check("set_state");
     return true;
 }
@@ -1248,7 +1390,7 @@ void Engine::snapshot(int id, void* out) {
     cudaMemcpyAsync(p + 8ull * ns, a_.vs + P.solid_begin, 8ull * ns, cudaMemcpyDeviceToHost, st_);
     cudaMemcpyAsync(p + 16ull * ns, a_.vols + P.solid_begin, 4ull * ns, cudaMemcpyDeviceToHost,
                     st_);
-    cudaStreamSynchronize(st_);
+    host_wait(st_);
     check("snapshot");
 }
 
@@ -1288,7 +1430,7 @@ void Engine::restore(int id, void const* data, size_t bytes) {
         launch_scatter_d2(a_, b, n, a_.tx64 + b, a_.x64, st_);
         p += 16ull * n;
     }
-    cudaStreamSynchronize(st_);
+    host_wait(st_);
     check("restore");
     float const* sxy = reinterpret_cast<float const*>(p);
     set_solid(id, sxy, sxy + 2ull * ns, sxy + 4ull * ns);
@@ -1297,7 +1439,7 @@ void Engine::restore(int id, void const* data, size_t bytes) {
     int32_t const active = scenes_[id].active ? 1 : 0;
     s.active = active;
     cudaMemcpyAsync(d_ss_ + id, &s, sizeof(s), cudaMemcpyHostToDevice, st_);
-    cudaStreamSynchronize(st_);
+    host_wait(st_);
     check("restore");
 }
 
@@ -1308,7 +1450,7 @@ void Engine::get_solid(int id, float* xy, float* volumes) {
         cudaMemcpyAsync(volumes, a_.vols + P.solid_begin, 4ull * P.solid_count,
                         cudaMemcpyDeviceToHost, st_);
     }
-    cudaStreamSynchronize(st_);
+    host_wait(st_);
     check("get_solid");
 }
 
@@ -1319,7 +1461,7 @@ void Engine::set_solid(int id, float const* xy, float const* v, float const* vol
     if (!n) return;
     if (xy) {
         cudaMemcpyAsync(a_.xs + b, xy, 8ull * n, cudaMemcpyHostToDevice, st_);
-        cudaStreamSynchronize(st_);
+        host_wait(st_);
         if (sc.near_words) near_words_.release(P.near_begin, sc.near_words);
         build_near_map(sc, xy, n);
         upload_params(id);
@@ -1331,7 +1473,7 @@ void Engine::set_solid(int id, float const* xy, float const* v, float const* vol
     } else if (xy) {
         launch("solid_volumes", [&] { launch_solid_volumes(a_, ext_stiles_, 1.7f, id, st_); });
     }
-    cudaStreamSynchronize(st_);
+    host_wait(st_);
     check("set_solid");
 }
 
@@ -1393,7 +1535,7 @@ bool Engine::get_array(int id, std::string const& name, float* out, int& width) 
             launch_gather_f(a_, b, n, static_cast<float const*>(src), a_.tkdiv + b, st_);
             cudaMemcpyAsync(out, a_.tkdiv + b, 4ull * n, cudaMemcpyDeviceToHost, st_);
         }
-        cudaStreamSynchronize(st_);
+        host_wait(st_);
         check("get_array");
     }
     return true;
@@ -1428,7 +1570,7 @@ void Engine::get_neighbors(int id, bool solid, uint8_t* counts, uint32_t* idx, f
     std::vector<uint32_t> oid(n), slot_of(n);
     cudaMemcpyAsync(oid.data(), a_.oid + P.fluid_begin, 4ull * n, cudaMemcpyDeviceToHost, st_);
     cudaMemcpyAsync(slot_of.data(), a_.slot_of + P.fluid_begin, 4ull * n, cudaMemcpyDeviceToHost, st_);
-    cudaStreamSynchronize(st_);
+    host_wait(st_);
     check("get_neighbors");
     uint32_t const base = solid ? P.solid_begin : P.fluid_begin;
     for (uint32_t i = 0; i < n; ++i) {
@@ -1505,7 +1647,7 @@ size_t Engine::get_sort(int id, bool solid, int32_t* gc, uint64_t* z, uint64_t* 
     cudaMemcpyAsync(hpi.data(), d_pi, 4 * words, cudaMemcpyDeviceToHost, st_);
     if (block_indices) cudaMemcpyAsync(block_indices, d_bi, 4 * words, cudaMemcpyDeviceToHost, st_);
     cudaMemcpyAsync(hbl.data(), d_bl, 8 * words, cudaMemcpyDeviceToHost, st_);
-    cudaStreamSynchronize(st_);
+    host_wait(st_);
     cudaFree(out);
     check("get_sort");
     if (pair_index) {

@@ -76,8 +76,8 @@ public:
     struct TuneReport {
         Tuning chosen;
         int count;               // candidates timed
-        Tuning candidates[8];
-        float ms[8];             // mean sub-step time of each candidate
+        Tuning candidates[16];
+        float ms[16];            // mean sub-step time of each candidate
     };
     Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes);
     ~Engine();
@@ -189,6 +189,13 @@ public:
     // Kernels this engine launched (graph nodes included, loop bodies
     // counted per executed iteration).
     int64_t kernel_launches();
+    // Times this engine waited on the host for the device.
+    int64_t host_waits() const { return host_waits_; }
+    // One frame of the single resident scene (emerald_sim_frame): with
+    // graphs, one graph launch (re-sort, then a conditional while node
+    // around the sub-step while the frame has sub-steps left) and one host
+    // wait; returns the sub-steps run and the scene's state after them.
+    int frame(int id, int32_t method, SceneState& out);
 
     void check(char const* what);
 
@@ -235,6 +242,18 @@ private:
     void update_sort_bases();
     int order_key_bits() const;
     void destroy_graphs();
+    void capture_frame(int32_t method, bool reorder);
+    void prepare_substep(int32_t method);
+    int64_t frames_launched_ = 0;
+    void host_wait(cudaStream_t s) {
+        ++host_waits_;
+        cudaStreamSynchronize(s);
+    }
+    int64_t host_waits_ = 0;
+    cudaStream_t frame_st_ = nullptr;                  // frame-loop body capture
+    std::map<int32_t, cudaGraphExec_t> frame_graphs_;  // key: method * 2 + reorder
+    std::map<int32_t, int64_t> frame_fixed_kernels_;   // per graph, outside the loop
+    int64_t frame_body_kernels_[5] = {0, 0, 0, 0, 0};  // per method, one frame iteration
     int max_iterations(int kind) const;
     void rebuild_solids();
     // Boundary-proximity map of a scene from its boundary positions.

@@ -23,6 +23,7 @@ namespace emerald {
 constexpr int kTile = 128;
 constexpr int kMaxNeighbors = 64;
 constexpr uint64_t kEmptyKey = ~0ull;
+constexpr int kLoopSlots = 9;  // Arena::loop_iterations entries
 
 enum Method : int { kPcisph = 0, kIisph = 1, kIisphAp = 2, kIisphPseudoAp = 3, kDfsph = 4 };
 
@@ -103,7 +104,7 @@ struct SceneState {
     int32_t stat_div_iters;
     int32_t error;
     int32_t substeps_total;
-    int32_t pad;
+    int32_t call_substeps;  // sub-steps run by the current frame-graph launch
     double err_sum_d;  // exact sum of the errors (DFSPH loops)
     double stat_avg_exact, stat_div_avg_exact;
 };
@@ -112,7 +113,9 @@ struct SceneState {
 struct Arena {
     SceneParams const* sp;
     SceneState* ss;
-    unsigned long long* loop_iterations;  // executed solver iterations per loop kind
+    // executed solver iterations per loop kind (0-3), then sub-steps run by
+    // frame graphs per method (4 + method)
+    unsigned long long* loop_iterations;
     int32_t const* tile_scene;   // fluid tile -> scene (-1: free)
     int32_t const* stile_scene;  // solid tile -> scene
     uint32_t stride;             // fluid arena capacity (multiple of kTile)

@@ -65,17 +65,30 @@ void launch_identity_order(Arena const& a, uint32_t begin, uint32_t count, cudaS
 
 // solver (solve_kernels.cu)
 void launch_max_v2(Arena const& a, uint32_t tiles, cudaStream_t st);
+// frame graphs: zero the per-launch sub-step counts; after each sub-step,
+// count it and set `cond` while an active scene's frame has sub-steps left
+void launch_frame_begin(Arena const& a, int nscenes, cudaStream_t st);
+void launch_frame_check(Arena const& a, int nscenes, int method, cudaGraphConditionalHandle cond,
+                        cudaStream_t st);
 void launch_begin_substep(Arena const& a, int nscenes, cudaStream_t st);
 void launch_zero_kappas(Arena const& a, uint32_t tiles, cudaStream_t st);
 void launch_iter_reset(Arena const& a, int nscenes, int kind, cudaStream_t st);
 void launch_iter_check(Arena const& a, int nscenes, int kind, int* running,
                        cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st);
 // comp: some resident scene is in compensated mode (selects the kernel variant)
-void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st);
+// persistent: the persistent-warp variant (same bits)
+void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st,
+                                bool persistent = false);
 // chunk: neighbour entries loaded together in the gather sums (1, 4 or 8;
 // every choice gives the same bits), plus kPrefetchLists to have each warp
 // ask L2 for its list rows before the sums
 constexpr int kPrefetchLists = 16;
+// kPersistentWarps selects the persistent-warp kernels of a gather family:
+// a grid of resident blocks whose warps walk their tiles with the next
+// tile's lists already requested into L2 (same bits; kPrefetchLists is
+// implied)
+constexpr int kPersistentWarps = 32;
+constexpr int kChunkMask = 15;
 void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int external,
                             int skip_done, bool comp, cudaStream_t st, int chunk = 4);
 void launch_dfsph_divergence(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st,
@@ -83,22 +96,25 @@ void launch_dfsph_divergence(Arena const& a, uint32_t tiles, bool comp, cudaStre
 void launch_dfsph_density(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st,
                           int chunk = 8);
 void launch_integrate_positions(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st);
-void launch_iisph_density_dii(Arena const& a, uint32_t tiles, cudaStream_t st);
-void launch_iisph_aii(Arena const& a, uint32_t tiles, cudaStream_t st);
-void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk = 4);
-void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st,
-                                int chunk = 4);
+// comp (the IISPH, IISPH_AP, IISPH_PSEUDO_AP and PCISPH kernels below): some
+// resident scene is in compensated mode; its neighbour sums are then
+// Kahan-compensated
+void launch_iisph_density_dii(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp);
+void launch_iisph_aii(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp);
+void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk, bool comp);
+void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk,
+                                bool comp);
 void launch_make_q(Arena const& a, uint32_t tiles, cudaStream_t st);
-void launch_apply_integrate(Arena const& a, uint32_t tiles, cudaStream_t st);
-void launch_ap_density(Arena const& a, uint32_t tiles, cudaStream_t st);
-void launch_ap_diag(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st);
-void launch_pressure_accel(Arena const& a, uint32_t tiles, cudaStream_t st);
-void launch_ap_iterate(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st);
-void launch_ap_finish(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st);
+void launch_apply_integrate(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp);
+void launch_ap_density(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp);
+void launch_ap_diag(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st, bool comp);
+void launch_pressure_accel(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp);
+void launch_ap_iterate(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st, bool comp);
+void launch_ap_finish(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st, bool comp);
 void launch_pc_init(Arena const& a, uint32_t tiles, cudaStream_t st);
 void launch_pc_predict(Arena const& a, uint32_t tiles, cudaStream_t st);
-void launch_pc_density(Arena const& a, uint32_t tiles, cudaStream_t st);
-void launch_pc_forces(Arena const& a, uint32_t tiles, cudaStream_t st);
+void launch_pc_density(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp);
+void launch_pc_forces(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp);
 void launch_pc_final(Arena const& a, uint32_t tiles, cudaStream_t st);
 
 }  // namespace emerald

@@ -11,6 +11,8 @@
 // reference's error reductions per scene (integer sum of error*1000 and the
 // maximum), and a one-block check kernel applies the reference's exit test
 // and marks finished scenes, whose later iteration launches return at once.
+#include <algorithm>
+
 #include "engine_types.cuh"
 #include "kernels.cuh"
 #include "sph_math.cuh"
@@ -184,6 +186,33 @@ __global__ void k_begin_substep(Arena a, int nscenes) {
     S.max_v2 = 0;
 }
 
+// Start of a frame-graph launch: no sub-step of it has run yet.
+__global__ void k_frame_begin(Arena a, int nscenes) {
+    int const s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nscenes) a.ss[s].call_substeps = 0;
+}
+
+// End of one sub-step inside a frame graph: counts it, and keeps the frame
+// loop going while an active scene's frame has sub-steps left (the host
+// loop of std_adaptive_time_step, emerald/sph2d_box/adaptive_time_step.h:74-103,
+// as a while node).
+__global__ void k_frame_check(Arena a, int nscenes, int method, cudaGraphConditionalHandle cond) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int s = threadIdx.x; s < nscenes; s += blockDim.x) {
+        SceneState& S = a.ss[s];
+        if (!S.active) continue;
+        S.call_substeps += 1;
+        if (S.remaining > 0) any = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        a.loop_iterations[4 + method] += 1ull;
+        cudaGraphSetConditional(cond, any ? 1u : 0u);
+    }
+}
+
 // Per-frame reset of the DFSPH kappas (dfsph_p.cpp:214-229), fixed-dt mode.
 __global__ void k_zero_kappas(Arena a) {
     Ctx c;
@@ -343,28 +372,31 @@ __device__ __forceinline__ void fold_fluid_list(Arena const& a, uint32_t i, int 
     }
 }
 
-// compute_densities (emerald/sph_common/density.cpp:10-73).
+// compute_densities (emerald/sph_common/density.cpp:10-73); with K each
+// sum is Kahan-compensated.
+template <bool K = false>
 __device__ __forceinline__ float density_of(Arena const& a, SceneParams const& P, uint32_t i) {
     size_t const stride = a.stride;
     float const rho0 = P.rho0;
     float const fmass = rho0 * P.fluid_volume;
-    float d = P.fluid_volume * rho0 * P.w0;
+    SumF<K> d(P.fluid_volume * rho0 * P.w0);
     int const c = a.nf_cnt[i];
     #pragma unroll 4
 
-    for (int k = 0; k < c; ++k) d += a.nf_w[k * stride + i] * fmass;
+    for (int k = 0; k < c; ++k) d.add(a.nf_w[k * stride + i] * fmass);
+    float out = d.get();
     int const cs = a.ns_cnt[i];
     if (cs) {
-        float db = 0.0f;
+        SumF<K> db;
         #pragma unroll 4
 
         for (int k = 0; k < cs; ++k) {
             size_t const e = k * stride + i;
-            db += a.ns_w[e] * (rho0 * a.vols[a.ns_idx[e]]);
+            db.add(a.ns_w[e] * (rho0 * a.vols[a.ns_idx[e]]));
         }
-        d += db;
+        out += db.get();
     }
-    return d;
+    return out;
 }
 
 // compute_divergences (emerald/sph_common/divergence.cpp:5-74).
@@ -461,7 +493,9 @@ __device__ __forceinline__ float2 apply_pressure_of(Arena const& a, SceneParams 
     return v;
 }
 
-// compute_pressure_accelerations (emerald/sph_common/pressure.cpp:83-178).
+// compute_pressure_accelerations (emerald/sph_common/pressure.cpp:83-178);
+// with K each sum is Kahan-compensated.
+template <bool K = false>
 __device__ __forceinline__ float2 pressure_accel_of(Arena const& a, SceneParams const& P, uint32_t i,
                                                     float const* q) {
     size_t const stride = a.stride;
@@ -471,25 +505,25 @@ __device__ __forceinline__ float2 pressure_accel_of(Arena const& a, SceneParams 
     float2 out = mk2(0.0f, 0.0f);
     int const c = a.nf_cnt[i];
     if (c) {
-        float2 acc = mk2(0.0f, 0.0f);
+        SumF2<K> acc;
         #pragma unroll 4
 
         for (int k = 0; k < c; ++k) {
             size_t const e = k * stride + i;
-            acc = add2(acc, scl2(neg_fmass * (qi + q[a.nf_idx[e]]), a.nf_gw[e]));
+            acc.add(scl2(neg_fmass * (qi + q[a.nf_idx[e]]), a.nf_gw[e]));
         }
-        out = acc;
+        out = acc.get();
     }
     int const cs = a.ns_cnt[i];
     if (cs) {
-        float2 acc = mk2(0.0f, 0.0f);
+        SumF2<K> acc;
         #pragma unroll 4
 
         for (int k = 0; k < cs; ++k) {
             size_t const e = k * stride + i;
-            acc = add2(acc, scl2(-(rho0 * a.vols[a.ns_idx[e]]) * qi, a.ns_gw[e]));
+            acc.add(scl2(-(rho0 * a.vols[a.ns_idx[e]]) * qi, a.ns_gw[e]));
         }
-        out = add2(out, acc);
+        out = add2(out, acc.get());
     }
     return out;
 }
@@ -713,6 +747,230 @@ __global__ void k_dfsph_density(Arena a) {
                      err, c.live, true);
 }
 
+// ------------------------------------------ persistent-warp gather kernels
+//
+// The DFSPH sums above, launched as one grid of resident blocks: warp w of
+// the G warps folds the 32-particle warp tiles w, w + G, w + 2G, ... (a warp
+// tile lies inside one 128-particle tile, so in one scene). While it folds
+// tile t, the list rows, count bytes and per-particle inputs of tile t + G
+// are already on their way into L2 (asked for with the counts it loaded one
+// tile earlier) and the counts of tile t + 2G are loading, so the lists
+// stream from HBM behind the folds instead of in front of them. Each
+// particle's sums are the same operations in the same order as in the
+// block-per-tile kernels, so the bits are theirs. Error sums gather per warp
+// and go to the scene's accumulators when the warp's next tile belongs to
+// another scene, and at the end.
+
+__device__ __forceinline__ void prefetch_l2(void const* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// L2 requests for a warp tile's fluid list rows (rows below the warp's
+// largest count; kernel values or indices, and the gradients) and for up to
+// five 128-byte lines of per-particle data, lane k asking for line k.
+template <bool W>
+__device__ __forceinline__ void prefetch_warp_tile(Arena const& a, uint32_t base, int count,
+                                                   void const* l0, void const* l1, void const* l2,
+                                                   void const* l3 = nullptr,
+                                                   void const* l4 = nullptr) {
+    int const lane = threadIdx.x & 31;
+    int const rows = static_cast<int>(__reduce_max_sync(0xffffffffu, uint32_t(count)));
+    if (lane < rows) {
+        size_t const e = static_cast<size_t>(lane) * a.stride + base;
+        prefetch_l2(W ? static_cast<void const*>(a.nf_w + e) : static_cast<void const*>(a.nf_idx + e));
+        prefetch_l2(a.nf_gw + e);
+        prefetch_l2(a.nf_gw + e + 16);
+    }
+    void const* const p = lane == 0 ? l0
+                        : lane == 1 ? l1
+                        : lane == 2 ? l2
+                        : lane == 3 ? l3
+                        : lane == 4 ? l4
+                                    : nullptr;
+    if (p) prefetch_l2(p);
+}
+
+struct WarpErr {
+    int32_t scene;
+    unsigned long long sum;
+    uint32_t max;
+    double exact;
+};
+
+__device__ __forceinline__ void flush_err(Arena const& a, WarpErr& e) {
+    if (e.scene >= 0) {
+        unsigned long long v = e.sum;
+        uint32_t m = e.max;
+        double d = e.exact;
+        for (int o = 16; o; o >>= 1) {
+            v += __shfl_xor_sync(0xffffffffu, v, o);
+            m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+            d += __shfl_xor_sync(0xffffffffu, d, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            SceneState* S = &a.ss[e.scene];
+            if (v) atomicAdd(&S->err_sum, v);
+            if (m) atomicMax(&S->err_max, m);
+            if (d != 0.0) atomicAdd(&S->err_sum_d, d);
+        }
+    }
+    e = WarpErr{-1, 0ull, 0u, 0.0};
+}
+
+// accumulate_error's contribution of one particle, kept in the warp.
+__device__ __forceinline__ void add_err(Arena const& a, WarpErr& e, int32_t scene, float err,
+                                        bool live) {
+    if (scene != e.scene) {
+        flush_err(a, e);
+        e.scene = scene;
+    }
+    if (live) {
+        e.sum += static_cast<unsigned long long>(static_cast<long long>(err * 1000.0f));
+        if (err == err && err > 0.0f) {
+            e.max = max(e.max, __float_as_uint(err));
+            e.exact += static_cast<double>(err);
+        }
+    }
+}
+
+// Walks this warp's tiles: prefetch(base, count) asks L2 for a tile's data,
+// body(scene, i, live) folds particle i of an active tile. Every lane of
+// the warp runs every iteration (tile checks are warp-uniform).
+template <class Prefetch, class Body>
+__device__ __forceinline__ void walk_warp_tiles(Arena const& a, uint32_t wtiles, bool skip_done,
+                                                Prefetch prefetch, Body body) {
+    uint32_t const lane = threadIdx.x & 31u;
+    uint32_t const G = (gridDim.x * blockDim.x) >> 5;
+    uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (t >= wtiles) return;
+    int cnt_next = (t + G < wtiles) ? int(a.nf_cnt[(t + G) * 32u + lane]) : 0;
+    prefetch(t * 32u, int(a.nf_cnt[t * 32u + lane]));
+    for (; t < wtiles; t += G) {
+        uint32_t const tn = t + G;
+        int cnt_after = 0;
+        if (tn < wtiles) {
+            prefetch(tn * 32u, cnt_next);
+            if (tn + G < wtiles) cnt_after = int(a.nf_cnt[(tn + G) * 32u + lane]);
+        }
+        int32_t const s = a.tile_scene[t / (kTile / 32)];
+        if (s >= 0) {
+            SceneState const& S = a.ss[s];
+            if (S.active && !(skip_done && S.done)) {
+                SceneParams const& P = a.sp[s];
+                uint32_t const i = t * 32u + lane;
+                body(s, i, (i - P.fluid_begin) < P.fluid_count);
+            }
+        }
+        cnt_next = cnt_after;
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kTile) k_dfsph_density_alpha_pw(Arena a, uint32_t wtiles) {
+    walk_warp_tiles(
+      a, wtiles, false,
+      [&](uint32_t base, int count) {
+          prefetch_warp_tile<true>(a, base, count, a.ns_cnt + base, a.kdiv + base, a.kdens + base);
+      },
+      [&](int32_t s, uint32_t i, bool live) {
+          if (!live) return;
+          Ctx const c{s, i, true};
+          if (MODE && a.sp[s].precision) {
+              dfsph_density_alpha<true>(a, c);
+          } else {
+              dfsph_density_alpha<false>(a, c);
+          }
+      });
+}
+
+template <int MODE, int CH>
+__global__ void __launch_bounds__(kTile) k_apply_pressures_pw(Arena a, uint32_t wtiles, int which_q,
+                                                            int external, int skip_done) {
+    float const* q = which_q ? a.qdens : a.qdiv;
+    walk_warp_tiles(
+      a, wtiles, skip_done != 0,
+      [&](uint32_t base, int count) {
+          prefetch_warp_tile<false>(a, base, count, a.ns_cnt + base, a.v + base, a.v + base + 16,
+                                    q + base);
+      },
+      [&](int32_t s, uint32_t i, bool live) {
+          if (!live) return;
+          SceneParams const& P = a.sp[s];
+          float const dt = a.ss[s].dt;
+          float2 v = a.v[i];
+          if (external) v = integrate_external(a, P, i, v, dt);
+          a.v[i] = (MODE && P.precision) ? apply_pressure_of<true, CH>(a, P, i, v, q, dt)
+                                         : apply_pressure_of<false, CH>(a, P, i, v, q, dt);
+      });
+}
+
+template <int MODE, int CH>
+__global__ void __launch_bounds__(kTile) k_dfsph_divergence_pw(Arena a, uint32_t wtiles) {
+    WarpErr e{-1, 0ull, 0u, 0.0};
+    walk_warp_tiles(
+      a, wtiles, true,
+      [&](uint32_t base, int count) {
+          prefetch_warp_tile<false>(a, base, count, a.ns_cnt + base, a.v + base, a.v + base + 16,
+                                    a.alpha + base, a.rho + base);
+      },
+      [&](int32_t s, uint32_t i, bool live) {
+          SceneParams const& P = a.sp[s];
+          float const dt = a.ss[s].dt;
+          float err = 0.0f;
+          if (live) {
+              float const d = (MODE && P.precision) ? divergence_of<true, CH>(a, P, i)
+                                                    : divergence_of<false, CH>(a, P, i);
+              a.rho_star[i] = d;
+              float kappa = 0.0f;
+              if (!(d <= 0.0f)) {
+                  float const numer = d * a.alpha[i];
+                  kappa = safe_f(numer, dt) ? numer / dt : 0.0f;
+              }
+              a.kdiv[i] = kappa;
+              a.qdiv[i] = p_over_rho2(kappa, a.rho[i]);
+              err = d <= 0.0f ? 0.0f : (dt * d / P.rho0);
+          }
+          add_err(a, e, s, err, live);
+      });
+    flush_err(a, e);
+}
+
+template <int MODE, int CH>
+__global__ void __launch_bounds__(kTile) k_dfsph_density_pw(Arena a, uint32_t wtiles) {
+    WarpErr e{-1, 0ull, 0u, 0.0};
+    walk_warp_tiles(
+      a, wtiles, true,
+      [&](uint32_t base, int count) {
+          prefetch_warp_tile<false>(a, base, count, a.ns_cnt + base, a.v + base, a.v + base + 16,
+                                    a.alpha + base, a.rho + base);
+      },
+      [&](int32_t s, uint32_t i, bool live) {
+          SceneParams const& P = a.sp[s];
+          float const dt = a.ss[s].dt;
+          float const rho0 = P.rho0;
+          float err = 0.0f;
+          if (live) {
+              float const rho = a.rho[i];
+              float const div = (MODE && P.precision) ? divergence_of<true, CH>(a, P, i)
+                                                      : divergence_of<false, CH>(a, P, i);
+              float const star = max_0x(rho + (dt * div));
+              a.rho_star[i] = star;
+              float const delta = star - rho0;
+              float kappa = 0.0f;
+              if (!(delta <= 0.0f)) {
+                  float const numer = delta * a.alpha[i];
+                  float const dd = sqrf(dt);
+                  kappa = safe_f(numer, dd) ? numer / dd : 0.0f;
+              }
+              a.kdens[i] = kappa;
+              a.qdens[i] = p_over_rho2(kappa, rho);
+              err = delta <= 0.0f ? 0.0f : (delta / rho0);
+          }
+          add_err(a, e, s, err, live);
+      });
+    flush_err(a, e);
+}
+
 // integrate_positions_in_place (dynamics.cpp:46-51). Compensated mode
 // accumulates the positions in double and stores their float rounding.
 // x_i += dt * v (+ shift): the reference's FP32 update, or for a
@@ -755,15 +1013,16 @@ __global__ void k_integrate_positions(Arena a) {
 
 // compute_densities, integrate_velocities_in_place and iisph_compute_diis
 // (iisph_ops.cpp:20-90), plus the zero initial pressures (iisph.cpp:76).
-__global__ void k_iisph_density_dii(Arena a) {
-    Ctx c;
-    if (!enter(a, false, c) || !c.live) return;
+// MODE 1 launches (some resident scene in compensated mode) Kahan-compensate
+// the sums of compensated scenes, here and in the kernels below.
+template <bool K>
+__device__ __forceinline__ void iisph_density_dii(Arena const& a, Ctx const& c) {
     SceneParams const& P = a.sp[c.s];
     uint32_t const i = c.i;
     size_t const stride = a.stride;
     float const dt = a.ss[c.s].dt;
     float const rho0 = P.rho0;
-    float const d = density_of(a, P, i);
+    float const d = density_of<K>(a, P, i);
     a.rho[i] = d;
     a.v[i] = integrate_external(a, P, i, a.v[i], dt);
     float const neg_dt2 = -sqrf(dt);
@@ -772,33 +1031,43 @@ __global__ void k_iisph_density_dii(Arena a) {
     int const cf = a.nf_cnt[i];
     if (cf) {
         float const fmass = rho0 * P.fluid_volume;
-        float2 g = mk2(0.0f, 0.0f);
+        SumF2<K> g;
         #pragma unroll 4
 
-        for (int k = 0; k < cf; ++k) g = add2(g, scl2(fmass, a.nf_gw[k * stride + i]));
-        float2 const numer = scl2(neg_dt2, g);
+        for (int k = 0; k < cf; ++k) g.add(scl2(fmass, a.nf_gw[k * stride + i]));
+        float2 const numer = scl2(neg_dt2, g.get());
         dii = safe_v(numer, denom) ? div2(numer, denom) : mk2(0.0f, 0.0f);
     }
     int const cs = a.ns_cnt[i];
     if (cs) {
-        float2 g = mk2(0.0f, 0.0f);
+        SumF2<K> g;
         #pragma unroll 4
 
         for (int k = 0; k < cs; ++k) {
             size_t const e = k * stride + i;
-            g = add2(g, scl2(rho0 * a.vols[a.ns_idx[e]], a.ns_gw[e]));
+            g.add(scl2(rho0 * a.vols[a.ns_idx[e]], a.ns_gw[e]));
         }
-        float2 const numer = scl2(neg_dt2, g);
+        float2 const numer = scl2(neg_dt2, g.get());
         dii = add2(dii, safe_v(numer, denom) ? div2(numer, denom) : mk2(0.0f, 0.0f));
     }
     a.dii[i] = dii;
     a.pbuf0[i] = 0.0f;
 }
 
-// iisph_compute_aiis_and_density_stars (iisph_ops.cpp:92-200).
-__global__ void k_iisph_aii(Arena a) {
+template <int MODE>
+__global__ void k_iisph_density_dii(Arena a) {
     Ctx c;
     if (!enter(a, false, c) || !c.live) return;
+    if (MODE && a.sp[c.s].precision) {
+        iisph_density_dii<true>(a, c);
+    } else {
+        iisph_density_dii<false>(a, c);
+    }
+}
+
+// iisph_compute_aiis_and_density_stars (iisph_ops.cpp:92-200).
+template <bool K>
+__device__ __forceinline__ void iisph_aii(Arena const& a, Ctx const& c) {
     SceneParams const& P = a.sp[c.s];
     uint32_t const i = c.i;
     size_t const stride = a.stride;
@@ -812,7 +1081,7 @@ __global__ void k_iisph_aii(Arena a) {
     int const cf = a.nf_cnt[i];
     if (cf) {
         float const mass = P.fluid_volume * rho0;
-        float dd = 0.0f;
+        SumF<K> af, dd;
         #pragma unroll 4
 
         for (int k = 0; k < cf; ++k) {
@@ -823,16 +1092,16 @@ __global__ void k_iisph_aii(Arena a) {
             float const denom = sqrf(a.rho[j]);
             if (safe_v(numer, denom)) {
                 float2 const dji = neg2(div2(numer, denom));
-                aii += mass * dot2(sub2(dii, dji), gw);
+                af.add(mass * dot2(sub2(dii, dji), gw));
             }
-            dd += dt * mass * dot2(sub2(vi, a.v[j]), gw);
+            dd.add(dt * mass * dot2(sub2(vi, a.v[j]), gw));
         }
-        star = a.rho[i] + dd;
+        aii = af.get();
+        star = a.rho[i] + dd.get();
     }
     int const cs = a.ns_cnt[i];
     if (cs) {
-        float ab = 0.0f;
-        float dd = 0.0f;
+        SumF<K> ab, dd;
         #pragma unroll 4
 
         for (int k = 0; k < cs; ++k) {
@@ -840,23 +1109,30 @@ __global__ void k_iisph_aii(Arena a) {
             uint32_t const j = a.ns_idx[e];
             float2 const gw = a.ns_gw[e];
             float const mass = a.vols[j] * rho0;
-            ab += mass * dot2(dii, gw);
-            dd += dt * mass * dot2(sub2(vi, a.vs[j]), gw);
+            ab.add(mass * dot2(dii, gw));
+            dd.add(dt * mass * dot2(sub2(vi, a.vs[j]), gw));
         }
-        aii += ab;
-        star += dd;
+        aii += ab.get();
+        star += dd.get();
     }
     a.aii[i] = aii;
     a.rho_star[i] = star;
 }
 
-// iisph_compute_sum_dij_pjs (iisph_ops.cpp:202-235).
-template <int CH, int PF>
-__global__ void k_iisph_sum_dij(Arena a) {
+template <int MODE>
+__global__ void k_iisph_aii(Arena a) {
     Ctx c;
-    if (!enter(a, true, c)) return;
-    if (PF) prefetch_fluid_lists(a, c.live ? int(a.nf_cnt[c.i]) : 0);
-    if (!c.live) return;
+    if (!enter(a, false, c) || !c.live) return;
+    if (MODE && a.sp[c.s].precision) {
+        iisph_aii<true>(a, c);
+    } else {
+        iisph_aii<false>(a, c);
+    }
+}
+
+// iisph_compute_sum_dij_pjs (iisph_ops.cpp:202-235).
+template <bool K, int CH>
+__device__ __forceinline__ void iisph_sum_dij(Arena const& a, Ctx const& c) {
     SceneParams const& P = a.sp[c.s];
     SceneState const& S = a.ss[c.s];
     uint32_t const i = c.i;
@@ -865,7 +1141,7 @@ __global__ void k_iisph_sum_dij(Arena a) {
     float const* p = pressures_cur(a, S);
     float const mass = P.fluid_volume * P.rho0;
     float const neg_dt2 = -sqrf(dt);
-    float2 sum = mk2(0.0f, 0.0f);
+    SumF2<K> sum;
     int const cf = a.nf_cnt[i];
     (void)stride;
     fold_fluid_list<CH>(
@@ -873,23 +1149,33 @@ __global__ void k_iisph_sum_dij(Arena a) {
       [&](float2 prho, float2 g) {
           float2 const numer = scl2(neg_dt2 * mass * prho.x, g);
           float const denom = sqrf(prho.y);
-          if (safe_v(numer, denom)) sum = add2(sum, div2(numer, denom));
+          if (safe_v(numer, denom)) sum.add(div2(numer, denom));
       });
-    a.sdp[i] = sum;
+    a.sdp[i] = sum.get();
+}
+
+template <int MODE, int CH, int PF>
+__global__ void k_iisph_sum_dij(Arena a) {
+    Ctx c;
+    if (!enter(a, true, c)) return;
+    if (PF) prefetch_fluid_lists(a, c.live ? int(a.nf_cnt[c.i]) : 0);
+    if (!c.live) return;
+    if (MODE && a.sp[c.s].precision) {
+        iisph_sum_dij<true, CH>(a, c);
+    } else {
+        iisph_sum_dij<false, CH>(a, c);
+    }
 }
 
 // iisph_compute_betas (iisph_ops.cpp:237-330) followed by
 // iisph_compute_new_pressures for the same particle (iisph_ops.cpp:332-425).
-template <int CH, int PF>
-__global__ void k_iisph_beta_pressure(Arena a) {
-    Ctx c;
-    if (!enter(a, true, c)) return;
+// Returns whether the particle's error counts (a_ii != 0).
+template <bool K, int CH>
+__device__ __forceinline__ bool iisph_beta_pressure(Arena const& a, Ctx const& c, SceneState* S,
+                                                    float& err) {
     SceneParams const& P = a.sp[c.s];
-    SceneState* S = &a.ss[c.s];
-    float err = 0.0f;
     bool counted = false;
-    if (PF) prefetch_fluid_lists(a, c.live ? int(a.nf_cnt[c.i]) : 0);
-    if (c.live) {
+    {
         uint32_t const i = c.i;
         size_t const stride = a.stride;
         float const dt = S->dt;
@@ -903,6 +1189,7 @@ __global__ void k_iisph_beta_pressure(Arena a) {
         int const cf = a.nf_cnt[i];
         if (cf) {
             float const mass = rho0 * P.fluid_volume;
+            SumF<K> bf;
             fold_fluid_list<CH>(
               a, i, cf,
               [&](uint32_t j) { return IisphNeighbor{a.rho[j], p[j], a.sdp[j], a.dii[j]}; },
@@ -913,19 +1200,20 @@ __global__ void k_iisph_beta_pressure(Arena a) {
                   float2 const dji = neg2(dij);
                   float2 const skni = sub2(nb.sdp, scl2(pi, dji));
                   float2 const t = sub2(sub2(si, scl2(nb.p, nb.dii)), skni);
-                  beta += mass * dot2(t, gw);
+                  bf.add(mass * dot2(t, gw));
               });
+            beta = bf.get();
         }
         int const cs = a.ns_cnt[i];
         if (cs) {
-            float bb = 0.0f;
+            SumF<K> bb;
             #pragma unroll 4
 
             for (int k = 0; k < cs; ++k) {
                 size_t const e = k * stride + i;
-                bb += (rho0 * a.vols[a.ns_idx[e]]) * dot2(si, a.ns_gw[e]);
+                bb.add((rho0 * a.vols[a.ns_idx[e]]) * dot2(si, a.ns_gw[e]));
             }
-            beta += bb;
+            beta += bb.get();
         }
         float const alpha = a.aii[i];
         float out = pi;
@@ -941,6 +1229,21 @@ __global__ void k_iisph_beta_pressure(Arena a) {
         }
         pn[i] = out;
     }
+    return counted;
+}
+
+template <int MODE, int CH, int PF>
+__global__ void k_iisph_beta_pressure(Arena a) {
+    Ctx c;
+    if (!enter(a, true, c)) return;
+    SceneState* S = &a.ss[c.s];
+    float err = 0.0f;
+    bool counted = false;
+    if (PF) prefetch_fluid_lists(a, c.live ? int(a.nf_cnt[c.i]) : 0);
+    if (c.live) {
+        counted = (MODE && a.sp[c.s].precision) ? iisph_beta_pressure<true, CH>(a, c, S, err)
+                                                : iisph_beta_pressure<false, CH>(a, c, S, err);
+    }
     accumulate_error(S, counted ? static_cast<unsigned long long>(err * 1000.0f) : 0ull, err,
                      c.live && counted);
 }
@@ -955,12 +1258,14 @@ __global__ void k_make_q(Arena a) {
 
 // apply_pressures_in_place then integrate_positions_in_place
 // (iisph.cpp:138-150).
+template <int MODE>
 __global__ void k_apply_integrate(Arena a) {
     Ctx c;
     if (!enter(a, false, c) || !c.live) return;
     SceneParams const& P = a.sp[c.s];
     float const dt = a.ss[c.s].dt;
-    float2 const v = apply_pressure_of(a, P, c.i, a.v[c.i], a.qdens, dt);
+    float2 const v = (MODE && P.precision) ? apply_pressure_of<true>(a, P, c.i, a.v[c.i], a.qdens, dt)
+                                           : apply_pressure_of<false>(a, P, c.i, a.v[c.i], a.qdens, dt);
     a.v[c.i] = v;
     advance_position(a, P, c.i, dt, v);
 }
@@ -968,12 +1273,13 @@ __global__ void k_apply_integrate(Arena a) {
 // ------------------------------------------------- IISPH_AP / PSEUDO_AP
 
 // compute_densities, integrate_velocities_in_place, zero pressures.
+template <int MODE>
 __global__ void k_ap_density(Arena a) {
     Ctx c;
     if (!enter(a, false, c) || !c.live) return;
     SceneParams const& P = a.sp[c.s];
     float const dt = a.ss[c.s].dt;
-    a.rho[c.i] = density_of(a, P, c.i);
+    a.rho[c.i] = (MODE && P.precision) ? density_of<true>(a, P, c.i) : density_of<false>(a, P, c.i);
     a.v[c.i] = integrate_external(a, P, c.i, a.v[c.i], dt);
     a.pbuf0[c.i] = 0.0f;
     a.qdens[c.i] = 0.0f;
@@ -981,9 +1287,8 @@ __global__ void k_ap_density(Arena a) {
 
 // iisph_ap_density_stars_and_diagonals (iisph_ap_ops.cpp:19-103) and the
 // pseudo variant (iisph_pseudo_ap_ops.cpp:19-117).
-__global__ void k_ap_diag(Arena a, int pseudo) {
-    Ctx c;
-    if (!enter(a, false, c) || !c.live) return;
+template <bool K>
+__device__ __forceinline__ void ap_diag(Arena const& a, Ctx const& c, int pseudo) {
     SceneParams const& P = a.sp[c.s];
     uint32_t const i = c.i;
     size_t const stride = a.stride;
@@ -999,18 +1304,17 @@ __global__ void k_ap_diag(Arena a, int pseudo) {
     }
     float const self_mass = P.fluid_volume * rho0;
     float2 const vi = a.v[i];
-    float2 sum = mk2(0.0f, 0.0f);
-    float sdot = 0.0f;
-    float div = 0.0f;
+    SumF2<K> sum_acc;
+    SumF<K> sdot_acc, div_acc;
     float const fmass = P.fluid_volume * rho0;
     #pragma unroll 4
 
     for (int k = 0; k < cf; ++k) {
         size_t const e = k * stride + i;
         float2 const gw = a.nf_gw[e];
-        sum = add2(sum, scl2(fmass, gw));
-        sdot += fmass * dot2(gw, gw);
-        div += fmass * dot2(sub2(vi, a.v[a.nf_idx[e]]), gw);
+        sum_acc.add(scl2(fmass, gw));
+        sdot_acc.add(fmass * dot2(gw, gw));
+        div_acc.add(fmass * dot2(sub2(vi, a.v[a.nf_idx[e]]), gw));
     }
     #pragma unroll 4
 
@@ -1019,9 +1323,12 @@ __global__ void k_ap_diag(Arena a, int pseudo) {
         uint32_t const j = a.ns_idx[e];
         float2 const gw = a.ns_gw[e];
         float const mass = a.vols[j] * rho0;
-        sum = add2(sum, scl2(mass, gw));
-        div += mass * dot2(sub2(vi, a.vs[j]), gw);
+        sum_acc.add(scl2(mass, gw));
+        div_acc.add(mass * dot2(sub2(vi, a.vs[j]), gw));
     }
+    float2 const sum = sum_acc.get();
+    float const sdot = sdot_acc.get();
+    float const div = div_acc.get();
     float const denom = sqrf(rho);
     float const numer = pseudo ? -(dot2(sum, sum) + self_mass * sdot)
                                : -sqrf(dt) * (dot2(sum, sum) + self_mass * sdot);
@@ -1029,17 +1336,54 @@ __global__ void k_ap_diag(Arena a, int pseudo) {
     a.rho_star[i] = rho + dt * div;
 }
 
+template <int MODE>
+__global__ void k_ap_diag(Arena a, int pseudo) {
+    Ctx c;
+    if (!enter(a, false, c) || !c.live) return;
+    if (MODE && a.sp[c.s].precision) {
+        ap_diag<true>(a, c, pseudo);
+    } else {
+        ap_diag<false>(a, c, pseudo);
+    }
+}
+
 // compute_pressure_accelerations over the cached p/rho^2 (also the pseudo
 // pressure displacements, iisph_pseudo_ap_ops.cpp:119-224).
+template <int MODE>
 __global__ void k_pressure_accel(Arena a) {
     Ctx c;
     if (!enter(a, true, c) || !c.live) return;
     SceneParams const& P = a.sp[c.s];
-    a.acc[c.i] = pressure_accel_of(a, P, c.i, a.qdens);
+    a.acc[c.i] = (MODE && P.precision) ? pressure_accel_of<true>(a, P, c.i, a.qdens)
+                                       : pressure_accel_of<false>(a, P, c.i, a.qdens);
 }
 
 // iisph_ap_iterate_pressures_in_place (iisph_ap_ops.cpp:105-194) and the
 // pseudo variant (iisph_pseudo_ap_ops.cpp:226-323).
+template <bool K>
+__device__ __forceinline__ float ap_neighbor_sum(Arena const& a, SceneParams const& P, uint32_t i,
+                                                 int cf, int cs) {
+    size_t const stride = a.stride;
+    float const rho0 = P.rho0;
+    SumF<K> api;
+    float2 const ai = a.acc[i];
+    float const fmass = rho0 * P.fluid_volume;
+    #pragma unroll 4
+
+    for (int k = 0; k < cf; ++k) {
+        size_t const e = k * stride + i;
+        api.add(fmass * dot2(sub2(ai, a.acc[a.nf_idx[e]]), a.nf_gw[e]));
+    }
+    #pragma unroll 4
+
+    for (int k = 0; k < cs; ++k) {
+        size_t const e = k * stride + i;
+        api.add((rho0 * a.vols[a.ns_idx[e]]) * dot2(ai, a.ns_gw[e]));
+    }
+    return api.get();
+}
+
+template <int MODE>
 __global__ void k_ap_iterate(Arena a, int pseudo) {
     Ctx c;
     if (!enter(a, true, c)) return;
@@ -1049,7 +1393,6 @@ __global__ void k_ap_iterate(Arena a, int pseudo) {
     bool counted = false;
     if (c.live) {
         uint32_t const i = c.i;
-        size_t const stride = a.stride;
         float const rho0 = P.rho0;
         int const cf = a.nf_cnt[i];
         int const cs = a.ns_cnt[i];
@@ -1060,21 +1403,8 @@ __global__ void k_ap_iterate(Arena a, int pseudo) {
         } else if (pseudo && diag == 0.0f) {
             pnew = 0.0f;
         } else {
-            float api = 0.0f;
-            float2 const ai = a.acc[i];
-            float const fmass = rho0 * P.fluid_volume;
-            #pragma unroll 4
-
-            for (int k = 0; k < cf; ++k) {
-                size_t const e = k * stride + i;
-                api += fmass * dot2(sub2(ai, a.acc[a.nf_idx[e]]), a.nf_gw[e]);
-            }
-            #pragma unroll 4
-
-            for (int k = 0; k < cs; ++k) {
-                size_t const e = k * stride + i;
-                api += (rho0 * a.vols[a.ns_idx[e]]) * dot2(ai, a.ns_gw[e]);
-            }
+            float api = (MODE && P.precision) ? ap_neighbor_sum<true>(a, P, i, cf, cs)
+                                              : ap_neighbor_sum<false>(a, P, i, cf, cs);
             if (!pseudo) api *= sqrf(S->dt);
             float const source = rho0 - a.rho_star[i];
             float const r = api - source;
@@ -1095,13 +1425,15 @@ __global__ void k_ap_iterate(Arena a, int pseudo) {
 // (integrate_velocities_and_positions_in_place, dynamics.cpp:53-63) or
 // iisph_pseudo_ap_integrate_velocities_and_positions_in_place
 // (iisph_pseudo_ap_ops.cpp:325-343).
+template <int MODE>
 __global__ void k_ap_finish(Arena a, int pseudo) {
     Ctx c;
     if (!enter(a, false, c) || !c.live) return;
     SceneParams const& P = a.sp[c.s];
     float const dt = a.ss[c.s].dt;
     uint32_t const i = c.i;
-    float2 const acc = pressure_accel_of(a, P, i, a.qdens);
+    float2 const acc = (MODE && P.precision) ? pressure_accel_of<true>(a, P, i, a.qdens)
+                                             : pressure_accel_of<false>(a, P, i, a.qdens);
     a.acc[i] = acc;
     if (!pseudo) {
         float2 const v = add2(a.v[i], scl2(dt, acc));
@@ -1147,6 +1479,35 @@ __global__ void k_pc_predict(Arena a) {
 // neighborhoods_from_state.cpp:103-128), pcisph_compute_densities,
 // pcisph_accumulate_density_from_solids and pcisph_update_pressures
 // (pcisph_ops.cpp:18-76), plus the max density error (common.cpp:78-85).
+template <bool K>
+__device__ __forceinline__ float pc_density_of(Arena const& a, SceneParams const& P, uint32_t i) {
+    size_t const stride = a.stride;
+    float const h = P.support;
+    float2 const pos = a.xstar[i];
+    int const cf = a.nf_cnt[i];
+    SumF<K> ws(P.w0);
+    #pragma unroll 4
+
+    for (int k = 0; k < cf; ++k) {
+        uint32_t const j = a.nf_idx[k * stride + i];
+        ws.add(kernel_w(length2f(sub2(a.xstar[j], pos)), h));
+    }
+    float d = P.mass * ws.get();
+    int const cs = a.ns_cnt[i];
+    if (cs) {
+        SumF<K> vf;
+        #pragma unroll 4
+
+        for (int k = 0; k < cs; ++k) {
+            uint32_t const j = a.ns_idx[k * stride + i];
+            vf.add(a.vols[j] * kernel_w(length2f(sub2(a.xs[j], pos)), h));
+        }
+        d += P.rho0 * vf.get();
+    }
+    return d;
+}
+
+template <int MODE>
 __global__ void k_pc_density(Arena a) {
     Ctx c;
     if (!enter(a, true, c)) return;
@@ -1155,29 +1516,8 @@ __global__ void k_pc_density(Arena a) {
     float err = 0.0f;
     if (c.live) {
         uint32_t const i = c.i;
-        size_t const stride = a.stride;
-        float const h = P.support;
-        float2 const pos = a.xstar[i];
-        int const cf = a.nf_cnt[i];
-        float ws = P.w0;
-        #pragma unroll 4
-
-        for (int k = 0; k < cf; ++k) {
-            uint32_t const j = a.nf_idx[k * stride + i];
-            ws += kernel_w(length2f(sub2(a.xstar[j], pos)), h);
-        }
-        float d = P.mass * ws;
-        int const cs = a.ns_cnt[i];
-        if (cs) {
-            float vf = 0.0f;
-            #pragma unroll 4
-
-            for (int k = 0; k < cs; ++k) {
-                uint32_t const j = a.ns_idx[k * stride + i];
-                vf += a.vols[j] * kernel_w(length2f(sub2(a.xs[j], pos)), h);
-            }
-            d += P.rho0 * vf;
-        }
+        float const d = (MODE && P.precision) ? pc_density_of<true>(a, P, i)
+                                              : pc_density_of<false>(a, P, i);
         a.rho[i] = d;
         float const p = a.pbuf0[i] + max_x0(d - P.rho0) / P.pcisph_denom;
         a.pbuf0[i] = p;
@@ -1189,9 +1529,8 @@ __global__ void k_pc_density(Arena a) {
 
 // pcisph_accumulate_pressure_forces and ..._from_solids (pcisph_ops.cpp:78-178)
 // on the fixed neighbour lists at the predicted positions.
-__global__ void k_pc_forces(Arena a) {
-    Ctx c;
-    if (!enter(a, true, c) || !c.live) return;
+template <bool K>
+__device__ __forceinline__ void pc_forces(Arena const& a, Ctx const& c) {
     SceneParams const& P = a.sp[c.s];
     uint32_t const i = c.i;
     size_t const stride = a.stride;
@@ -1205,7 +1544,7 @@ __global__ void k_pc_forces(Arena a) {
         float2 const vi = a.vstar[i];
         float const rho = a.rho[i];
         float const pors = a.qdens[i];
-        float2 pf = mk2(0.0f, 0.0f);
+        SumF2<K> pf;
         #pragma unroll 4
 
         for (int k = 0; k < cf; ++k) {
@@ -1214,31 +1553,42 @@ __global__ void k_pc_forces(Arena a) {
             float const dist = length2f(vto);
             float2 const gw = kernel_grad_w(neg2(vto), h);
             float const rho_j = a.rho[j];
-            pf = add2(pf, scl2(pors + a.qdens[j], gw));
+            pf.add(scl2(pors + a.qdens[j], gw));
             float2 const dv = sub2(a.vstar[j], vi);
             float const dvr = dot2(vto, dv);
             if (dvr < 0.0f) {
                 float const mu = h * dvr / (dist + N2);
                 float const den = (rho + rho_j) / 2.0f;
-                pf = add2(pf, scl2(((-1.0f * P.viscosity * mu) + (2.0f * sqrf(mu))) / den, gw));
+                pf.add(scl2(((-1.0f * P.viscosity * mu) + (2.0f * sqrf(mu))) / den, gw));
             }
         }
-        f = add2(f, scl2(-(m * m), pf));
+        f = add2(f, scl2(-(m * m), pf.get()));
     }
     int const cs = a.ns_cnt[i];
     if (cs) {
         float const pors = a.pbuf0[i] / sqrf(a.rho[i]);
-        float2 vg = mk2(0.0f, 0.0f);
+        SumF2<K> vg;
         #pragma unroll 4
 
         for (int k = 0; k < cs; ++k) {
             uint32_t const j = a.ns_idx[k * stride + i];
             float2 const gw = kernel_grad_w(neg2(sub2(a.xs[j], pos)), h);
-            vg = add2(vg, scl2(a.vols[j], gw));
+            vg.add(scl2(a.vols[j], gw));
         }
-        f = add2(f, scl2(-m * P.rho0 * pors, vg));
+        f = add2(f, scl2(-m * P.rho0 * pors, vg.get()));
     }
     a.fp[i] = f;
+}
+
+template <int MODE>
+__global__ void k_pc_forces(Arena a) {
+    Ctx c;
+    if (!enter(a, true, c) || !c.live) return;
+    if (MODE && a.sp[c.s].precision) {
+        pc_forces<true>(a, c);
+    } else {
+        pc_forces<false>(a, c);
+    }
 }
 
 // Final velocity and position update (pcisph.cpp:151-163).
@@ -1258,6 +1608,24 @@ __global__ void k_pc_final(Arena a) {
 
 // Launches K(mode, chunk, prefetch) for the runtime choice: mode 1 when
 // `comp`, chunk 1, 4 or 8 (anything else: 8), prefetch 0 or 1.
+// Blocks of a persistent-warp launch: the resident blocks of `kernel` on
+// every multiprocessor, no more than the tiles to cover.
+template <class K>
+unsigned persistent_grid(K kernel, uint32_t tiles) {
+    static thread_local int dev_cached = -1;
+    static thread_local int sms = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != dev_cached) {
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        dev_cached = dev;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTile, 0);
+    uint64_t const g = uint64_t(std::max(per_sm, 1)) * uint64_t(std::max(sms, 1));
+    return unsigned(std::max<uint64_t>(1, std::min<uint64_t>(g, tiles)));
+}
+
 #define EMLD_DISPATCH(K, comp, ch, pf)                                        \
     do {                                                                      \
         if (comp) {                                                           \
@@ -1275,6 +1643,13 @@ __global__ void k_pc_final(Arena a) {
         }                                                                     \
     } while (0)
 
+void launch_frame_begin(Arena const& a, int nscenes, cudaStream_t st) {
+    k_frame_begin<<<(nscenes + 127) / 128, 128, 0, st>>>(a, nscenes);
+}
+void launch_frame_check(Arena const& a, int nscenes, int method, cudaGraphConditionalHandle cond,
+                        cudaStream_t st) {
+    k_frame_check<<<1, 128, 0, st>>>(a, nscenes, method, cond);
+}
 void launch_max_v2(Arena const& a, uint32_t tiles, cudaStream_t st) {
     k_max_v2<<<tiles, kTile, 0, st>>>(a);
 }
@@ -1291,31 +1666,80 @@ void launch_iter_check(Arena const& a, int nscenes, int kind, int* running,
                        cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st) {
     k_iter_check<<<1, 256, 0, st>>>(a, nscenes, kind, running, cond, use_cond);
 }
-void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st) {
+void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st,
+                                bool persistent) {
+    if (!tiles) return;
+    if (persistent) {
+        uint32_t const wt = tiles * (kTile / 32);
+        if (comp) {
+            k_dfsph_density_alpha_pw<1>
+              <<<persistent_grid(k_dfsph_density_alpha_pw<1>, tiles), kTile, 0, st>>>(a, wt);
+        } else {
+            k_dfsph_density_alpha_pw<0>
+              <<<persistent_grid(k_dfsph_density_alpha_pw<0>, tiles), kTile, 0, st>>>(a, wt);
+        }
+        return;
+    }
     if (comp) {
         k_dfsph_density_alpha<1><<<tiles, kTile, 0, st>>>(a);
     } else {
         k_dfsph_density_alpha<0><<<tiles, kTile, 0, st>>>(a);
     }
 }
+#define EMLD_PW_DISPATCH(K, comp, ch)                                          \
+    do {                                                                      \
+        if (comp) {                                                           \
+            if ((ch) == 1) K(1, 1); else if ((ch) == 4) K(1, 4); else K(1, 8); \
+        } else {                                                              \
+            if ((ch) == 1) K(0, 1); else if ((ch) == 4) K(0, 4); else K(0, 8); \
+        }                                                                     \
+    } while (0)
+
 void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int external,
                             int skip_done, bool comp, cudaStream_t st, int chunk) {
+    if (!tiles) return;
     bool const pf = (chunk & kPrefetchLists) != 0;
-    int const ch = chunk & ~kPrefetchLists;
+    int const ch = chunk & kChunkMask;
+    if (chunk & kPersistentWarps) {
+#define EMLD_APPLY_PW(M, C)                                                                     \
+    k_apply_pressures_pw<M, C><<<persistent_grid(k_apply_pressures_pw<M, C>, tiles), kTile, 0, st>>>( \
+      a, tiles * (kTile / 32), which_q, external, skip_done)
+        EMLD_PW_DISPATCH(EMLD_APPLY_PW, comp, ch);
+#undef EMLD_APPLY_PW
+        return;
+    }
 #define EMLD_APPLY(M, C, F) k_apply_pressures<M, C, F><<<tiles, kTile, 0, st>>>(a, which_q, external, skip_done)
     EMLD_DISPATCH(EMLD_APPLY, comp, ch, pf);
 #undef EMLD_APPLY
 }
 void launch_dfsph_divergence(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st, int chunk) {
+    if (!tiles) return;
     bool const pf = (chunk & kPrefetchLists) != 0;
-    int const ch = chunk & ~kPrefetchLists;
+    int const ch = chunk & kChunkMask;
+    if (chunk & kPersistentWarps) {
+#define EMLD_DIV_PW(M, C)                                                                         \
+    k_dfsph_divergence_pw<M, C><<<persistent_grid(k_dfsph_divergence_pw<M, C>, tiles), kTile, 0, st>>>( \
+      a, tiles * (kTile / 32))
+        EMLD_PW_DISPATCH(EMLD_DIV_PW, comp, ch);
+#undef EMLD_DIV_PW
+        return;
+    }
 #define EMLD_DIV(M, C, F) k_dfsph_divergence<M, C, F><<<tiles, kTile, 0, st>>>(a)
     EMLD_DISPATCH(EMLD_DIV, comp, ch, pf);
 #undef EMLD_DIV
 }
 void launch_dfsph_density(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st, int chunk) {
+    if (!tiles) return;
     bool const pf = (chunk & kPrefetchLists) != 0;
-    int const ch = chunk & ~kPrefetchLists;
+    int const ch = chunk & kChunkMask;
+    if (chunk & kPersistentWarps) {
+#define EMLD_DENS_PW(M, C)                                                                    \
+    k_dfsph_density_pw<M, C><<<persistent_grid(k_dfsph_density_pw<M, C>, tiles), kTile, 0, st>>>( \
+      a, tiles * (kTile / 32))
+        EMLD_PW_DISPATCH(EMLD_DENS_PW, comp, ch);
+#undef EMLD_DENS_PW
+        return;
+    }
 #define EMLD_DENS(M, C, F) k_dfsph_density<M, C, F><<<tiles, kTile, 0, st>>>(a)
     EMLD_DISPATCH(EMLD_DENS, comp, ch, pf);
 #undef EMLD_DENS
@@ -1327,46 +1751,79 @@ void launch_integrate_positions(Arena const& a, uint32_t tiles, bool comp, cudaS
         k_integrate_positions<0><<<tiles, kTile, 0, st>>>(a);
     }
 }
-void launch_iisph_density_dii(Arena const& a, uint32_t tiles, cudaStream_t st) {
-    k_iisph_density_dii<<<tiles, kTile, 0, st>>>(a);
+void launch_iisph_density_dii(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp) {
+    if (comp) {
+        k_iisph_density_dii<1><<<tiles, kTile, 0, st>>>(a);
+    } else {
+        k_iisph_density_dii<0><<<tiles, kTile, 0, st>>>(a);
+    }
 }
-void launch_iisph_aii(Arena const& a, uint32_t tiles, cudaStream_t st) {
-    k_iisph_aii<<<tiles, kTile, 0, st>>>(a);
+void launch_iisph_aii(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp) {
+    if (comp) {
+        k_iisph_aii<1><<<tiles, kTile, 0, st>>>(a);
+    } else {
+        k_iisph_aii<0><<<tiles, kTile, 0, st>>>(a);
+    }
 }
-void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk) {
+void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk, bool comp) {
     bool const pf = (chunk & kPrefetchLists) != 0;
-    int const ch = chunk & ~kPrefetchLists;
-#define EMLD_SUM(M, C, F) k_iisph_sum_dij<C, F><<<tiles, kTile, 0, st>>>(a)
-    EMLD_DISPATCH(EMLD_SUM, false, ch, pf);
+    int const ch = chunk & kChunkMask;
+#define EMLD_SUM(M, C, F) k_iisph_sum_dij<M, C, F><<<tiles, kTile, 0, st>>>(a)
+    EMLD_DISPATCH(EMLD_SUM, comp, ch, pf);
 #undef EMLD_SUM
 }
-void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk) {
+void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk,
+                                bool comp) {
     bool const pf = (chunk & kPrefetchLists) != 0;
-    int const ch = chunk & ~kPrefetchLists;
-#define EMLD_BETA(M, C, F) k_iisph_beta_pressure<C, F><<<tiles, kTile, 0, st>>>(a)
-    EMLD_DISPATCH(EMLD_BETA, false, ch, pf);
+    int const ch = chunk & kChunkMask;
+#define EMLD_BETA(M, C, F) k_iisph_beta_pressure<M, C, F><<<tiles, kTile, 0, st>>>(a)
+    EMLD_DISPATCH(EMLD_BETA, comp, ch, pf);
 #undef EMLD_BETA
 }
 void launch_make_q(Arena const& a, uint32_t tiles, cudaStream_t st) {
     k_make_q<<<tiles, kTile, 0, st>>>(a);
 }
-void launch_apply_integrate(Arena const& a, uint32_t tiles, cudaStream_t st) {
-    k_apply_integrate<<<tiles, kTile, 0, st>>>(a);
+void launch_apply_integrate(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp) {
+    if (comp) {
+        k_apply_integrate<1><<<tiles, kTile, 0, st>>>(a);
+    } else {
+        k_apply_integrate<0><<<tiles, kTile, 0, st>>>(a);
+    }
 }
-void launch_ap_density(Arena const& a, uint32_t tiles, cudaStream_t st) {
-    k_ap_density<<<tiles, kTile, 0, st>>>(a);
+void launch_ap_density(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp) {
+    if (comp) {
+        k_ap_density<1><<<tiles, kTile, 0, st>>>(a);
+    } else {
+        k_ap_density<0><<<tiles, kTile, 0, st>>>(a);
+    }
 }
-void launch_ap_diag(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st) {
-    k_ap_diag<<<tiles, kTile, 0, st>>>(a, pseudo);
+void launch_ap_diag(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st, bool comp) {
+    if (comp) {
+        k_ap_diag<1><<<tiles, kTile, 0, st>>>(a, pseudo);
+    } else {
+        k_ap_diag<0><<<tiles, kTile, 0, st>>>(a, pseudo);
+    }
 }
-void launch_pressure_accel(Arena const& a, uint32_t tiles, cudaStream_t st) {
-    k_pressure_accel<<<tiles, kTile, 0, st>>>(a);
+void launch_pressure_accel(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp) {
+    if (comp) {
+        k_pressure_accel<1><<<tiles, kTile, 0, st>>>(a);
+    } else {
+        k_pressure_accel<0><<<tiles, kTile, 0, st>>>(a);
+    }
 }
-void launch_ap_iterate(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st) {
-    k_ap_iterate<<<tiles, kTile, 0, st>>>(a, pseudo);
+void launch_ap_iterate(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st, bool comp) {
+    if (comp) {
+        k_ap_iterate<1><<<tiles, kTile, 0, st>>>(a, pseudo);
+    } else {
+        k_ap_iterate<0><<<tiles, kTile, 0, st>>>(a, pseudo);
+    }
 }
-void launch_ap_finish(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st) {
-    k_ap_finish<<<tiles, kTile, 0, st>>>(a, pseudo);
+void launch_ap_finish(Arena const& a, uint32_t tiles, int pseudo, cudaStream_t st, bool comp) {
+    if (comp) {
+        k_ap_finish<1><<<tiles, kTile, 0, st>>>(a, pseudo);
+    } else {
+        k_ap_finish<0><<<tiles, kTile, 0, st>>>(a, pseudo);
+    }
 }
 void launch_pc_init(Arena const& a, uint32_t tiles, cudaStream_t st) {
     k_pc_init<<<tiles, kTile, 0, st>>>(a);
@@ -1374,11 +1831,19 @@ void launch_pc_init(Arena const& a, uint32_t tiles, cudaStream_t st) {
 void launch_pc_predict(Arena const& a, uint32_t tiles, cudaStream_t st) {
     k_pc_predict<<<tiles, kTile, 0, st>>>(a);
 }
-void launch_pc_density(Arena const& a, uint32_t tiles, cudaStream_t st) {
-    k_pc_density<<<tiles, kTile, 0, st>>>(a);
+void launch_pc_density(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp) {
+    if (comp) {
+        k_pc_density<1><<<tiles, kTile, 0, st>>>(a);
+    } else {
+        k_pc_density<0><<<tiles, kTile, 0, st>>>(a);
+    }
 }
-void launch_pc_forces(Arena const& a, uint32_t tiles, cudaStream_t st) {
-    k_pc_forces<<<tiles, kTile, 0, st>>>(a);
+void launch_pc_forces(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp) {
+    if (comp) {
+        k_pc_forces<1><<<tiles, kTile, 0, st>>>(a);
+    } else {
+        k_pc_forces<0><<<tiles, kTile, 0, st>>>(a);
+    }
 }
 void launch_pc_final(Arena const& a, uint32_t tiles, cudaStream_t st) {
     k_pc_final<<<tiles, kTile, 0, st>>>(a);

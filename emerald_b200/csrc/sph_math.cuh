@@ -91,6 +91,40 @@ EMLD_HD void kahan_add(KahanF2& k, float2 v) {
     kahan_add(k.y, v.y);
 }
 
+// A running sum of float (SumF) or float2 (SumF2) terms: with K = false
+// exactly the reference's s += t, with K = true Kahan-compensated.
+template <bool K>
+struct SumF {
+    float s;
+    EMLD_HD explicit SumF(float init = 0.0f) : s(init) {}
+    EMLD_HD void add(float v) { s += v; }
+    EMLD_HD float get() const { return s; }
+};
+template <>
+struct SumF<true> {
+    KahanF k;
+    EMLD_HD explicit SumF(float init = 0.0f) : k{init, 0.0f} {}
+    EMLD_HD void add(float v) { kahan_add(k, v); }
+    EMLD_HD float get() const { return k.s; }
+};
+template <bool K>
+struct SumF2 {
+    float2 s;
+    EMLD_HD SumF2() : s{0.0f, 0.0f} {}
+    EMLD_HD void add(float2 v) {
+        s.x += v.x;
+        s.y += v.y;
+    }
+    EMLD_HD float2 get() const { return s; }
+};
+template <>
+struct SumF2<true> {
+    KahanF2 k;
+    EMLD_HD SumF2() : k{{0.0f, 0.0f}, {0.0f, 0.0f}} {}
+    EMLD_HD void add(float2 v) { kahan_add(k, v); }
+    EMLD_HD float2 get() const { return float2{k.x.s, k.y.s}; }
+};
+
 // Cubic spline with the reference's 3D normalisation 1/(pi h^3), support 2h
 // (emerald/sph_common/kernels.h:12-64).
 constexpr float kPi = 3.14159274101257324218750f;

@@ -170,7 +170,11 @@ int emerald_sim_sub_step(emerald_sim* sim, int32_t method, float t, float dt,
 
 /* One frame, as X_simulation_step through EZ_EXAMPLE_SIM::step
  * (emerald/sph2d_box/simulation.cpp:41-93): CFL-adaptive sub-steps
- * (adaptive_time_step.h:35-122) or PCISPH's fixed sub-steps. */
+ * (adaptive_time_step.h:35-122) or PCISPH's fixed sub-steps. With graphs on
+ * (the default) the whole frame is one CUDA graph launch, its sub-step loop
+ * a conditional while node on the device, and the call waits for the
+ * device once; a frame that started earlier (after emerald_sim_advance) is
+ * finished. stats->sub_steps counts the sub-steps this call ran. */
 int emerald_sim_frame(emerald_sim* sim, int32_t method, emerald_step_stats* stats);
 
 /* Advances n adaptive sub-steps, continuing and starting frames exactly as
@@ -307,6 +311,10 @@ int emerald_sim_set_graphs(emerald_sim* sim, int32_t graphs);
 
 /* Kernels this simulation has launched (graph nodes included, loop bodies
  * counted once per executed iteration). */
+/* Times the simulation waited on the host for the device (stream or event
+ * synchronisations). No counterpart in the reference; with graphs on, a
+ * frame costs one. */
+int emerald_sim_host_waits(emerald_sim* sim, int64_t* count);
 int emerald_sim_kernel_launches(emerald_sim* sim, int64_t* count);
 
 /* Number of kernel launches this library issued from the host since the
@@ -354,28 +362,36 @@ int emerald_batch_kernel_launches(emerald_batch* batch, int64_t* count);
 /* -------------------------------------------------------------- autotuning */
 
 /* Neighbour entries each gather-sum kernel loads together (1, 4 or 8), and
- * whether its warps first ask L2 for their list rows (prefetch 1). Every
- * choice gives the same bits. Autotuning (DFSPH_P and IISPH) times a few
- * whole sub-steps of `method` with each candidate setting, every candidate
- * from the same state (restored afterwards, so the simulation is left as it
- * was), after at least one sub-step of that method, and keeps the fastest,
- * also for later simulations and batches of the same method and size class
- * (log2 of the active particle count). candidate_ms[k]: mean sub-step time
- * of candidate k, whose chunks and prefetch flags are candidate_chunks[k]
- * and candidate_prefetch[k] (apply, divergence, iisph_sum, iisph_beta;
- * prefetch[] in the same order). No counterpart in the reference. */
+ * how it brings its lists in (prefetch): 0 loads them as the sums need
+ * them; 1 has each warp first ask L2 for its list rows;
+ * EMERALD_TUNE_PERSISTENT (2; DFSPH_P families only) launches one grid of
+ * resident blocks whose warps walk their 32-particle tiles and request the
+ * next tile's lists and inputs into L2 while they fold the current one.
+ * Every choice gives the same bits. Autotuning (DFSPH_P and IISPH) times a
+ * few whole sub-steps of `method` with each candidate setting, every
+ * candidate from the same state (restored afterwards, so the simulation is
+ * left as it was), after at least one sub-step of that method, and keeps
+ * the fastest, also for later simulations and batches of the same method
+ * and size class (log2 of the active particle count). candidate_ms[k]: mean
+ * sub-step time of candidate k, whose chunks and prefetch modes are
+ * candidate_chunks[k] and candidate_prefetch[k] (apply, divergence,
+ * iisph_sum, iisph_beta; prefetch[] in the same order; the divergence
+ * family's mode also applies to the DFSPH density and alpha pass). No
+ * counterpart in the reference. */
+#define EMERALD_TUNE_PERSISTENT 2
+#define EMERALD_TUNE_CANDIDATES 16
 typedef struct emerald_tuning {
     int32_t apply_chunk, divergence_chunk, iisph_sum_chunk, iisph_beta_chunk;
     int32_t candidates;
-    int32_t candidate_chunks[8][4];
-    float candidate_ms[8];
+    int32_t candidate_chunks[EMERALD_TUNE_CANDIDATES][4];
+    float candidate_ms[EMERALD_TUNE_CANDIDATES];
     int32_t prefetch[4];
-    int32_t candidate_prefetch[8][4];
+    int32_t candidate_prefetch[EMERALD_TUNE_CANDIDATES][4];
 } emerald_tuning;
 
 int emerald_sim_autotune(emerald_sim* sim, int32_t method, emerald_tuning* out);
 int emerald_batch_autotune(emerald_batch* batch, int32_t method, emerald_tuning* out);
-/* Pins the settings of *tuning (its chunks and prefetch flags; the candidate
+/* Pins the settings of *tuning (its chunks and prefetch modes; the candidate
  * fields are ignored) until the next call; NULL returns to the tuned or
  * default settings. */
 int emerald_sim_set_tuning(emerald_sim* sim, emerald_tuning const* tuning);

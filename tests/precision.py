@@ -6,7 +6,9 @@ each sub-step with the same dt, frame boundaries and iteration counts (and
 the same relaxation omega, viscosity and PCISPH denominator), so the two
 differ only in arithmetic precision. Reported per checkpoint: per-particle density error (relative,
 L_inf and RMS), position error (in units of the particle spacing, max and
-RMS) and the kinetic-energy difference."""
+RMS), the kinetic-energy difference, and the drift of the total mechanical
+energy (kinetic plus gravitational, m g y summed) from its initial value in
+both runs."""
 import numpy as np
 
 from cpu_checkers import FP64Oracle
@@ -44,7 +46,9 @@ def compare(E, n_side, steps, checkpoints, precision, seed=1, offset=0.0, method
     ref = FP64Oracle().sim(p.support, p.target_density, p.mass_per_particle, p.gravity,
                            solid, scene.solid_volumes, fluid)
     mass = float(p.mass_per_particle)
+    g = float(p.gravity)
     dx = float(scene.dx)
+    e0 = mass * g * float(np.sum(fluid[:, 1].astype(np.float64)))
     tps = int(p.time_per_step_flicks)
     rows = []
     for step in range(1, steps + 1):
@@ -71,6 +75,8 @@ def compare(E, n_side, steps, checkpoints, precision, seed=1, offset=0.0, method
             dpos = np.hypot(*(x.astype(np.float64) - x64).T) / dx
             ke = 0.5 * mass * float(np.sum(v.astype(np.float64) ** 2))
             ke64 = 0.5 * mass * float(np.sum(v64 ** 2))
+            e32 = ke + mass * g * float(np.sum(x[:, 1].astype(np.float64)))
+            e64 = ke64 + mass * g * float(np.sum(x64[:, 1]))
             extra = {}
             if method in ("iisph", "iisph_ap", "iisph_pseudo_ap"):
                 pr = sim.array("pressures").astype(np.float64)
@@ -87,6 +93,8 @@ def compare(E, n_side, steps, checkpoints, precision, seed=1, offset=0.0, method
                              position_rms_dx=float(np.sqrt(np.mean(dpos ** 2))),
                              kinetic_energy=ke, kinetic_energy_fp64=ke64,
                              energy_rel_diff=abs(ke - ke64) / ke64 if ke64 else 0.0,
+                             energy_drift=(e32 - e0) / abs(e0) if e0 else 0.0,
+                             energy_drift_fp64=(e64 - e0) / abs(e0) if e0 else 0.0,
                              iterations=st["pressure_iterations"], **extra))
     ref.close()
     sim.close()

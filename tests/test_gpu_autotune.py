@@ -53,6 +53,7 @@ def test_batch_tuning(E):
     b.step("iisph", 2)
     t = b.autotune("iisph")
     assert len(t["candidates"]) == 8 and all(c["ms_per_substep"] > 0 for c in t["candidates"])
+    assert all(m in (0, 1) for c in t["candidates"] for m in c["prefetch"].values())
     b.step("iisph", 4)
     for sid, s in zip(ids, scs):
         sim = E.Simulation.from_block_scene(s)
@@ -79,6 +80,9 @@ def test_every_candidate_gives_the_same_bits(E, method):
     probe.advance(method, 1)
     cands = probe.autotune(method)["candidates"]
     assert any(any(c["prefetch"].values()) for c in cands)
+    if method == "dfsph_p":
+        # the persistent-warp kernels are among the candidates
+        assert any(c["prefetch"]["apply"] == 2 for c in cands)
     for c in cands:
         sim = E.Simulation.from_block_scene(sc)
         sim.set_tuning(c["chunks"], c["prefetch"])
@@ -94,6 +98,11 @@ def test_set_tuning_rejects_bad_values(E):
         sim.set_tuning({"apply": 3, "divergence": 4, "iisph_sum": 4, "iisph_beta": 4})
     with pytest.raises(E.EmeraldError):
         sim.set_tuning({"apply": 4, "divergence": 4, "iisph_sum": 4, "iisph_beta": 4},
-                       {"apply": 2})
+                       {"apply": 3})
+    with pytest.raises(E.EmeraldError):  # no persistent-warp IISPH kernels
+        sim.set_tuning({"apply": 4, "divergence": 4, "iisph_sum": 4, "iisph_beta": 4},
+                       {"iisph_sum": 2})
+    sim.set_tuning({"apply": 4, "divergence": 8, "iisph_sum": 4, "iisph_beta": 4},
+                   {"apply": 2, "divergence": 2})
     sim.set_tuning()
     sim.close()
