@@ -420,8 +420,10 @@ def run_gpu(args):
         flush1 = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
         result["side1m"] = run_side1m(args, torch, E, flush1)
         del flush1
-    if args.serving_requests > 0 and world == 1:
-        result["serving"] = run_serving(args, torch, E)
+    if args.serving_requests > 0:
+        serving = run_serving(args, torch, E, rank, world, barrier)
+        if rank == 0:
+            result["serving"] = serving
     if args.literal_steps > 0 and world == 1:
         result["pcisph_h2dx"] = run_pcisph_literal(args, torch, E, flush)
     if world > 1:
@@ -561,25 +563,33 @@ def run_batched(args, torch, E, rank, world, barrier):
     return out
 
 
-def run_serving(args, torch, E):
-    """The served workload: a Poisson stream (200 requests/s) of DFSPH dam
-    breaks, fluid count log-uniform in [2048, 262144], sub-step count uniform
-    in [50, 500], admitted under a 120 GB device-memory budget and stepped
-    by continuous batching. Compared with the same requests served one at a
-    time by the single-scene API (scene set-up, sub-steps and result copy of
-    each, back to back)."""
+def run_serving(args, torch, E, rank=0, world=1, barrier=None):
+    """The served workload: a Poisson stream (200 requests/s per GPU) of
+    DFSPH dam breaks, fluid count log-uniform in [2048, 262144], sub-step
+    count uniform in [50, 500], admitted under a 120 GB device-memory budget
+    and stepped by continuous batching. With N GPUs the stream has N times
+    the requests at N times the rate, and each request is routed as it
+    arrives to one GPU's request loop (workloads.route_requests: least work
+    routed so far); the ranks exchange nothing but the final timing. On one
+    GPU it is compared with the same requests served one at a time by the
+    single-scene API (scene set-up, sub-steps and result copy of each, back
+    to back)."""
     import threading
     from emerald_b200 import workloads as W
-    reqs = W.serving_requests(args.serving_requests)
-    scenes = [W.scene_for(r["nx"], r["ny"], r["seed"]) for r in reqs]
-    srv = E.Server(120 * 10**9, "dfsph_p", max_scenes=max(64, len(reqs)),
+    reqs = W.serving_requests(args.serving_requests * world, rate=200.0 * world)
+    mine = W.route_requests(reqs, world)[rank]
+    my_reqs = [reqs[k] for k in mine]
+    scenes = [W.scene_for(r["nx"], r["ny"], r["seed"]) for r in my_reqs]
+    srv = E.Server(120 * 10**9, "dfsph_p", max_scenes=max(64, len(my_reqs)),
                    max_substeps_per_launch=args.serving_substeps, lanes=args.serving_lanes,
                    order=args.serving_order)
-    ids = [None] * len(reqs)
+    ids = [None] * len(my_reqs)
+    if barrier is not None:
+        barrier()
     t_start = time.perf_counter()
 
     def client():
-        for k, (r, sc) in enumerate(zip(reqs, scenes)):
+        for k, (r, sc) in enumerate(zip(my_reqs, scenes)):
             delay = t_start + r["arrival"] - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
@@ -593,22 +603,39 @@ def run_serving(args, torch, E):
     st = srv.stats()
     srv.close()
     total_ms = [d[3]["total_ms"] for d in done]
-    particle_steps = sum(len(sc.fluid) * r["substeps"] for r, sc in zip(reqs, scenes))
-    out = {"workload": "%d DFSPH dam-break requests, Poisson 200/s, fluid count log-uniform in "
-                       "[2048, 262144], sub-steps uniform in [50, 500], 120 GB budget, "
-                       "continuous batching (admission every <= 8 sub-steps)" % len(reqs),
+    particle_steps = sum(len(sc.fluid) * r["substeps"] for r, sc in zip(my_reqs, scenes))
+    mine_stats = [wall, float(np.percentile(total_ms, 99)) if total_ms else 0.0,
+                  st["step_ms_p99"], particle_steps]
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor(mine_stats[:3], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ps = torch.tensor([particle_steps], dtype=torch.float64, device="cuda")
+        dist.all_reduce(ps, op=dist.ReduceOp.SUM)
+        wall, req_p99_all, step_p99_all = (float(v) for v in t.tolist())
+        particle_steps = float(ps.item())
+    else:
+        req_p99_all, step_p99_all = mine_stats[1], mine_stats[2]
+    out = {"workload": "%d DFSPH dam-break requests, Poisson %d/s, fluid count log-uniform in "
+                       "[2048, 262144], sub-steps uniform in [50, 500], 120 GB budget per GPU, "
+                       "continuous batching (admission every <= 8 sub-steps)%s" % (
+                           len(reqs), 200 * world,
+                           ", routed to %d per-GPU request loops" % world if world > 1 else ""),
            "requests": len(reqs), "wall_s": round(wall, 3),
            "scenes_per_s": round(len(reqs) / wall, 3),
            "particle_steps_per_s": round(particle_steps / wall, 1),
-           "step_ms_p50": round(st["step_ms_p50"], 3), "step_ms_p99": round(st["step_ms_p99"], 3),
+           "step_ms_p50": round(st["step_ms_p50"], 3), "step_ms_p99": round(step_p99_all, 3),
            "request_ms_p50": round(float(np.percentile(total_ms, 50)), 1),
-           "request_ms_p99": round(float(np.percentile(total_ms, 99)), 1),
+           "request_ms_p99": round(req_p99_all, 1),
            "queue_ms_p99": round(st["queue_ms_p99"], 1),
            "resident_peak": st["resident_peak"], "arena_bytes": st["device_bytes"],
            "lanes": args.serving_lanes, "order": args.serving_order,
            "substeps_per_launch": args.serving_substeps,
            "max_avg_density_error": max(d[2]["error_average"] for d in done),
            "requests_above_0.1%": int(sum(d[2]["error_average"] > TOL_0_1 for d in done))}
+    if world > 1:
+        out["routed_to_rank0"] = len(my_reqs) if rank == 0 else None
+        return out
     # the same requests one at a time, bounded in time
     t0 = time.perf_counter()
     served = 0

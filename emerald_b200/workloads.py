@@ -86,3 +86,19 @@ def assign_scenes(sizes, world):
     for lst in out:
         lst.sort()
     return out
+
+
+def route_requests(requests, world):
+    """Routes a request stream (serving_requests dicts, in arrival order) to
+    `world` GPUs, each with its own request loop: every request goes, as it
+    arrives, to the rank with the least work routed so far (fluid particles
+    x sub-steps; ties to the lower rank). Returns a list of request-index
+    lists, one per rank, each in arrival order. Deterministic, so every
+    process computes the same routing without exchanging anything."""
+    load = [0] * world
+    out = [[] for _ in range(world)]
+    for k, r in enumerate(requests):
+        j = min(range(world), key=lambda q: (load[q], q))
+        out[j].append(k)
+        load[j] += int(r["nx"]) * int(r["ny"]) * int(r["substeps"])
+    return out
