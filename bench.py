@@ -424,6 +424,8 @@ def run_gpu(args):
         serving = run_serving(args, torch, E, rank, world, barrier)
         if rank == 0:
             result["serving"] = serving
+    if args.config1 and world == 1:
+        result["config1"] = run_config1(args, torch, E, flush)
     if args.literal_steps > 0 and world == 1:
         result["pcisph_h2dx"] = run_pcisph_literal(args, torch, E, flush)
     if world > 1:
@@ -431,6 +433,64 @@ def run_gpu(args):
         dist.barrier()
         dist.destroy_process_group()
     return result
+
+
+def run_config1(args, torch, E, flush):
+    """The first configuration: the IISPH dam break of 128 x 128 = 16,384
+    fluid particles at dx = 1/256 (support = dx, boundary volumes m / rho0,
+    square-lattice mass), fixed dt = 1e-4 s, at most 50 pressure iterations
+    at 0.1% average density error, 100 sub-steps from rest, timed as one
+    stretch with CUDA events (the L2 flushed before it). The reference's CPU
+    time for the same 100 sub-steps is timed beside it on the host cores
+    (oracle/_ref)."""
+    dx = np.float32(1.0 / 256)
+    scene = E.BlockScene(128, dx=dx, seed=1, time_per_step_flicks=TPS_FLICKS, sub_steps=4,
+                         iisph_max_pressure_iterations=50,
+                         iisph_error_average_threshold=np.float32(0.001))
+    sim = E.Simulation.from_block_scene(scene)
+    n = sim.n
+    sim.begin_frame("iisph")
+    flush.zero_()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    last = None
+    for k in range(100):
+        last = sim.sub_step("iisph", np.float32(k * 1e-4), np.float32(1e-4))
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    sim.close()
+    out = {"workload": "IISPH dam break, 128x128=16384 fluid particles, dx=1/256, support=dx, "
+                       "fixed dt=1e-4 s, 50 iterations at most, 0.1% tolerance, 100 sub-steps "
+                       "from rest",
+           "steps": 100, "ms_total": round(ms, 3), "ms_per_step": round(ms / 100, 4),
+           "particle_steps_per_s": round(n * 100 / (ms / 1000.0), 1),
+           "last_step": {k: last[k] for k in ("pressure_iterations", "error_average")},
+           "note": "each sub-step reads its statistics back (one host wait per sub-step)"}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from cpu_checkers import Reference, RefParams
+        if Reference.available:
+            R = Reference()
+            threads = os.cpu_count() or 1
+            R.set_threads(threads)
+            d = scene.params.as_dict()
+            rp = {k: d[k] for k, _ in RefParams._fields_ if k in d}
+            rp.update(mass_per_particle_override=d["mass_per_particle"],
+                      pressure_correction_denom_override=d["pressure_correction_denom"])
+            ref = R.sim(rp, scene.solid, scene.fluid, None, scene.solid_volumes)
+            ref.begin_frame("iisph")
+            t0 = time.perf_counter()
+            for k in range(100):
+                ref.sub_step("iisph", np.float32(k * 1e-4), np.float32(1e-4))
+            cpu_s = time.perf_counter() - t0
+            out["cpu_baseline"] = {"value": round(n * 100 / cpu_s, 1),
+                                   "unit": "particle-steps/s", "cores": threads,
+                                   "kind": "reference", "seconds": round(cpu_s, 3),
+                                   "sample": "the same 100 fixed-dt IISPH sub-steps on the "
+                                             "reference's CPU code (oracle/_ref)"}
+    return out
 
 
 def run_pcisph_literal(args, torch, E, flush):
@@ -775,6 +835,8 @@ def main():
                     help="request loop queue order")
     ap.add_argument("--literal-steps", type=int, default=20,
                     help="PCISPH sub-steps of the scene at the literal support h = 2 dx (0: skip)")
+    ap.add_argument("--no-config1", dest="config1", action="store_false",
+                    help="skip the 16,384-particle fixed-dt IISPH configuration")
     ap.add_argument("--no-side1m", dest="side1m", action="store_false",
                     help="skip the 1,048,576-particle north-star scene")
     ap.add_argument("--side", type=int, default=512,

@@ -622,8 +622,10 @@ int autotune_into(Engine& engine, int32_t method, emerald_tuning* out) {
                 *out = emerald_tuning{};
                 auto split = [](int v, int32_t& chunk, int32_t& prefetch) {
                     chunk = v & kChunkMask;
-                    prefetch = (v & kPersistentWarps) ? EMERALD_TUNE_PERSISTENT
-                                                      : ((v & kPrefetchLists) ? 1 : 0);
+                    prefetch = (v & kPersistentWarps)
+                                 ? ((v & kPersistentBlocks256) ? EMERALD_TUNE_PERSISTENT_256
+                                                               : EMERALD_TUNE_PERSISTENT)
+                                 : ((v & kPrefetchLists) ? 1 : 0);
                 };
                 split(r.chosen.apply, out->apply_chunk, out->prefetch[0]);
                 split(r.chosen.divergence, out->divergence_chunk, out->prefetch[1]);
@@ -661,12 +663,12 @@ int set_tuning_of(Engine& engine, emerald_tuning const* t) {
             return fail(EMERALD_EINVAL, "chunks must be 1, 4 or 8");
         }
         int32_t const mode = t->prefetch[k];
-        bool const persistent_ok = k < 2;  // the DFSPH_P families
-        if (mode != 0 && mode != 1 && !(mode == EMERALD_TUNE_PERSISTENT && persistent_ok)) {
-            return fail(EMERALD_EINVAL, "prefetch must be 0 or 1, or 2 for apply and divergence");
+        if (mode < 0 || mode > EMERALD_TUNE_PERSISTENT_256) {
+            return fail(EMERALD_EINVAL, "prefetch must be 0, 1, 2 or 3");
         }
         v[k] = chunks[k] | (mode == 1 ? kPrefetchLists : 0) |
-               (mode == EMERALD_TUNE_PERSISTENT ? kPersistentWarps : 0);
+               (mode >= EMERALD_TUNE_PERSISTENT ? kPersistentWarps : 0) |
+               (mode == EMERALD_TUNE_PERSISTENT_256 ? kPersistentBlocks256 : 0);
     }
     Engine::Tuning tu;
     tu.apply = v[0];

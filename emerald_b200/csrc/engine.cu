@@ -870,8 +870,7 @@ void Engine::emit_substep(int32_t method, bool reorder) {
     switch (method) {
     case kDfsph:
         launch("dfsph_density_alpha", [&] {
-            launch_dfsph_density_alpha(a_, tiles, compensated_, st,
-                                       (tuning_.divergence & kPersistentWarps) != 0);
+            launch_dfsph_density_alpha(a_, tiles, compensated_, st, tuning_.divergence);
         });
         launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 0, compensated_, st, tuning_.apply); });
         run_loop(2, max_iterations(2), method);
@@ -1185,9 +1184,12 @@ Engine::TuneReport Engine::autotune(int32_t method, int substeps) {
         // and with kPersistentWarps (W), the persistent-warp kernels
         int const P = kPrefetchLists;
         int const W = kPersistentWarps;
+        // (W2: the same in blocks of 256 threads)
+        int const W2 = kPersistentWarps | kPersistentBlocks256;
         int const opts[][2] = {{4, 8}, {1, 4}, {4, 4}, {1, 8}, {8, 8},
                                {1 | P, 4 | P}, {4 | P, 8 | P}, {1 | P, 4},
-                               {1 | W, 4 | W}, {4 | W, 4 | W}, {1 | W, 1 | W}, {4 | W, 8 | W}};
+                               {1 | W, 4 | W}, {4 | W, 4 | W}, {1 | W, 1 | W}, {4 | W, 8 | W},
+                               {1 | W2, 4 | W2}, {4 | W2, 4 | W2}};
         for (auto const& o : opts) {
             Tuning t = tuning_;
             t.apply = o[0];
@@ -1196,8 +1198,11 @@ Engine::TuneReport Engine::autotune(int32_t method, int substeps) {
         }
     } else {
         int const P = kPrefetchLists;
+        int const W = kPersistentWarps;
+        int const W2 = kPersistentWarps | kPersistentBlocks256;
         int const opts[][2] = {{4, 4}, {1, 1}, {1, 4}, {4, 1}, {8, 4},
-                               {4 | P, 4 | P}, {1 | P, 1 | P}, {4 | P, 1 | P}};
+                               {4 | P, 4 | P}, {1 | P, 1 | P}, {4 | P, 1 | P},
+                               {4 | W, 4 | W}, {1 | W, 1 | W}, {1 | W, 4 | W}, {4 | W2, 4 | W2}};
         for (auto const& o : opts) {
             Tuning t = tuning_;
             t.iisph_sum = o[0];

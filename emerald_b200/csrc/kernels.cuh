@@ -76,9 +76,10 @@ void launch_iter_reset(Arena const& a, int nscenes, int kind, cudaStream_t st);
 void launch_iter_check(Arena const& a, int nscenes, int kind, int* running,
                        cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st);
 // comp: some resident scene is in compensated mode (selects the kernel variant)
-// persistent: the persistent-warp variant (same bits)
+// mode: the divergence family's tuning value; with kPersistentWarps the
+// persistent-warp variant (same bits)
 void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st,
-                                bool persistent = false);
+                                int mode = 0);
 // chunk: neighbour entries loaded together in the gather sums (1, 4 or 8;
 // every choice gives the same bits), plus kPrefetchLists to have each warp
 // ask L2 for its list rows before the sums
@@ -88,6 +89,8 @@ constexpr int kPrefetchLists = 16;
 // tile's lists already requested into L2 (same bits; kPrefetchLists is
 // implied)
 constexpr int kPersistentWarps = 32;
+// with kPersistentWarps: blocks of 256 threads instead of 128
+constexpr int kPersistentBlocks256 = 64;
 constexpr int kChunkMask = 15;
 void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int external,
                             int skip_done, bool comp, cudaStream_t st, int chunk = 4);

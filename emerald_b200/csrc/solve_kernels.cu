@@ -817,18 +817,19 @@ __device__ __forceinline__ void flush_err(Arena const& a, WarpErr& e) {
     e = WarpErr{-1, 0ull, 0u, 0.0};
 }
 
-// accumulate_error's contribution of one particle, kept in the warp.
-__device__ __forceinline__ void add_err(Arena const& a, WarpErr& e, int32_t scene, float err,
-                                        bool live) {
+// accumulate_error's contribution of one particle (its integer v and
+// error m, the exact sum too when `exact`), kept in the warp.
+__device__ __forceinline__ void add_err(Arena const& a, WarpErr& e, int32_t scene,
+                                        unsigned long long v, float m, bool live, bool exact) {
     if (scene != e.scene) {
         flush_err(a, e);
         e.scene = scene;
     }
     if (live) {
-        e.sum += static_cast<unsigned long long>(static_cast<long long>(err * 1000.0f));
-        if (err == err && err > 0.0f) {
-            e.max = max(e.max, __float_as_uint(err));
-            e.exact += static_cast<double>(err);
+        e.sum += v;
+        if (m == m && m > 0.0f) {
+            e.max = max(e.max, __float_as_uint(m));
+            if (exact) e.exact += static_cast<double>(m);
         }
     }
 }
@@ -866,7 +867,7 @@ __device__ __forceinline__ void walk_warp_tiles(Arena const& a, uint32_t wtiles,
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kTile) k_dfsph_density_alpha_pw(Arena a, uint32_t wtiles) {
+__global__ void __launch_bounds__(256) k_dfsph_density_alpha_pw(Arena a, uint32_t wtiles) {
     walk_warp_tiles(
       a, wtiles, false,
       [&](uint32_t base, int count) {
@@ -884,7 +885,7 @@ __global__ void __launch_bounds__(kTile) k_dfsph_density_alpha_pw(Arena a, uint3
 }
 
 template <int MODE, int CH>
-__global__ void __launch_bounds__(kTile) k_apply_pressures_pw(Arena a, uint32_t wtiles, int which_q,
+__global__ void __launch_bounds__(256) k_apply_pressures_pw(Arena a, uint32_t wtiles, int which_q,
                                                             int external, int skip_done) {
     float const* q = which_q ? a.qdens : a.qdiv;
     walk_warp_tiles(
@@ -905,7 +906,7 @@ __global__ void __launch_bounds__(kTile) k_apply_pressures_pw(Arena a, uint32_t 
 }
 
 template <int MODE, int CH>
-__global__ void __launch_bounds__(kTile) k_dfsph_divergence_pw(Arena a, uint32_t wtiles) {
+__global__ void __launch_bounds__(256) k_dfsph_divergence_pw(Arena a, uint32_t wtiles) {
     WarpErr e{-1, 0ull, 0u, 0.0};
     walk_warp_tiles(
       a, wtiles, true,
@@ -930,13 +931,15 @@ __global__ void __launch_bounds__(kTile) k_dfsph_divergence_pw(Arena a, uint32_t
               a.qdiv[i] = p_over_rho2(kappa, a.rho[i]);
               err = d <= 0.0f ? 0.0f : (dt * d / P.rho0);
           }
-          add_err(a, e, s, err, live);
+          add_err(a, e, s,
+                  static_cast<unsigned long long>(static_cast<long long>(err * 1000.0f)), err,
+                  live, true);
       });
     flush_err(a, e);
 }
 
 template <int MODE, int CH>
-__global__ void __launch_bounds__(kTile) k_dfsph_density_pw(Arena a, uint32_t wtiles) {
+__global__ void __launch_bounds__(256) k_dfsph_density_pw(Arena a, uint32_t wtiles) {
     WarpErr e{-1, 0ull, 0u, 0.0};
     walk_warp_tiles(
       a, wtiles, true,
@@ -966,7 +969,9 @@ __global__ void __launch_bounds__(kTile) k_dfsph_density_pw(Arena a, uint32_t wt
               a.qdens[i] = p_over_rho2(kappa, rho);
               err = delta <= 0.0f ? 0.0f : (delta / rho0);
           }
-          add_err(a, e, s, err, live);
+          add_err(a, e, s,
+                  static_cast<unsigned long long>(static_cast<long long>(err * 1000.0f)), err,
+                  live, true);
       });
     flush_err(a, e);
 }
@@ -1246,6 +1251,50 @@ __global__ void k_iisph_beta_pressure(Arena a) {
     }
     accumulate_error(S, counted ? static_cast<unsigned long long>(err * 1000.0f) : 0ull, err,
                      c.live && counted);
+}
+
+// The two IISPH gather kernels as persistent warps (see the DFSPH ones
+// above): the batched workload's per-iteration sums.
+template <int MODE, int CH>
+__global__ void __launch_bounds__(256) k_iisph_sum_dij_pw(Arena a, uint32_t wtiles) {
+    walk_warp_tiles(
+      a, wtiles, true,
+      [&](uint32_t base, int count) {
+          prefetch_warp_tile<false>(a, base, count, nullptr, nullptr, nullptr);
+      },
+      [&](int32_t s, uint32_t i, bool live) {
+          if (!live) return;
+          Ctx const c{s, i, true};
+          if (MODE && a.sp[s].precision) {
+              iisph_sum_dij<true, CH>(a, c);
+          } else {
+              iisph_sum_dij<false, CH>(a, c);
+          }
+      });
+}
+
+template <int MODE, int CH>
+__global__ void __launch_bounds__(256) k_iisph_beta_pressure_pw(Arena a, uint32_t wtiles) {
+    WarpErr e{-1, 0ull, 0u, 0.0};
+    walk_warp_tiles(
+      a, wtiles, true,
+      [&](uint32_t base, int count) {
+          prefetch_warp_tile<false>(a, base, count, a.ns_cnt + base, a.sdp + base,
+                                    a.sdp + base + 16, a.aii + base, a.rho_star + base);
+      },
+      [&](int32_t s, uint32_t i, bool live) {
+          SceneState* S = &a.ss[s];
+          float err = 0.0f;
+          bool counted = false;
+          if (live) {
+              Ctx const c{s, i, true};
+              counted = (MODE && a.sp[s].precision) ? iisph_beta_pressure<true, CH>(a, c, S, err)
+                                                    : iisph_beta_pressure<false, CH>(a, c, S, err);
+          }
+          add_err(a, e, s, counted ? static_cast<unsigned long long>(err * 1000.0f) : 0ull, err,
+                  live && counted, false);
+      });
+    flush_err(a, e);
 }
 
 // q = safe_divide(p, rho^2) of the final pressures, for apply_pressures.
@@ -1611,7 +1660,7 @@ __global__ void k_pc_final(Arena a) {
 // Blocks of a persistent-warp launch: the resident blocks of `kernel` on
 // every multiprocessor, no more than the tiles to cover.
 template <class K>
-unsigned persistent_grid(K kernel, uint32_t tiles) {
+unsigned persistent_grid(K kernel, uint32_t tiles, int threads = kTile) {
     static thread_local int dev_cached = -1;
     static thread_local int sms = 0;
     int dev = 0;
@@ -1621,9 +1670,10 @@ unsigned persistent_grid(K kernel, uint32_t tiles) {
         dev_cached = dev;
     }
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTile, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
     uint64_t const g = uint64_t(std::max(per_sm, 1)) * uint64_t(std::max(sms, 1));
-    return unsigned(std::max<uint64_t>(1, std::min<uint64_t>(g, tiles)));
+    uint64_t const need = (uint64_t(tiles) * kTile + threads - 1) / threads;
+    return unsigned(std::max<uint64_t>(1, std::min<uint64_t>(g, need)));
 }
 
 #define EMLD_DISPATCH(K, comp, ch, pf)                                        \
@@ -1667,16 +1717,17 @@ void launch_iter_check(Arena const& a, int nscenes, int kind, int* running,
     k_iter_check<<<1, 256, 0, st>>>(a, nscenes, kind, running, cond, use_cond);
 }
 void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st,
-                                bool persistent) {
+                                int mode) {
     if (!tiles) return;
-    if (persistent) {
+    if (mode & kPersistentWarps) {
         uint32_t const wt = tiles * (kTile / 32);
+        int const th = (mode & kPersistentBlocks256) ? 256 : kTile;
         if (comp) {
             k_dfsph_density_alpha_pw<1>
-              <<<persistent_grid(k_dfsph_density_alpha_pw<1>, tiles), kTile, 0, st>>>(a, wt);
+              <<<persistent_grid(k_dfsph_density_alpha_pw<1>, tiles, th), th, 0, st>>>(a, wt);
         } else {
             k_dfsph_density_alpha_pw<0>
-              <<<persistent_grid(k_dfsph_density_alpha_pw<0>, tiles), kTile, 0, st>>>(a, wt);
+              <<<persistent_grid(k_dfsph_density_alpha_pw<0>, tiles, th), th, 0, st>>>(a, wt);
         }
         return;
     }
@@ -1701,8 +1752,9 @@ void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int ext
     bool const pf = (chunk & kPrefetchLists) != 0;
     int const ch = chunk & kChunkMask;
     if (chunk & kPersistentWarps) {
+        int const th = (chunk & kPersistentBlocks256) ? 256 : kTile;
 #define EMLD_APPLY_PW(M, C)                                                                     \
-    k_apply_pressures_pw<M, C><<<persistent_grid(k_apply_pressures_pw<M, C>, tiles), kTile, 0, st>>>( \
+    k_apply_pressures_pw<M, C><<<persistent_grid(k_apply_pressures_pw<M, C>, tiles, th), th, 0, st>>>( \
       a, tiles * (kTile / 32), which_q, external, skip_done)
         EMLD_PW_DISPATCH(EMLD_APPLY_PW, comp, ch);
 #undef EMLD_APPLY_PW
@@ -1717,8 +1769,9 @@ void launch_dfsph_divergence(Arena const& a, uint32_t tiles, bool comp, cudaStre
     bool const pf = (chunk & kPrefetchLists) != 0;
     int const ch = chunk & kChunkMask;
     if (chunk & kPersistentWarps) {
+        int const th = (chunk & kPersistentBlocks256) ? 256 : kTile;
 #define EMLD_DIV_PW(M, C)                                                                         \
-    k_dfsph_divergence_pw<M, C><<<persistent_grid(k_dfsph_divergence_pw<M, C>, tiles), kTile, 0, st>>>( \
+    k_dfsph_divergence_pw<M, C><<<persistent_grid(k_dfsph_divergence_pw<M, C>, tiles, th), th, 0, st>>>( \
       a, tiles * (kTile / 32))
         EMLD_PW_DISPATCH(EMLD_DIV_PW, comp, ch);
 #undef EMLD_DIV_PW
@@ -1733,8 +1786,9 @@ void launch_dfsph_density(Arena const& a, uint32_t tiles, bool comp, cudaStream_
     bool const pf = (chunk & kPrefetchLists) != 0;
     int const ch = chunk & kChunkMask;
     if (chunk & kPersistentWarps) {
+        int const th = (chunk & kPersistentBlocks256) ? 256 : kTile;
 #define EMLD_DENS_PW(M, C)                                                                    \
-    k_dfsph_density_pw<M, C><<<persistent_grid(k_dfsph_density_pw<M, C>, tiles), kTile, 0, st>>>( \
+    k_dfsph_density_pw<M, C><<<persistent_grid(k_dfsph_density_pw<M, C>, tiles, th), th, 0, st>>>( \
       a, tiles * (kTile / 32))
         EMLD_PW_DISPATCH(EMLD_DENS_PW, comp, ch);
 #undef EMLD_DENS_PW
@@ -1766,16 +1820,36 @@ void launch_iisph_aii(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp
     }
 }
 void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk, bool comp) {
+    if (!tiles) return;
     bool const pf = (chunk & kPrefetchLists) != 0;
     int const ch = chunk & kChunkMask;
+    if (chunk & kPersistentWarps) {
+        int const th = (chunk & kPersistentBlocks256) ? 256 : kTile;
+#define EMLD_SUM_PW(M, C)                                                                       \
+    k_iisph_sum_dij_pw<M, C><<<persistent_grid(k_iisph_sum_dij_pw<M, C>, tiles, th), th, 0, st>>>( \
+      a, tiles * (kTile / 32))
+        EMLD_PW_DISPATCH(EMLD_SUM_PW, comp, ch);
+#undef EMLD_SUM_PW
+        return;
+    }
 #define EMLD_SUM(M, C, F) k_iisph_sum_dij<M, C, F><<<tiles, kTile, 0, st>>>(a)
     EMLD_DISPATCH(EMLD_SUM, comp, ch, pf);
 #undef EMLD_SUM
 }
 void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk,
                                 bool comp) {
+    if (!tiles) return;
     bool const pf = (chunk & kPrefetchLists) != 0;
     int const ch = chunk & kChunkMask;
+    if (chunk & kPersistentWarps) {
+        int const th = (chunk & kPersistentBlocks256) ? 256 : kTile;
+#define EMLD_BETA_PW(M, C)                                                                   \
+    k_iisph_beta_pressure_pw<M, C>                                                           \
+      <<<persistent_grid(k_iisph_beta_pressure_pw<M, C>, tiles, th), th, 0, st>>>(a, tiles * (kTile / 32))
+        EMLD_PW_DISPATCH(EMLD_BETA_PW, comp, ch);
+#undef EMLD_BETA_PW
+        return;
+    }
 #define EMLD_BETA(M, C, F) k_iisph_beta_pressure<M, C, F><<<tiles, kTile, 0, st>>>(a)
     EMLD_DISPATCH(EMLD_BETA, comp, ch, pf);
 #undef EMLD_BETA

@@ -364,9 +364,10 @@ int emerald_batch_kernel_launches(emerald_batch* batch, int64_t* count);
 /* Neighbour entries each gather-sum kernel loads together (1, 4 or 8), and
  * how it brings its lists in (prefetch): 0 loads them as the sums need
  * them; 1 has each warp first ask L2 for its list rows;
- * EMERALD_TUNE_PERSISTENT (2; DFSPH_P families only) launches one grid of
- * resident blocks whose warps walk their 32-particle tiles and request the
- * next tile's lists and inputs into L2 while they fold the current one.
+ * EMERALD_TUNE_PERSISTENT (2) launches one grid of resident blocks of 128
+ * threads whose warps walk their 32-particle tiles and request the next
+ * tile's lists and inputs into L2 while they fold the current one;
+ * EMERALD_TUNE_PERSISTENT_256 (3) the same in blocks of 256 threads.
  * Every choice gives the same bits. Autotuning (DFSPH_P and IISPH) times a
  * few whole sub-steps of `method` with each candidate setting, every
  * candidate from the same state (restored afterwards, so the simulation is
@@ -379,6 +380,7 @@ int emerald_batch_kernel_launches(emerald_batch* batch, int64_t* count);
  * family's mode also applies to the DFSPH density and alpha pass). No
  * counterpart in the reference. */
 #define EMERALD_TUNE_PERSISTENT 2
+#define EMERALD_TUNE_PERSISTENT_256 3
 #define EMERALD_TUNE_CANDIDATES 16
 typedef struct emerald_tuning {
     int32_t apply_chunk, divergence_chunk, iisph_sum_chunk, iisph_beta_chunk;
