@@ -817,6 +817,53 @@ __device__ __forceinline__ void flush_err(Arena const& a, WarpErr& e) {
     e = WarpErr{-1, 0ull, 0u, 0.0};
 }
 
+// The warps' remaining sums, combined per block in shared memory and sent
+// to the scene's accumulators with one set of atomics per block (a warp
+// whose scene differs from the block's first flushing warp sends its own).
+// Every thread of the block calls it.
+__device__ __forceinline__ void flush_err_block(Arena const& a, WarpErr& e) {
+    __shared__ unsigned long long b_sum;
+    __shared__ uint32_t b_max;
+    __shared__ double b_exact;
+    __shared__ int b_scene;
+    if (threadIdx.x == 0) {
+        b_sum = 0ull;
+        b_max = 0u;
+        b_exact = 0.0;
+        b_scene = -1;
+    }
+    __syncthreads();
+    unsigned long long v = e.sum;
+    uint32_t m = e.max;
+    double d = e.exact;
+    for (int o = 16; o; o >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+        m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        d += __shfl_xor_sync(0xffffffffu, d, o);
+    }
+    if ((threadIdx.x & 31) == 0 && e.scene >= 0) {
+        int const prev = atomicCAS(&b_scene, -1, e.scene);
+        if (prev == -1 || prev == e.scene) {
+            atomicAdd(&b_sum, v);
+            atomicMax(&b_max, m);
+            atomicAdd(&b_exact, d);
+        } else {
+            SceneState* S = &a.ss[e.scene];
+            if (v) atomicAdd(&S->err_sum, v);
+            if (m) atomicMax(&S->err_max, m);
+            if (d != 0.0) atomicAdd(&S->err_sum_d, d);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && b_scene >= 0) {
+        SceneState* S = &a.ss[b_scene];
+        if (b_sum) atomicAdd(&S->err_sum, b_sum);
+        if (b_max) atomicMax(&S->err_max, b_max);
+        if (b_exact != 0.0) atomicAdd(&S->err_sum_d, b_exact);
+    }
+    e = WarpErr{-1, 0ull, 0u, 0.0};
+}
+
 // accumulate_error's contribution of one particle (its integer v and
 // error m, the exact sum too when `exact`), kept in the warp.
 __device__ __forceinline__ void add_err(Arena const& a, WarpErr& e, int32_t scene,
@@ -836,16 +883,17 @@ __device__ __forceinline__ void add_err(Arena const& a, WarpErr& e, int32_t scen
 
 // Walks this warp's tiles: prefetch(base, count) asks L2 for a tile's data,
 // body(scene, i, live) folds particle i of an active tile. Every lane of
-// the warp runs every iteration (tile checks are warp-uniform).
+// the warp runs every iteration (tile checks are warp-uniform), and every
+// thread of the block returns from it (no early exit, so the kernels can
+// meet at a block barrier afterwards).
 template <class Prefetch, class Body>
 __device__ __forceinline__ void walk_warp_tiles(Arena const& a, uint32_t wtiles, bool skip_done,
                                                 Prefetch prefetch, Body body) {
     uint32_t const lane = threadIdx.x & 31u;
     uint32_t const G = (gridDim.x * blockDim.x) >> 5;
     uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (t >= wtiles) return;
     int cnt_next = (t + G < wtiles) ? int(a.nf_cnt[(t + G) * 32u + lane]) : 0;
-    prefetch(t * 32u, int(a.nf_cnt[t * 32u + lane]));
+    if (t < wtiles) prefetch(t * 32u, int(a.nf_cnt[t * 32u + lane]));
     for (; t < wtiles; t += G) {
         uint32_t const tn = t + G;
         int cnt_after = 0;
@@ -935,7 +983,7 @@ __global__ void __launch_bounds__(256) k_dfsph_divergence_pw(Arena a, uint32_t w
                   static_cast<unsigned long long>(static_cast<long long>(err * 1000.0f)), err,
                   live, true);
       });
-    flush_err(a, e);
+    flush_err_block(a, e);
 }
 
 template <int MODE, int CH>
@@ -973,7 +1021,7 @@ __global__ void __launch_bounds__(256) k_dfsph_density_pw(Arena a, uint32_t wtil
                   static_cast<unsigned long long>(static_cast<long long>(err * 1000.0f)), err,
                   live, true);
       });
-    flush_err(a, e);
+    flush_err_block(a, e);
 }
 
 // integrate_positions_in_place (dynamics.cpp:46-51). Compensated mode
@@ -1294,7 +1342,7 @@ __global__ void __launch_bounds__(256) k_iisph_beta_pressure_pw(Arena a, uint32_
           add_err(a, e, s, counted ? static_cast<unsigned long long>(err * 1000.0f) : 0ull, err,
                   live && counted, false);
       });
-    flush_err(a, e);
+    flush_err_block(a, e);
 }
 
 // q = safe_divide(p, rho^2) of the final pressures, for apply_pressures.
