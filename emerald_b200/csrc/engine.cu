@@ -960,10 +960,16 @@ void Engine::capture_frame(int32_t method, bool reorder) {
     cur_ = cap_st_;
     cudaGraph_t g = nullptr;
     auto abort = [&] {
-        cudaGraph_t dead = nullptr;
-        cudaStreamEndCapture(frame_st_, &dead);
-        cudaStreamEndCapture(cap_st_, &dead);
-        if (dead) cudaGraphDestroy(dead);
+        for (cudaStream_t sst : {body_st_, frame_st_, cap_st_}) {
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            if (cudaStreamIsCapturing(sst, &cs) == cudaSuccess &&
+                cs != cudaStreamCaptureStatusNone) {
+                cudaGraph_t dead = nullptr;
+                cudaStreamEndCapture(sst, &dead);
+                if (dead) cudaGraphDestroy(dead);
+            }
+        }
+        cudaGetLastError();
         capturing_ = false;
         cur_ = st_;
     };
@@ -1037,7 +1043,7 @@ void Engine::capture_frame(int32_t method, bool reorder) {
 
 int Engine::frame(int id, int32_t method, SceneState& out) {
     if (!use_graphs_ || timing_ || has_force_callbacks() || active_scenes() != 1 ||
-        !scenes_[id].active) {
+        !scenes_[id].active || !frame_graphs_ok_) {
         // host loop: one sub-step at a time, the frame's end read after each
         int n = 0;
         do {
@@ -1053,7 +1059,15 @@ int Engine::frame(int id, int32_t method, SceneState& out) {
     int const key = method * 2 + (reorder ? 1 : 0);
     auto it = frame_graphs_.find(key);
     if (it == frame_graphs_.end()) {
-        capture_frame(method, reorder);
+        try {
+            capture_frame(method, reorder);
+        } catch (std::runtime_error const&) {
+            // a device or driver without the frame graph's nested
+            // conditional nodes: frames keep the host loop from now on
+            frame_graphs_ok_ = false;
+            --frames_launched_;
+            return frame(id, method, out);
+        }
         it = frame_graphs_.find(key);
     }
     if (cudaGraphLaunch(it->second, st_) != cudaSuccess) {

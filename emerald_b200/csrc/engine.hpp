@@ -245,6 +245,7 @@ private:
     void capture_frame(int32_t method, bool reorder);
     void prepare_substep(int32_t method);
     int64_t frames_launched_ = 0;
+    bool frame_graphs_ok_ = true;
     void host_wait(cudaStream_t s) {
         ++host_waits_;
         cudaStreamSynchronize(s);
