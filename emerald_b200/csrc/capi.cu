@@ -624,7 +624,8 @@ int autotune_into(Engine& engine, int32_t method, emerald_tuning* out) {
                     chunk = v & kChunkMask;
                     prefetch = (v & kPersistentWarps)
                                  ? ((v & kPersistentBlocks256) ? EMERALD_TUNE_PERSISTENT_256
-                                                               : EMERALD_TUNE_PERSISTENT)
+                                                               : EMERALD_TUNE_PERSISTENT) +
+                                     ((v & kFusedExitTest) ? 2 : 0)
                                  : ((v & kPrefetchLists) ? 1 : 0);
                 };
                 split(r.chosen.apply, out->apply_chunk, out->prefetch[0]);
@@ -663,12 +664,15 @@ int set_tuning_of(Engine& engine, emerald_tuning const* t) {
             return fail(EMERALD_EINVAL, "chunks must be 1, 4 or 8");
         }
         int32_t const mode = t->prefetch[k];
-        if (mode < 0 || mode > EMERALD_TUNE_PERSISTENT_256) {
-            return fail(EMERALD_EINVAL, "prefetch must be 0, 1, 2 or 3");
+        if (mode < 0 || mode > EMERALD_TUNE_PERSISTENT_256_FUSED) {
+            return fail(EMERALD_EINVAL, "prefetch must be between 0 and 5");
         }
         v[k] = chunks[k] | (mode == 1 ? kPrefetchLists : 0) |
                (mode >= EMERALD_TUNE_PERSISTENT ? kPersistentWarps : 0) |
-               (mode == EMERALD_TUNE_PERSISTENT_256 ? kPersistentBlocks256 : 0);
+               ((mode == EMERALD_TUNE_PERSISTENT_256 || mode == EMERALD_TUNE_PERSISTENT_256_FUSED)
+                  ? kPersistentBlocks256
+                  : 0) |
+               (mode >= EMERALD_TUNE_PERSISTENT_FUSED ? kFusedExitTest : 0);
     }
     Engine::Tuning tu;
     tu.apply = v[0];

@@ -119,7 +119,7 @@ size_t Engine::footprint(uint32_t fluid_capacity, uint32_t solid_capacity, int m
     bytes += r(8 * stab) + r(4 * (stab + 1)) + r(4 * stab); // solid cell table
     size_t const scan_words = std::max(scan_scratch_words(uint32_t(ftab)),
                                        scan_scratch_words(uint32_t(stab))) + 64;
-    bytes += r(4 * scan_words) + r(sizeof(int)) + r(sizeof(uint32_t)) +
+    bytes += r(4 * scan_words) + r(sizeof(int)) + 2 * r(sizeof(uint32_t)) +
              r(sizeof(unsigned long long) * kLoopSlots);
     return bytes;
 }
@@ -227,6 +227,8 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
     d_scan_ = static_cast<uint32_t*>(dev(4ull * scan_words));
     d_running_ = static_cast<int*>(dev(sizeof(int)));
     d_flag_ = static_cast<uint32_t*>(dev(sizeof(uint32_t)));
+    d_check_counter_ = static_cast<unsigned int*>(dev(sizeof(unsigned int)));
+    cudaMemset(d_check_counter_, 0, sizeof(unsigned int));
     d_loop_iters_ = static_cast<unsigned long long*>(dev(sizeof(unsigned long long) * kLoopSlots));
     a_.loop_iterations = d_loop_iters_;
     cudaMemset(d_loop_iters_, 0, sizeof(unsigned long long) * kLoopSlots);
@@ -729,19 +731,29 @@ void Engine::emit_loop_body(int kind, int32_t method, cudaGraphConditionalHandle
     // loop kernels are counted on the device, once per executed iteration
     bool const was_counting = count_host_;
     count_host_ = false;
+    // the exit test in the last block of the iteration's final kernel, when
+    // that kernel is a persistent-warp one tuned to carry it
+    auto fused = [&](int v) {
+        return (v & kPersistentWarps) && (v & kFusedExitTest) && !timing_;
+    };
+    LoopCheck const lc{d_check_counter_, d_running_, cond, max_scenes_, kind, use_cond ? 1 : 0};
+    LoopCheck const none{nullptr, nullptr, 0, 0, 0, 0};
+    bool carried = false;
     switch (method) {
     case kDfsph:
+        carried = fused(tuning_.apply);
         if (kind == 2) {
             launch("dfsph_divergence", [&] { launch_dfsph_divergence(a_, tiles, compensated_, st, tuning_.divergence); });
-            launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 1, compensated_, st, tuning_.apply); });
+            launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 0, 0, 1, compensated_, st, tuning_.apply, carried ? lc : none); });
         } else {
             launch("dfsph_density", [&] { launch_dfsph_density(a_, tiles, compensated_, st, tuning_.divergence); });
-            launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 1, 0, 1, compensated_, st, tuning_.apply); });
+            launch("apply_pressures", [&] { launch_apply_pressures(a_, tiles, 1, 0, 1, compensated_, st, tuning_.apply, carried ? lc : none); });
         }
         break;
     case kIisph:
+        carried = fused(tuning_.iisph_beta);
         launch("iisph_sum_dij", [&] { launch_iisph_sum_dij(a_, tiles, st, tuning_.iisph_sum, compensated_); });
-        launch("iisph_beta_pressure", [&] { launch_iisph_beta_pressure(a_, tiles, st, tuning_.iisph_beta, compensated_); });
+        launch("iisph_beta_pressure", [&] { launch_iisph_beta_pressure(a_, tiles, st, tuning_.iisph_beta, compensated_, carried ? lc : none); });
         break;
     case kIisphAp:
     case kIisphPseudoAp: {
@@ -757,21 +769,22 @@ void Engine::emit_loop_body(int kind, int32_t method, cudaGraphConditionalHandle
         break;
     default: break;
     }
-    launch("iter_check", [&] {
-        launch_iter_check(a_, max_scenes_, kind, d_running_, cond, use_cond ? 1 : 0, st);
-    });
+    if (!carried) {
+        launch("iter_check", [&] {
+            launch_iter_check(a_, max_scenes_, kind, d_running_, cond, use_cond ? 1 : 0, st);
+        });
+    }
+    // kernels per executed iteration of this loop kind (body + check)
+    loop_kernels_[kind] = (kind == 3 ? 4 : 3) - (carried ? 1 : 0);
     count_host_ = was_counting;
 }
-
-// Kernels per executed iteration of each loop kind (body kernels + check).
-static int loop_body_kernels(int kind) { return kind == 3 ? 4 : 3; }
 
 int64_t Engine::kernel_launches() {
     unsigned long long it[kLoopSlots] = {};
     cudaMemcpyAsync(it, d_loop_iters_, sizeof(it), cudaMemcpyDeviceToHost, st_);
     host_wait(st_);
     int64_t n = host_launches_;
-    for (int k = 0; k < 4; ++k) n += int64_t(it[k]) * loop_body_kernels(k);
+    for (int k = 0; k < 4; ++k) n += int64_t(it[k]) * loop_kernels_[k];
     for (int m = 0; m < 5; ++m) n += int64_t(it[4 + m]) * frame_body_kernels_[m];
     return n;
 }
@@ -1200,10 +1213,13 @@ Engine::TuneReport Engine::autotune(int32_t method, int substeps) {
         int const W = kPersistentWarps;
         // (W2: the same in blocks of 256 threads)
         int const W2 = kPersistentWarps | kPersistentBlocks256;
+        // (F: the loop's exit test fused into the apply kernel's last block)
+        int const F = kFusedExitTest;
         int const opts[][2] = {{4, 8}, {1, 4}, {4, 4}, {1, 8}, {8, 8},
                                {1 | P, 4 | P}, {4 | P, 8 | P}, {1 | P, 4},
                                {1 | W, 4 | W}, {4 | W, 4 | W}, {1 | W, 1 | W}, {4 | W, 8 | W},
-                               {1 | W2, 4 | W2}, {4 | W2, 4 | W2}};
+                               {1 | W2, 4 | W2}, {4 | W2, 4 | W2},
+                               {1 | W | F, 4 | W}, {1 | W2 | F, 4 | W2}};
         for (auto const& o : opts) {
             Tuning t = tuning_;
             t.apply = o[0];
@@ -1214,9 +1230,11 @@ Engine::TuneReport Engine::autotune(int32_t method, int substeps) {
         int const P = kPrefetchLists;
         int const W = kPersistentWarps;
         int const W2 = kPersistentWarps | kPersistentBlocks256;
+        int const F = kFusedExitTest;
         int const opts[][2] = {{4, 4}, {1, 1}, {1, 4}, {4, 1}, {8, 4},
                                {4 | P, 4 | P}, {1 | P, 1 | P}, {4 | P, 1 | P},
-                               {4 | W, 4 | W}, {1 | W, 1 | W}, {1 | W, 4 | W}, {4 | W2, 4 | W2}};
+                               {4 | W, 4 | W}, {1 | W, 1 | W}, {1 | W, 4 | W}, {4 | W2, 4 | W2},
+                               {4 | W, 4 | W | F}, {4 | W2, 4 | W2 | F}};
         for (auto const& o : opts) {
             Tuning t = tuning_;
             t.iisph_sum = o[0];

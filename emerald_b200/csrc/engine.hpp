@@ -283,6 +283,8 @@ private:
     int* h_running_ = nullptr;
     uint32_t* d_flag_ = nullptr;
     uint32_t* h_flag_ = nullptr;
+    unsigned int* d_check_counter_ = nullptr;  // finished blocks of a fused exit test
+    int loop_kernels_[4] = {3, 3, 3, 4};        // kernels per iteration of each loop kind
     std::vector<Scene> scenes_;
     std::vector<int32_t> tile_scene_, stile_scene_;
     RangeAllocator fluid_tiles_, solid_tiles_, ftab_, stab_, near_words_;

@@ -91,9 +91,23 @@ constexpr int kPrefetchLists = 16;
 constexpr int kPersistentWarps = 32;
 // with kPersistentWarps: blocks of 256 threads instead of 128
 constexpr int kPersistentBlocks256 = 64;
+// with kPersistentWarps, on a solver loop's final kernel (DFSPH apply,
+// IISPH beta): the iteration's exit test runs in that kernel's last block
+constexpr int kFusedExitTest = 128;
 constexpr int kChunkMask = 15;
+// An iteration's exit test fused into the last block of its final
+// persistent-warp kernel (counter != nullptr; needs kPersistentWarps): the
+// loop kind, the scenes, the host-visible running flag, the loop's while
+// condition and a device counter of finished blocks (zero between launches).
+struct LoopCheck {
+    unsigned int* counter;
+    int* running;
+    cudaGraphConditionalHandle cond;
+    int nscenes, kind, use_cond;
+};
 void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int external,
-                            int skip_done, bool comp, cudaStream_t st, int chunk = 4);
+                            int skip_done, bool comp, cudaStream_t st, int chunk = 4,
+                            LoopCheck lc = LoopCheck{nullptr, nullptr, 0, 0, 0, 0});
 void launch_dfsph_divergence(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st,
                              int chunk = 8);
 void launch_dfsph_density(Arena const& a, uint32_t tiles, bool comp, cudaStream_t st,
@@ -106,7 +120,7 @@ void launch_iisph_density_dii(Arena const& a, uint32_t tiles, cudaStream_t st, b
 void launch_iisph_aii(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp);
 void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk, bool comp);
 void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk,
-                                bool comp);
+                                bool comp, LoopCheck lc = LoopCheck{nullptr, nullptr, 0, 0, 0, 0});
 void launch_make_q(Arena const& a, uint32_t tiles, cudaStream_t st);
 void launch_apply_integrate(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp);
 void launch_ap_density(Arena const& a, uint32_t tiles, cudaStream_t st, bool comp);

@@ -243,8 +243,13 @@ __global__ void k_iter_reset(Arena a, int nscenes, int kind) {
 // 2: DFSPH divergence (:187-211), 3: PCISPH (pcisph.cpp:144-148).
 // One block; *running is set when any scene still iterates and, inside a
 // captured graph, the loop's while condition takes the same value.
-__global__ void k_iter_check(Arena a, int nscenes, int kind, int* running,
-                             cudaGraphConditionalHandle cond, int use_cond) {
+// The exit test of one solver iteration for every scene (kind 0: IISPH
+// family, iisph.cpp:119-128; 1: DFSPH density, dfsph_p.cpp:113-133; 2: DFSPH
+// divergence, :187-211; 3: PCISPH, pcisph.cpp:144-148), run by one block.
+// With `fresh`, the scenes' error accumulators were written by other blocks
+// of the same kernel and are read through atomics (L2), not L1.
+__device__ void exit_test(Arena const& a, int nscenes, int kind, int* running,
+                          cudaGraphConditionalHandle cond, int use_cond, bool fresh) {
     __shared__ int any;
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
@@ -252,14 +257,17 @@ __global__ void k_iter_check(Arena a, int nscenes, int kind, int* running,
         SceneParams const& P = a.sp[s];
         SceneState& S = a.ss[s];
         if (!S.active || S.done) continue;
+        unsigned long long const err_sum = fresh ? atomicAdd(&S.err_sum, 0ull) : S.err_sum;
+        uint32_t const err_max = fresh ? atomicMax(&S.err_max, 0u) : S.err_max;
+        double const err_sum_d = fresh ? atomicAdd(&S.err_sum_d, 0.0) : S.err_sum_d;
         double const n = static_cast<double>(1000ull * P.fluid_count);
         float const avg = P.fluid_count
-                            ? static_cast<float>(static_cast<double>(S.err_sum) / n)
+                            ? static_cast<float>(static_cast<double>(err_sum) / n)
                             : 0.0f;
         // the exact mean of the errors, reported beside the reference's
         // metric (which drops each particle's error below 0.1%)
-        double const exact = P.fluid_count ? S.err_sum_d / static_cast<double>(P.fluid_count) : 0.0;
-        float const mx = __uint_as_float(S.err_max);
+        double const exact = P.fluid_count ? err_sum_d / static_cast<double>(P.fluid_count) : 0.0;
+        float const mx = __uint_as_float(err_max);
         bool conv = false;
         int const max_iter = iteration_cap(P, kind);
         if (kind == 0) {
@@ -306,6 +314,36 @@ __global__ void k_iter_check(Arena a, int nscenes, int kind, int* running,
         a.loop_iterations[kind] += 1ull;
         *running = any;
         if (use_cond) cudaGraphSetConditional(cond, any ? 1u : 0u);
+    }
+}
+
+// Exit test after one solver iteration, as its own one-block launch.
+// *running is set when any scene still iterates and, inside a captured
+// graph, the loop's while condition takes the same value.
+__global__ void k_iter_check(Arena a, int nscenes, int kind, int* running,
+                             cudaGraphConditionalHandle cond, int use_cond) {
+    exit_test(a, nscenes, kind, running, cond, use_cond, false);
+}
+
+// The exit test run by the last block of an iteration's final
+// persistent-warp kernel instead of its own launch: each block counts
+// itself done; the one that completes the count runs exit_test and resets
+// the counter for the next launch. `fence`: this kernel itself wrote the
+// error accumulators the test reads (IISPH's beta pass), so the blocks'
+// writes are fenced before they count themselves done.
+__device__ __forceinline__ void fused_exit_test(Arena const& a, LoopCheck const& lc, bool fence) {
+    if (!lc.counter) return;
+    __shared__ int last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (fence) __threadfence();
+        last = atomicAdd(lc.counter, 1u) == gridDim.x - 1 ? 1 : 0;
+        if (last) __threadfence();
+    }
+    __syncthreads();
+    if (last) {
+        exit_test(a, lc.nscenes, lc.kind, lc.running, lc.cond, lc.use_cond, true);
+        if (threadIdx.x == 0) *lc.counter = 0u;
     }
 }
 
@@ -934,7 +972,8 @@ __global__ void __launch_bounds__(256) k_dfsph_density_alpha_pw(Arena a, uint32_
 
 template <int MODE, int CH>
 __global__ void __launch_bounds__(256) k_apply_pressures_pw(Arena a, uint32_t wtiles, int which_q,
-                                                            int external, int skip_done) {
+                                                            int external, int skip_done,
+                                                            LoopCheck lc) {
     float const* q = which_q ? a.qdens : a.qdiv;
     walk_warp_tiles(
       a, wtiles, skip_done != 0,
@@ -951,6 +990,7 @@ __global__ void __launch_bounds__(256) k_apply_pressures_pw(Arena a, uint32_t wt
           a.v[i] = (MODE && P.precision) ? apply_pressure_of<true, CH>(a, P, i, v, q, dt)
                                          : apply_pressure_of<false, CH>(a, P, i, v, q, dt);
       });
+    fused_exit_test(a, lc, false);
 }
 
 template <int MODE, int CH>
@@ -1322,7 +1362,8 @@ __global__ void __launch_bounds__(256) k_iisph_sum_dij_pw(Arena a, uint32_t wtil
 }
 
 template <int MODE, int CH>
-__global__ void __launch_bounds__(256) k_iisph_beta_pressure_pw(Arena a, uint32_t wtiles) {
+__global__ void __launch_bounds__(256) k_iisph_beta_pressure_pw(Arena a, uint32_t wtiles,
+                                                                LoopCheck lc) {
     WarpErr e{-1, 0ull, 0u, 0.0};
     walk_warp_tiles(
       a, wtiles, true,
@@ -1343,6 +1384,7 @@ __global__ void __launch_bounds__(256) k_iisph_beta_pressure_pw(Arena a, uint32_
                   live && counted, false);
       });
     flush_err_block(a, e);
+    fused_exit_test(a, lc, true);
 }
 
 // q = safe_divide(p, rho^2) of the final pressures, for apply_pressures.
@@ -1795,7 +1837,7 @@ void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, bool comp, cudaS
     } while (0)
 
 void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int external,
-                            int skip_done, bool comp, cudaStream_t st, int chunk) {
+                            int skip_done, bool comp, cudaStream_t st, int chunk, LoopCheck lc) {
     if (!tiles) return;
     bool const pf = (chunk & kPrefetchLists) != 0;
     int const ch = chunk & kChunkMask;
@@ -1803,7 +1845,7 @@ void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int ext
         int const th = (chunk & kPersistentBlocks256) ? 256 : kTile;
 #define EMLD_APPLY_PW(M, C)                                                                     \
     k_apply_pressures_pw<M, C><<<persistent_grid(k_apply_pressures_pw<M, C>, tiles, th), th, 0, st>>>( \
-      a, tiles * (kTile / 32), which_q, external, skip_done)
+      a, tiles * (kTile / 32), which_q, external, skip_done, lc)
         EMLD_PW_DISPATCH(EMLD_APPLY_PW, comp, ch);
 #undef EMLD_APPLY_PW
         return;
@@ -1885,7 +1927,7 @@ void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st, int c
 #undef EMLD_SUM
 }
 void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st, int chunk,
-                                bool comp) {
+                                bool comp, LoopCheck lc) {
     if (!tiles) return;
     bool const pf = (chunk & kPrefetchLists) != 0;
     int const ch = chunk & kChunkMask;
@@ -1893,7 +1935,7 @@ void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st,
         int const th = (chunk & kPersistentBlocks256) ? 256 : kTile;
 #define EMLD_BETA_PW(M, C)                                                                   \
     k_iisph_beta_pressure_pw<M, C>                                                           \
-      <<<persistent_grid(k_iisph_beta_pressure_pw<M, C>, tiles, th), th, 0, st>>>(a, tiles * (kTile / 32))
+      <<<persistent_grid(k_iisph_beta_pressure_pw<M, C>, tiles, th), th, 0, st>>>(a, tiles * (kTile / 32), lc)
         EMLD_PW_DISPATCH(EMLD_BETA_PW, comp, ch);
 #undef EMLD_BETA_PW
         return;

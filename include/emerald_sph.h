@@ -367,7 +367,11 @@ int emerald_batch_kernel_launches(emerald_batch* batch, int64_t* count);
  * EMERALD_TUNE_PERSISTENT (2) launches one grid of resident blocks of 128
  * threads whose warps walk their 32-particle tiles and request the next
  * tile's lists and inputs into L2 while they fold the current one;
- * EMERALD_TUNE_PERSISTENT_256 (3) the same in blocks of 256 threads.
+ * EMERALD_TUNE_PERSISTENT_256 (3) the same in blocks of 256 threads;
+ * EMERALD_TUNE_PERSISTENT_FUSED (4) and EMERALD_TUNE_PERSISTENT_256_FUSED (5)
+ * the same, and on a solver loop's final kernel (apply for DFSPH_P, beta for
+ * IISPH) the iteration's exit test runs in that kernel's last block instead
+ * of a launch of its own.
  * Every choice gives the same bits. Autotuning (DFSPH_P and IISPH) times a
  * few whole sub-steps of `method` with each candidate setting, every
  * candidate from the same state (restored afterwards, so the simulation is
@@ -381,6 +385,8 @@ int emerald_batch_kernel_launches(emerald_batch* batch, int64_t* count);
  * counterpart in the reference. */
 #define EMERALD_TUNE_PERSISTENT 2
 #define EMERALD_TUNE_PERSISTENT_256 3
+#define EMERALD_TUNE_PERSISTENT_FUSED 4
+#define EMERALD_TUNE_PERSISTENT_256_FUSED 5
 #define EMERALD_TUNE_CANDIDATES 16
 typedef struct emerald_tuning {
     int32_t apply_chunk, divergence_chunk, iisph_sum_chunk, iisph_beta_chunk;

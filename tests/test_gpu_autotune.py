@@ -52,8 +52,8 @@ def test_batch_tuning(E):
     ids = [b.add_block_scene(s) for s in scs]
     b.step("iisph", 2)
     t = b.autotune("iisph")
-    assert len(t["candidates"]) == 12 and all(c["ms_per_substep"] > 0 for c in t["candidates"])
-    assert all(m in (0, 1, 2, 3) for c in t["candidates"] for m in c["prefetch"].values())
+    assert len(t["candidates"]) == 14 and all(c["ms_per_substep"] > 0 for c in t["candidates"])
+    assert all(0 <= m <= 5 for c in t["candidates"] for m in c["prefetch"].values())
     b.step("iisph", 4)
     for sid, s in zip(ids, scs):
         sim = E.Simulation.from_block_scene(s)
@@ -80,9 +80,12 @@ def test_every_candidate_gives_the_same_bits(E, method):
     probe.advance(method, 1)
     cands = probe.autotune(method)["candidates"]
     assert any(any(c["prefetch"].values()) for c in cands)
-    # the persistent-warp kernels, in both block sizes, are among the candidates
+    # the persistent-warp kernels, in both block sizes, and with the exit
+    # test fused into the loop's final kernel, are among the candidates
     fam = "apply" if method == "dfsph_p" else "iisph_sum"
+    last = "apply" if method == "dfsph_p" else "iisph_beta"
     assert {c["prefetch"][fam] for c in cands} >= {2, 3}
+    assert {c["prefetch"][last] for c in cands} >= {4, 5}
     for c in cands:
         sim = E.Simulation.from_block_scene(sc)
         sim.set_tuning(c["chunks"], c["prefetch"])
@@ -98,7 +101,7 @@ def test_set_tuning_rejects_bad_values(E):
         sim.set_tuning({"apply": 3, "divergence": 4, "iisph_sum": 4, "iisph_beta": 4})
     with pytest.raises(E.EmeraldError):
         sim.set_tuning({"apply": 4, "divergence": 4, "iisph_sum": 4, "iisph_beta": 4},
-                       {"apply": 4})
+                       {"apply": 6})
     sim.set_tuning({"apply": 4, "divergence": 8, "iisph_sum": 4, "iisph_beta": 4},
                    {"apply": 2, "divergence": 2})
     sim.set_tuning()
