@@ -790,9 +790,12 @@ int64_t Engine::kernel_launches() {
 }
 
 void Engine::run_loop(int kind, int max_iter, int32_t method) {
-    launch("iter_reset", [&] { launch_iter_reset(a_, max_scenes_, kind, cur_); });
+    if (!capturing_) {
+        launch("iter_reset", [&] { launch_iter_reset(a_, max_scenes_, kind, cur_); });
+    }
     if (capturing_) {
-        // while (any scene iterates) { body; check } as a conditional node
+        // while (any scene iterates) { body; check } as a conditional node,
+        // opened by the reset kernel every time the loop is reached
         cudaStreamCaptureStatus status;
         cudaGraph_t g = nullptr;
         cudaGraphNode_t const* deps = nullptr;
@@ -804,6 +807,11 @@ void Engine::run_loop(int kind, int max_iter, int32_t method) {
         cudaGraphConditionalHandle cond;
         if (cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
             throw std::runtime_error("graph capture: conditional handle");
+        }
+        launch("iter_reset", [&] { launch_iter_reset(a_, max_scenes_, kind, cur_, cond, 1); });
+        if (cudaStreamGetCaptureInfo(cur_, &status, nullptr, &g, &deps, &ndeps) != cudaSuccess ||
+            status != cudaStreamCaptureStatusActive) {
+            throw std::runtime_error("graph capture: no active capture");
         }
         cudaGraphNodeParams params{};
         params.type = cudaGraphNodeTypeConditional;

@@ -72,7 +72,9 @@ void launch_frame_check(Arena const& a, int nscenes, int method, cudaGraphCondit
                         cudaStream_t st);
 void launch_begin_substep(Arena const& a, int nscenes, cudaStream_t st);
 void launch_zero_kappas(Arena const& a, uint32_t tiles, cudaStream_t st);
-void launch_iter_reset(Arena const& a, int nscenes, int kind, cudaStream_t st);
+// use_cond: also set `cond` (the loop's while condition) to 1
+void launch_iter_reset(Arena const& a, int nscenes, int kind, cudaStream_t st,
+                       cudaGraphConditionalHandle cond = 0, int use_cond = 0);
 void launch_iter_check(Arena const& a, int nscenes, int kind, int* running,
                        cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st);
 // comp: some resident scene is in compensated mode (selects the kernel variant)

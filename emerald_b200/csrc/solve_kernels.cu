@@ -226,9 +226,15 @@ __device__ __forceinline__ int iteration_cap(SceneParams const& P, int kind) {
 }
 
 // Starts a solver loop; a scene whose cap is zero runs no iteration, as the
-// reference's for-loop would.
-__global__ void k_iter_reset(Arena a, int nscenes, int kind) {
+// reference's for-loop would. Inside a captured graph it also opens the
+// loop's while node: a condition handle's default is applied when the graph
+// that owns it is launched, and a loop nested in a frame graph's sub-step
+// loop is reached once per sub-step of one launch, after the previous
+// sub-step's exit test closed it.
+__global__ void k_iter_reset(Arena a, int nscenes, int kind, cudaGraphConditionalHandle cond,
+                             int use_cond) {
     int const s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (use_cond && s == 0) cudaGraphSetConditional(cond, 1u);
     if (s >= nscenes) return;
     SceneState& S = a.ss[s];
     S.iter = 0;
@@ -1799,8 +1805,9 @@ void launch_begin_substep(Arena const& a, int nscenes, cudaStream_t st) {
 void launch_zero_kappas(Arena const& a, uint32_t tiles, cudaStream_t st) {
     k_zero_kappas<<<tiles, kTile, 0, st>>>(a);
 }
-void launch_iter_reset(Arena const& a, int nscenes, int kind, cudaStream_t st) {
-    k_iter_reset<<<(nscenes + 127) / 128, 128, 0, st>>>(a, nscenes, kind);
+void launch_iter_reset(Arena const& a, int nscenes, int kind, cudaStream_t st,
+                       cudaGraphConditionalHandle cond, int use_cond) {
+    k_iter_reset<<<(nscenes + 127) / 128, 128, 0, st>>>(a, nscenes, kind, cond, use_cond);
 }
 void launch_iter_check(Arena const& a, int nscenes, int kind, int* running,
                        cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st) {
