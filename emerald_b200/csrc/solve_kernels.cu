@@ -1767,9 +1767,17 @@ unsigned persistent_grid(K kernel, uint32_t tiles, int threads = kTile) {
     }
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
-    uint64_t const g = uint64_t(std::max(per_sm, 1)) * uint64_t(std::max(sms, 1));
-    uint64_t const need = (uint64_t(tiles) * kTile + threads - 1) / threads;
-    return unsigned(std::max<uint64_t>(1, std::min<uint64_t>(g, need)));
+    uint64_t const resident = uint64_t(std::max(per_sm, 1)) * uint64_t(std::max(sms, 1));
+    // The fewest blocks that still give no warp more warp tiles than the
+    // resident grid would: every warp then walks the same number of tiles
+    // (8,192 warp tiles on 5,328 resident warps are 2 each on 4,096 warps,
+    // not 2 on some and 1 on the rest).
+    uint64_t const wpb = uint64_t(threads / 32);
+    uint64_t const wtiles = uint64_t(tiles) * (kTile / 32);
+    uint64_t const per_warp = (wtiles + resident * wpb - 1) / (resident * wpb);
+    uint64_t const warps = (wtiles + per_warp - 1) / per_warp;
+    uint64_t const blocks = (warps + wpb - 1) / wpb;
+    return unsigned(std::max<uint64_t>(1, std::min<uint64_t>(resident, blocks)));
 }
 
 #define EMLD_DISPATCH(K, comp, ch, pf)                                        \
