@@ -50,10 +50,13 @@ def scene_1m(E):
                         dfsph_density_error_average_threshold=F(0.0005))
 
 
-def compare_lists(sim, other, solid, what):
+def compare_lists(sim, other, solid, what, kernels=True):
+    """Counts, indices and (with `kernels`) W and grad W of one list."""
     a = sim.neighbors(solid)
     b = other.neighbors(solid)
     names = ("counts", "indices", "W", "grad W")
+    if not kernels:
+        names, a, b = names[:2], a[:2], b[:2]
     live = np.arange(64)[None, :] < a[0][:, None]
     for name, u, w in zip(names, a, b):
         if name != "counts":
@@ -124,7 +127,8 @@ def test_north_star_scene_iterations_match_oracle(oracle):
 
 def test_pcisph_262k_matches_reference():
     """PCISPH on the 262,144-particle scene: two fixed sub-steps of
-    time_per_step / sub_steps = 5e-4 s against the compiled reference."""
+    time_per_step / sub_steps = 5e-4 s against the compiled reference:
+    positions, velocities and the neighbour lists' counts and indices."""
     import emerald_b200 as E
     from cpu_checkers import Reference
     R = Reference()
@@ -141,6 +145,9 @@ def test_pcisph_262k_matches_reference():
     rx, rv = ref.state()
     assert_bitwise(x, rx, "PCISPH 262k positions")
     assert_bitwise(v, rv, "PCISPH 262k velocities")
-    compare_lists(sim, ref, False, "PCISPH 262k")
-    compare_lists(sim, ref, True, "PCISPH 262k")
+    # The reference rewrites its lists' W and grad W at every iteration's
+    # predicted positions (pcisph.cpp:90-91) and this path evaluates those
+    # in registers without storing them, so only the list structure compares.
+    compare_lists(sim, ref, False, "PCISPH 262k", kernels=False)
+    compare_lists(sim, ref, True, "PCISPH 262k", kernels=False)
     sim.close()

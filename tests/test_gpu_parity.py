@@ -392,15 +392,19 @@ def test_frame_is_one_graph_launch(E, oracle, method):
     while node around the sub-step) and waits on the host once: after the
     first frame (which captures the graphs), every frame costs one host
     wait, runs the oracle's sub-step count and ends on its state bit for
-    bit. A frame begun by emerald_sim_advance is finished, not restarted."""
+    bit. Frames alternate between two graphs, one that re-sorts the
+    particles' storage order first and one that does not, so the first two
+    frames capture. A frame begun by emerald_sim_advance is finished, not
+    restarted."""
     scene = E.BlockScene(40, dx=F(1 / 80), seed=13, time_per_step_flicks=1411200, sub_steps=4,
                          dfsph_divergence_error_average_threshold=F(0.001),
                          dfsph_density_error_average_threshold=F(0.0005))
     sim = E.Simulation.from_block_scene(scene)
     osim = oracle.sim(oracle_params(E, scene.params), scene.solid, scene.solid_volumes,
                       scene.fluid)
-    sim.frame(method)
-    osim.frame(method)
+    for _ in range(2):
+        sim.frame(method)
+        osim.frame(method)
     waits = []
     for _ in range(3):
         w0 = sim.host_waits()
@@ -408,9 +412,9 @@ def test_frame_is_one_graph_launch(E, oracle, method):
         waits.append(sim.host_waits() - w0)
         assert st["sub_steps"] == osim.frame(method)
     assert waits == [1, 1, 1], waits
-    assert_bitwise(sim.state()[0], osim.state()[0], "%s positions after 4 frames" % method)
-    assert_bitwise(sim.state()[1], osim.state()[1], "%s velocities after 4 frames" % method)
-    # two sub-steps into the fifth frame, then the frame call finishes it
+    assert_bitwise(sim.state()[0], osim.state()[0], "%s positions after 5 frames" % method)
+    assert_bitwise(sim.state()[1], osim.state()[1], "%s velocities after 5 frames" % method)
+    # two sub-steps into the sixth frame, then the frame call finishes it
     sim.advance(method, 2, stats=False)
     st = sim.frame(method)
     k = osim.frame(method)
