@@ -223,6 +223,16 @@ EXPORTS = {
     "emerald_batch_autotune": (c_i32, [c_vp, c_i32, ctypes.POINTER(Tuning)]),
     "emerald_compute_grid_coords": (c_i32, [c_sz, c_f, c_f, c_f, c_vp, c_vp, c_vp]),
     "emerald_compute_z_indices": (c_i32, [c_sz, c_vp, c_vp, c_vp]),
+    "emerald_compute_index_pairs": (c_i32, [c_sz, c_vp, c_vp, c_vp]),
+    "emerald_index_pairs_workspace": (c_i32, [c_sz, ctypes.POINTER(c_sz)]),
+    "emerald_sort_index_pairs": (c_i32, [c_sz, c_vp, c_vp, c_sz, c_vp]),
+    "emerald_compute_block_indices": (c_i32, [c_sz, c_vp, c_vp, c_vp, c_sz, c_vp]),
+    "emerald_fill_blocks": (c_i32, [c_sz, c_vp, c_vp, c_vp]),
+    "emerald_block_map_create": (c_i32, [ctypes.POINTER(c_vp)]),
+    "emerald_block_map_destroy": (c_i32, [c_vp]),
+    "emerald_create_block_map": (c_i32, [c_sz, c_vp, c_vp, c_vp, c_vp]),
+    "emerald_create_regular_neighborhoods": (c_i32, [c_sz, c_f, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                                     c_vp, c_vp, c_vp, c_vp, c_vp]),
     "emerald_compute_neighbor_distances_and_vectors_to": (c_i32, [c_sz, c_vp, c_vp, c_vp, c_vp,
                                                                   c_vp, c_vp, c_vp]),
     "emerald_compute_neighbor_kernels": (c_i32, [c_sz, c_f, c_vp, c_vp, c_vp, c_vp]),

@@ -17,7 +17,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["build_kernels.cu", "solve_kernels.cu", "sort_kernels.cu", "engine.cu", "capi.cu",
            "scene.cpp", "noalloc.cu", "reorder_kernels.cu", "server.cpp", "common_ops.cu",
-           "solver_ops.cu"]
+           "solver_ops.cu", "sort_ops.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -504,6 +504,57 @@ int emerald_compute_grid_coords(size_t n, float cell_size, float bounds_min_x, f
 /* compute_z_indices (emerald/sph_common/common.cpp:69-76). */
 int emerald_compute_z_indices(size_t n, uint64_t* z_indices, int32_t const* grid_coords,
                               void* stream);
+
+/* The z-order sort and the neighbour search (emerald/sph_common/neighborhood.h:41-97,
+ * neighborhood.cpp:10-152). The reference's std::pair<uint64_t, size_t>
+ * arrays (index pairs (z, index), blocks [begin, end)) are interleaved
+ * uint64 pairs, their own memory layout on LP64. n is below 2^32 - 1. */
+/* compute_index_pairs (neighborhood.cpp:10-16): index_pairs[i] = (z_indices[i], i). */
+int emerald_compute_index_pairs(size_t n, uint64_t* index_pairs, uint64_t const* z_indices,
+                                void* stream);
+/* Bytes of device workspace emerald_sort_index_pairs and
+ * emerald_compute_block_indices need for n pairs (256-byte aligned). */
+int emerald_index_pairs_workspace(size_t n, size_t* bytes);
+/* sort_index_pairs (neighborhood.cpp:18-26): ascending (z, index) order,
+ * the order std::sort gives the pairs, in place. */
+int emerald_sort_index_pairs(size_t n, uint64_t* index_pairs, void* workspace,
+                             size_t workspace_bytes, void* stream);
+/* compute_block_indices (neighborhood.cpp:28-64): per sorted pair, the
+ * number of z changes before it (0 0 0 1 1 2 ...). The block count is
+ * block_indices[n - 1] + 1, read by the caller as the reference's driver
+ * does (emerald/sph2d_box/neighborhoods_from_state.cpp:32). */
+int emerald_compute_block_indices(size_t n, uint32_t* block_indices,
+                                  uint64_t const* sorted_index_pairs, void* workspace,
+                                  size_t workspace_bytes, void* stream);
+/* fill_blocks (neighborhood.cpp:66-93): blocks[b] = [first, last + 1) of
+ * the pairs whose block index is b (non-decreasing block indices, as
+ * emerald_compute_block_indices makes them). */
+int emerald_fill_blocks(size_t n, uint64_t* blocks, uint32_t const* block_indices, void* stream);
+/* Block_map (neighborhood.h:21-35): z key -> block, as a device hash table.
+ * emerald_create_block_map (create_block_map, neighborhood.cpp:95-110)
+ * clears the map and inserts every block under the z key of its first pair;
+ * the table holds at least twice block_count slots and grows on demand, as
+ * the reference's rehash does (growing waits for `stream`). A map is used
+ * on the device that filled it. */
+typedef struct emerald_block_map emerald_block_map;
+int emerald_block_map_create(emerald_block_map** map);
+int emerald_block_map_destroy(emerald_block_map* map);
+int emerald_create_block_map(size_t block_count, emerald_block_map* into, uint64_t const* blocks,
+                             uint64_t const* sorted_index_pairs, void* stream);
+/* create_regular_neighborhoods (neighborhood.cpp:112-136, the search of
+ * neighborhood.h:199-282): for each particle the other set's particles in
+ * the 3x3 cells around its grid coordinate, closer than max_distance (the
+ * particle itself excluded when other_positions == self_positions), at most
+ * 64 taken in the reference's visiting order, sorted by (distance, index).
+ * Rows are the Neighborhood_pointers layout (64 entries per particle);
+ * entries past a particle's count are left as they were. */
+int emerald_create_regular_neighborhoods(size_t n, float max_distance, uint8_t* counts,
+                                         uint64_t* indices, float* distances, float* vectors_to,
+                                         float const* self_positions,
+                                         int32_t const* self_grid_coords,
+                                         float const* other_positions,
+                                         uint64_t const* other_sorted_index_pairs,
+                                         emerald_block_map const* other_block_map, void* stream);
 /* compute_neighbor_distances_and_vectors_to (emerald/sph_common/neighborhood.cpp:154-176). */
 int emerald_compute_neighbor_distances_and_vectors_to(size_t n, float* distances,
                                                       float* vectors_to,

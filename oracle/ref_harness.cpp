@@ -803,6 +803,90 @@ void ref_common_z_indices(size_t n, uint64_t* z, int32_t const* gc) {
     compute_z_indices(n, z, g.data());
 }
 
+// compute_index_pairs / sort_index_pairs / compute_block_indices /
+// fill_blocks (emerald/sph_common/neighborhood.cpp:10-93) on interleaved
+// (z, index) and (begin, end) uint64 pairs.
+namespace {
+std::vector<std::pair<uint64_t, size_t>> pairs_from(size_t n, uint64_t const* flat) {
+    std::vector<std::pair<uint64_t, size_t>> p(n);
+    for (size_t i = 0; i < n; ++i) p[i] = {flat[2 * i], size_t(flat[2 * i + 1])};
+    return p;
+}
+void pairs_to(std::vector<std::pair<uint64_t, size_t>> const& p, uint64_t* flat) {
+    for (size_t i = 0; i < p.size(); ++i) {
+        flat[2 * i] = p[i].first;
+        flat[2 * i + 1] = p[i].second;
+    }
+}
+}  // namespace
+
+void ref_common_index_pairs(size_t n, uint64_t* pairs, uint64_t const* z) {
+    std::vector<std::pair<uint64_t, size_t>> p(n);
+    compute_index_pairs(n, p.data(), z);
+    pairs_to(p, pairs);
+}
+
+void ref_common_sort_index_pairs(size_t n, uint64_t* pairs) {
+    auto p = pairs_from(n, pairs);
+    sort_index_pairs(n, p.data());
+    pairs_to(p, pairs);
+}
+
+void ref_common_block_indices(size_t n, uint32_t* block_indices, uint64_t const* pairs) {
+    auto const p = pairs_from(n, pairs);
+    compute_block_indices(n, block_indices, p.data());
+}
+
+void ref_common_fill_blocks(size_t n, size_t block_count, uint64_t* blocks,
+                            uint32_t* block_indices) {
+    std::vector<std::pair<size_t, size_t>> b(block_count);
+    for (size_t k = 0; k < block_count; ++k) b[k] = {size_t(blocks[2 * k]), size_t(blocks[2 * k + 1])};
+    fill_blocks(n, b.data(), block_indices);
+    for (size_t k = 0; k < block_count; ++k) {
+        blocks[2 * k] = b[k].first;
+        blocks[2 * k + 1] = b[k].second;
+    }
+}
+
+// create_block_map + create_regular_neighborhoods (neighborhood.cpp:95-136):
+// the other set's block map from its blocks and sorted pairs, then the
+// lists (row-major, 64 entries per particle). With `same` the other set is
+// the self set (one positions array, so the reference skips each particle
+// itself).
+void ref_common_regular_neighborhoods(size_t n, size_t n_other, float max_distance,
+                                      uint8_t* counts, uint64_t* idx, float* dist, float* vec,
+                                      float const* self_xy, int32_t const* self_gc,
+                                      float const* other_xy, int same, size_t n_pairs,
+                                      uint64_t const* other_pairs, size_t block_count,
+                                      uint64_t const* other_blocks) {
+    auto const p = to_v2f(self_xy, n);
+    auto const o = same ? std::vector<V2f>() : to_v2f(other_xy, n_other);
+    std::vector<V2i> gc(n);
+    for (size_t i = 0; i < n; ++i) gc[i] = V2i{self_gc[2 * i], self_gc[2 * i + 1]};
+    auto const pairs = pairs_from(n_pairs, other_pairs);
+    std::vector<std::pair<size_t, size_t>> blocks(block_count);
+    for (size_t k = 0; k < block_count; ++k) {
+        blocks[k] = {size_t(other_blocks[2 * k]), size_t(other_blocks[2 * k + 1])};
+    }
+    Block_map map{block_count * 2};
+    map = create_block_map(block_count, std::move(map), blocks.data(), pairs.data());
+    Neighborhood_vectors nb;
+    nb.resize(n);
+    create_regular_neighborhoods(n, max_distance, nb.counts.data(), nb.indices.data(),
+                                 nb.distances.data(), nb.vectors_to.data(), p.data(), gc.data(),
+                                 same ? p.data() : o.data(), pairs.data(), map);
+    for (size_t i = 0; i < n; ++i) {
+        counts[i] = nb.counts[i];
+        for (size_t k = 0; k < nb.counts[i]; ++k) {
+            size_t const e = i * NEIGHBORHOOD_MAX_COUNT + k;
+            idx[e] = nb.indices[i][k];
+            dist[e] = nb.distances[i][k];
+            vec[2 * e] = nb.vectors_to[i][k][0];
+            vec[2 * e + 1] = nb.vectors_to[i][k][1];
+        }
+    }
+}
+
 void ref_common_distances_vectors(size_t n, size_t n_other, float* dist, float* vec,
                                   float const* self_xy, float const* other_xy,
                                   uint8_t const* counts, uint64_t const* idx) {

@@ -297,6 +297,12 @@ class Reference:
         # the sph_common functions on flat arrays (row-major 64-entry lists)
         L.ref_common_grid_coords.argtypes = [c_sz, c_f, c_f, c_f, c_vp, c_vp]
         L.ref_common_z_indices.argtypes = [c_sz, c_vp, c_vp]
+        L.ref_common_index_pairs.argtypes = [c_sz, c_vp, c_vp]
+        L.ref_common_sort_index_pairs.argtypes = [c_sz, c_vp]
+        L.ref_common_block_indices.argtypes = [c_sz, c_vp, c_vp]
+        L.ref_common_fill_blocks.argtypes = [c_sz, c_sz, c_vp, c_vp]
+        L.ref_common_regular_neighborhoods.argtypes = [c_sz, c_sz, c_f] + [c_vp] * 7 + \
+            [ctypes.c_int, c_sz, c_vp, c_sz, c_vp]
         L.ref_common_distances_vectors.argtypes = [c_sz, c_sz, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]
         L.ref_common_kernels.argtypes = [c_sz, c_f, c_vp, c_vp, c_vp, c_vp, c_vp]
         L.ref_common_densities.argtypes = [c_sz, c_f, c_f] + [c_vp] * 9

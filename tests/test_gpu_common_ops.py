@@ -214,3 +214,165 @@ def test_empty_and_invalid(E):
     assert E.lib.emerald_compute_densities(0, F(0.01), F(1000), None, None, E.Neighborhood(),
                                            None, E.Neighborhood(), None) == 0
     assert E.lib.emerald_compute_neighbor_kernels(10, F(0.0), None, None, None, None) == 22
+
+
+# ---------------------------------------------- z-order sort and the search
+
+def workspace(E, n):
+    import ctypes
+    b = ctypes.c_size_t()
+    check(E.lib.emerald_index_pairs_workspace(n, ctypes.byref(b)))
+    import torch
+    return torch.empty(max(b.value, 1), dtype=torch.uint8, device="cuda")
+
+
+def device_sort(E, pairs):
+    """emerald_sort_index_pairs on a copy of the interleaved (z, index) pairs."""
+    n = len(pairs)
+    d = dev(pairs)
+    ws = workspace(E, n)
+    check(E.lib.emerald_sort_index_pairs(n, d.data_ptr(), ws.data_ptr(), ws.numel(), None))
+    return host(d)
+
+
+def reference_sort(reference, pairs):
+    out = np.ascontiguousarray(pairs.copy())
+    reference.L.ref_common_sort_index_pairs(len(out), ptr(out))
+    return out
+
+
+def sorted_set(E, reference, xy, cell):
+    """The reference's chain (neighborhoods_from_state.cpp:15-44) for one
+    point set with the grid at the origin, through the device functions:
+    grid coords, z keys, sorted pairs, block indices, blocks, the block map.
+    Each product is compared with the reference's on the way."""
+    n = len(xy)
+    K = Keep()
+    gc = dev(np.zeros((n, 2), np.int32))
+    check(E.lib.emerald_compute_grid_coords(n, cell, F(0.0), F(0.0), gc.data_ptr(), K(xy), None))
+    z = dev(np.zeros(n, np.uint64))
+    check(E.lib.emerald_compute_z_indices(n, z.data_ptr(), gc.data_ptr(), None))
+    pairs = dev(np.zeros((n, 2), np.uint64))
+    check(E.lib.emerald_compute_index_pairs(n, pairs.data_ptr(), z.data_ptr(), None))
+    rpairs = np.zeros((n, 2), np.uint64)
+    reference.L.ref_common_index_pairs(n, ptr(rpairs), ptr(host(z)))
+    assert_bitwise(host(pairs), rpairs, "index pairs")
+    ws = workspace(E, n)
+    check(E.lib.emerald_sort_index_pairs(n, pairs.data_ptr(), ws.data_ptr(), ws.numel(), None))
+    reference.L.ref_common_sort_index_pairs(n, ptr(rpairs))
+    assert_bitwise(host(pairs), rpairs, "sorted pairs")
+    bi = dev(np.zeros(n, np.uint32))
+    check(E.lib.emerald_compute_block_indices(n, bi.data_ptr(), pairs.data_ptr(), ws.data_ptr(),
+                                              ws.numel(), None))
+    rbi = np.zeros(n, np.uint32)
+    reference.L.ref_common_block_indices(n, ptr(rbi), ptr(rpairs))
+    assert_bitwise(host(bi), rbi, "block indices")
+    nb = int(rbi[-1]) + 1
+    blocks = dev(np.zeros((nb, 2), np.uint64))
+    check(E.lib.emerald_fill_blocks(n, blocks.data_ptr(), bi.data_ptr(), None))
+    rblocks = np.zeros((nb, 2), np.uint64)
+    reference.L.ref_common_fill_blocks(n, nb, ptr(rblocks), ptr(rbi))
+    assert_bitwise(host(blocks), rblocks, "blocks")
+    return dict(n=n, xy=xy, gc=gc, pairs=pairs, rpairs=rpairs, blocks=blocks, rblocks=rblocks,
+                nb=nb, keep=K)
+
+
+def compare_search(E, reference, self_set, other_set, cell, bmap, what):
+    import ctypes
+    n = self_set["n"]
+    same = other_set is self_set
+    x = dev(self_set["xy"])
+    ox = x if same else dev(other_set["xy"])
+    check(E.lib.emerald_create_block_map(other_set["nb"], bmap, other_set["blocks"].data_ptr(),
+                                         other_set["pairs"].data_ptr(), None))
+    counts = dev(np.full(n, 255, np.uint8))
+    idx = dev(np.zeros((n, 64), np.uint64))
+    dist = dev(np.zeros((n, 64), np.float32))
+    vec = dev(np.zeros((n, 64, 2), np.float32))
+    check(E.lib.emerald_create_regular_neighborhoods(
+        n, cell, counts.data_ptr(), idx.data_ptr(), dist.data_ptr(), vec.data_ptr(), x.data_ptr(),
+        self_set["gc"].data_ptr(), ox.data_ptr(), other_set["pairs"].data_ptr(), bmap, None))
+    rc = np.zeros(n, np.uint8)
+    ri = np.zeros((n, 64), np.uint64)
+    rd = np.zeros((n, 64), np.float32)
+    rv = np.zeros((n, 64, 2), np.float32)
+    reference.L.ref_common_regular_neighborhoods(
+        n, other_set["n"], cell, ptr(rc), ptr(ri), ptr(rd), ptr(rv), ptr(self_set["xy"]),
+        ptr(host(self_set["gc"])), ptr(other_set["xy"]), 1 if same else 0, other_set["n"],
+        ptr(other_set["rpairs"]), other_set["nb"], ptr(other_set["rblocks"]))
+    c = host(counts)
+    assert_bitwise(c, rc, "%s counts" % what)
+    live = np.arange(64)[None, :] < c[:, None]
+    assert_bitwise(np.where(live, host(idx), 0), ri, "%s indices" % what)
+    assert_bitwise(np.where(live, host(dist), 0), rd, "%s distances" % what)
+    assert_bitwise(np.where(live[..., None], host(vec), 0), rv, "%s vectors_to" % what)
+    return c
+
+
+@pytest.fixture()
+def block_map(E):
+    import ctypes
+    m = ctypes.c_void_p()
+    check(E.lib.emerald_block_map_create(ctypes.byref(m)))
+    yield m.value
+    check(E.lib.emerald_block_map_destroy(m.value))
+
+
+def test_index_pair_sort_matches_reference(E, reference):
+    """Random pairs with many equal z keys, indices out of order and equal
+    pairs, the all-ones z key of cell (-1, -1), and 2^20 pairs: the device
+    sort gives std::sort's order."""
+    rng = np.random.Generator(np.random.PCG64(17))
+    for n, zmax, imax in ((2, 3, 2), (37, 4, 10), (5000, 300, 1 << 40), (1 << 20, 1 << 30, 1 << 20)):
+        z = rng.integers(0, zmax, n, dtype=np.uint64)
+        z[rng.integers(0, n, max(1, n // 50))] = np.uint64(0xFFFFFFFFFFFFFFFF)
+        pairs = np.stack([z, rng.integers(0, imax, n, dtype=np.uint64)], axis=1)
+        assert_bitwise(device_sort(E, pairs), reference_sort(reference, pairs),
+                       "sorted pairs n=%d" % n)
+    # nothing to do for 0 or 1 pair (neighborhood.cpp:20)
+    one = np.array([[5, 9]], np.uint64)
+    assert_bitwise(device_sort(E, one), one, "one pair")
+    assert E.lib.emerald_sort_index_pairs(0, None, None, 0, None) == 0
+
+
+def test_sort_products_and_search_match_reference(E, reference, case, block_map):
+    """The tank case (fluid against itself and against its walls, whose
+    cells reach negative coordinates and cell (-1, -1)) through the device
+    chain, every product against the reference's."""
+    cell = case["cell"]
+    fluid = sorted_set(E, reference, case["fluid"], cell)
+    solid = sorted_set(E, reference, case["solid"], cell)
+    assert (host(solid["gc"]) < 0).any()
+    assert np.uint64(0xFFFFFFFFFFFFFFFF) in host(solid["pairs"])[:, 0]
+    cf = compare_search(E, reference, fluid, fluid, cell, block_map, "fluid")
+    cs = compare_search(E, reference, fluid, solid, cell, block_map, "boundary")
+    assert cf.max() > 10 and cs.max() > 0
+
+
+def test_search_caps_dense_cells_like_the_reference(E, reference, block_map):
+    """Cells holding far more than 64 candidates: the search keeps the first
+    64 accepted in the reference's visiting order and sorts those, so the
+    lists equal the reference's, not the 64 nearest. The map is refilled with
+    more blocks afterwards (its table grows)."""
+    rng = np.random.Generator(np.random.PCG64(23))
+    cell = F(0.05)
+    dense = rng.uniform(0.0, 0.1, (900, 2)).astype(np.float32)
+    sparse = rng.uniform(-0.5, 1.5, (3000, 2)).astype(np.float32)
+    xy = np.concatenate([dense, sparse]).astype(np.float32)
+    s = sorted_set(E, reference, xy, cell)
+    c = compare_search(E, reference, s, s, cell, block_map, "dense")
+    assert (c == 64).sum() > 100
+    big = rng.uniform(-2.0, 2.0, (20000, 2)).astype(np.float32)
+    b = sorted_set(E, reference, big, F(0.01))
+    assert b["nb"] > 4 * s["nb"]
+    compare_search(E, reference, b, b, F(0.01), block_map, "after growing")
+    # a map of no blocks finds nothing
+    check(E.lib.emerald_create_block_map(0, block_map, None, None, None))
+    counts = dev(np.full(4, 7, np.uint8))
+    K = Keep()
+    check(E.lib.emerald_create_regular_neighborhoods(
+        4, cell, counts.data_ptr(), K(np.zeros((4, 64), np.uint64)),
+        K(np.zeros((4, 64), np.float32)), K(np.zeros((4, 64, 2), np.float32)), K(xy[:4]),
+        K(np.zeros((4, 2), np.int32)), K(xy[:4]), K(np.zeros((1, 2), np.uint64)), block_map,
+        None))
+    assert (host(counts) == 0).all()

@@ -176,3 +176,33 @@ def test_non_finite_inputs_are_rejected_before_any_device_work():
     assert b"not finite" in E.lib.emerald_last_error()
     out = np.zeros(4, np.float32)
     assert E.lib.emerald_config(ctypes.byref(q), E._ptr(out)) == 22
+
+
+def test_sort_entry_points_host_side():
+    """The z-order sort and search entry points: the workspace size grows with
+    n, a block map is created and destroyed on the host, and NULL arguments
+    are refused before any device work (no GPU needed)."""
+    import emerald_b200 as E
+    sizes = []
+    for n in (0, 1, 1000, 1 << 20):
+        b = ctypes.c_size_t()
+        assert E.lib.emerald_index_pairs_workspace(n, ctypes.byref(b)) == 0
+        assert b.value > 0
+        sizes.append(b.value)
+    assert sizes == sorted(sizes) and sizes[-1] >= 16 << 20
+    assert E.lib.emerald_index_pairs_workspace(1 << 33, ctypes.byref(ctypes.c_size_t())) == 22
+    assert E.lib.emerald_index_pairs_workspace(10, None) == 22
+    m = ctypes.c_void_p()
+    assert E.lib.emerald_block_map_create(ctypes.byref(m)) == 0 and m.value
+    assert E.lib.emerald_create_regular_neighborhoods(5, 0.1, None, None, None, None, None, None,
+                                                      None, None, m.value, None) == 22
+    # a map that was never filled is refused
+    fake = ctypes.c_void_p(8)
+    assert E.lib.emerald_create_regular_neighborhoods(5, 0.1, fake, fake, fake, fake, fake, fake,
+                                                      fake, fake, m.value, None) == 22
+    assert b"filled" in E.lib.emerald_last_error()
+    assert E.lib.emerald_block_map_destroy(m.value) == 0
+    assert E.lib.emerald_block_map_destroy(None) == 0
+    assert E.lib.emerald_create_block_map(3, None, None, None, None) == 22
+    assert E.lib.emerald_sort_index_pairs(10, None, None, 0, None) == 22
+    assert E.lib.emerald_compute_block_indices(10, None, None, None, 0, None) == 22

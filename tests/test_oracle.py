@@ -78,6 +78,46 @@ def test_fixture_sort_matches_reference(oracle, fixture7927):
     assert np.all(s["blocks"][1:, 0] == s["blocks"][:-1, 1])
 
 
+def test_reference_sort_functions_match_fixture(reference, oracle, fixture7927):
+    """The harness's per-function wrappers around the reference's own
+    compute_index_pairs, sort_index_pairs, compute_block_indices,
+    fill_blocks, create_block_map and create_regular_neighborhoods (the
+    checkers of the device versions) reproduce the fixture's sort products
+    and lists, with the grid at the origin."""
+    from cpu_checkers import ptr
+    xy = np.ascontiguousarray(fixture7927["xy"], np.float32)
+    n = len(xy)
+    L = reference.L
+    gc = np.zeros((n, 2), np.int32)
+    L.ref_common_grid_coords(n, F(2.1), F(0.0), F(0.0), ptr(gc), ptr(xy))
+    assert_bitwise(gc, fixture7927["grid_coords"], "grid coords")
+    z = np.zeros(n, np.uint64)
+    L.ref_common_z_indices(n, ptr(z), ptr(gc))
+    pairs = np.zeros((n, 2), np.uint64)
+    L.ref_common_index_pairs(n, ptr(pairs), ptr(z))
+    assert_bitwise(pairs[:, 1], np.arange(n, dtype=np.uint64), "unsorted pair indices")
+    L.ref_common_sort_index_pairs(n, ptr(pairs))
+    assert_bitwise(pairs[:, 1], fixture7927["pair_index"].astype(np.uint64), "sorted pairs")
+    bi = np.zeros(n, np.uint32)
+    L.ref_common_block_indices(n, ptr(bi), ptr(pairs))
+    assert_bitwise(bi, fixture7927["block_indices"], "block indices")
+    nb = int(bi[-1]) + 1
+    blocks = np.zeros((nb, 2), np.uint64)
+    L.ref_common_fill_blocks(n, nb, ptr(blocks), ptr(bi))
+    assert_bitwise(blocks, oracle.sort(xy, F(2.1))["blocks"].astype(np.uint64), "blocks")
+    counts = np.zeros(n, np.uint8)
+    idx = np.zeros((n, 64), np.uint64)
+    dist = np.zeros((n, 64), np.float32)
+    vec = np.zeros((n, 64, 2), np.float32)
+    L.ref_common_regular_neighborhoods(n, n, F(2.1), ptr(counts), ptr(idx), ptr(dist), ptr(vec),
+                                       ptr(xy), ptr(gc), ptr(xy), 1, n, ptr(pairs), nb,
+                                       ptr(blocks))
+    assert_bitwise(counts, fixture7927["counts"], "counts")
+    live = np.arange(64)[None, :] < counts[:, None]
+    assert_bitwise(np.where(live, idx, 0), np.where(live, fixture7927["idx"], 0).astype(np.uint64),
+                   "indices")
+
+
 def test_fixture_neighbors_match_reference(oracle, fixture7927):
     xy = fixture7927["xy"]
     counts, idx, dist, vec = oracle.neighborhoods(xy, xy, True, F(2.1))
