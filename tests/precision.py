@@ -13,6 +13,10 @@ import numpy as np
 
 from cpu_checkers import FP64Oracle
 
+# Speed (m/s) above which a particle counts as ejected: the dam break's
+# bulk flow stays below 10 m/s.
+FAST = 50.0
+
 
 def dfsph_scene(E, n_side, precision, seed=1):
     return E.BlockScene(n_side, dx=np.float32(1.0 / (2 * n_side)), seed=seed,
@@ -91,6 +95,9 @@ def compare(E, n_side, steps, checkpoints, precision, seed=1, offset=0.0, method
                              density_rms=float(np.sqrt(np.mean(drel ** 2))),
                              position_max_dx=float(dpos.max()),
                              position_rms_dx=float(np.sqrt(np.mean(dpos ** 2))),
+                             position_p99_dx=float(np.percentile(dpos, 99)),
+                             fast_fp32=int(np.sum(np.hypot(*v.astype(np.float64).T) > FAST)),
+                             fast_fp64=int(np.sum(np.hypot(*v64.T) > FAST)),
                              kinetic_energy=ke, kinetic_energy_fp64=ke64,
                              energy_rel_diff=abs(ke - ke64) / ke64 if ke64 else 0.0,
                              energy_drift=(e32 - e0) / abs(e0) if e0 else 0.0,

@@ -29,18 +29,21 @@ def main():
           "GPU oracle with the same sub-steps and iteration counts\n" % (
               args.method.upper(), args.n_side, args.n_side, args.n_side ** 2, 2 * args.n_side))
     print("| mode | sub-step | density err L_inf | density err RMS | position err max (dx) | "
-          "position err RMS (dx) | kinetic energy rel. diff | energy drift FP32 | "
-          "energy drift FP64 | iterations |")
-    print("|---|---:|---:|---:|---:|---:|---:|---:|---:|---:|")
+          "position err RMS (dx) | position err p99 (dx) | kinetic energy rel. diff | "
+          "energy drift FP32 | energy drift FP64 | particles > 50 m/s FP32 / FP64 | "
+          "iterations |")
+    print("|---|---:|---:|---:|---:|---:|---:|---:|---:|---:|---:|---:|")
     for name, mode in (("reference FP32", E.PRECISION_REFERENCE),
                        ("compensated", E.PRECISION_COMPENSATED)):
         t0 = time.time()
         rows = compare(E, args.n_side, args.steps, at, mode, method=args.method)
         for r in rows:
-            print("| %s | %d | %.3e | %.3e | %.3e | %.3e | %.3e | %.3e | %.3e | %d |" % (
-                name, r["step"], r["density_linf"], r["density_rms"], r["position_max_dx"],
-                r["position_rms_dx"], r["energy_rel_diff"], r["energy_drift"],
-                r["energy_drift_fp64"], r["iterations"]), flush=True)
+            print("| %s | %d | %.3e | %.3e | %.3e | %.3e | %.3e | %.3e | %.3e | %.3e | %d / %d | "
+                  "%d |" % (
+                      name, r["step"], r["density_linf"], r["density_rms"], r["position_max_dx"],
+                      r["position_rms_dx"], r["position_p99_dx"], r["energy_rel_diff"],
+                      r["energy_drift"], r["energy_drift_fp64"], r["fast_fp32"], r["fast_fp64"],
+                      r["iterations"]), flush=True)
         print("<!-- %s: %.1f s -->" % (name, time.time() - t0), flush=True)
 
 
