@@ -925,35 +925,50 @@ __device__ __forceinline__ void add_err(Arena const& a, WarpErr& e, int32_t scen
     }
 }
 
+// The scene of warp tile t when it takes part in this launch (active and,
+// with skip_done, its solver loop still running), else -1. The answer does
+// not change while a walk runs: the loop state moves only in the exit test.
+__device__ __forceinline__ int32_t live_tile_scene(Arena const& a, uint32_t t, bool skip_done) {
+    int32_t const s = a.tile_scene[t / (kTile / 32)];
+    if (s < 0) return -1;
+    SceneState const& S = a.ss[s];
+    return (S.active && !(skip_done && S.done)) ? s : -1;
+}
+
 // Walks this warp's tiles: prefetch(base, count) asks L2 for a tile's data,
-// body(scene, i, live) folds particle i of an active tile. Every lane of
-// the warp runs every iteration (tile checks are warp-uniform), and every
-// thread of the block returns from it (no early exit, so the kernels can
-// meet at a block barrier afterwards).
+// body(scene, i, live) folds particle i of a tile whose scene takes part;
+// tiles of scenes that sit out (finished loops in a batch) are neither
+// prefetched nor folded. Every lane of the warp runs every iteration (tile
+// checks are warp-uniform), and every thread of the block returns from it
+// (no early exit, so the kernels can meet at a block barrier afterwards).
 template <class Prefetch, class Body>
 __device__ __forceinline__ void walk_warp_tiles(Arena const& a, uint32_t wtiles, bool skip_done,
                                                 Prefetch prefetch, Body body) {
     uint32_t const lane = threadIdx.x & 31u;
     uint32_t const G = (gridDim.x * blockDim.x) >> 5;
     uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int cnt_next = (t + G < wtiles) ? int(a.nf_cnt[(t + G) * 32u + lane]) : 0;
-    if (t < wtiles) prefetch(t * 32u, int(a.nf_cnt[t * 32u + lane]));
+    int32_t s_cur = t < wtiles ? live_tile_scene(a, t, skip_done) : -1;
+    int32_t s_next = t + G < wtiles ? live_tile_scene(a, t + G, skip_done) : -1;
+    int cnt_next = s_next >= 0 ? int(a.nf_cnt[(t + G) * 32u + lane]) : 0;
+    if (s_cur >= 0) prefetch(t * 32u, int(a.nf_cnt[t * 32u + lane]));
     for (; t < wtiles; t += G) {
         uint32_t const tn = t + G;
+        int32_t s_after = -1;
         int cnt_after = 0;
         if (tn < wtiles) {
-            prefetch(tn * 32u, cnt_next);
-            if (tn + G < wtiles) cnt_after = int(a.nf_cnt[(tn + G) * 32u + lane]);
-        }
-        int32_t const s = a.tile_scene[t / (kTile / 32)];
-        if (s >= 0) {
-            SceneState const& S = a.ss[s];
-            if (S.active && !(skip_done && S.done)) {
-                SceneParams const& P = a.sp[s];
-                uint32_t const i = t * 32u + lane;
-                body(s, i, (i - P.fluid_begin) < P.fluid_count);
+            if (s_next >= 0) prefetch(tn * 32u, cnt_next);
+            if (tn + G < wtiles) {
+                s_after = live_tile_scene(a, tn + G, skip_done);
+                if (s_after >= 0) cnt_after = int(a.nf_cnt[(tn + G) * 32u + lane]);
             }
         }
+        if (s_cur >= 0) {
+            SceneParams const& P = a.sp[s_cur];
+            uint32_t const i = t * 32u + lane;
+            body(s_cur, i, (i - P.fluid_begin) < P.fluid_count);
+        }
+        s_cur = s_next;
+        s_next = s_after;
         cnt_next = cnt_after;
     }
 }
