@@ -121,6 +121,7 @@ size_t Engine::footprint(uint32_t fluid_capacity, uint32_t solid_capacity, int m
                                        scan_scratch_words(uint32_t(stab))) + 64;
     bytes += r(4 * scan_words) + r(sizeof(int)) + 2 * r(sizeof(uint32_t)) +
              r(sizeof(unsigned long long) * kLoopSlots);
+    bytes += r(4 * M) + r(4 * (M + 1)) + r(4);              // solver-loop work list
     return bytes;
 }
 
@@ -232,6 +233,11 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
     d_loop_iters_ = static_cast<unsigned long long*>(dev(sizeof(unsigned long long) * kLoopSlots));
     a_.loop_iterations = d_loop_iters_;
     cudaMemset(d_loop_iters_, 0, sizeof(unsigned long long) * kLoopSlots);
+    a_.loop_scene = static_cast<int32_t*>(dev(4ull * max_scenes_));
+    a_.loop_wt0 = static_cast<uint32_t*>(dev(4ull * (max_scenes_ + 1)));
+    a_.loop_n = static_cast<uint32_t*>(dev(4));
+    cudaMemset(a_.loop_n, 0, 4);
+    cudaMemset(a_.loop_wt0, 0, 4);
     if (cudaStreamCreateWithFlags(&cap_st_, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&body_st_, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&frame_st_, cudaStreamNonBlocking) != cudaSuccess ||

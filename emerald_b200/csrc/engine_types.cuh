@@ -116,6 +116,13 @@ struct Arena {
     // executed solver iterations per loop kind (0-3), then sub-steps run by
     // frame graphs per method (4 + method)
     unsigned long long* loop_iterations;
+    // Solver-loop work list of the persistent-warp loop kernels: the scenes
+    // whose loop still runs (loop_scene[0, *loop_n)) and the exclusive prefix
+    // of their warp tiles (loop_wt0, *loop_n + 1 entries), rebuilt by every
+    // loop reset and exit test.
+    int32_t* loop_scene;
+    uint32_t* loop_wt0;
+    uint32_t* loop_n;
     int32_t const* tile_scene;   // fluid tile -> scene (-1: free)
     int32_t const* stile_scene;  // solid tile -> scene
     uint32_t stride;             // fluid arena capacity (multiple of kTile)

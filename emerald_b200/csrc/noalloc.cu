@@ -120,6 +120,9 @@ extern "C" int emerald_neighbors_static(void const* d_xy, uint32_t n, float supp
     a.sp = reinterpret_cast<SceneParams const*>(base + kOffParams);
     a.ss = reinterpret_cast<SceneState*>(base + kOffState);
     a.loop_iterations = reinterpret_cast<unsigned long long*>(base + kOffLoops);
+    a.loop_scene = nullptr;  // the neighbour build runs no solver loop
+    a.loop_wt0 = nullptr;
+    a.loop_n = nullptr;
     a.tile_scene = reinterpret_cast<int32_t const*>(base + kOffTiles);
     a.stride = stride;
     a.x = const_cast<float2*>(static_cast<float2 const*>(d_xy));

@@ -225,23 +225,92 @@ __device__ __forceinline__ int iteration_cap(SceneParams const& P, int kind) {
     return kind == 0 ? P.iisph_max_iter : (kind == 3 ? 6 : P.dfsph_max_iter);
 }
 
+// Rebuilds the solver-loop work list (Arena::loop_scene, loop_wt0,
+// loop_n): the active scenes whose loop still runs and have particles, in
+// scene order, with the exclusive prefix of their warp tiles (32 particles
+// each). Run by every thread of one block after the scenes' done flags are
+// final; a block-wide scan over the scenes, blockDim.x at a time.
+__device__ void build_loop_list(Arena const& a, int nscenes) {
+    __shared__ uint32_t base_wt, base_n;
+    __shared__ uint32_t warp_wt[32], warp_n[32];
+    int const lane = threadIdx.x & 31;
+    int const warp = threadIdx.x >> 5;
+    int const nwarps = (blockDim.x + 31) >> 5;
+    if (threadIdx.x == 0) {
+        base_wt = 0u;
+        base_n = 0u;
+    }
+    __syncthreads();
+    for (int s0 = 0; s0 < nscenes; s0 += blockDim.x) {
+        int const s = s0 + threadIdx.x;
+        uint32_t wt = 0u;
+        if (s < nscenes) {
+            SceneState const& S = a.ss[s];
+            if (S.active && !S.done) wt = (a.sp[s].fluid_count + 31u) / 32u;
+        }
+        uint32_t const on = wt ? 1u : 0u;
+        // inclusive scans of (wt, on) within the warp, then across warps
+        uint32_t iw = wt, in = on;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t const yw = __shfl_up_sync(0xffffffffu, iw, o);
+            uint32_t const yn = __shfl_up_sync(0xffffffffu, in, o);
+            if (lane >= o) {
+                iw += yw;
+                in += yn;
+            }
+        }
+        if (lane == 31) {
+            warp_wt[warp] = iw;
+            warp_n[warp] = in;
+        }
+        __syncthreads();
+        uint32_t pw = 0u, pn = 0u, tw = 0u, tn = 0u;
+        for (int w = 0; w < nwarps; ++w) {
+            if (w < warp) {
+                pw += warp_wt[w];
+                pn += warp_n[w];
+            }
+            tw += warp_wt[w];
+            tn += warp_n[w];
+        }
+        if (on) {
+            uint32_t const k = base_n + pn + in - 1u;
+            a.loop_scene[k] = s;
+            a.loop_wt0[k] = base_wt + pw + iw - wt;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            base_wt += tw;
+            base_n += tn;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        a.loop_wt0[base_n] = base_wt;
+        *a.loop_n = base_n;
+    }
+}
+
 // Starts a solver loop; a scene whose cap is zero runs no iteration, as the
 // reference's for-loop would. Inside a captured graph it also opens the
 // loop's while node: a condition handle's default is applied when the graph
 // that owns it is launched, and a loop nested in a frame graph's sub-step
 // loop is reached once per sub-step of one launch, after the previous
-// sub-step's exit test closed it.
+// sub-step's exit test closed it. One block: it also builds the loop's first
+// work list.
 __global__ void k_iter_reset(Arena a, int nscenes, int kind, cudaGraphConditionalHandle cond,
                              int use_cond) {
-    int const s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (use_cond && s == 0) cudaGraphSetConditional(cond, 1u);
-    if (s >= nscenes) return;
-    SceneState& S = a.ss[s];
-    S.iter = 0;
-    S.done = (S.active && iteration_cap(a.sp[s], kind) > 0) ? 0 : 1;
-    S.err_sum = 0ull;
-    S.err_max = 0u;
-    S.err_sum_d = 0.0;
+    if (use_cond && threadIdx.x == 0) cudaGraphSetConditional(cond, 1u);
+    for (int s = threadIdx.x; s < nscenes; s += blockDim.x) {
+        SceneState& S = a.ss[s];
+        S.iter = 0;
+        S.done = (S.active && iteration_cap(a.sp[s], kind) > 0) ? 0 : 1;
+        S.err_sum = 0ull;
+        S.err_max = 0u;
+        S.err_sum_d = 0.0;
+    }
+    __syncthreads();
+    build_loop_list(a, nscenes);
 }
 
 // Exit test after one solver iteration. kind 0: IISPH family
@@ -316,6 +385,7 @@ __device__ void exit_test(Arena const& a, int nscenes, int kind, int* running,
         }
     }
     __syncthreads();
+    build_loop_list(a, nscenes);
     if (threadIdx.x == 0) {
         a.loop_iterations[kind] += 1ull;
         *running = any;
@@ -925,50 +995,83 @@ __device__ __forceinline__ void add_err(Arena const& a, WarpErr& e, int32_t scen
     }
 }
 
-// The scene of warp tile t when it takes part in this launch (active and,
-// with skip_done, its solver loop still running), else -1. The answer does
-// not change while a walk runs: the loop state moves only in the exit test.
-__device__ __forceinline__ int32_t live_tile_scene(Arena const& a, uint32_t t, bool skip_done) {
+// The scene of warp tile t when it takes part in this launch (active), else
+// -1.
+__device__ __forceinline__ int32_t live_tile_scene(Arena const& a, uint32_t t) {
     int32_t const s = a.tile_scene[t / (kTile / 32)];
     if (s < 0) return -1;
-    SceneState const& S = a.ss[s];
-    return (S.active && !(skip_done && S.done)) ? s : -1;
+    return a.ss[s].active ? s : -1;
+}
+
+// Warp tile w of the solver-loop work list (w < the list's total): its scene
+// and its warp tile in the arena, by bisection of the prefix loop_wt0.
+__device__ __forceinline__ void loop_list_tile(Arena const& a, uint32_t n, uint32_t w,
+                                               int32_t& s, uint32_t& t) {
+    uint32_t lo = 0u, hi = n;  // loop_wt0[lo] <= w < loop_wt0[hi]
+    while (hi - lo > 1u) {
+        uint32_t const mid = (lo + hi) >> 1;
+        if (a.loop_wt0[mid] <= w) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    s = a.loop_scene[lo];
+    t = a.sp[s].fluid_begin / 32u + (w - a.loop_wt0[lo]);
 }
 
 // Walks this warp's tiles: prefetch(base, count) asks L2 for a tile's data,
-// body(scene, i, live) folds particle i of a tile whose scene takes part;
-// tiles of scenes that sit out (finished loops in a batch) are neither
-// prefetched nor folded. Every lane of the warp runs every iteration (tile
-// checks are warp-uniform), and every thread of the block returns from it
-// (no early exit, so the kernels can meet at a block barrier afterwards).
+// body(scene, i, live) folds particle i of the tile. With skip_done (the
+// kernels of a solver-loop iteration) the walk covers the warp tiles of the
+// loop's work list only, so a batch whose other scenes have converged costs
+// only the tiles still iterating; otherwise every tile of an active scene.
+// Every lane of the warp runs every iteration (tile choices are
+// warp-uniform), and every thread of the block returns from it (no early
+// exit, so the kernels can meet at a block barrier afterwards).
 template <class Prefetch, class Body>
 __device__ __forceinline__ void walk_warp_tiles(Arena const& a, uint32_t wtiles, bool skip_done,
                                                 Prefetch prefetch, Body body) {
     uint32_t const lane = threadIdx.x & 31u;
     uint32_t const G = (gridDim.x * blockDim.x) >> 5;
-    uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int32_t s_cur = t < wtiles ? live_tile_scene(a, t, skip_done) : -1;
-    int32_t s_next = t + G < wtiles ? live_tile_scene(a, t + G, skip_done) : -1;
-    int cnt_next = s_next >= 0 ? int(a.nf_cnt[(t + G) * 32u + lane]) : 0;
-    if (s_cur >= 0) prefetch(t * 32u, int(a.nf_cnt[t * 32u + lane]));
-    for (; t < wtiles; t += G) {
-        uint32_t const tn = t + G;
+    uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t const n = skip_done ? *a.loop_n : 0u;
+    uint32_t const total = skip_done ? a.loop_wt0[n] : wtiles;
+    // position w of the walk -> scene (-1: sits out) and warp tile
+    auto locate = [&](uint32_t k, int32_t& s, uint32_t& t) {
+        if (skip_done) {
+            loop_list_tile(a, n, k, s, t);
+        } else {
+            t = k;
+            s = live_tile_scene(a, k);
+        }
+    };
+    int32_t s_cur = -1, s_next = -1;
+    uint32_t t_cur = 0u, t_next = 0u;
+    if (w < total) locate(w, s_cur, t_cur);
+    if (w + G < total) locate(w + G, s_next, t_next);
+    int cnt_next = s_next >= 0 ? int(a.nf_cnt[t_next * 32u + lane]) : 0;
+    if (s_cur >= 0) prefetch(t_cur * 32u, int(a.nf_cnt[t_cur * 32u + lane]));
+    for (; w < total; w += G) {
+        uint32_t const wn = w + G;
         int32_t s_after = -1;
+        uint32_t t_after = 0u;
         int cnt_after = 0;
-        if (tn < wtiles) {
-            if (s_next >= 0) prefetch(tn * 32u, cnt_next);
-            if (tn + G < wtiles) {
-                s_after = live_tile_scene(a, tn + G, skip_done);
-                if (s_after >= 0) cnt_after = int(a.nf_cnt[(tn + G) * 32u + lane]);
+        if (wn < total) {
+            if (s_next >= 0) prefetch(t_next * 32u, cnt_next);
+            if (wn + G < total) {
+                locate(wn + G, s_after, t_after);
+                if (s_after >= 0) cnt_after = int(a.nf_cnt[t_after * 32u + lane]);
             }
         }
         if (s_cur >= 0) {
             SceneParams const& P = a.sp[s_cur];
-            uint32_t const i = t * 32u + lane;
+            uint32_t const i = t_cur * 32u + lane;
             body(s_cur, i, (i - P.fluid_begin) < P.fluid_count);
         }
         s_cur = s_next;
+        t_cur = t_next;
         s_next = s_after;
+        t_next = t_after;
         cnt_next = cnt_after;
     }
 }
@@ -1830,7 +1933,7 @@ void launch_zero_kappas(Arena const& a, uint32_t tiles, cudaStream_t st) {
 }
 void launch_iter_reset(Arena const& a, int nscenes, int kind, cudaStream_t st,
                        cudaGraphConditionalHandle cond, int use_cond) {
-    k_iter_reset<<<(nscenes + 127) / 128, 128, 0, st>>>(a, nscenes, kind, cond, use_cond);
+    k_iter_reset<<<1, 256, 0, st>>>(a, nscenes, kind, cond, use_cond);
 }
 void launch_iter_check(Arena const& a, int nscenes, int kind, int* running,
                        cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st) {
