@@ -238,6 +238,7 @@ Engine::Engine(uint32_t fluid_capacity, uint32_t solid_capacity, int max_scenes)
     a_.loop_n = static_cast<uint32_t*>(dev(4));
     cudaMemset(a_.loop_n, 0, 4);
     cudaMemset(a_.loop_wt0, 0, 4);
+    a_.batch = max_scenes_ > 1 ? 1 : 0;
     if (cudaStreamCreateWithFlags(&cap_st_, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&body_st_, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&frame_st_, cudaStreamNonBlocking) != cudaSuccess ||

@@ -123,6 +123,7 @@ struct Arena {
     int32_t* loop_scene;
     uint32_t* loop_wt0;
     uint32_t* loop_n;
+    int32_t batch;  // the arena holds more than one scene slot (loop kernels walk the work list)
     int32_t const* tile_scene;   // fluid tile -> scene (-1: free)
     int32_t const* stile_scene;  // solid tile -> scene
     uint32_t stride;             // fluid arena capacity (multiple of kTile)

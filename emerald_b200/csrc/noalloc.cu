@@ -123,6 +123,7 @@ extern "C" int emerald_neighbors_static(void const* d_xy, uint32_t n, float supp
     a.loop_scene = nullptr;  // the neighbour build runs no solver loop
     a.loop_wt0 = nullptr;
     a.loop_n = nullptr;
+    a.batch = 0;
     a.tile_scene = reinterpret_cast<int32_t const*>(base + kOffTiles);
     a.stride = stride;
     a.x = const_cast<float2*>(static_cast<float2 const*>(d_xy));

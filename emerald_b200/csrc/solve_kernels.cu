@@ -997,10 +997,11 @@ __device__ __forceinline__ void add_err(Arena const& a, WarpErr& e, int32_t scen
 
 // The scene of warp tile t when it takes part in this launch (active), else
 // -1.
-__device__ __forceinline__ int32_t live_tile_scene(Arena const& a, uint32_t t) {
+__device__ __forceinline__ int32_t live_tile_scene(Arena const& a, uint32_t t, bool skip_done) {
     int32_t const s = a.tile_scene[t / (kTile / 32)];
     if (s < 0) return -1;
-    return a.ss[s].active ? s : -1;
+    SceneState const& S = a.ss[s];
+    return (S.active && !(skip_done && S.done)) ? s : -1;
 }
 
 // Warp tile w of the solver-loop work list (w < the list's total): its scene
@@ -1021,64 +1022,82 @@ __device__ __forceinline__ void loop_list_tile(Arena const& a, uint32_t n, uint3
 }
 
 // Walks this warp's tiles: prefetch(base, count) asks L2 for a tile's data,
-// body(scene, i, live) folds particle i of the tile. With skip_done (the
-// kernels of a solver-loop iteration) the walk covers the warp tiles of the
-// loop's work list only, so a batch whose other scenes have converged costs
-// only the tiles still iterating; otherwise every tile of an active scene.
-// Every lane of the warp runs every iteration (tile choices are
-// warp-uniform), and every thread of the block returns from it (no early
-// exit, so the kernels can meet at a block barrier afterwards).
-template <class Prefetch, class Body>
+// body(scene, i, live) folds particle i of the tile. LIST (the solver-loop
+// kernels of a batch) walks the warp tiles of the loop's work list only, so
+// the scenes that have converged cost nothing; otherwise the walk covers
+// every tile and skips those of inactive scenes (and, with skip_done, of
+// scenes whose loop has ended). The list walk holds more registers, so
+// single scenes keep the plain walk. Every lane of the warp runs every
+// iteration (tile choices are warp-uniform), and every thread of the block
+// returns from it (no early exit, so the kernels can meet at a block
+// barrier afterwards).
+template <bool LIST, class Prefetch, class Body>
 __device__ __forceinline__ void walk_warp_tiles(Arena const& a, uint32_t wtiles, bool skip_done,
                                                 Prefetch prefetch, Body body) {
     uint32_t const lane = threadIdx.x & 31u;
     uint32_t const G = (gridDim.x * blockDim.x) >> 5;
     uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    uint32_t const n = skip_done ? *a.loop_n : 0u;
-    uint32_t const total = skip_done ? a.loop_wt0[n] : wtiles;
-    // position w of the walk -> scene (-1: sits out) and warp tile
-    auto locate = [&](uint32_t k, int32_t& s, uint32_t& t) {
-        if (skip_done) {
-            loop_list_tile(a, n, k, s, t);
-        } else {
-            t = k;
-            s = live_tile_scene(a, k);
-        }
-    };
-    int32_t s_cur = -1, s_next = -1;
-    uint32_t t_cur = 0u, t_next = 0u;
-    if (w < total) locate(w, s_cur, t_cur);
-    if (w + G < total) locate(w + G, s_next, t_next);
-    int cnt_next = s_next >= 0 ? int(a.nf_cnt[t_next * 32u + lane]) : 0;
-    if (s_cur >= 0) prefetch(t_cur * 32u, int(a.nf_cnt[t_cur * 32u + lane]));
-    for (; w < total; w += G) {
-        uint32_t const wn = w + G;
-        int32_t s_after = -1;
-        uint32_t t_after = 0u;
-        int cnt_after = 0;
-        if (wn < total) {
-            if (s_next >= 0) prefetch(t_next * 32u, cnt_next);
-            if (wn + G < total) {
-                locate(wn + G, s_after, t_after);
-                if (s_after >= 0) cnt_after = int(a.nf_cnt[t_after * 32u + lane]);
+    if constexpr (LIST) {
+        uint32_t const n = *a.loop_n;
+        uint32_t const total = a.loop_wt0[n];
+        int32_t s_cur = -1, s_next = -1;
+        uint32_t t_cur = 0u, t_next = 0u;
+        if (w < total) loop_list_tile(a, n, w, s_cur, t_cur);
+        if (w + G < total) loop_list_tile(a, n, w + G, s_next, t_next);
+        int cnt_next = s_next >= 0 ? int(a.nf_cnt[t_next * 32u + lane]) : 0;
+        if (s_cur >= 0) prefetch(t_cur * 32u, int(a.nf_cnt[t_cur * 32u + lane]));
+        for (; w < total; w += G) {
+            uint32_t const wn = w + G;
+            int32_t s_after = -1;
+            uint32_t t_after = 0u;
+            int cnt_after = 0;
+            if (wn < total) {
+                if (s_next >= 0) prefetch(t_next * 32u, cnt_next);
+                if (wn + G < total) {
+                    loop_list_tile(a, n, wn + G, s_after, t_after);
+                    cnt_after = int(a.nf_cnt[t_after * 32u + lane]);
+                }
             }
-        }
-        if (s_cur >= 0) {
             SceneParams const& P = a.sp[s_cur];
             uint32_t const i = t_cur * 32u + lane;
             body(s_cur, i, (i - P.fluid_begin) < P.fluid_count);
+            s_cur = s_next;
+            t_cur = t_next;
+            s_next = s_after;
+            t_next = t_after;
+            cnt_next = cnt_after;
         }
-        s_cur = s_next;
-        t_cur = t_next;
-        s_next = s_after;
-        t_next = t_after;
-        cnt_next = cnt_after;
+    } else {
+        int32_t s_cur = w < wtiles ? live_tile_scene(a, w, skip_done) : -1;
+        int32_t s_next = w + G < wtiles ? live_tile_scene(a, w + G, skip_done) : -1;
+        int cnt_next = s_next >= 0 ? int(a.nf_cnt[(w + G) * 32u + lane]) : 0;
+        if (s_cur >= 0) prefetch(w * 32u, int(a.nf_cnt[w * 32u + lane]));
+        for (; w < wtiles; w += G) {
+            uint32_t const wn = w + G;
+            int32_t s_after = -1;
+            int cnt_after = 0;
+            if (wn < wtiles) {
+                if (s_next >= 0) prefetch(wn * 32u, cnt_next);
+                if (wn + G < wtiles) {
+                    s_after = live_tile_scene(a, wn + G, skip_done);
+                    if (s_after >= 0) cnt_after = int(a.nf_cnt[(wn + G) * 32u + lane]);
+                }
+            }
+            if (s_cur >= 0) {
+                SceneParams const& P = a.sp[s_cur];
+                uint32_t const i = w * 32u + lane;
+                body(s_cur, i, (i - P.fluid_begin) < P.fluid_count);
+            }
+            s_cur = s_next;
+            s_next = s_after;
+            cnt_next = cnt_after;
+        }
     }
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_dfsph_density_alpha_pw(Arena a, uint32_t wtiles) {
-    walk_warp_tiles(
+    walk_warp_tiles<false>(
       a, wtiles, false,
       [&](uint32_t base, int count) {
           prefetch_warp_tile<true>(a, base, count, a.ns_cnt + base, a.kdiv + base, a.kdens + base);
@@ -1094,12 +1113,12 @@ __global__ void __launch_bounds__(256) k_dfsph_density_alpha_pw(Arena a, uint32_
       });
 }
 
-template <int MODE, int CH>
+template <int MODE, int CH, bool LIST>
 __global__ void __launch_bounds__(256) k_apply_pressures_pw(Arena a, uint32_t wtiles, int which_q,
                                                             int external, int skip_done,
                                                             LoopCheck lc) {
     float const* q = which_q ? a.qdens : a.qdiv;
-    walk_warp_tiles(
+    walk_warp_tiles<LIST>(
       a, wtiles, skip_done != 0,
       [&](uint32_t base, int count) {
           prefetch_warp_tile<false>(a, base, count, a.ns_cnt + base, a.v + base, a.v + base + 16,
@@ -1117,10 +1136,10 @@ __global__ void __launch_bounds__(256) k_apply_pressures_pw(Arena a, uint32_t wt
     fused_exit_test(a, lc, false);
 }
 
-template <int MODE, int CH>
+template <int MODE, int CH, bool LIST>
 __global__ void __launch_bounds__(256) k_dfsph_divergence_pw(Arena a, uint32_t wtiles) {
     WarpErr e{-1, 0ull, 0u, 0.0};
-    walk_warp_tiles(
+    walk_warp_tiles<LIST>(
       a, wtiles, true,
       [&](uint32_t base, int count) {
           prefetch_warp_tile<false>(a, base, count, a.ns_cnt + base, a.v + base, a.v + base + 16,
@@ -1150,10 +1169,10 @@ __global__ void __launch_bounds__(256) k_dfsph_divergence_pw(Arena a, uint32_t w
     flush_err_block(a, e);
 }
 
-template <int MODE, int CH>
+template <int MODE, int CH, bool LIST>
 __global__ void __launch_bounds__(256) k_dfsph_density_pw(Arena a, uint32_t wtiles) {
     WarpErr e{-1, 0ull, 0u, 0.0};
-    walk_warp_tiles(
+    walk_warp_tiles<LIST>(
       a, wtiles, true,
       [&](uint32_t base, int count) {
           prefetch_warp_tile<false>(a, base, count, a.ns_cnt + base, a.v + base, a.v + base + 16,
@@ -1467,9 +1486,9 @@ __global__ void k_iisph_beta_pressure(Arena a) {
 
 // The two IISPH gather kernels as persistent warps (see the DFSPH ones
 // above): the batched workload's per-iteration sums.
-template <int MODE, int CH>
+template <int MODE, int CH, bool LIST>
 __global__ void __launch_bounds__(256) k_iisph_sum_dij_pw(Arena a, uint32_t wtiles) {
-    walk_warp_tiles(
+    walk_warp_tiles<LIST>(
       a, wtiles, true,
       [&](uint32_t base, int count) {
           prefetch_warp_tile<false>(a, base, count, nullptr, nullptr, nullptr);
@@ -1485,11 +1504,11 @@ __global__ void __launch_bounds__(256) k_iisph_sum_dij_pw(Arena a, uint32_t wtil
       });
 }
 
-template <int MODE, int CH>
+template <int MODE, int CH, bool LIST>
 __global__ void __launch_bounds__(256) k_iisph_beta_pressure_pw(Arena a, uint32_t wtiles,
                                                                 LoopCheck lc) {
     WarpErr e{-1, 0ull, 0u, 0.0};
-    walk_warp_tiles(
+    walk_warp_tiles<LIST>(
       a, wtiles, true,
       [&](uint32_t base, int count) {
           prefetch_warp_tile<false>(a, base, count, a.ns_cnt + base, a.sdp + base,
@@ -1960,6 +1979,19 @@ void launch_dfsph_density_alpha(Arena const& a, uint32_t tiles, bool comp, cudaS
         k_dfsph_density_alpha<0><<<tiles, kTile, 0, st>>>(a);
     }
 }
+// A persistent-warp loop kernel with the work-list walk (`list`: the
+// solver loops of a batch) or the plain walk.
+#define EMLD_PW_LAUNCH(KERNEL, M, C, ...)                                                      \
+    do {                                                                                       \
+        if (list) {                                                                            \
+            KERNEL<M, C, true>                                                                 \
+              <<<persistent_grid(KERNEL<M, C, true>, tiles, th), th, 0, st>>>(__VA_ARGS__);    \
+        } else {                                                                               \
+            KERNEL<M, C, false>                                                                \
+              <<<persistent_grid(KERNEL<M, C, false>, tiles, th), th, 0, st>>>(__VA_ARGS__);   \
+        }                                                                                      \
+    } while (0)
+
 #define EMLD_PW_DISPATCH(K, comp, ch)                                          \
     do {                                                                      \
         if (comp) {                                                           \
@@ -1976,9 +2008,10 @@ void launch_apply_pressures(Arena const& a, uint32_t tiles, int which_q, int ext
     int const ch = chunk & kChunkMask;
     if (chunk & kPersistentWarps) {
         int const th = (chunk & kPersistentBlocks256) ? 256 : kTile;
+        bool const list = a.batch && skip_done;
 #define EMLD_APPLY_PW(M, C)                                                                     \
-    k_apply_pressures_pw<M, C><<<persistent_grid(k_apply_pressures_pw<M, C>, tiles, th), th, 0, st>>>( \
-      a, tiles * (kTile / 32), which_q, external, skip_done, lc)
+    EMLD_PW_LAUNCH(k_apply_pressures_pw, M, C, a, tiles * (kTile / 32), which_q, external,     \
+                   skip_done, lc)
         EMLD_PW_DISPATCH(EMLD_APPLY_PW, comp, ch);
 #undef EMLD_APPLY_PW
         return;
@@ -1993,9 +2026,8 @@ void launch_dfsph_divergence(Arena const& a, uint32_t tiles, bool comp, cudaStre
     int const ch = chunk & kChunkMask;
     if (chunk & kPersistentWarps) {
         int const th = (chunk & kPersistentBlocks256) ? 256 : kTile;
-#define EMLD_DIV_PW(M, C)                                                                         \
-    k_dfsph_divergence_pw<M, C><<<persistent_grid(k_dfsph_divergence_pw<M, C>, tiles, th), th, 0, st>>>( \
-      a, tiles * (kTile / 32))
+        bool const list = a.batch != 0;
+#define EMLD_DIV_PW(M, C) EMLD_PW_LAUNCH(k_dfsph_divergence_pw, M, C, a, tiles * (kTile / 32))
         EMLD_PW_DISPATCH(EMLD_DIV_PW, comp, ch);
 #undef EMLD_DIV_PW
         return;
@@ -2010,9 +2042,8 @@ void launch_dfsph_density(Arena const& a, uint32_t tiles, bool comp, cudaStream_
     int const ch = chunk & kChunkMask;
     if (chunk & kPersistentWarps) {
         int const th = (chunk & kPersistentBlocks256) ? 256 : kTile;
-#define EMLD_DENS_PW(M, C)                                                                    \
-    k_dfsph_density_pw<M, C><<<persistent_grid(k_dfsph_density_pw<M, C>, tiles, th), th, 0, st>>>( \
-      a, tiles * (kTile / 32))
+        bool const list = a.batch != 0;
+#define EMLD_DENS_PW(M, C) EMLD_PW_LAUNCH(k_dfsph_density_pw, M, C, a, tiles * (kTile / 32))
         EMLD_PW_DISPATCH(EMLD_DENS_PW, comp, ch);
 #undef EMLD_DENS_PW
         return;
@@ -2048,9 +2079,8 @@ void launch_iisph_sum_dij(Arena const& a, uint32_t tiles, cudaStream_t st, int c
     int const ch = chunk & kChunkMask;
     if (chunk & kPersistentWarps) {
         int const th = (chunk & kPersistentBlocks256) ? 256 : kTile;
-#define EMLD_SUM_PW(M, C)                                                                       \
-    k_iisph_sum_dij_pw<M, C><<<persistent_grid(k_iisph_sum_dij_pw<M, C>, tiles, th), th, 0, st>>>( \
-      a, tiles * (kTile / 32))
+        bool const list = a.batch != 0;
+#define EMLD_SUM_PW(M, C) EMLD_PW_LAUNCH(k_iisph_sum_dij_pw, M, C, a, tiles * (kTile / 32))
         EMLD_PW_DISPATCH(EMLD_SUM_PW, comp, ch);
 #undef EMLD_SUM_PW
         return;
@@ -2066,9 +2096,9 @@ void launch_iisph_beta_pressure(Arena const& a, uint32_t tiles, cudaStream_t st,
     int const ch = chunk & kChunkMask;
     if (chunk & kPersistentWarps) {
         int const th = (chunk & kPersistentBlocks256) ? 256 : kTile;
+        bool const list = a.batch != 0;
 #define EMLD_BETA_PW(M, C)                                                                   \
-    k_iisph_beta_pressure_pw<M, C>                                                           \
-      <<<persistent_grid(k_iisph_beta_pressure_pw<M, C>, tiles, th), th, 0, st>>>(a, tiles * (kTile / 32), lc)
+    EMLD_PW_LAUNCH(k_iisph_beta_pressure_pw, M, C, a, tiles * (kTile / 32), lc)
         EMLD_PW_DISPATCH(EMLD_BETA_PW, comp, ch);
 #undef EMLD_BETA_PW
         return;

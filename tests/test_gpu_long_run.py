@@ -1,16 +1,18 @@
-"""The benchmark scene over a long run, bit for bit: 120 frames (about 1,500
-CFL-adaptive DFSPH_P sub-steps) of the 512 x 512 dam break at dx = 1/1024,
+"""The benchmark scenes over long runs, bit for bit: 120 frames (2,141
+CFL-adaptive DFSPH_P sub-steps) of the 512 x 512 dam break at dx = 1/1024 and
+95 frames (about 1,900 sub-steps) of the 1024 x 1024 one at dx = 1/2048,
 support = dx, through emerald_sim_frame (one graph launch per frame), with
 the state's SHA-256 after every 5th frame equal to the compiled reference's
-(tests/golden/long_run_dfsph_262k.npz, made by
+(tests/golden/long_run_dfsph_262k.npz and long_run_dfsph_1m.npz, made by
 tests/golden/make_long_run.py through the reference's own frame loop).
 
-The run covers the collapse of the dam, the splash on the far wall and,
-near frame 105, the ejection of a single particle at about 2,600 m/s that
-this small-support scene shows in the reference itself: equal digests
-before and after it mean the ejection is the reference's trajectory, not
-a fault of the GPU path. The energy drift and the largest speed stored
-beside the digests state the same."""
+The runs cover the collapse of the dam, the splash on the far wall and the
+instability this small-support scene develops in the reference itself: at
+262,144 particles the ejection of a single particle at about 2,600 m/s near
+frame 105, at 1,048,576 particles a few ejections near frame 84 and a
+cascade from frame 88 on. Equal digests before and after them mean they are
+the reference's trajectory, not a fault of the GPU path. The energy drift
+and the largest speed stored beside the digests state the same."""
 import hashlib
 import os
 
@@ -21,24 +23,29 @@ import bench
 
 pytestmark = pytest.mark.gpu
 
-GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
-                      "long_run_dfsph_262k.npz")
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
-def test_long_run_digests_match_reference():
+@pytest.mark.parametrize("side,name", [(512, "long_run_dfsph_262k.npz"),
+                                       (1024, "long_run_dfsph_1m.npz")])
+def test_long_run_digests_match_reference(side, name):
     import emerald_b200 as E
-    g = np.load(GOLDEN)
+    g = np.load(os.path.join(GOLDEN, name))
     want = dict(zip(g["frames"].tolist(), g["digests"].tolist()))
     flicks = dict(zip(g["frames"].tolist(), g["flicks"].tolist()))
-    sim = E.Simulation.from_block_scene(E.BlockScene(bench.N_SIDE, **bench.scene_kwargs()))
-    assert bench.N_SIDE == 512
+    bench.configure_scene(side)
+    try:
+        sim = E.Simulation.from_block_scene(E.BlockScene(side, **bench.scene_kwargs()))
+    finally:
+        bench.configure_scene(512)
     last = int(g["frames"].max())
     for f in range(1, last + 1):
         sim.frame("dfsph_p")
         if f in want:
             x, v = sim.state()
             got = hashlib.sha256(x.tobytes() + v.tobytes()).hexdigest()
-            assert got == want[f], "frame %d: state differs from the reference's" % f
+            assert got == want[f], "side %d frame %d: state differs from the reference's" % (
+                side, f)
             assert sim.time() == flicks[f], f
     # the stored run does contain the ejection it is kept for
     assert g["max_speed"].max() > 1000.0 and g["max_speed"][0] < 10.0
