@@ -296,8 +296,8 @@ __device__ void build_loop_list(Arena const& a, int nscenes) {
 // loop's while node: a condition handle's default is applied when the graph
 // that owns it is launched, and a loop nested in a frame graph's sub-step
 // loop is reached once per sub-step of one launch, after the previous
-// sub-step's exit test closed it. One block: it also builds the loop's first
-// work list.
+// sub-step's exit test closed it. One block: in a batch it also builds the
+// loop's first work list.
 __global__ void k_iter_reset(Arena a, int nscenes, int kind, cudaGraphConditionalHandle cond,
                              int use_cond) {
     if (use_cond && threadIdx.x == 0) cudaGraphSetConditional(cond, 1u);
@@ -310,7 +310,7 @@ __global__ void k_iter_reset(Arena a, int nscenes, int kind, cudaGraphConditiona
         S.err_sum_d = 0.0;
     }
     __syncthreads();
-    build_loop_list(a, nscenes);
+    if (a.batch) build_loop_list(a, nscenes);
 }
 
 // Exit test after one solver iteration. kind 0: IISPH family
@@ -385,7 +385,7 @@ __device__ void exit_test(Arena const& a, int nscenes, int kind, int* running,
         }
     }
     __syncthreads();
-    build_loop_list(a, nscenes);
+    if (a.batch) build_loop_list(a, nscenes);
     if (threadIdx.x == 0) {
         a.loop_iterations[kind] += 1ull;
         *running = any;
