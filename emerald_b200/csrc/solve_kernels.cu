@@ -1038,34 +1038,27 @@ __device__ __forceinline__ void walk_warp_tiles(Arena const& a, uint32_t wtiles,
     uint32_t const G = (gridDim.x * blockDim.x) >> 5;
     uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if constexpr (LIST) {
+        // one tile ahead (fewer registers than the plain walk's two)
         uint32_t const n = *a.loop_n;
         uint32_t const total = a.loop_wt0[n];
-        int32_t s_cur = -1, s_next = -1;
-        uint32_t t_cur = 0u, t_next = 0u;
-        if (w < total) loop_list_tile(a, n, w, s_cur, t_cur);
-        if (w + G < total) loop_list_tile(a, n, w + G, s_next, t_next);
-        int cnt_next = s_next >= 0 ? int(a.nf_cnt[t_next * 32u + lane]) : 0;
-        if (s_cur >= 0) prefetch(t_cur * 32u, int(a.nf_cnt[t_cur * 32u + lane]));
+        int32_t s_cur = -1;
+        uint32_t t_cur = 0u;
+        if (w < total) {
+            loop_list_tile(a, n, w, s_cur, t_cur);
+            prefetch(t_cur * 32u, int(a.nf_cnt[t_cur * 32u + lane]));
+        }
         for (; w < total; w += G) {
-            uint32_t const wn = w + G;
-            int32_t s_after = -1;
-            uint32_t t_after = 0u;
-            int cnt_after = 0;
-            if (wn < total) {
-                if (s_next >= 0) prefetch(t_next * 32u, cnt_next);
-                if (wn + G < total) {
-                    loop_list_tile(a, n, wn + G, s_after, t_after);
-                    cnt_after = int(a.nf_cnt[t_after * 32u + lane]);
-                }
+            int32_t s_next = -1;
+            uint32_t t_next = 0u;
+            if (w + G < total) {
+                loop_list_tile(a, n, w + G, s_next, t_next);
+                prefetch(t_next * 32u, int(a.nf_cnt[t_next * 32u + lane]));
             }
             SceneParams const& P = a.sp[s_cur];
             uint32_t const i = t_cur * 32u + lane;
             body(s_cur, i, (i - P.fluid_begin) < P.fluid_count);
             s_cur = s_next;
             t_cur = t_next;
-            s_next = s_after;
-            t_next = t_after;
-            cnt_next = cnt_after;
         }
     } else {
         int32_t s_cur = w < wtiles ? live_tile_scene(a, w, skip_done) : -1;
@@ -1170,7 +1163,7 @@ __global__ void __launch_bounds__(256) k_dfsph_divergence_pw(Arena a, uint32_t w
 }
 
 template <int MODE, int CH, bool LIST>
-__global__ void __launch_bounds__(256) k_dfsph_density_pw(Arena a, uint32_t wtiles) {
+__global__ void __launch_bounds__(256, LIST ? 3 : 1) k_dfsph_density_pw(Arena a, uint32_t wtiles) {
     WarpErr e{-1, 0ull, 0u, 0.0};
     walk_warp_tiles<LIST>(
       a, wtiles, true,
@@ -1505,7 +1498,7 @@ __global__ void __launch_bounds__(256) k_iisph_sum_dij_pw(Arena a, uint32_t wtil
 }
 
 template <int MODE, int CH, bool LIST>
-__global__ void __launch_bounds__(256) k_iisph_beta_pressure_pw(Arena a, uint32_t wtiles,
+__global__ void __launch_bounds__(256, LIST ? 3 : 1) k_iisph_beta_pressure_pw(Arena a, uint32_t wtiles,
                                                                 LoopCheck lc) {
     WarpErr e{-1, 0ull, 0u, 0.0};
     walk_warp_tiles<LIST>(
