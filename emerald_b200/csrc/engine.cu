@@ -1122,7 +1122,9 @@ uint64_t Engine::tuning_key(int32_t method) const {
     for (auto const& sc : scenes_) {
         if (sc.used && sc.active) n += sc.p.fluid_count;
     }
-    return uint64_t(method) * 64u + ceil_log2(std::max<uint64_t>(n, 1));
+    // batches and single scenes keep separate tunings
+    return uint64_t(method) * 128u + (max_scenes_ > 1 ? 64u : 0u) +
+           ceil_log2(std::max<uint64_t>(n, 1));
 }
 
 // Tuning cache lookup and per-scene method parameters before a sub-step or
@@ -1256,6 +1258,20 @@ Engine::TuneReport Engine::autotune(int32_t method, int substeps) {
             t.iisph_beta = o[1];
             cand.push_back(t);
         }
+    }
+    if (max_scenes_ > 1) {
+        // A batch's loops run as long as its slowest scene's; only the
+        // persistent-warp kernels walk just the scenes still iterating, so a
+        // batch chooses among them (a few sub-steps after the start, where
+        // the tuner times them, do not yet show the slow scenes' long loops)
+        bool const dfsph = method == kDfsph;
+        cand.erase(std::remove_if(cand.begin(), cand.end(),
+                                  [&](Tuning const& t) {
+                                      int const x = dfsph ? t.apply : t.iisph_sum;
+                                      int const y = dfsph ? t.divergence : t.iisph_beta;
+                                      return !((x & kPersistentWarps) && (y & kPersistentWarps));
+                                  }),
+                   cand.end());
     }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);

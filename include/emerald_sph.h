@@ -376,8 +376,11 @@ int emerald_batch_kernel_launches(emerald_batch* batch, int64_t* count);
  * few whole sub-steps of `method` with each candidate setting, every
  * candidate from the same state (restored afterwards, so the simulation is
  * left as it was), after at least one sub-step of that method, and keeps
- * the fastest, also for later simulations and batches of the same method
- * and size class (log2 of the active particle count). candidate_ms[k]: mean
+ * the fastest, also for later simulations (or, found on a batch, later
+ * batches) of the same method and size class (log2 of the active particle
+ * count). A batch times the persistent-warp candidates only (modes 2 to 5):
+ * its solver loops run as long as its slowest scene's, and those kernels
+ * walk just the scenes still iterating. candidate_ms[k]: mean
  * sub-step time of candidate k, whose chunks and prefetch modes are
  * candidate_chunks[k] and candidate_prefetch[k] (apply, divergence,
  * iisph_sum, iisph_beta; prefetch[] in the same order; the divergence
